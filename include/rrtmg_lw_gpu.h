@@ -1,0 +1,154 @@
+/*
+ * rrtmg_lw_gpu.h -- C ABI of the B200 RRTMG longwave column path.
+ *
+ * The library (ccpp_physics_b200/librrtmg_lw_gpu.so) replaces the two public
+ * entry points of the Fortran module rrtmg_lw in ccpp-physics:
+ *
+ *   rlwinit       physics/Radiation/RRTMG/radlw_main.F90:1322-1324
+ *   rrtmg_lw_run  physics/Radiation/RRTMG/radlw_main.F90:419-434
+ *                 (argument declarations radlw_main.F90:609-656,
+ *                  CCPP metadata radlw_main.meta:1-444)
+ *
+ * A Fortran host reaches these through an ISO_C_BINDING shim that keeps the
+ * original rlwinit / rrtmg_lw_run interfaces.  Every
+ * array is the caller's Fortran array, column-major, kind_phys = real(8):
+ * element (i, k) of an (npts, nlay) array is at ptr[(i-1) + (k-1)*ldim],
+ * element (i, k, b) of an (npts, nlay, nbands) array at
+ * ptr[(i-1) + ldim*((k-1) + nlay*(b-1))].  Fortran logicals are passed as
+ * int32 0/1.  Optional Fortran arguments are NULL when absent.
+ *
+ * Error convention (radlw_main.F90:713-760, 1415-1420): the functions return
+ * errflg (0 = success, 1 = error) and copy errmsg into the caller's buffer
+ * (NUL-terminated, truncated to errmsg_len).  Calls never abort the process.
+ *
+ * Threading: rrtmg_lw_gpu_run* may be called concurrently from several host
+ * threads (the CCPP host calls rrtmg_lw_run once per physics block from
+ * OpenMP threads).  Each host thread gets its own CUDA stream and device
+ * workspace; the only shared state is the immutable device tables written
+ * by rrtmg_lw_gpu_init.
+ */
+#ifndef RRTMG_LW_GPU_H
+#define RRTMG_LW_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RRTMG_LW_NBANDS 16   /* radlw_param.f:103 */
+#define RRTMG_LW_NGPT 140    /* radlw_param.f:104 */
+
+/* Arguments of rlwinit (radlw_main.F90:1322-1324), plus the CUDA device. */
+typedef struct rrtmg_lw_init_args {
+  int32_t me;            /* print control: banner when me == 0 */
+  int32_t rad_hr_units;  /* 1: heating rates in K/day, otherwise K/s */
+  int32_t inc_minor_gas; /* logical; only affects the banner (as in rlwinit) */
+  int32_t ilwcliq;
+  int32_t isubclw;
+  int32_t iovr, iovr_rand, iovr_maxrand, iovr_max, iovr_dcorr, iovr_exp,
+      iovr_exprand;
+  int32_t device;        /* CUDA device ordinal (extension; 0 by default) */
+} rrtmg_lw_init_args;
+
+/* Arguments of rrtmg_lw_run (radlw_main.F90:419-434), same names. */
+typedef struct rrtmg_lw_run_args {
+  int32_t npts, nlay, nlp1;
+  int32_t ldim;          /* leading dimension of (npts,...) arrays; 0 = npts */
+  int32_t lprnt, lslwr, top_at_1, inc_minor_gas;
+  int32_t iovr, iovr_rand, iovr_maxrand, iovr_max, iovr_dcorr, iovr_exp,
+      iovr_exprand;
+  int32_t ilwcliq, ilwcice, isubclw;
+  /* inputs */
+  const double *plyr, *plvl, *tlyr, *tlvl, *qlyr, *olyr;
+  const double *gasvmr_co2, *gasvmr_n2o, *gasvmr_ch4, *gasvmr_o2, *gasvmr_co,
+      *gasvmr_cfc11, *gasvmr_cfc12, *gasvmr_cfc22, *gasvmr_ccl4;
+  const int32_t *icseed;                 /* (npts) */
+  const double *aeraod, *aerssa;         /* (npts, nlay, nbands) */
+  const double *sfemis, *sfgtmp;         /* (npts) */
+  const double *dzlyr, *delpin;          /* (npts, nlay) */
+  const double *de_lgth;                 /* (npts) */
+  const double *alpha;                   /* (npts, nlay) */
+  const double *cld_cf;                  /* (npts, nlay) */
+  /* optional cloud inputs (ilwcliq > 0 needs the first eight, else cld_od) */
+  const double *cld_lwp, *cld_ref_liq, *cld_iwp, *cld_ref_ice, *cld_rwp,
+      *cld_ref_rain, *cld_swp, *cld_ref_snow, *cld_od;
+  /* outputs */
+  double *hlwc;    /* (npts, nlay) total-sky heating rate */
+  double *topflx;  /* (npts) records {upfxc, upfx0} = topflw_type */
+  double *sfcflx;  /* (npts) records {upfxc, upfx0, dnfxc, dnfx0} = sfcflw_type */
+  double *cldtau;  /* (npts, nlay) band-7 layer cloud optical depth */
+  /* optional outputs (NULL = not present) */
+  double *hlw0;    /* (npts, nlay) clear-sky heating rate */
+  double *hlwb;    /* (npts, nlay, nbands) spectral-band heating rates */
+  double *flxprf;  /* (npts, nlp1) records {upfxc, dnfxc, upfx0, dnfx0} = proflw_type */
+} rrtmg_lw_run_args;
+
+/* Execution options (extension, no counterpart in the reference). */
+enum rrtmg_lw_precision {
+  RRTMG_LW_FP64 = 0,       /* plain FP64 path, matches the Fortran within 1e-10 */
+  RRTMG_LW_FP32 = 1,       /* FP32 gas optics + transfer, FP64 interpolation weights
+                              and flux divergence */
+  RRTMG_LW_SURROGATE = 2   /* learned gas optics (BF16 MLP) + FP32 transfer */
+};
+enum rrtmg_lw_memory {
+  RRTMG_LW_HOST = 0,       /* every pointer is host memory (pageable or pinned) */
+  RRTMG_LW_DEVICE = 1      /* every pointer is device memory on the init device */
+};
+typedef struct rrtmg_lw_exec {
+  int32_t precision;       /* enum rrtmg_lw_precision */
+  int32_t memory;          /* enum rrtmg_lw_memory */
+  void *stream;            /* cudaStream_t; NULL = the calling thread's stream */
+  int32_t sync;            /* 1 = return after the results are in place (host
+                              memory always syncs); 0 = leave work queued */
+  int32_t reserved;
+} rrtmg_lw_exec;
+
+/* rlwinit (radlw_main.F90:1322): validates iovr, sets fluxfac/heatfac, builds
+ * the transmittance/tau-transition tables (radlw_main.F90:1474-1501) and
+ * uploads every coefficient table to the device.  Returns errflg. */
+int rrtmg_lw_gpu_init(const rrtmg_lw_init_args *args, char *errmsg,
+                      int32_t errmsg_len);
+
+/* rrtmg_lw_run (radlw_main.F90:419) on the GPU, FP64, host pointers.
+ * Returns errflg. */
+int rrtmg_lw_gpu_run(const rrtmg_lw_run_args *args, char *errmsg,
+                     int32_t errmsg_len);
+
+/* rrtmg_lw_run with explicit precision / memory space / stream. */
+int rrtmg_lw_gpu_run_ex(const rrtmg_lw_run_args *args,
+                        const rrtmg_lw_exec *exec, char *errmsg,
+                        int32_t errmsg_len);
+
+/* McICA sub-column generator alone (mcica_subcol, radlw_main.F90:1847-2107,
+ * with the GFS Mersenne Twister, mersenne_twister.f:285-372), on the GPU.
+ * For each column i: seed[i], cldf (ldim, nlay) layer cloud fraction already
+ * floored as in cldprop (radlw_main.F90:1805-1811), dz (ldim, nlay) [km],
+ * de_lgth (npts), alpha (ldim, nlay).  Writes lcloudy as bits:
+ * bits[(i*RRTMG_LW_NGPT + ig) * nwords + (k >> 5)] bit (k & 31) for g-point
+ * ig (0-based) and layer k (0-based, surface first), nwords = (nlay+31)/32.
+ * Device pointers only.  Returns errflg. */
+int rrtmg_lw_gpu_mcica(int32_t npts, int32_t nlay, int32_t ldim, int32_t iovr,
+                       const int32_t *seed, const double *cldf,
+                       const double *dz, const double *de_lgth,
+                       const double *alpha, uint32_t *bits, void *stream,
+                       char *errmsg, int32_t errmsg_len);
+
+/* Gas optics alone (setcoef + taumol, radlw_main.F90:2151-2406, 3836-6840)
+ * for the same inputs as rrtmg_lw_run, device pointers, internal (surface
+ * first) layer order: writes taug[(i*nlay + k)*140 + ig] (gas optical depth
+ * before aerosol is added) and fracs[(i*nlay + k)*140 + ig] (Planck
+ * fraction), precision RRTMG_LW_FP64 or RRTMG_LW_FP32 (outputs are always
+ * double).  Used to generate training data for the learned gas optics and
+ * for stage-level parity tests.  Returns errflg. */
+int rrtmg_lw_gpu_gas_optics(const rrtmg_lw_run_args *args, int32_t precision,
+                            double *taug, double *fracs, void *stream,
+                            char *errmsg, int32_t errmsg_len);
+
+/* Release device tables and per-thread workspaces (call once at exit). */
+void rrtmg_lw_gpu_finalize(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RRTMG_LW_GPU_H */
