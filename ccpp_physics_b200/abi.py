@@ -56,7 +56,8 @@ class RunArgs(C.Structure):
 
 class ExecArgs(C.Structure):
     _fields_ = [("precision", C.c_int32), ("memory", C.c_int32),
-                ("stream", C.c_void_p), ("sync", C.c_int32), ("reserved", C.c_int32)]
+                ("stream", C.c_void_p), ("sync", C.c_int32), ("reserved", C.c_int32),
+                ("kernel_ms", C.POINTER(C.c_float))]
 
 
 FP64, FP32, SURROGATE = 0, 1, 2

@@ -1,0 +1,91 @@
+// lw_common.cuh -- shared definitions of the B200 RRTMG-LW kernels.
+//
+// Band layout and constants follow physics/Radiation/RRTMG/radlw_param.f
+// (:103-142) and radlw_main.F90 (RLM:309-354); the coefficient tables are
+// the DATA of radlw_datatb.f, extracted into rrtmg_lw_tables.bin whose
+// offsets are in rrtmg_lw_table_layout.h (namespace lwtab).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../data/rrtmg_lw_table_layout.h"
+
+namespace lw {
+
+constexpr int NBANDS = 16;
+constexpr int NGPT = 140;
+constexpr int NTBL = 10000;
+
+// g-points per band and first g-point of each band (radlw_param.f:111-120)
+__host__ __device__ constexpr int ng_of(int b) {
+  return b == 0 ? 10 : b == 1 ? 12 : b == 2 ? 16 : b == 3 ? 14 : b == 4 ? 16 : b == 5 ? 8
+       : b == 6 ? 12 : b == 7 ? 8 : b == 8 ? 12 : b == 9 ? 6 : b == 10 ? 8 : b == 11 ? 8
+       : b == 12 ? 4 : 2;
+}
+__host__ __device__ constexpr int ns_of(int b) {
+  return b == 0 ? 0 : ns_of(b - 1) + ng_of(b - 1);
+}
+// reference-atmosphere counts per band (RLM:326-327); nspb(16) = 0 is kept
+__host__ __device__ constexpr int nspa_of(int b) {
+  return (b == 2 || b == 3 || b == 4 || b == 6 || b == 8 || b == 11 || b == 12 || b == 14 || b == 15) ? 9 : 1;
+}
+__host__ __device__ constexpr int nspb_of(int b) {
+  return (b == 2 || b == 3 || b == 4) ? 5 : (b == 5 || b == 11 || b == 12 || b == 14 || b == 15) ? 0 : 1;
+}
+
+// Run-time constants shared by every column of a call.
+struct Consts {
+  double fluxfac, heatfac;
+};
+
+// Coefficient tables in device memory, in the arithmetic precision R.
+template <typename R>
+struct Tables {
+  const R* kt;       // every radlw_datatb.f array (offsets lwtab::*)
+  const R* exp_tbl;  // rlwinit tables, 0..NTBL (RLM:1474-1501)
+  const R* tfn_tbl;
+  const R* tau_tbl;
+};
+
+// Device-side view of one physics block (the arrays of one rrtmg_lw_run call).
+enum InField {
+  F_PLYR, F_PLVL, F_TLYR, F_TLVL, F_QLYR, F_OLYR, F_CO2, F_N2O, F_CH4, F_O2, F_CO, F_CFC11,
+  F_CFC12, F_CFC22, F_CCL4, F_AERAOD, F_AERSSA, F_SFEMIS, F_SFGTMP, F_DZLYR, F_DELPIN,
+  F_DELGTH, F_ALPHA, F_CLDCF, F_LWP, F_RELIQ, F_IWP, F_REICE, F_RWP, F_RERAIN, F_SWP,
+  F_RESNOW, F_CLDOD, N_IN
+};
+enum OutField { O_HLWC, O_TOPFLX, O_SFCFLX, O_CLDTAU, O_HLW0, O_HLWB, O_FLXPRF, N_OUT };
+
+struct Block {
+  const double* in[N_IN];
+  const int32_t* icseed;
+  double* out[N_OUT];
+  int npts;   // columns in this block
+  int ld;     // leading dimension of its (npts, ...) arrays
+  int col0;   // global index of its first column (prefix sum)
+  int pad;
+};
+
+// Flags common to every block of a launch.
+struct Flags {
+  int nlay, top_at_1, inc_minor_gas, iovr, iovr_dcorr, iovr_exp, iovr_exprand;
+  int ilwcliq, ilwcice, isubclw;
+  int want_hlw0, want_hlwb, want_flxprf;
+  int gas_only;        // 1: write taug/fracs only (training data / stage tests)
+};
+
+// Locate the block of a global column (blocks sorted by col0).
+__device__ __forceinline__ int find_block(const Block* blocks, int nblocks, int col) {
+  int lo = 0, hi = nblocks - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (blocks[mid].col0 <= col) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename T>
+__device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
+
+}  // namespace lw

@@ -102,6 +102,8 @@ typedef struct rrtmg_lw_exec {
   int32_t sync;            /* 1 = return after the results are in place (host
                               memory always syncs); 0 = leave work queued */
   int32_t reserved;
+  float *kernel_ms;        /* optional float[2]: device time of the McICA and
+                              column kernels of this call (forces a sync) */
 } rrtmg_lw_exec;
 
 /* rlwinit (radlw_main.F90:1322): validates iovr, sets fluxfac/heatfac, builds

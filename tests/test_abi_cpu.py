@@ -1,0 +1,72 @@
+"""CPU-side checks of the C ABI: the CUDA library loads without a GPU and
+exports every function declared in include/*.h; host-side validation paths
+return errors instead of crashing."""
+import ctypes as C
+import glob
+import os
+import re
+
+import pytest
+
+from ccpp_physics_b200 import abi
+
+ROOT = os.path.join(os.path.dirname(__file__), "..")
+
+
+def _declared():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        txt = open(h).read()
+        names |= set(re.findall(r"^\s*(?:int|void)\s+(rrtmg_lw_gpu_\w+)\s*\(", txt, re.M))
+    return names
+
+
+def test_library_exports_header_symbols():
+    from ccpp_physics_b200 import rrtmg_lw as lw
+    L = lw.lib()
+    declared = _declared()
+    assert {"rrtmg_lw_gpu_init", "rrtmg_lw_gpu_run", "rrtmg_lw_gpu_run_ex"} <= declared
+    for n in sorted(declared):
+        assert hasattr(L, n), n
+
+
+def test_struct_layout_matches_header(tmp_path):
+    """ctypes mirror == C header: sizeof and every field offset, from gcc."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not available")
+    structs = {"rrtmg_lw_run_args": abi.RunArgs, "rrtmg_lw_init_args": abi.InitArgs,
+               "rrtmg_lw_exec": abi.ExecArgs}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rrtmg_lw_gpu.h"', 'int main(void){']
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0;}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                  check=True).stdout.splitlines())
+    for cname, py in structs.items():
+        assert int(got[cname]) == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(py, fname).offset, (cname, fname)
+
+
+def test_run_before_init_reports_error():
+    import numpy as np
+    from ccpp_physics_b200 import rrtmg_lw as lw, synthetic
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("checks the no-GPU path")
+    except ImportError:
+        pass
+    prof = synthetic.make_profiles(2, 10, seed=1)
+    msg, err = lw.run_profile(prof, abi.alloc_outputs(2, 10))
+    assert err == 1 and "init" in msg
+    rc, msg = lw.rlwinit()
+    assert rc == 1 and "CUDA" in msg
