@@ -157,9 +157,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncols", type=int, default=0, help="override the column count (profiling runs)")
+    ap.add_argument("--quick", action="store_true", help="FP64 device-resident loop only (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.ncols:
+        cfg["ncols"] = args.ncols
+        cfg["name"] = f"{cfg['name']}_first{args.ncols}"
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -186,7 +191,10 @@ def main():
     prof = synthetic.make_profiles(ncols, nlay, seed=1, cloudy=cfg["cloudy"], col_offset=rank * ncols,
                                    device="cuda")
     out = abi.alloc_outputs(ncols, nlay, hlw0=True, like="cuda")
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library and the CUDA events must share it (the
+    # legacy default stream does not order work of non-blocking streams)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
 
     def step(precision="fp64", o=out, kernel_ms=None):
@@ -227,6 +235,11 @@ def main():
         ms64 = timed(lambda: step("fp64"), args.steps)
     value = world * ncols * args.steps / (ms64 / 1e3)
     ref64 = {k: v.clone() for k, v in out.items()}
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "value": value, "ms_per_step": ms64 / args.steps,
+                              "config": cfg["name"]}), flush=True)
+        return
 
     # per-kernel device time (dominant kernel for the roofline)
     import ctypes as C

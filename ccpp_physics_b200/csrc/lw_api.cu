@@ -218,7 +218,8 @@ namespace {
 
 // Validate arguments the way rrtmg_lw_run reports errors (RLM:713-760);
 // returns -1 when the call is a no-op (lslwr false or npts == 0).
-int validate(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg, int32_t errmsg_len) {
+int validate(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg, int32_t errmsg_len,
+             bool need_outputs = true) {
   if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_lw_run: null argument struct"); return 1; }
   if (!a->lslwr) return -1;                                  // RLM:727
   if (a->nlay < 1 || a->nlp1 != a->nlay + 1 || a->npts < 0 || (a->ldim != 0 && a->ldim < a->npts)) {
@@ -255,9 +256,13 @@ int validate(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg, i
   const double* req[] = {a->plyr, a->plvl, a->tlyr, a->tlvl, a->qlyr, a->olyr, a->gasvmr_co2, a->gasvmr_n2o,
                          a->gasvmr_ch4, a->gasvmr_o2, a->gasvmr_co, a->gasvmr_cfc11, a->gasvmr_cfc12,
                          a->gasvmr_cfc22, a->gasvmr_ccl4, a->aeraod, a->aerssa, a->sfemis, a->sfgtmp,
-                         a->dzlyr, a->delpin, a->cld_cf, a->hlwc, a->topflx, a->sfcflx, a->cldtau};
+                         a->dzlyr, a->delpin, a->cld_cf};
   for (const double* p : req)
-    if (!p) { set_msg(errmsg, errmsg_len, "rrtmg_lw_run: a required array pointer is NULL"); return 1; }
+    if (!p) { set_msg(errmsg, errmsg_len, "rrtmg_lw_run: a required input array pointer is NULL"); return 1; }
+  const double* outs[] = {a->hlwc, a->topflx, a->sfcflx, a->cldtau};
+  if (need_outputs)
+    for (const double* p : outs)
+      if (!p) { set_msg(errmsg, errmsg_len, "rrtmg_lw_run: a required output array pointer is NULL"); return 1; }
   if (a->isubclw == 2 && !a->icseed) { set_msg(errmsg, errmsg_len, "rrtmg_lw_run: icseed is NULL"); return 1; }
   if (x && x->precision != RRTMG_LW_FP64 && x->precision != RRTMG_LW_FP32) {
     set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: precision %d not available in this build", x->precision);
@@ -515,7 +520,7 @@ extern "C" int rrtmg_lw_gpu_gas_optics(const rrtmg_lw_run_args* a, int32_t preci
   rrtmg_lw_exec x{precision, RRTMG_LW_DEVICE, stream, 1, 0, nullptr};
   rrtmg_lw_run_args a2 = *a;
   a2.lslwr = 1;
-  int v = validate(&a2, &x, errmsg, errmsg_len);
+  int v = validate(&a2, &x, errmsg, errmsg_len, false);
   if (v == -1) return 0;
   if (v) return 1;
   if (!taug || !fracs) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_gas_optics: NULL output"); return 1; }

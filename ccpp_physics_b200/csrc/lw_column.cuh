@@ -391,7 +391,7 @@ lw_column_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, 
       s.ci[3] = min(180, max(1, (int)(tz0 - 159.0)));
     }
     // McICA sub-column flags of this column
-    const bool mc = lcf1 && f.isubclw > 0;
+    const bool mc = lcf1 && f.isubclw > 0 && !f.gas_only;   // gas-only launches have no McICA flags
     if (mc) {
       const uint32_t* src = bits_g + (size_t)c * NGPT * nw;
       for (int w = t; w < NGPT * nw; w += 32 * V) s.bits[w] = src[w];
