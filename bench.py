@@ -243,13 +243,15 @@ def main():
 
     # per-kernel device time (dominant kernel for the roofline)
     import ctypes as C
-    kms = (C.c_float * 2)()
+    kms = (C.c_float * 3)()
     kt = []
     for _ in range(3):
         step("fp64", kernel_ms=kms)
-        kt.append((kms[0], kms[1]))
+        kt.append((kms[0], kms[1], kms[2]))
     mcica_ms = sum(k[0] for k in kt) / len(kt)
-    col_ms = sum(k[1] for k in kt) / len(kt)
+    gas_ms = sum(k[1] for k in kt) / len(kt)
+    rt_ms = sum(k[2] for k in kt) / len(kt)
+    col_ms = gas_ms + rt_ms
 
     # ---- FP32 path ----
     out32 = abi.alloc_outputs(ncols, nlay, hlw0=True, like="cuda")
@@ -261,8 +263,8 @@ def main():
         return float(torch.sqrt(torch.mean((a - b) ** 2)).item())
 
     paths = {
-        "fp64": {"value": value, "ms_per_step": ms64 / args.steps, "column_kernel_ms": col_ms,
-                 "mcica_kernel_ms": mcica_ms},
+        "fp64": {"value": value, "ms_per_step": ms64 / args.steps, "gas_kernel_ms": gas_ms,
+                 "rt_kernel_ms": rt_ms, "mcica_kernel_ms": mcica_ms},
         "fp32": {"value": world * ncols * args.steps / (ms32 / 1e3), "ms_per_step": ms32 / args.steps,
                  "flux_rmse_wm2": rmse(torch.cat([out32["topflx"], out32["sfcflx"]], 1),
                                        torch.cat([ref64["topflx"], ref64["sfcflx"]], 1)),

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -27,14 +28,14 @@ extern "C" const unsigned char rrtmg_lw_tables_blob[];
 extern "C" const unsigned char rrtmg_lw_tables_blob_end[];
 
 namespace lw {
-cudaError_t prepare_column_fp64();
-cudaError_t prepare_column_fp32();
+size_t scratch_per_column_fp64(int V);
+size_t scratch_per_column_fp32(int V);
 cudaError_t launch_column_fp64(int V, bool hlwb, const Block*, int, const Block&, int, const Flags&, const Consts&,
-                               const Tables<double>&, const Tables<double>&, const uint32_t*, double*,
-                               double*, int, cudaStream_t);
+                               const Tables<double>&, const Tables<double>&, const uint32_t*, void*, size_t,
+                               double*, double*, int, cudaStream_t, cudaEvent_t);
 cudaError_t launch_column_fp32(int V, bool hlwb, const Block*, int, const Block&, int, const Flags&, const Consts&,
-                               const Tables<float>&, const Tables<double>&, const uint32_t*, double*,
-                               double*, int, cudaStream_t);
+                               const Tables<float>&, const Tables<double>&, const uint32_t*, void*, size_t,
+                               double*, double*, int, cudaStream_t, cudaEvent_t);
 cudaError_t mcica_upload_powers();
 cudaError_t mcica_launch(const Block*, int, const Block&, int, int, int, int, int, const double*,
                          const int32_t*, int, uint32_t*, int, cudaStream_t);
@@ -65,6 +66,8 @@ struct Workspace {
   size_t dbuf_bytes = 0;
   uint32_t* bits = nullptr;   // McICA sub-column flags
   size_t bits_bytes = 0;
+  char* scratch = nullptr;    // gas optics -> transfer hand-off (kernel A -> B)
+  size_t scratch_bytes = 0;
   Block* dblocks = nullptr;   // block descriptors on the device
   size_t dblocks_n = 0;
   Block* hblocks = nullptr;   // pinned host copy of the descriptors
@@ -204,11 +207,13 @@ extern "C" int rrtmg_lw_gpu_init(const rrtmg_lw_init_args* a, char* errmsg, int3
   CK(cudaMemcpy(g.tbl64, tb.data(), tb.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
   CK(cudaMemcpy(g.tbl32, tb32.data(), tb32.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
   CK(mcica_upload_powers(), "mcica powers upload");
-  CK(prepare_column_fp64(), "kernel attributes (fp64)");
-  CK(prepare_column_fp32(), "kernel attributes (fp32)");
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, g.device), "cudaDeviceGetAttribute");
   CK(mcica_prepare(optin), "kernel attributes (mcica)");
+  // per-thread stack for the spilled kernels (a context setting, gone with the process)
+  size_t stack = 0;
+  CK(cudaDeviceGetLimit(&stack, cudaLimitStackSize), "cudaDeviceGetLimit");
+  if (stack < 4096) CK(cudaDeviceSetLimit(cudaLimitStackSize, 4096), "cudaDeviceSetLimit(stack)");
   g.ready = true;
   return errflg;
 }
@@ -273,6 +278,9 @@ int validate(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg, i
 
 int pick_v(int nlay) { return nlay <= 63 ? 2 : nlay <= 127 ? 4 : 8; }
 
+// Device scratch budget of one call (columns are processed in chunks that fit).
+constexpr size_t kScratchBudget = (size_t)6 << 30;
+
 // Sizes (in doubles) of each input/output field for one block.
 struct FieldSizes { size_t n2, n2l, n3, n1; };
 FieldSizes sizes_of(const rrtmg_lw_run_args* a) {
@@ -318,7 +326,7 @@ void block_from_args(const rrtmg_lw_run_args* a, Block* B) {
 int launch(Workspace* w, const Block* hblocks, int nblocks, int ncols, const Flags& f, int precision,
            float* kernel_ms, char* errmsg, int32_t errmsg_len) {
   cudaStream_t st = w->stream;
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   if (kernel_ms)
     for (auto& e : ev) CK(cudaEventCreate(&e), "cudaEventCreate");
   const Block* dblk = nullptr;
@@ -354,23 +362,30 @@ int launch(Workspace* w, const Block* hblocks, int nblocks, int ncols, const Fla
   const int V = pick_v(f.nlay);
   const bool hlwb = f.want_hlwb != 0;
   if (kernel_ms) CK(cudaEventRecord(ev[1], st), "cudaEventRecord");
+  // scratch between the gas-optics and transfer kernels, in chunks of columns
+  const size_t per = (precision == RRTMG_LW_FP64) ? scratch_per_column_fp64(V) : scratch_per_column_fp32(V);
+  size_t budget = kScratchBudget;
+  if (const char* env = std::getenv("RRTMG_LW_GPU_SCRATCH_MB")) budget = (size_t)std::atol(env) << 20;
+  const size_t want = std::min<size_t>((size_t)ncols * per, std::max<size_t>(budget, per));
+  CK(grow(&w->scratch, &w->scratch_bytes, want), "cudaMalloc(scratch)");
   if (precision == RRTMG_LW_FP64) {
     Tables<double> t{g.kt64, g.tbl64, g.tbl64 + (NTBL + 1), g.tbl64 + 2 * (NTBL + 1)};
-    CK(launch_column_fp64(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t, t, w->bits, nullptr, nullptr,
-                          g.num_sms, st),
-       "column kernel launch (fp64)");
+    CK(launch_column_fp64(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t, t, w->bits, w->scratch, w->scratch_bytes,
+                          nullptr, nullptr, g.num_sms, st, ev[3]),
+       "column kernels launch (fp64)");
   } else {
     Tables<float> t{g.kt32, g.tbl32, g.tbl32 + (NTBL + 1), g.tbl32 + 2 * (NTBL + 1)};
     Tables<double> t64{g.kt64, g.tbl64, g.tbl64 + (NTBL + 1), g.tbl64 + 2 * (NTBL + 1)};
-    CK(launch_column_fp32(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t, t64, w->bits, nullptr, nullptr,
-                          g.num_sms, st),
-       "column kernel launch (fp32)");
+    CK(launch_column_fp32(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t, t64, w->bits, w->scratch,
+                          w->scratch_bytes, nullptr, nullptr, g.num_sms, st, ev[3]),
+       "column kernels launch (fp32)");
   }
   if (kernel_ms) {
     CK(cudaEventRecord(ev[2], st), "cudaEventRecord");
     CK(cudaEventSynchronize(ev[2]), "kernel execution");
     CK(cudaEventElapsedTime(&kernel_ms[0], ev[0], ev[1]), "cudaEventElapsedTime");
-    CK(cudaEventElapsedTime(&kernel_ms[1], ev[1], ev[2]), "cudaEventElapsedTime");
+    CK(cudaEventElapsedTime(&kernel_ms[1], ev[1], ev[3]), "cudaEventElapsedTime");
+    CK(cudaEventElapsedTime(&kernel_ms[2], ev[3], ev[2]), "cudaEventElapsedTime");
     for (auto& e : ev) cudaEventDestroy(e);
   }
   return 0;
@@ -412,6 +427,7 @@ extern "C" int rrtmg_lw_gpu_run_ex(const rrtmg_lw_run_args* a, const rrtmg_lw_ex
     int r = launch(&wl, &B, 1, a->npts, f, x->precision, x->kernel_ms, errmsg, errmsg_len);
     // launch() may have grown buffers
     w->bits = wl.bits; w->bits_bytes = wl.bits_bytes; w->dblocks = wl.dblocks; w->dblocks_n = wl.dblocks_n;
+    w->scratch = wl.scratch; w->scratch_bytes = wl.scratch_bytes;
     w->hblocks = wl.hblocks; w->hblocks_n = wl.hblocks_n;
     if (r) return r;
     if (x->sync) CK(cudaStreamSynchronize(st), "kernel execution");
@@ -469,6 +485,7 @@ extern "C" int rrtmg_lw_gpu_run_ex(const rrtmg_lw_run_args* a, const rrtmg_lw_ex
   wl.stream = st;
   int r = launch(&wl, &B, 1, a->npts, f, x->precision, x->kernel_ms, errmsg, errmsg_len);
   w->bits = wl.bits; w->bits_bytes = wl.bits_bytes; w->dblocks = wl.dblocks; w->dblocks_n = wl.dblocks_n;
+    w->scratch = wl.scratch; w->scratch_bytes = wl.scratch_bytes;
   w->hblocks = wl.hblocks; w->hblocks_n = wl.hblocks_n;
   if (r) return r;
   for (int k = 0; k < nout; ++k) {
@@ -538,11 +555,13 @@ extern "C" int rrtmg_lw_gpu_gas_optics(const rrtmg_lw_run_args* a, int32_t preci
   const int V = pick_v(a2.nlay);
   Tables<double> t64{g.kt64, g.tbl64, g.tbl64 + (NTBL + 1), g.tbl64 + 2 * (NTBL + 1)};
   if (precision == RRTMG_LW_FP64) {
-    CK(launch_column_fp64(V, false, nullptr, 1, B, a2.npts, f, g.cs, t64, t64, nullptr, taug, fracs, g.num_sms, st),
+    CK(launch_column_fp64(V, false, nullptr, 1, B, a2.npts, f, g.cs, t64, t64, nullptr, nullptr, 0, taug, fracs,
+                          g.num_sms, st, nullptr),
        "gas optics launch");
   } else {
     Tables<float> t{g.kt32, g.tbl32, g.tbl32 + (NTBL + 1), g.tbl32 + 2 * (NTBL + 1)};
-    CK(launch_column_fp32(V, false, nullptr, 1, B, a2.npts, f, g.cs, t, t64, nullptr, taug, fracs, g.num_sms, st),
+    CK(launch_column_fp32(V, false, nullptr, 1, B, a2.npts, f, g.cs, t, t64, nullptr, nullptr, 0, taug, fracs,
+                          g.num_sms, st, nullptr),
        "gas optics launch");
   }
   CK(cudaStreamSynchronize(st), "gas optics execution");
@@ -557,6 +576,7 @@ extern "C" void rrtmg_lw_gpu_finalize(void) {
     if (w->stream) cudaStreamSynchronize(w->stream);
     if (w->dbuf) cudaFree(w->dbuf);
     if (w->bits) cudaFree(w->bits);
+    if (w->scratch) cudaFree(w->scratch);
     if (w->dblocks) cudaFree(w->dblocks);
     if (w->hblocks) cudaFreeHost(w->hblocks);
     if (w->stream) cudaStreamDestroy(w->stream);

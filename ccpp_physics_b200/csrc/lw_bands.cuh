@@ -11,6 +11,17 @@
 
 #include "lw_common.cuh"
 
+// Unrolling of the per-band g-point loops: fully unrolled (the default), every
+// table gather of the band uses a constant offset from a per-layer row pointer.
+#ifndef LW_GLOOP_FULL
+#define LW_GLOOP_FULL 1
+#endif
+#if LW_GLOOP_FULL
+#define LW_GLOOP _Pragma("unroll")
+#else
+#define LW_GLOOP _Pragma("unroll 1")
+#endif
+
 namespace lw {
 
 // Per-layer state produced by setcoef (RLM:2151-2406) and the driver
@@ -27,16 +38,62 @@ struct Lay {
   bool lower;          // k <= laytrop
 };
 
+// Shared-memory SoA record of the per-layer state (fields below), read by
+// each band routine for the fields it needs, so the record does not occupy
+// registers across the band loop.
+enum LayField {
+  LF_FAC00, LF_FAC01, LF_FAC10, LF_FAC11, LF_SELFFAC, LF_SELFFRAC, LF_FORFAC, LF_FORFRAC, LF_MINORFRAC,
+  LF_SCALEMINOR, LF_SCALEMINORN2, LF_COL1, LF_COL2, LF_COL3, LF_COL4, LF_COL5, LF_COL6, LF_COL7,
+  LF_COLDRY, LF_COLBRD, LF_WX1, LF_WX2, LF_WX3, LF_WX4, LF_PAVEL, N_LF
+};
+
+template <typename R>
+struct LayRef {
+  const R* sc;      // [N_LF][nlp]
+  const int* si;    // [nlp] packed indices
+  int t, nlp;
+  bool lower;
+  __device__ __forceinline__ Lay<R> load() const {
+    Lay<R> L;
+    L.fac00 = sc[LF_FAC00 * nlp + t]; L.fac01 = sc[LF_FAC01 * nlp + t];
+    L.fac10 = sc[LF_FAC10 * nlp + t]; L.fac11 = sc[LF_FAC11 * nlp + t];
+    L.selffac = sc[LF_SELFFAC * nlp + t]; L.selffrac = sc[LF_SELFFRAC * nlp + t];
+    L.forfac = sc[LF_FORFAC * nlp + t]; L.forfrac = sc[LF_FORFRAC * nlp + t];
+    L.minorfrac = sc[LF_MINORFRAC * nlp + t];
+    L.scaleminor = sc[LF_SCALEMINOR * nlp + t]; L.scaleminorn2 = sc[LF_SCALEMINORN2 * nlp + t];
+#pragma unroll
+    for (int m = 0; m < 7; ++m) L.col[m] = sc[(LF_COL1 + m) * nlp + t];
+    L.coldry = sc[LF_COLDRY * nlp + t]; L.colbrd = sc[LF_COLBRD * nlp + t];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) L.wx[m] = sc[(LF_WX1 + m) * nlp + t];
+    L.pavel = sc[LF_PAVEL * nlp + t];
+    const int i0 = si[t];
+    L.jp = i0 & 0xff; L.jt = (i0 >> 8) & 0xf; L.jt1 = (i0 >> 12) & 0xf;
+    L.indself = (i0 >> 16) & 0xf; L.indfor = (i0 >> 20) & 0xf; L.indminor = (i0 >> 24) & 0x1f;
+    L.lower = lower;
+    // For a pressure profile that is not monotonic the count-based split
+    // (laytrop) can send a layer to the branch of the other atmosphere, where
+    // the reference indexes its tables out of bounds; keep indices in range.
+    if (L.lower) { L.jp = min(L.jp, 12); L.indself = max(L.indself, 1); }
+    else L.jp = max(L.jp, 13);
+    return L;
+  }
+};
+
 template <typename R>
 struct KT {
   const R* __restrict__ p;
   // Fortran-order accessors, 1-based indices
-  __device__ __forceinline__ R a1(int off, int i) const { return ldg(p + off + (i - 1)); }
+  __device__ __forceinline__ R at(long long o) const {
+    if (!LW_OK(o >= 0 && o < RRTMG_LW_TABLES_NDOUBLE, 1, o)) return R(0);
+    return ldg(p + o);
+  }
+  __device__ __forceinline__ R a1(int off, int i) const { return at(off + (i - 1)); }
   __device__ __forceinline__ R a2(int off, int n1, int i, int j) const {
-    return ldg(p + off + (i - 1) + n1 * (j - 1));
+    return at(off + (i - 1) + n1 * (j - 1));
   }
   __device__ __forceinline__ R a3(int off, int n1, int n2, int i, int j, int k) const {
-    return ldg(p + off + (i - 1) + n1 * ((j - 1) + n2 * (k - 1)));
+    return at(off + (i - 1) + n1 * ((j - 1) + n2 * (k - 1)));
   }
   __device__ __forceinline__ R chi(int m, int j) const { return a2(lwtab::chi_mls, 7, m, j); }
 };
@@ -187,14 +244,15 @@ __device__ __forceinline__ R adjcol(R col, R ref, R thresh, R base, R expo) {
 // ---------------------------------------------------------------------------
 
 template <typename R, typename E>  // taugb01, RLM:4023-4125
-__device__ void taugb01(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb01(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 10;
   R scalen2 = L.colbrd * L.scaleminorn2;
   if (L.lower) {
     int i0 = lo0<R, 0>(L), i1 = lo1<R, 0>(L);
     R pp = L.pavel;
     R corradj = (pp < R(250)) ? one<R>() - R(0.15) * (R(250) - pp) / R(154.4) : one<R>();
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b01_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b01_forref, ng, ig, L);
@@ -205,7 +263,7 @@ __device__ void taugb01(const KT<R>& t, const Lay<R>& L, E emit) {
   } else {
     int i0 = up0<R, 0>(L), i1 = up1<R, 0>(L);
     R corradj = one<R>() - R(0.15) * (L.pavel / R(95.6));
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R taufor = forc(t, lwtab::b01_forref, ng, ig, L);
       R taun2 = scalen2 * minor2(t, lwtab::b01_kb_mn2, ng, ig, L);
@@ -216,12 +274,13 @@ __device__ void taugb01(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb02, RLM:4131-4203
-__device__ void taugb02(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb02(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 12;
   if (L.lower) {
     int i0 = lo0<R, 1>(L), i1 = lo1<R, 1>(L);
     R corradj = one<R>() - R(0.05) * (L.pavel - R(100)) / R(900);
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b02_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b02_forref, ng, ig, L);
@@ -230,7 +289,7 @@ __device__ void taugb02(const KT<R>& t, const Lay<R>& L, E emit) {
     }
   } else {
     int i0 = up0<R, 1>(L), i1 = up1<R, 1>(L);
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R taufor = forc(t, lwtab::b02_forref, ng, ig, L);
       emit(ig - 1, L.col[0] * absk(t, lwtab::b02_absb, ng, ig, L, i0, i1) + taufor, t.a1(lwtab::b02_fracrefb, ig));
@@ -239,7 +298,8 @@ __device__ void taugb02(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb03, RLM:4210-4512
-__device__ void taugb03(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb03(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 16;
   R adjcoln2o = adjcol<R>(L.col[3], L.coldry * t.chi(4, L.jp + 1), R(1.5), R(0.5), R(0.65));
   if (L.lower) {
@@ -247,7 +307,7 @@ __device__ void taugb03(const KT<R>& t, const Lay<R>& L, E emit) {
     Low<R> o = low_setup<R, 2>(L, L.col[0], t.chi(1, L.jp) / t.chi(2, L.jp), t.chi(1, L.jp + 1) / t.chi(2, L.jp + 1), L.col[1]);
     Spec<R> sm = spec<R>(L.col[0], rma, L.col[1], R(8));
     Spec<R> sp = spec<R>(L.col[0], rpa, L.col[1], R(8));
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b03_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b03_forref, ng, ig, L);
@@ -262,7 +322,7 @@ __device__ void taugb03(const KT<R>& t, const Lay<R>& L, E emit) {
     Up<R> u = up_setup<R, 2>(L, L.col[0], t.chi(1, L.jp) / t.chi(2, L.jp), t.chi(1, L.jp + 1) / t.chi(2, L.jp + 1), L.col[1]);
     Spec<R> sm = spec<R>(L.col[0], rmb, L.col[1], R(4));
     Spec<R> sp = spec<R>(L.col[0], rpb, L.col[1], R(4));
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R taufor = forc(t, lwtab::b03_forref, ng, ig, L);
       R absn2o = minor3(t, lwtab::b03_kb_mn2o, ng, 5, ig, sm.js, sm.fs, L);
@@ -273,13 +333,14 @@ __device__ void taugb03(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb04, RLM:4518-4757
-__device__ void taugb04(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb04(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 14;
   if (L.lower) {
     R rpa = t.chi(1, 11) / t.chi(2, 11);
     Low<R> o = low_setup<R, 3>(L, L.col[0], t.chi(1, L.jp) / t.chi(2, L.jp), t.chi(1, L.jp + 1) / t.chi(2, L.jp + 1), L.col[1]);
     Spec<R> sp = spec<R>(L.col[0], rpa, L.col[1], R(8));
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b04_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b04_forref, ng, ig, L);
@@ -293,7 +354,7 @@ __device__ void taugb04(const KT<R>& t, const Lay<R>& L, E emit) {
     Spec<R> sp = spec<R>(L.col[2], rpb, L.col[1], R(4));
     // empirical scalings of g-points 8..14 (RLM:4746-4752)
     const R sc[14] = {R(1), R(1), R(1), R(1), R(1), R(1), R(1), R(0.92), R(0.88), R(1.07), R(1.1), R(0.99), R(0.88), R(0.943)};
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tau = up_major(t, lwtab::b04_absb, ng, ig, u);
       if (ig >= 8) tau = tau * sc[ig - 1];
@@ -303,14 +364,15 @@ __device__ void taugb04(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb05, RLM:4764-5023
-__device__ void taugb05(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb05(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 16;
   if (L.lower) {
     R rpa = t.chi(1, 5) / t.chi(2, 5), rma = t.chi(1, 7) / t.chi(2, 7);
     Low<R> o = low_setup<R, 4>(L, L.col[0], t.chi(1, L.jp) / t.chi(2, L.jp), t.chi(1, L.jp + 1) / t.chi(2, L.jp + 1), L.col[1]);
     Spec<R> sm = spec<R>(L.col[0], rma, L.col[1], R(8));
     Spec<R> sp = spec<R>(L.col[0], rpa, L.col[1], R(8));
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b05_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b05_forref, ng, ig, L);
@@ -323,7 +385,7 @@ __device__ void taugb05(const KT<R>& t, const Lay<R>& L, E emit) {
     R rpb = t.chi(3, 43) / t.chi(2, 43);
     Up<R> u = up_setup<R, 4>(L, L.col[2], t.chi(3, L.jp) / t.chi(2, L.jp), t.chi(3, L.jp + 1) / t.chi(2, L.jp + 1), L.col[1]);
     Spec<R> sp = spec<R>(L.col[2], rpb, L.col[1], R(4));
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig)
       emit(ig - 1, up_major(t, lwtab::b05_absb, ng, ig, u) + L.wx[0] * t.a1(lwtab::b05_ccl4, ig),
            planck(t, lwtab::b05_fracrefb, ng, ig, sp.js, sp.fs));
@@ -331,12 +393,13 @@ __device__ void taugb05(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb06, RLM:5030-5111
-__device__ void taugb06(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb06(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 8;
   if (L.lower) {
     int i0 = lo0<R, 5>(L), i1 = lo1<R, 5>(L);
     R adjcolco2 = adjcol<R>(L.col[1], L.coldry * t.chi(2, L.jp + 1), R(3), R(2), R(0.77));
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b06_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b06_forref, ng, ig, L);
@@ -346,7 +409,7 @@ __device__ void taugb06(const KT<R>& t, const Lay<R>& L, E emit) {
            t.a1(lwtab::b06_fracrefa, ig));
     }
   } else {
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig)
       emit(ig - 1, L.wx[1] * t.a1(lwtab::b06_cfc11adj, ig) + L.wx[2] * t.a1(lwtab::b06_cfc12, ig),
            t.a1(lwtab::b06_fracrefa, ig));
@@ -354,7 +417,8 @@ __device__ void taugb06(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb07, RLM:5118-5375
-__device__ void taugb07(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb07(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 12;
   if (L.lower) {
     R rpa = t.chi(1, 3) / t.chi(3, 3), rma = t.chi(1, 3) / t.chi(3, 3);
@@ -362,7 +426,7 @@ __device__ void taugb07(const KT<R>& t, const Lay<R>& L, E emit) {
     Spec<R> sm = spec<R>(L.col[0], rma, L.col[2], R(8));
     Spec<R> sp = spec<R>(L.col[0], rpa, L.col[2], R(8));
     R adjcolco2 = adjcol<R>(L.col[1], L.coldry * t.chi(2, L.jp + 1), R(3), R(3), R(0.79));
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b07_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b07_forref, ng, ig, L);
@@ -375,7 +439,7 @@ __device__ void taugb07(const KT<R>& t, const Lay<R>& L, E emit) {
     int i0 = up0<R, 6>(L), i1 = up1<R, 6>(L);
     // RLM:5366-5371
     const R sc[12] = {R(1), R(1), R(1), R(1), R(1), R(0.92), R(0.88), R(1.07), R(1.1), R(0.99), R(0.855), R(1)};
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R absco2 = minor2(t, lwtab::b07_kb_mco2, ng, ig, L);
       R tau = L.col[2] * absk(t, lwtab::b07_absb, ng, ig, L, i0, i1) + adjcolco2 * absco2;
@@ -386,12 +450,13 @@ __device__ void taugb07(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb08, RLM:5382-5501
-__device__ void taugb08(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb08(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 8;
   R adjcolco2 = adjcol<R>(L.col[1], L.coldry * t.chi(2, L.jp + 1), R(3), R(2), R(0.65));
   if (L.lower) {
     int i0 = lo0<R, 7>(L), i1 = lo1<R, 7>(L);
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b08_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b08_forref, ng, ig, L);
@@ -405,7 +470,7 @@ __device__ void taugb08(const KT<R>& t, const Lay<R>& L, E emit) {
     }
   } else {
     int i0 = up0<R, 7>(L), i1 = up1<R, 7>(L);
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R absco2 = minor2(t, lwtab::b08_kb_mco2, ng, ig, L);
       R absn2o = minor2(t, lwtab::b08_kb_mn2o, ng, ig, L);
@@ -417,7 +482,8 @@ __device__ void taugb08(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb09, RLM:5508-5753
-__device__ void taugb09(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb09(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 12;
   R adjcoln2o = adjcol<R>(L.col[3], L.coldry * t.chi(4, L.jp + 1), R(1.5), R(0.5), R(0.65));
   if (L.lower) {
@@ -425,7 +491,7 @@ __device__ void taugb09(const KT<R>& t, const Lay<R>& L, E emit) {
     Low<R> o = low_setup<R, 8>(L, L.col[0], t.chi(1, L.jp) / t.chi(6, L.jp), t.chi(1, L.jp + 1) / t.chi(6, L.jp + 1), L.col[4]);
     Spec<R> sm = spec<R>(L.col[0], rma, L.col[4], R(8));
     Spec<R> sp = spec<R>(L.col[0], rpa, L.col[4], R(8));
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b09_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b09_forref, ng, ig, L);
@@ -435,7 +501,7 @@ __device__ void taugb09(const KT<R>& t, const Lay<R>& L, E emit) {
     }
   } else {
     int i0 = up0<R, 8>(L), i1 = up1<R, 8>(L);
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R absn2o = minor2(t, lwtab::b09_kb_mn2o, ng, ig, L);
       emit(ig - 1, L.col[4] * absk(t, lwtab::b09_absb, ng, ig, L, i0, i1) + adjcoln2o * absn2o,
@@ -445,11 +511,12 @@ __device__ void taugb09(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb10, RLM:5759-5829
-__device__ void taugb10(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb10(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 6;
   if (L.lower) {
     int i0 = lo0<R, 9>(L), i1 = lo1<R, 9>(L);
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b10_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b10_forref, ng, ig, L);
@@ -457,7 +524,7 @@ __device__ void taugb10(const KT<R>& t, const Lay<R>& L, E emit) {
     }
   } else {
     int i0 = up0<R, 9>(L), i1 = up1<R, 9>(L);
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R taufor = forc(t, lwtab::b10_forref, ng, ig, L);
       emit(ig - 1, L.col[0] * absk(t, lwtab::b10_absb, ng, ig, L, i0, i1) + taufor, t.a1(lwtab::b10_fracrefb, ig));
@@ -466,12 +533,13 @@ __device__ void taugb10(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb11, RLM:5836-5923
-__device__ void taugb11(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb11(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 8;
   R scaleo2 = L.col[5] * L.scaleminor;
   if (L.lower) {
     int i0 = lo0<R, 10>(L), i1 = lo1<R, 10>(L);
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b11_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b11_forref, ng, ig, L);
@@ -481,7 +549,7 @@ __device__ void taugb11(const KT<R>& t, const Lay<R>& L, E emit) {
     }
   } else {
     int i0 = up0<R, 10>(L), i1 = up1<R, 10>(L);
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R taufor = forc(t, lwtab::b11_forref, ng, ig, L);
       R tauo2 = scaleo2 * minor2(t, lwtab::b11_kb_mo2, ng, ig, L);
@@ -491,7 +559,8 @@ __device__ void taugb11(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb12, RLM:5929-6111
-__device__ void taugb12(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb12(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 8;
   if (L.lower) {
     R rpa = t.chi(1, 10) / t.chi(2, 10);
@@ -503,7 +572,7 @@ __device__ void taugb12(const KT<R>& t, const Lay<R>& L, E emit) {
     R mult = R(8) * parm;
     int jpl = min(8, max(1, 1 + (int)mult));
     R fpl = fracpart(mult);
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b12_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b12_forref, ng, ig, L);
@@ -515,7 +584,8 @@ __device__ void taugb12(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb13, RLM:6117-6361
-__device__ void taugb13(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb13(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 4;
   if (L.lower) {
     R rpa = t.chi(1, 5) / t.chi(4, 5), rma = t.chi(1, 1) / t.chi(4, 1), rma3 = t.chi(1, 3) / t.chi(4, 3);
@@ -524,7 +594,7 @@ __device__ void taugb13(const KT<R>& t, const Lay<R>& L, E emit) {
     Spec<R> smco = spec<R>(L.col[0], rma3, L.col[3], R(8));
     Spec<R> sp = spec<R>(L.col[0], rpa, L.col[3], R(8));
     R adjcolco2 = adjcol<R>(L.col[1], L.coldry * R(3.55e-4), R(3), R(2), R(0.68));
-#pragma unroll 1
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig) {
       R tauself = selfc(t, lwtab::b13_selfref, ng, ig, L);
       R taufor = forc(t, lwtab::b13_forref, ng, ig, L);
@@ -534,14 +604,15 @@ __device__ void taugb13(const KT<R>& t, const Lay<R>& L, E emit) {
            planck(t, lwtab::b13_fracrefa, ng, ig, sp.js, sp.fs));
     }
   } else {
-#pragma unroll 2
+LW_GLOOP
     for (int ig = 1; ig <= ng; ++ig)
       emit(ig - 1, L.col[2] * minor2(t, lwtab::b13_kb_mo3, ng, ig, L), t.a1(lwtab::b13_fracrefb, ig));
   }
 }
 
 template <typename R, typename E>  // taugb14, RLM:6367-6431
-__device__ void taugb14(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb14(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 2;
   if (L.lower) {
     int i0 = lo0<R, 13>(L), i1 = lo1<R, 13>(L);
@@ -558,7 +629,8 @@ __device__ void taugb14(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb15, RLM:6438-6644
-__device__ void taugb15(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb15(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 2;
   if (L.lower) {
     R rpa = t.chi(4, 1) / t.chi(2, 1), rma = t.chi(4, 1) / t.chi(2, 1);
@@ -579,7 +651,8 @@ __device__ void taugb15(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>  // taugb16, RLM:6650-6840
-__device__ void taugb16(const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ void taugb16(const KT<R>& t, const LayRef<R>& LR, E emit) {
+  const Lay<R> L = LR.load();
   constexpr int ng = 2;
   if (L.lower) {
     R rpa = t.chi(1, 6) / t.chi(6, 6);
@@ -599,7 +672,7 @@ __device__ void taugb16(const KT<R>& t, const Lay<R>& L, E emit) {
 }
 
 template <typename R, typename E>
-__device__ __forceinline__ void band_gas_optics(int b, const KT<R>& t, const Lay<R>& L, E emit) {
+__device__ __forceinline__ void band_gas_optics(int b, const KT<R>& t, const LayRef<R>& L, E emit) {
   switch (b) {
     case 0: taugb01(t, L, emit); break;
     case 1: taugb02(t, L, emit); break;

@@ -3,10 +3,12 @@
 // Planck integrals, cloud optics and the flux sums / flux divergence stay
 // FP64 inside the kernel.
 #include <algorithm>
+#include <cstdio>
 
-#include "lw_column.cuh"
+#include "lw_rt.cuh"
 
 #define REAL float
-#define LW_PREPARE_FN prepare_column_fp32
+#define LW_SCRATCH_FN scratch_per_column_fp32
 #define LW_LAUNCH_FN launch_column_fp32
+#define LW_DBG_FN rrtmg_lw_gpu_debug_read_fp32
 #include "lw_column_launch.inc"

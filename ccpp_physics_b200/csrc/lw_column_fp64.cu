@@ -1,10 +1,12 @@
 // FP64 instantiation of the column kernel.  Built with -fmad=false so that
 // every multiply and add rounds separately, in the order of the Fortran.
 #include <algorithm>
+#include <cstdio>
 
-#include "lw_column.cuh"
+#include "lw_rt.cuh"
 
 #define REAL double
-#define LW_PREPARE_FN prepare_column_fp64
+#define LW_SCRATCH_FN scratch_per_column_fp64
 #define LW_LAUNCH_FN launch_column_fp64
+#define LW_DBG_FN rrtmg_lw_gpu_debug_read_fp64
 #include "lw_column_launch.inc"

@@ -23,9 +23,12 @@ __host__ __device__ constexpr int ng_of(int b) {
        : b == 6 ? 12 : b == 7 ? 8 : b == 8 ? 12 : b == 9 ? 6 : b == 10 ? 8 : b == 11 ? 8
        : b == 12 ? 4 : 2;
 }
-__host__ __device__ constexpr int ns_of(int b) {
-  return b == 0 ? 0 : ns_of(b - 1) + ng_of(b - 1);
+__host__ __device__ constexpr int ns_of(int b) {   // first g-point of band b (flat, no recursion)
+  return b == 0 ? 0 : b == 1 ? 10 : b == 2 ? 22 : b == 3 ? 38 : b == 4 ? 52 : b == 5 ? 68 : b == 6 ? 76
+       : b == 7 ? 88 : b == 8 ? 96 : b == 9 ? 108 : b == 10 ? 114 : b == 11 ? 122 : b == 12 ? 130
+       : b == 13 ? 134 : b == 14 ? 136 : 138;
 }
+static_assert(ns_of(15) + ng_of(15) == NGPT, "band layout");
 // reference-atmosphere counts per band (RLM:326-327); nspb(16) = 0 is kept
 __host__ __device__ constexpr int nspa_of(int b) {
   return (b == 2 || b == 3 || b == 4 || b == 6 || b == 8 || b == 11 || b == 12 || b == 14 || b == 15) ? 9 : 1;
@@ -40,12 +43,15 @@ struct Consts {
 };
 
 // Coefficient tables in device memory, in the arithmetic precision R.
+// rlwinit tables (RLM:1474-1501) are one allocation: exp_tbl[0..NTBL], then
+// tfn_tbl, then tau_tbl, each NTBL+1 long (the kernels index them from
+// exp_tbl with constant offsets).
 template <typename R>
 struct Tables {
   const R* kt;       // every radlw_datatb.f array (offsets lwtab::*)
-  const R* exp_tbl;  // rlwinit tables, 0..NTBL (RLM:1474-1501)
-  const R* tfn_tbl;
-  const R* tau_tbl;
+  const R* exp_tbl;
+  const R* tfn_tbl;  // = exp_tbl + NTBL + 1
+  const R* tau_tbl;  // = exp_tbl + 2 * (NTBL + 1)
 };
 
 // Device-side view of one physics block (the arrays of one rrtmg_lw_run call).
@@ -87,5 +93,30 @@ __device__ __forceinline__ int find_block(const Block* blocks, int nblocks, int 
 
 template <typename T>
 __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
+
+// Debug builds (-DLW_DEBUG_CHECKS=1) bounds-check every table, scratch,
+// input and output access of the column kernels: the first violation is
+// recorded in lw_dbg_err {site, index, block, thread} and the access is
+// skipped.  Release builds compile the checks out.
+#ifndef LW_DEBUG_CHECKS
+#define LW_DEBUG_CHECKS 0
+#endif
+#if LW_DEBUG_CHECKS
+static __device__ unsigned int lw_dbg_err[8];
+__device__ __forceinline__ bool lw_ok(bool cond, unsigned site, long long idx) {
+  if (cond) return true;
+  if (atomicCAS(&lw_dbg_err[0], 0u, site) == 0u) {
+    lw_dbg_err[1] = (unsigned)(idx & 0xffffffffll);
+    lw_dbg_err[2] = (unsigned)((unsigned long long)idx >> 32);
+    lw_dbg_err[3] = blockIdx.x;
+    lw_dbg_err[4] = threadIdx.x;
+    __threadfence();
+  }
+  return false;
+}
+#define LW_OK(cond, site, idx) lw_ok((cond), (site), (long long)(idx))
+#else
+#define LW_OK(cond, site, idx) true
+#endif
 
 }  // namespace lw

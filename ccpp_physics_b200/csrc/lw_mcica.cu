@@ -18,6 +18,7 @@
 // the FP64 comparisons/products of the walk are IEEE operations, so the
 // sub-column flags equal the Fortran's bit for bit.
 #include <cstdint>
+#include <cstdio>
 #include <cuda_runtime.h>
 
 #include "lw_common.cuh"
@@ -221,6 +222,12 @@ cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int 
   int grid = min((ncols + wpb - 1) / wpb, num_sms * per_sm);
   if (grid < 1) return cudaSuccess;
   lw_mcica_kernel<<<grid, wpb * 32, smem, st>>>(blocks, nblocks, b0, ncols, a, cldf_dev, seed_dev, dev_ld, bits);
+#if LW_DEBUG_CHECKS
+  {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { fprintf(stderr, "lw debug: mcica kernel failed\n"); return e; }
+  }
+#endif
   return cudaGetLastError();
 }
 

@@ -1,0 +1,331 @@
+// lw_rt.cuh -- kernel B of the RRTMG-LW path: McICA radiative transfer.
+//
+// Replaces rtrnmc (physics/Radiation/RRTMG/radlw_main.F90, RLM:3420-3785)
+// and the output mapping of rrtmg_lw_run (RLM:1228-1304).  One warp owns
+// one column; lane l owns layers/levels V*l .. V*l+V-1 (surface first).  For
+// each g-point the down- and up-sweep recurrences of the two-stream solution
+// are affine maps per layer (radiance -> radiance*t + s): each lane composes
+// its V layers, a 5-step shuffle scan composes across lanes, and each lane
+// replays its layers from the radiance entering its segment, in the
+// Fortran's operation order.  Per-level flux sums stay in FP64 registers of
+// the lane that owns the level, so no cross-lane reduction over g-points is
+// needed.  Inputs come from kernel A (lw_gas.cuh) and the McICA kernel.
+#pragma once
+
+#include "lw_gas.cuh"
+
+namespace lw {
+
+template <typename R> __device__ __forceinline__ R shdn(R v, int d) { return __shfl_down_sync(0xffffffffu, v, d); }
+template <typename R> __device__ __forceinline__ R shup(R v, int d) { return __shfl_up_sync(0xffffffffu, v, d); }
+template <typename R> __device__ __forceinline__ R shidx(R v, int s) { return __shfl_sync(0xffffffffu, v, s); }
+
+// V consecutive values starting at a 16-byte aligned address; the scratch
+// written by kernel A is read once, so it is loaded evict-first (.cs).
+template <typename R, int V>
+__device__ __forceinline__ void load_vec(const R* __restrict__ p, R (&o)[V]) {
+  if constexpr (sizeof(R) == 8) {
+#pragma unroll
+    for (int j = 0; j < V; j += 2) {
+      double2 v = __ldcs(reinterpret_cast<const double2*>(p + j));
+      o[j] = v.x; o[j + 1] = v.y;
+    }
+  } else if constexpr (V % 4 == 0) {
+#pragma unroll
+    for (int j = 0; j < V; j += 4) {
+      float4 v = __ldcs(reinterpret_cast<const float4*>(p + j));
+      o[j] = v.x; o[j + 1] = v.y; o[j + 2] = v.z; o[j + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; j += 2) {
+      float2 v = __ldcs(reinterpret_cast<const float2*>(p + j));
+      o[j] = v.x; o[j + 1] = v.y;
+    }
+  }
+}
+
+// Per-layer two-stream coefficients of one g-point (RLM:3598-3660).
+template <typename R>
+struct LayRT {
+  R tr, gsd, gsu;       // clear-sky transmittance and layer sources
+  R ef, tsd, tsu;       // cloudy: efclrfr and total-sky sources
+};
+
+template <typename R>
+__device__ __forceinline__ void layer_rt(R tau, R frac, R secd, R blay, R plevu, R plevd, bool cloudy, R tcld,
+                                         const Tables<R>& tab, LayRT<R>& o) {
+  const R one = R(1);
+  R odepth = fmax(R(0), secd * tau);
+  R atrgas, trng, gasfac;
+  if (odepth <= R(0.06)) {
+    atrgas = odepth - R(0.5) * odepth * odepth;
+    trng = one - atrgas;
+    gasfac = R(kRec6) * odepth;
+  } else {
+    R tblind = odepth / (R(kBpade) + odepth);
+    int itgas = min(NTBL, max(0, (int)(R(kTblint) * tblind + R(0.5))));
+    if (!LW_OK(itgas >= 0 && itgas <= NTBL, 22, itgas)) itgas = 0;
+    const R* e = tab.exp_tbl + itgas;          // exp, tfn, tau tables are contiguous
+    trng = ldg(e);
+    atrgas = one - trng;
+    gasfac = ldg(e + (NTBL + 1));
+    odepth = ldg(e + 2 * (NTBL + 1));
+  }
+  R dplnku = plevu - blay;
+  R dplnkd = plevd - blay;
+  R bbdgas = frac * (blay + dplnkd * gasfac);
+  R bbugas = frac * (blay + dplnku * gasfac);
+  o.gsd = bbdgas * atrgas;
+  o.gsu = bbugas * atrgas;
+  o.tr = trng;
+  if (cloudy) {
+    R odcld = secd * tcld;
+    o.ef = one - (one - exp(-odcld)) * one;   // clfm = 1 for a McICA cloudy sub-column
+    R odtot = odepth + odcld;
+    R totfac, atrtot;
+    if (odtot < R(0.06)) {
+      totfac = R(kRec6) * odtot;
+      atrtot = odtot - R(0.5) * odtot * odtot;
+    } else {
+      R tblind = odtot / (R(kBpade) + odtot);
+      int ittot = min(NTBL, max(0, (int)(R(kTblint) * tblind + R(0.5))));
+      const R* e = tab.exp_tbl + ittot;
+      totfac = ldg(e + (NTBL + 1));
+      atrtot = one - ldg(e);
+    }
+    R bbdtot = frac * (blay + dplnkd * totfac);
+    R bbutot = frac * (blay + dplnku * totfac);
+    o.tsd = bbdtot * atrtot;
+    o.tsu = bbutot * atrtot;
+  }
+}
+
+template <typename R, int V, bool HLWB>
+__global__ void __launch_bounds__(128, LW_RT_MINB)
+lw_rt_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int ncols, Flags f, Consts cs,
+             Tables<R> tab, Scratch<R> sc, const uint32_t* __restrict__ bits_g) {
+  constexpr int NLP = 32 * V;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int nlay = f.nlay, nlp1 = nlay + 1;
+  const int nw = (nlay + 31) >> 5;
+  const int k0 = V * lane;
+  const double flxfac = 0.5 * cs.fluxfac;   // wtdiff * fluxfac
+
+  for (int cc = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; cc < ncols; cc += nwarps) {
+    const int c = sc.c0 + cc;
+    const Block& B = (nblocks == 1) ? b0 : blocks[find_block(blocks, nblocks, c)];
+    const int i = c - B.col0;
+    const size_t ld = (size_t)B.ld;
+    const bool top = f.top_at_1 != 0;
+    if (!LW_OK(cc < sc.cap && c < sc.ntot && i >= 0 && i < B.npts, 21, cc)) continue;
+    const double* crec = sc.col + (size_t)cc * kColRec;
+    const bool mc = crec[33] != 0.0 && f.isubclw > 0;
+    const R semis = R(crec[32]);
+    const R reflct = R(1) - semis;
+    const R* tcol = sc.tau + (size_t)cc * NGPT * NLP + k0;
+    const R* fcol = sc.frac + (size_t)cc * NGPT * NLP + k0;
+    const R* bcol = sc.band + (size_t)cc * 3 * NBANDS * NLP + k0;
+    const uint32_t* cbw = bits_g + (size_t)c * NGPT * nw + (k0 >> 5);
+    const uint32_t lmask = (k0 >= nlay) ? 0u : (nlay - k0 >= V ? (1u << V) - 1u : (1u << (nlay - k0)) - 1u);
+
+    double acc_tu[V], acc_td[V], acc_cu[V], acc_cd[V];
+    double bnd_tu[HLWB ? V : 1], bnd_td[HLWB ? V : 1];
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      acc_tu[j] = acc_td[j] = acc_cu[j] = acc_cd[j] = 0.0;
+      if constexpr (HLWB) bnd_tu[j] = bnd_td[j] = 0.0;
+    }
+
+#pragma unroll 1
+    for (int b = 0; b < NBANDS; ++b) {
+      // band terms of the lane's layers: pklay(b,k+1), pklev(b,k..k+1), taucld(b,k+1)
+      R blay[V], plev[V], tcld[V];
+      load_vec<R, V>(bcol + (0 * NBANDS + b) * NLP, blay);
+      load_vec<R, V>(bcol + (1 * NBANDS + b) * NLP, plev);
+      load_vec<R, V>(bcol + (2 * NBANDS + b) * NLP, tcld);
+      const R plev_top = shdn(plev[0], 1);    // pklev of the level above the segment
+      const R secd = R(crec[b]);
+      const R pk0 = R(crec[16 + b]);          // pklay(b, 0): surface (RLM:2251-2262)
+      const int ns = ns_of(b), ng = ng_of(b);
+      // inputs of the first g-point of the band; each iteration prefetches the next
+      R ntau[V], nfrac[V];
+      load_vec<R, V>(tcol + (size_t)ns * NLP, ntau);
+      load_vec<R, V>(fcol + (size_t)ns * NLP, nfrac);
+      uint32_t nbits = (mc && lmask && LW_OK((k0 >> 5) < nw, 27, k0)) ? __ldg(cbw + (size_t)ns * nw) : 0u;
+#pragma unroll 1
+      for (int g = ns; g < ns + ng; ++g) {
+        R tau[V], frac[V];
+#pragma unroll
+        for (int j = 0; j < V; ++j) { tau[j] = ntau[j]; frac[j] = nfrac[j]; }
+        const uint32_t cbits = (nbits >> (k0 & 31)) & lmask;
+        if (g + 1 < ns + ng && LW_OK(g + 1 < NGPT, 26, g)) {
+          load_vec<R, V>(tcol + (size_t)(g + 1) * NLP, ntau);
+          load_vec<R, V>(fcol + (size_t)(g + 1) * NLP, nfrac);
+          if (mc && lmask) nbits = __ldg(cbw + (size_t)(g + 1) * nw);
+        }
+        LayRT<R> rt[V];
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+          if (k0 + j < nlay) {
+            const R pu = (j + 1 < V) ? plev[j + 1] : plev_top;
+            layer_rt<R>(tau[j], frac[j], secd, blay[j], pu, plev[j], (cbits >> j) & 1u, tcld[j], tab, rt[j]);
+          } else {
+            rt[j].tr = R(1); rt[j].gsd = R(0); rt[j].gsu = R(0);
+          }
+        }
+        const bool any_cloud = __any_sync(0xffffffffu, cbits != 0);
+
+        // ---- down sweep (RLM:3598-3673): compose, suffix scan, replay ----
+        R Ac = R(1), Bc = R(0), At = R(1), Bt = R(0);
+#pragma unroll
+        for (int j = V - 1; j >= 0; --j) {
+          Bc = rt[j].tr * Bc + rt[j].gsd; Ac = rt[j].tr * Ac;
+          if (any_cloud) {
+            if ((cbits >> j) & 1u) {
+              const R a = rt[j].tr * rt[j].ef;
+              Bt = a * Bt + (rt[j].gsd + (rt[j].tsd - rt[j].gsd)); At = a * At;
+            } else {
+              Bt = rt[j].tr * Bt + rt[j].gsd; At = rt[j].tr * At;
+            }
+          }
+        }
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const R ac = shdn(Ac, d), bc = shdn(Bc, d);
+          R at = R(0), bt = R(0);
+          if (any_cloud) { at = shdn(At, d); bt = shdn(Bt, d); }
+          if (lane + d < 32) {
+            Bc = Ac * bc + Bc; Ac = Ac * ac;
+            if (any_cloud) { Bt = At * bt + Bt; At = At * at; }
+          }
+        }
+        R xc = shdn(Bc, 1), xt = any_cloud ? shdn(Bt, 1) : R(0);
+        if (lane == 31) { xc = R(0); xt = R(0); }
+#pragma unroll
+        for (int j = V - 1; j >= 0; --j) {
+          xc = xc * rt[j].tr + rt[j].gsd;
+          if (any_cloud) {
+            if ((cbits >> j) & 1u) xt = xt * rt[j].tr * rt[j].ef + rt[j].gsd + R(1) * (rt[j].tsd - rt[j].gsd);
+            else xt = xt * rt[j].tr + rt[j].gsd;
+          } else {
+            xt = xc;
+          }
+          acc_cd[j] += (double)xc;
+          acc_td[j] += (double)xt;
+          if constexpr (HLWB) bnd_td[j] += (double)xt;
+        }
+        // ---- surface emission and reflection (RLM:3682-3691) ----
+        const R rad0 = semis * shidx(frac[0], 0) * pk0;
+        const R r0c = rad0 + reflct * shidx(xc, 0);
+        const R r0t = rad0 + reflct * shidx(xt, 0);
+        // ---- up sweep (RLM:3700-3730): compose, prefix scan, replay ----
+        Ac = R(1); Bc = R(0); At = R(1); Bt = R(0);
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+          Bc = rt[j].tr * Bc + rt[j].gsu; Ac = rt[j].tr * Ac;
+          if (any_cloud) {
+            if ((cbits >> j) & 1u) {
+              const R a = rt[j].tr * rt[j].ef;
+              Bt = a * Bt + (rt[j].gsu + (rt[j].tsu - rt[j].gsu)); At = a * At;
+            } else {
+              Bt = rt[j].tr * Bt + rt[j].gsu; At = rt[j].tr * At;
+            }
+          }
+        }
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const R ac = shup(Ac, d), bc = shup(Bc, d);
+          R at = R(0), bt = R(0);
+          if (any_cloud) { at = shup(At, d); bt = shup(Bt, d); }
+          if (lane >= d) {
+            Bc = Ac * bc + Bc; Ac = Ac * ac;
+            if (any_cloud) { Bt = At * bt + Bt; At = At * at; }
+          }
+        }
+        {
+          const R pac = shup(Ac, 1), pbc = shup(Bc, 1);
+          xc = (lane == 0) ? r0c : pac * r0c + pbc;
+          if (any_cloud) {
+            const R pat = shup(At, 1), pbt = shup(Bt, 1);
+            xt = (lane == 0) ? r0t : pat * r0t + pbt;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+          acc_cu[j] += (double)xc;
+          const double ut = any_cloud ? (double)xt : (double)xc;
+          acc_tu[j] += ut;
+          if constexpr (HLWB) bnd_tu[j] += ut;
+          xc = xc * rt[j].tr + rt[j].gsu;
+          if (any_cloud) {
+            if ((cbits >> j) & 1u) xt = xt * rt[j].tr * rt[j].ef + rt[j].gsu + R(1) * (rt[j].tsu - rt[j].gsu);
+            else xt = xt * rt[j].tr + rt[j].gsu;
+          }
+        }
+      }
+      if constexpr (HLWB) {
+        // spectral band heating rate (RLM:3772-3780)
+        double fn[V];
+#pragma unroll
+        for (int j = 0; j < V; ++j) { fn[j] = (bnd_tu[j] - bnd_td[j]) * flxfac; bnd_tu[j] = bnd_td[j] = 0.0; }
+        const double fn_top = __shfl_down_sync(0xffffffffu, fn[0], 1);
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+          const int k = k0 + j;
+          if (k < nlay && LW_OK(k >= 0, 23, k)) {
+            const int r = top ? nlp1 - (k + 1) - 1 : k;
+            const double above = (j + 1 < V) ? fn[j + 1] : fn_top;
+            const double rfdelp = cs.heatfac / B.in[F_DELPIN][i + ld * r];
+            B.out[O_HLWB][i + ld * ((size_t)r + (size_t)nlay * b)] = (fn[j] - above) * rfdelp;
+          }
+        }
+      }
+    }
+
+    // ------------------------------ fluxes and heating rates --------------
+    double fnet[V], fnetc[V];
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const int lv = k0 + j;
+      const double tu = acc_tu[j] * flxfac, td = acc_td[j] * flxfac;
+      const double cu = acc_cu[j] * flxfac, cd = acc_cd[j] * flxfac;
+      fnet[j] = tu - td;
+      fnetc[j] = cu - cd;
+      if (lv <= nlay && LW_OK(lv >= 0, 25, lv)) {
+        if (lv == nlay) {
+          B.out[O_TOPFLX][2 * i + 0] = tu;
+          B.out[O_TOPFLX][2 * i + 1] = cu;
+        }
+        if (lv == 0) {
+          B.out[O_SFCFLX][4 * i + 0] = tu;
+          B.out[O_SFCFLX][4 * i + 1] = cu;
+          B.out[O_SFCFLX][4 * i + 2] = td;
+          B.out[O_SFCFLX][4 * i + 3] = cd;
+        }
+        if (f.want_flxprf) {
+          const int rl = top ? nlp1 - lv - 1 : lv;
+          double* p = B.out[O_FLXPRF] + 4 * (i + ld * (size_t)rl);
+          p[0] = tu; p[1] = td; p[2] = cu; p[3] = cd;
+        }
+      }
+    }
+    const double fn_top = __shfl_down_sync(0xffffffffu, fnet[0], 1);
+    const double fc_top = __shfl_down_sync(0xffffffffu, fnetc[0], 1);
+#pragma unroll
+    for (int j = 0; j < V; ++j) {   // RLM:3754-3770
+      const int k = k0 + j;
+      if (k < nlay && LW_OK(k >= 0 && (top ? nlp1 - (k + 1) - 1 : k) >= 0, 24, k)) {
+        const int r = top ? nlp1 - (k + 1) - 1 : k;
+        const double rfdelp = cs.heatfac / B.in[F_DELPIN][i + ld * r];
+        const double up = (j + 1 < V) ? fnet[j + 1] : fn_top;
+        const double upc = (j + 1 < V) ? fnetc[j + 1] : fc_top;
+        B.out[O_HLWC][i + ld * r] = (fnet[j] - up) * rfdelp;
+        if (f.want_hlw0) B.out[O_HLW0][i + ld * r] = (fnetc[j] - upc) * rfdelp;
+      }
+    }
+  }
+}
+
+}  // namespace lw

@@ -102,8 +102,9 @@ typedef struct rrtmg_lw_exec {
   int32_t sync;            /* 1 = return after the results are in place (host
                               memory always syncs); 0 = leave work queued */
   int32_t reserved;
-  float *kernel_ms;        /* optional float[2]: device time of the McICA and
-                              column kernels of this call (forces a sync) */
+  float *kernel_ms;        /* optional float[3]: device time in ms of the McICA,
+                              gas-optics and transfer kernels of this call
+                              (first chunk for the last two; forces a sync) */
 } rrtmg_lw_exec;
 
 /* rlwinit (radlw_main.F90:1322): validates iovr, sets fluxfac/heatfac, builds
