@@ -28,6 +28,15 @@ extern "C" const unsigned char rrtmg_lw_tables_blob[];
 extern "C" const unsigned char rrtmg_lw_tables_blob_end[];
 
 namespace lw {
+struct NoAllocView {
+  int ready, device, num_sms;
+  const double* kt64;
+  const float* kt32;
+  const double* tbl64;
+  const float* tbl32;
+  Consts cs;
+};
+NoAllocView noalloc_view();
 size_t scratch_per_column_fp64(int V);
 size_t scratch_per_column_fp32(int V);
 cudaError_t launch_column_fp64(int V, bool hlwb, const Block*, int, const Block&, int, const Flags&, const Consts&,
@@ -586,4 +595,11 @@ extern "C" void rrtmg_lw_gpu_finalize(void) {
   tl_ws = nullptr;
   cudaFree(g.kt64); cudaFree(g.kt32); cudaFree(g.tbl64); cudaFree(g.tbl32);
   g = DeviceState();
+}
+
+// Read-only view of the device tables for the allocation-free entry point
+// (lw_noalloc.cu).
+lw::NoAllocView lw::noalloc_view() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return NoAllocView{g.ready ? 1 : 0, g.device, g.num_sms, g.kt64, g.kt32, g.tbl64, g.tbl32, g.cs};
 }

@@ -148,6 +148,22 @@ int rrtmg_lw_gpu_gas_optics(const rrtmg_lw_run_args *args, int32_t precision,
                             double *taug, double *fracs, void *stream,
                             char *errmsg, int32_t errmsg_len);
 
+/* rrtmg_lw_run for callers that cannot allocate device memory during a run:
+ * hosts that give (nearly) all GPU memory to their own pool at start-up and
+ * time-step loops that must not call cudaMalloc/cudaFree, which synchronize
+ * the device.  No counterpart in the reference.  Same arguments and results
+ * as rrtmg_lw_gpu_run_ex with RRTMG_LW_DEVICE memory (every pointer is device
+ * memory owned by the caller), precision RRTMG_LW_FP64 or RRTMG_LW_FP32, work
+ * queued on `stream` (NULL = default stream) and synchronized before return.
+ * The kernels' scratch is a fixed 64 MiB array inside the library (held by
+ * every GPU that loads it until exit); calls whose columns do not fit are
+ * rejected with an error giving the maximum (about 190 columns of 127 layers
+ * in FP64).  All calls share that array: calls that overlap on the GPU race.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  Returns errflg. */
+int rrtmg_lw_gpu_run_noalloc(const rrtmg_lw_run_args *args, int32_t precision,
+                             void *stream, char *errmsg, int32_t errmsg_len);
+
 /* Release device tables and per-thread workspaces (call once at exit). */
 void rrtmg_lw_gpu_finalize(void);
 
