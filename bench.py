@@ -37,6 +37,16 @@ CONFIGS = {
 }
 
 
+def n_chunks(ncols, nlay, real_bytes=8, budget=6 << 30):
+    """Chunks the library splits a call into (its scratch budget, 6 GiB by
+    default): tau/frac (140 g-points) + 3x16 band fields per padded layer,
+    plus a 48-double column record."""
+    v = 2 if nlay <= 63 else 4 if nlay <= 127 else 8
+    per = (2 * 140 + 3 * 16) * 32 * v * real_bytes + 48 * 8
+    budget = int(os.environ.get("RRTMG_LW_GPU_SCRATCH_MB", budget >> 20)) << 20
+    return -(-ncols // max(1, budget // per))
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -302,11 +312,13 @@ def main():
     peak, peak_kind = _peaks()
     achieved = BYTES_PER_COL * ncols / (col_ms / 1e3) / 1e9
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "column_kernel_traffic.json")
+    tfile = os.path.join(ROOT, "profiles", "column_kernels_traffic.txt")
     if os.path.exists(tfile):
+        # "dram_bytes_per_column_fp64: N" lines from the ncu summary
         with open(tfile) as fh:
-            tr = json.load(fh)
-        traffic = tr["dram_bytes_per_column"] * ncols
+            tr = dict(l.split(":", 1) for l in fh if ":" in l and not l.startswith("#"))
+        if "dram_bytes_per_column_fp64" in tr:
+            traffic = float(tr["dram_bytes_per_column_fp64"]) * ncols
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -331,12 +343,12 @@ def main():
         "clocks": clk.summary(),
         "e2e": {"value": e2e, "unit": "columns/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "matches_device_run": ok_e2e},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": args.steps * (1 + 2 * n_chunks(ncols, nlay)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": "lw_column_kernel<double,4>",
-                     "note": "compulsory bytes 61,052 B/column / column-kernel time; the kernel is "
-                             "FP64-pipe bound, not HBM bound"},
+                     "kernel": "lw_gas_kernel<double,4> + lw_rt_kernel<double,4,0>",
+                     "note": "compulsory bytes 61,052 B/column / (gas + transfer kernel time); the "
+                             "kernels are FP64-issue and gather-latency bound, not HBM bound"},
         "cpu_baseline": cpu,
         "paths": paths,
     }
