@@ -60,6 +60,12 @@ class ExecArgs(C.Structure):
                 ("kernel_ms", C.POINTER(C.c_float))]
 
 
+class Tuning(C.Structure):
+    """rrtmg_lw_tuning: launch shape of the column kernels (0 = default)."""
+    _fields_ = [("rt_warps", C.c_int32), ("gas_per_sm", C.c_int32), ("chunk_cols", C.c_int32),
+                ("use_graph", C.c_int32)]
+
+
 FP64, FP32, SURROGATE = 0, 1, 2
 HOST, DEVICE = 0, 1
 

@@ -23,6 +23,7 @@
 
 #include "../../include/rrtmg_lw_gpu.h"
 #include "lw_common.cuh"
+#include "lw_launch.h"
 
 extern "C" const unsigned char rrtmg_lw_tables_blob[];
 extern "C" const unsigned char rrtmg_lw_tables_blob_end[];
@@ -37,18 +38,6 @@ struct NoAllocView {
   Consts cs;
 };
 NoAllocView noalloc_view();
-size_t scratch_per_column_fp64(int V);
-size_t scratch_per_column_fp32(int V);
-cudaError_t launch_column_fp64(int V, bool hlwb, const Block*, int, const Block&, int, const Flags&, const Consts&,
-                               const Tables<double>&, const Tables<double>&, const uint32_t*, void*, size_t,
-                               double*, double*, int, cudaStream_t, cudaEvent_t);
-cudaError_t launch_column_fp32(int V, bool hlwb, const Block*, int, const Block&, int, const Flags&, const Consts&,
-                               const Tables<float>&, const Tables<double>&, const uint32_t*, void*, size_t,
-                               double*, double*, int, cudaStream_t, cudaEvent_t);
-cudaError_t mcica_upload_powers();
-cudaError_t mcica_launch(const Block*, int, const Block&, int, int, int, int, int, const double*,
-                         const int32_t*, int, uint32_t*, int, cudaStream_t);
-cudaError_t mcica_prepare(int max_smem);
 }  // namespace lw
 
 using namespace lw;
@@ -64,9 +53,13 @@ struct DeviceState {
   double* tbl64 = nullptr;   // exp, tfn, tau (3 x (NTBL+1))
   float* tbl32 = nullptr;
   Consts cs{};
+  Shape tuned[2][9];         // autotuned launch shape per [fp32?][V]
+  bool has_tuned[2][9] = {};
 };
 DeviceState g;
 std::mutex g_mu;
+
+struct GraphEntry;
 
 struct Workspace {
   int device = -1;
@@ -81,7 +74,30 @@ struct Workspace {
   size_t dblocks_n = 0;
   Block* hblocks = nullptr;   // pinned host copy of the descriptors
   size_t hblocks_n = 0;
+  uint64_t gen = 0;           // bumped whenever bits/scratch move (graphs hold their addresses)
+  std::vector<GraphEntry*> graphs;
 };
+
+// A captured call of rrtmg_lw_gpu_run_blocks: the kernels of one block set
+// with its own device copy of the block descriptors.
+struct GraphEntry {
+  std::vector<Block> blocks;
+  Flags f;
+  int precision = 0;
+  Shape sh;
+  int ncols = 0;
+  uint64_t gen = 0;
+  uint64_t last_use = 0;
+  Block* dblocks = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+constexpr size_t kMaxGraphs = 8;   // per workspace; least recently used is dropped
+
+void drop_graph(GraphEntry* e) {
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->dblocks) cudaFree(e->dblocks);
+  delete e;
+}
 std::vector<Workspace*> g_workspaces;
 thread_local Workspace* tl_ws = nullptr;
 
@@ -219,6 +235,8 @@ extern "C" int rrtmg_lw_gpu_init(const rrtmg_lw_init_args* a, char* errmsg, int3
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, g.device), "cudaDeviceGetAttribute");
   CK(mcica_prepare(optin), "kernel attributes (mcica)");
+  CK(prepare_column_fp64(), "kernel attributes (column, fp64)");
+  CK(prepare_column_fp32(), "kernel attributes (column, fp32)");
   // per-thread stack for the spilled kernels (a context setting, gone with the process)
   size_t stack = 0;
   CK(cudaDeviceGetLimit(&stack, cudaLimitStackSize), "cudaDeviceGetLimit");
@@ -285,7 +303,6 @@ int validate(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg, i
   return 0;
 }
 
-int pick_v(int nlay) { return nlay <= 63 ? 2 : nlay <= 127 ? 4 : 8; }
 
 // Device scratch budget of one call (columns are processed in chunks that fit).
 constexpr size_t kScratchBudget = (size_t)6 << 30;
@@ -332,71 +349,186 @@ void block_from_args(const rrtmg_lw_run_args* a, Block* B) {
   B->pad = 0;
 }
 
-int launch(Workspace* w, const Block* hblocks, int nblocks, int ncols, const Flags& f, int precision,
-           float* kernel_ms, char* errmsg, int32_t errmsg_len) {
-  cudaStream_t st = w->stream;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  if (kernel_ms)
-    for (auto& e : ev) CK(cudaEventCreate(&e), "cudaEventCreate");
-  const Block* dblk = nullptr;
-  if (nblocks > 1) {
-  // descriptors: pinned host staging -> device
+// grow() for the buffers captured graphs refer to
+template <typename T>
+cudaError_t grow_ws(Workspace* w, T** p, size_t* have, size_t need_bytes) {
+  if (*have >= need_bytes && *p) return cudaSuccess;
+  ++w->gen;
+  return grow(p, have, need_bytes);
+}
+
+Shape default_shape(int precision, int V) {
+  const int pi = precision == RRTMG_LW_FP64 ? 0 : 1;
+  return g.has_tuned[pi][V] ? g.tuned[pi][V] : Shape();
+}
+
+size_t scratch_budget() {
+  size_t budget = kScratchBudget;
+  if (const char* env = std::getenv("RRTMG_LW_GPU_SCRATCH_MB")) budget = (size_t)std::atol(env) << 20;
+  return budget;
+}
+
+// Size the McICA flags and the kernel A -> B scratch for a call.
+int reserve(Workspace* w, int ncols, const Flags& f, int precision, const Shape& sh, char* errmsg,
+            int32_t errmsg_len) {
+  const int nw = (f.nlay + 31) / 32;
+  if (f.isubclw > 0 && !f.gas_only)
+    CK(grow_ws(w, &w->bits, &w->bits_bytes, (size_t)ncols * NGPT * nw * sizeof(uint32_t)), "cudaMalloc(mcica bits)");
+  const int V = pick_v(f.nlay);
+  const size_t per = (precision == RRTMG_LW_FP64) ? scratch_per_column_fp64(V) : scratch_per_column_fp32(V);
+  size_t cols = std::min<size_t>((size_t)ncols, std::max<size_t>(scratch_budget() / per, 1));
+  if (sh.chunk > 0) cols = std::min<size_t>(cols, (size_t)sh.chunk);
+  CK(grow_ws(w, &w->scratch, &w->scratch_bytes, cols * per), "cudaMalloc(scratch)");
+  return 0;
+}
+
+// Copy the block descriptors (nblocks > 1) to the workspace's device array.
+int upload_blocks(Workspace* w, cudaStream_t st, const Block* hblocks, int nblocks, const Block** dblk,
+                  char* errmsg, int32_t errmsg_len) {
+  *dblk = nullptr;
+  if (nblocks <= 1) return 0;
+  CK(cudaStreamSynchronize(st), "cudaStreamSynchronize");   // a previous call may still read the staging copy
   if (w->hblocks_n < (size_t)nblocks) {
     if (w->hblocks) cudaFreeHost(w->hblocks);
     w->hblocks = nullptr;
     w->hblocks_n = 0;
-    CK(cudaStreamSynchronize(st), "cudaStreamSynchronize");
     CK(cudaMallocHost((void**)&w->hblocks, sizeof(Block) * nblocks), "cudaMallocHost");
     w->hblocks_n = nblocks;
-  } else {
-    CK(cudaStreamSynchronize(st), "cudaStreamSynchronize");   // previous call done with the staging copy
   }
-  if (hblocks != w->hblocks) std::memcpy(w->hblocks, hblocks, sizeof(Block) * nblocks);
+  std::memcpy(w->hblocks, hblocks, sizeof(Block) * nblocks);
   size_t have = w->dblocks_n * sizeof(Block);
   CK(grow(&w->dblocks, &have, sizeof(Block) * nblocks), "cudaMalloc(blocks)");
   w->dblocks_n = have / sizeof(Block);
   CK(cudaMemcpyAsync(w->dblocks, w->hblocks, sizeof(Block) * nblocks, cudaMemcpyHostToDevice, st),
      "cudaMemcpyAsync(blocks)");
-  dblk = w->dblocks;
-  }
-  const Block& b0 = hblocks[0];
-  const int nw = (f.nlay + 31) / 32;
-  if (kernel_ms) CK(cudaEventRecord(ev[0], st), "cudaEventRecord");
+  *dblk = w->dblocks;
+  return 0;
+}
+
+// Enqueue the McICA and column kernels of a call (buffers already reserved).
+// ev (optional, 4 events): before McICA, before gas optics, end, and after
+// the first gas-optics launch.
+cudaError_t enqueue(Workspace* w, cudaStream_t st, const Block* dblk, const Block& b0, int nblocks, int ncols,
+                    const Flags& f, int precision, const Shape& sh, cudaEvent_t* ev) {
+  cudaError_t e;
+  if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return e;
   if (f.isubclw > 0 && !f.gas_only) {
-    CK(grow(&w->bits, &w->bits_bytes, (size_t)ncols * NGPT * nw * sizeof(uint32_t)), "cudaMalloc(mcica bits)");
-    CK(mcica_launch(dblk, nblocks, b0, ncols, f.nlay, f.iovr, f.isubclw, f.top_at_1, nullptr, nullptr, 0,
-                    w->bits, g.num_sms, st),
-       "McICA kernel launch");
+    e = mcica_launch(dblk, nblocks, b0, ncols, f.nlay, f.iovr, f.isubclw, f.top_at_1, nullptr, nullptr, 0, w->bits,
+                     g.num_sms, st);
+    if (e != cudaSuccess) return e;
   }
+  if (ev && (e = cudaEventRecord(ev[1], st)) != cudaSuccess) return e;
   const int V = pick_v(f.nlay);
   const bool hlwb = f.want_hlwb != 0;
-  if (kernel_ms) CK(cudaEventRecord(ev[1], st), "cudaEventRecord");
-  // scratch between the gas-optics and transfer kernels, in chunks of columns
-  const size_t per = (precision == RRTMG_LW_FP64) ? scratch_per_column_fp64(V) : scratch_per_column_fp32(V);
-  size_t budget = kScratchBudget;
-  if (const char* env = std::getenv("RRTMG_LW_GPU_SCRATCH_MB")) budget = (size_t)std::atol(env) << 20;
-  const size_t want = std::min<size_t>((size_t)ncols * per, std::max<size_t>(budget, per));
-  CK(grow(&w->scratch, &w->scratch_bytes, want), "cudaMalloc(scratch)");
+  Tables<double> t64{g.kt64, g.tbl64, g.tbl64 + (NTBL + 1), g.tbl64 + 2 * (NTBL + 1)};
   if (precision == RRTMG_LW_FP64) {
-    Tables<double> t{g.kt64, g.tbl64, g.tbl64 + (NTBL + 1), g.tbl64 + 2 * (NTBL + 1)};
-    CK(launch_column_fp64(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t, t, w->bits, w->scratch, w->scratch_bytes,
-                          nullptr, nullptr, g.num_sms, st, ev[3]),
-       "column kernels launch (fp64)");
+    e = launch_column_fp64(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t64, t64, w->bits, w->scratch,
+                           w->scratch_bytes, nullptr, nullptr, g.num_sms, sh, st, ev ? ev[3] : nullptr);
   } else {
     Tables<float> t{g.kt32, g.tbl32, g.tbl32 + (NTBL + 1), g.tbl32 + 2 * (NTBL + 1)};
-    Tables<double> t64{g.kt64, g.tbl64, g.tbl64 + (NTBL + 1), g.tbl64 + 2 * (NTBL + 1)};
-    CK(launch_column_fp32(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t, t64, w->bits, w->scratch,
-                          w->scratch_bytes, nullptr, nullptr, g.num_sms, st, ev[3]),
-       "column kernels launch (fp32)");
+    e = launch_column_fp32(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t, t64, w->bits, w->scratch,
+                           w->scratch_bytes, nullptr, nullptr, g.num_sms, sh, st, ev ? ev[3] : nullptr);
   }
+  if (e != cudaSuccess) return e;
+  if (ev && (e = cudaEventRecord(ev[2], st)) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+struct Events {
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  ~Events() { for (auto& e : ev) if (e) cudaEventDestroy(e); }
+  cudaError_t create() {
+    for (auto& e : ev) {
+      cudaError_t r = cudaEventCreate(&e);
+      if (r != cudaSuccess) return r;
+    }
+    return cudaSuccess;
+  }
+};
+
+int launch(Workspace* w, cudaStream_t st, const Block* hblocks, int nblocks, int ncols, const Flags& f,
+           int precision, const Shape& sh, float* kernel_ms, char* errmsg, int32_t errmsg_len) {
+  Events E;
+  if (kernel_ms) CK(E.create(), "cudaEventCreate");
+  int r = reserve(w, ncols, f, precision, sh, errmsg, errmsg_len);
+  if (r) return r;
+  const Block* dblk = nullptr;
+  if ((r = upload_blocks(w, st, hblocks, nblocks, &dblk, errmsg, errmsg_len))) return r;
+  CK(enqueue(w, st, dblk, hblocks[0], nblocks, ncols, f, precision, sh, kernel_ms ? E.ev : nullptr),
+     "kernel launch");
   if (kernel_ms) {
-    CK(cudaEventRecord(ev[2], st), "cudaEventRecord");
-    CK(cudaEventSynchronize(ev[2]), "kernel execution");
-    CK(cudaEventElapsedTime(&kernel_ms[0], ev[0], ev[1]), "cudaEventElapsedTime");
-    CK(cudaEventElapsedTime(&kernel_ms[1], ev[1], ev[3]), "cudaEventElapsedTime");
-    CK(cudaEventElapsedTime(&kernel_ms[2], ev[3], ev[2]), "cudaEventElapsedTime");
-    for (auto& e : ev) cudaEventDestroy(e);
+    CK(cudaEventSynchronize(E.ev[2]), "kernel execution");
+    CK(cudaEventElapsedTime(&kernel_ms[0], E.ev[0], E.ev[1]), "cudaEventElapsedTime");
+    CK(cudaEventElapsedTime(&kernel_ms[1], E.ev[1], E.ev[3]), "cudaEventElapsedTime");
+    CK(cudaEventElapsedTime(&kernel_ms[2], E.ev[3], E.ev[2]), "cudaEventElapsedTime");
   }
+  return 0;
+}
+
+// Launch a block set through a cached CUDA graph (captured on first use).
+int launch_graph(Workspace* w, cudaStream_t st, const std::vector<Block>& hb, int ncols, const Flags& f,
+                 int precision, const Shape& sh, char* errmsg, int32_t errmsg_len) {
+  static uint64_t tick = 0;
+  int r = reserve(w, ncols, f, precision, sh, errmsg, errmsg_len);   // may move buffers: bump gen first
+  if (r) return r;
+  GraphEntry* hit = nullptr;
+  for (size_t k = 0; k < w->graphs.size(); ++k) {
+    GraphEntry* e = w->graphs[k];
+    if (e->gen != w->gen) {            // refers to buffers that moved
+      drop_graph(e);
+      w->graphs.erase(w->graphs.begin() + k);
+      --k;
+      continue;
+    }
+    if (e->ncols == ncols && e->precision == precision && e->blocks.size() == hb.size() &&
+        std::memcmp(&e->f, &f, sizeof(Flags)) == 0 && std::memcmp(&e->sh, &sh, sizeof(Shape)) == 0 &&
+        std::memcmp(e->blocks.data(), hb.data(), sizeof(Block) * hb.size()) == 0) {
+      hit = e;
+      break;
+    }
+  }
+  if (!hit) {
+    if (w->graphs.size() >= kMaxGraphs) {
+      auto lru = std::min_element(w->graphs.begin(), w->graphs.end(),
+                                  [](GraphEntry* a, GraphEntry* b) { return a->last_use < b->last_use; });
+      CK(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+      drop_graph(*lru);
+      w->graphs.erase(lru);
+    }
+    GraphEntry* e = new GraphEntry();
+    e->blocks = hb;
+    e->f = f;
+    e->precision = precision;
+    e->sh = sh;
+    e->ncols = ncols;
+    e->gen = w->gen;
+    const Block* dblk = nullptr;
+    cudaError_t ce = cudaSuccess;
+    if (hb.size() > 1) {
+      ce = cudaMalloc((void**)&e->dblocks, sizeof(Block) * hb.size());
+      if (ce == cudaSuccess)
+        ce = cudaMemcpy(e->dblocks, hb.data(), sizeof(Block) * hb.size(), cudaMemcpyHostToDevice);
+      dblk = e->dblocks;
+    }
+    // capture on the workspace's private stream, then launch on the caller's
+    cudaGraph_t graph = nullptr;
+    if (ce == cudaSuccess) ce = cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+      cudaError_t ke = enqueue(w, w->stream, dblk, hb[0], (int)hb.size(), ncols, f, precision, sh, nullptr);
+      ce = cudaStreamEndCapture(w->stream, &graph);
+      if (ke != cudaSuccess) ce = ke;
+    }
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) {
+      drop_graph(e);
+      return cuda_fail(errmsg, errmsg_len, "CUDA graph capture", ce);
+    }
+    w->graphs.push_back(e);
+    hit = e;
+  }
+  hit->last_use = ++tick;
+  CK(cudaGraphLaunch(hit->exec, st), "cudaGraphLaunch");
   return 0;
 }
 
@@ -427,17 +559,12 @@ extern "C" int rrtmg_lw_gpu_run_ex(const rrtmg_lw_run_args* a, const rrtmg_lw_ex
   Flags f;
   fill_flags(a, &f);
   cudaStream_t st = x->stream ? (cudaStream_t)x->stream : w->stream;
-  Workspace wl = *w;            // launch on the caller's stream if given
-  wl.stream = st;
 
   if (x->memory == RRTMG_LW_DEVICE) {
     Block B;
     block_from_args(a, &B);
-    int r = launch(&wl, &B, 1, a->npts, f, x->precision, x->kernel_ms, errmsg, errmsg_len);
-    // launch() may have grown buffers
-    w->bits = wl.bits; w->bits_bytes = wl.bits_bytes; w->dblocks = wl.dblocks; w->dblocks_n = wl.dblocks_n;
-    w->scratch = wl.scratch; w->scratch_bytes = wl.scratch_bytes;
-    w->hblocks = wl.hblocks; w->hblocks_n = wl.hblocks_n;
+    int r = launch(w, st, &B, 1, a->npts, f, x->precision, default_shape(x->precision, pick_v(f.nlay)),
+                   x->kernel_ms, errmsg, errmsg_len);
     if (r) return r;
     if (x->sync) CK(cudaStreamSynchronize(st), "kernel execution");
     return 0;
@@ -490,12 +617,8 @@ extern "C" int rrtmg_lw_gpu_run_ex(const rrtmg_lw_run_args* a, const rrtmg_lw_ex
   }
   Block B;
   block_from_args(&d, &B);
-  wl = *w;
-  wl.stream = st;
-  int r = launch(&wl, &B, 1, a->npts, f, x->precision, x->kernel_ms, errmsg, errmsg_len);
-  w->bits = wl.bits; w->bits_bytes = wl.bits_bytes; w->dblocks = wl.dblocks; w->dblocks_n = wl.dblocks_n;
-    w->scratch = wl.scratch; w->scratch_bytes = wl.scratch_bytes;
-  w->hblocks = wl.hblocks; w->hblocks_n = wl.hblocks_n;
+  int r = launch(w, st, &B, 1, a->npts, f, x->precision, default_shape(x->precision, pick_v(f.nlay)),
+                 x->kernel_ms, errmsg, errmsg_len);
   if (r) return r;
   for (int k = 0; k < nout; ++k) {
     if (!host_out[k]) continue;
@@ -565,15 +688,175 @@ extern "C" int rrtmg_lw_gpu_gas_optics(const rrtmg_lw_run_args* a, int32_t preci
   Tables<double> t64{g.kt64, g.tbl64, g.tbl64 + (NTBL + 1), g.tbl64 + 2 * (NTBL + 1)};
   if (precision == RRTMG_LW_FP64) {
     CK(launch_column_fp64(V, false, nullptr, 1, B, a2.npts, f, g.cs, t64, t64, nullptr, nullptr, 0, taug, fracs,
-                          g.num_sms, st, nullptr),
+                          g.num_sms, Shape(), st, nullptr),
        "gas optics launch");
   } else {
     Tables<float> t{g.kt32, g.tbl32, g.tbl32 + (NTBL + 1), g.tbl32 + 2 * (NTBL + 1)};
     CK(launch_column_fp32(V, false, nullptr, 1, B, a2.npts, f, g.cs, t, t64, nullptr, nullptr, 0, taug, fracs,
-                          g.num_sms, st, nullptr),
+                          g.num_sms, Shape(), st, nullptr),
        "gas optics launch");
   }
   CK(cudaStreamSynchronize(st), "gas optics execution");
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+namespace {
+
+// Validate a block set for run_blocks / autotune and build its descriptors
+// (empty blocks dropped, col0 = prefix sums).  Returns -1 if nothing to do.
+int build_block_set(const rrtmg_lw_run_args* blocks, int32_t nblocks, const rrtmg_lw_exec* x, int64_t max_cols,
+                    std::vector<Block>* hb, Flags* f, int* ncols, char* errmsg, int32_t errmsg_len) {
+  if (nblocks < 0 || (nblocks > 0 && !blocks)) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_blocks: bad block array");
+    return 1;
+  }
+  if (x->memory != RRTMG_LW_DEVICE) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_blocks: every block must be in device memory (RRTMG_LW_DEVICE)");
+    return 1;
+  }
+  hb->clear();
+  long total = 0;
+  bool have_flags = false;
+  for (int b = 0; b < nblocks; ++b) {
+    int v = validate(&blocks[b], x, errmsg, errmsg_len);
+    if (v == -1) continue;
+    if (v) {
+      char tmp[400];
+      std::snprintf(tmp, sizeof(tmp), "%s", errmsg ? errmsg : "");
+      set_msg(errmsg, errmsg_len, "block %d: %s", b, tmp);
+      return 1;
+    }
+    Flags fb;
+    fill_flags(&blocks[b], &fb);
+    if (!have_flags) {
+      *f = fb;
+      have_flags = true;
+    } else if (std::memcmp(&fb, f, sizeof(Flags)) != 0) {
+      set_msg(errmsg, errmsg_len,
+              "rrtmg_lw_gpu_run_blocks: block %d differs from block 0 in nlay, flags or optional outputs", b);
+      return 1;
+    }
+    if (total + blocks[b].npts > (long)INT32_MAX) {
+      set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_blocks: more than 2^31-1 columns");
+      return 1;
+    }
+    Block B;
+    block_from_args(&blocks[b], &B);
+    B.col0 = (int)total;
+    total += blocks[b].npts;
+    hb->push_back(B);
+    if (max_cols > 0 && total >= max_cols) break;
+  }
+  *ncols = (int)total;
+  return hb->empty() ? -1 : 0;
+}
+
+}  // namespace
+
+extern "C" int rrtmg_lw_gpu_run_blocks(const rrtmg_lw_run_args* blocks, int32_t nblocks, const rrtmg_lw_exec* x,
+                                       const rrtmg_lw_tuning* tune, char* errmsg, int32_t errmsg_len) {
+  set_msg(errmsg, errmsg_len, "");
+  if (!g.ready) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: rrtmg_lw_gpu_init has not been called"); return 1; }
+  rrtmg_lw_exec dflt{RRTMG_LW_FP64, RRTMG_LW_DEVICE, nullptr, 1, 0, nullptr};
+  if (!x) x = &dflt;
+  std::vector<Block> hb;
+  Flags f;
+  int ncols = 0;
+  int v = build_block_set(blocks, nblocks, x, 0, &hb, &f, &ncols, errmsg, errmsg_len);
+  if (v == -1) return 0;
+  if (v) return 1;
+  CK(cudaSetDevice(g.device), "cudaSetDevice");
+  int rc = 0;
+  Workspace* w = workspace(errmsg, errmsg_len, &rc);
+  if (!w) return rc;
+  cudaStream_t st = x->stream ? (cudaStream_t)x->stream : w->stream;
+  Shape sh = default_shape(x->precision, pick_v(f.nlay));
+  bool graph = false;
+  if (tune) {
+    if (tune->rt_warps) sh.rt_warps = tune->rt_warps;
+    if (tune->gas_per_sm) sh.gas_per_sm = tune->gas_per_sm;
+    if (tune->chunk_cols) sh.chunk = tune->chunk_cols;
+    graph = tune->use_graph != 0;
+  }
+  if (sh.rt_warps != 1 && sh.rt_warps != 2 && sh.rt_warps != 4) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_blocks: rt_warps must be 1, 2 or 4 (got %d)", sh.rt_warps);
+    return 1;
+  }
+  if (sh.gas_per_sm < 0 || sh.chunk < 0) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_blocks: negative tuning value");
+    return 1;
+  }
+  int r = graph ? launch_graph(w, st, hb, ncols, f, x->precision, sh, errmsg, errmsg_len)
+                : launch(w, st, hb.data(), (int)hb.size(), ncols, f, x->precision, sh, x->kernel_ms, errmsg,
+                         errmsg_len);
+  if (r) return r;
+  if (x->sync) CK(cudaStreamSynchronize(st), "kernel execution");
+  return 0;
+}
+
+extern "C" int rrtmg_lw_gpu_autotune(const rrtmg_lw_run_args* blocks, int32_t nblocks, int32_t precision,
+                                     void* stream, int64_t sample_cols, rrtmg_lw_tuning* best, float* best_ms,
+                                     char* errmsg, int32_t errmsg_len) {
+  set_msg(errmsg, errmsg_len, "");
+  if (!g.ready) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: rrtmg_lw_gpu_init has not been called"); return 1; }
+  rrtmg_lw_exec x{precision, RRTMG_LW_DEVICE, stream, 1, 0, nullptr};
+  std::vector<Block> hb;
+  Flags f;
+  int ncols = 0;
+  int v = build_block_set(blocks, nblocks, &x, sample_cols, &hb, &f, &ncols, errmsg, errmsg_len);
+  if (v == -1) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_autotune: no columns to tune on"); return 1; }
+  if (v) return 1;
+  CK(cudaSetDevice(g.device), "cudaSetDevice");
+  int rc = 0;
+  Workspace* w = workspace(errmsg, errmsg_len, &rc);
+  if (!w) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : w->stream;
+  const int V = pick_v(f.nlay);
+  // candidates: transfer CTA of 1, 2, 4 columns x hand-off chunk (all, 1/2, 1/4 of the columns)
+  std::vector<Shape> cands;
+  for (int wv : {4, 2, 1})
+    for (long ch : {0L, (long)(ncols + 1) / 2, (long)(ncols + 3) / 4}) {
+      if (ch > 0 && ch < 1024) continue;
+      Shape s;
+      s.rt_warps = wv;
+      s.chunk = ch;
+      cands.push_back(s);
+    }
+  Events E;
+  CK(E.create(), "cudaEventCreate");
+  float best_t = -1.f;
+  Shape best_s;
+  for (const Shape& s : cands) {
+    int r = launch(w, st, hb.data(), (int)hb.size(), ncols, f, precision, s, nullptr, errmsg, errmsg_len);   // warm
+    if (r) return r;
+    CK(cudaEventRecord(E.ev[0], st), "cudaEventRecord");
+    for (int rep = 0; rep < 2; ++rep)
+      if ((r = launch(w, st, hb.data(), (int)hb.size(), ncols, f, precision, s, nullptr, errmsg, errmsg_len)))
+        return r;
+    CK(cudaEventRecord(E.ev[1], st), "cudaEventRecord");
+    CK(cudaEventSynchronize(E.ev[1]), "kernel execution");
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, E.ev[0], E.ev[1]), "cudaEventElapsedTime");
+    ms *= 0.5f;
+    if (best_t < 0.f || ms < best_t) {
+      best_t = ms;
+      best_s = s;
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    const int pi = precision == RRTMG_LW_FP64 ? 0 : 1;
+    g.tuned[pi][V] = best_s;
+    g.has_tuned[pi][V] = true;
+  }
+  if (best) {
+    best->rt_warps = best_s.rt_warps;
+    best->gas_per_sm = best_s.gas_per_sm;
+    best->chunk_cols = (int32_t)best_s.chunk;
+    best->use_graph = 0;
+  }
+  if (best_ms) *best_ms = best_t;
   return 0;
 }
 
@@ -583,6 +866,8 @@ extern "C" void rrtmg_lw_gpu_finalize(void) {
   cudaSetDevice(g.device);
   for (Workspace* w : g_workspaces) {
     if (w->stream) cudaStreamSynchronize(w->stream);
+    for (GraphEntry* e : w->graphs) drop_graph(e);
+    w->graphs.clear();
     if (w->dbuf) cudaFree(w->dbuf);
     if (w->bits) cudaFree(w->bits);
     if (w->scratch) cudaFree(w->scratch);

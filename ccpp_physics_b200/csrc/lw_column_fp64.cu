@@ -8,5 +8,7 @@
 #define REAL double
 #define LW_SCRATCH_FN scratch_per_column_fp64
 #define LW_LAUNCH_FN launch_column_fp64
+#define LW_PREPARE_FN prepare_column_fp64
+#define LW_NLAUNCH_FN launches_column_fp64
 #define LW_DBG_FN rrtmg_lw_gpu_debug_read_fp64
 #include "lw_column_launch.inc"

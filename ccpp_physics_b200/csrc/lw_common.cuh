@@ -81,6 +81,17 @@ struct Flags {
   int gas_only;        // 1: write taug/fracs only (training data / stage tests)
 };
 
+// Launch shape of the column kernels (host side; chosen by the autotuner
+// or defaulted).  rt_warps: columns (one warp each) per CTA of the transfer
+// kernel; chunk: columns per gas-optics -> transfer hand-off (0 = as many as
+// the scratch budget holds); gas_per_sm: resident gas CTAs per SM to launch
+// (0 = the occupancy limit).
+struct Shape {
+  int rt_warps = 4;
+  int gas_per_sm = 0;
+  long chunk = 0;
+};
+
 // Locate the block of a global column (blocks sorted by col0).
 __device__ __forceinline__ int find_block(const Block* blocks, int nblocks, int col) {
   int lo = 0, hi = nblocks - 1;

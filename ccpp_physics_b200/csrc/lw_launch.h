@@ -1,0 +1,39 @@
+// lw_launch.h -- host-side launchers of the column kernels, shared by the
+// entry points (lw_api.cu, lw_noalloc.cu).  Every launcher only enqueues
+// work on the given stream.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "lw_common.cuh"
+
+namespace lw {
+
+size_t scratch_per_column_fp64(int V);
+size_t scratch_per_column_fp32(int V);
+cudaError_t prepare_column_fp64();
+cudaError_t prepare_column_fp32();
+int launches_column_fp64(int V, int ncols, size_t scratch_bytes, const Shape& sh);
+int launches_column_fp32(int V, int ncols, size_t scratch_bytes, const Shape& sh);
+cudaError_t launch_column_fp64(int V, bool hlwb, const Block* blocks, int nblocks, const Block& b0, int ncols,
+                               const Flags& f, const Consts& cs, const Tables<double>& tab,
+                               const Tables<double>& tab64, const uint32_t* bits, void* scratch,
+                               size_t scratch_bytes, double* gas_taug, double* gas_fracs, int num_sms,
+                               const Shape& sh, cudaStream_t st, cudaEvent_t ev_mid);
+cudaError_t launch_column_fp32(int V, bool hlwb, const Block* blocks, int nblocks, const Block& b0, int ncols,
+                               const Flags& f, const Consts& cs, const Tables<float>& tab,
+                               const Tables<double>& tab64, const uint32_t* bits, void* scratch,
+                               size_t scratch_bytes, double* gas_taug, double* gas_fracs, int num_sms,
+                               const Shape& sh, cudaStream_t st, cudaEvent_t ev_mid);
+cudaError_t mcica_upload_powers();
+cudaError_t mcica_prepare(int max_smem);
+cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int ncols, int nlay, int iovr,
+                         int isubclw, int top_at_1, const double* cldf_dev, const int32_t* seed_dev, int dev_ld,
+                         uint32_t* bits, int num_sms, cudaStream_t st);
+
+// layers per lane of the column kernels (NLP = 32 V padded layers)
+inline int pick_v(int nlay) { return nlay <= 63 ? 2 : nlay <= 127 ? 4 : 8; }
+
+}  // namespace lw

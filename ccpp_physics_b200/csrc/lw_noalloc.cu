@@ -39,17 +39,9 @@
 #include "../../include/rrtmg_lw_gpu.h"
 #include "lw_common.cuh"
 
+#include "lw_launch.h"
+
 namespace lw {
-size_t scratch_per_column_fp64(int V);
-size_t scratch_per_column_fp32(int V);
-cudaError_t launch_column_fp64(int V, bool hlwb, const Block*, int, const Block&, int, const Flags&, const Consts&,
-                               const Tables<double>&, const Tables<double>&, const uint32_t*, void*, size_t,
-                               double*, double*, int, cudaStream_t, cudaEvent_t);
-cudaError_t launch_column_fp32(int V, bool hlwb, const Block*, int, const Block&, int, const Flags&, const Consts&,
-                               const Tables<float>&, const Tables<double>&, const uint32_t*, void*, size_t,
-                               double*, double*, int, cudaStream_t, cudaEvent_t);
-cudaError_t mcica_launch(const Block*, int, const Block&, int, int, int, int, int, const double*,
-                         const int32_t*, int, uint32_t*, int, cudaStream_t);
 // device tables and constants written by rrtmg_lw_gpu_init (lw_api.cu)
 struct NoAllocView {
   int ready, device, num_sms;
@@ -201,12 +193,12 @@ extern "C" int rrtmg_lw_gpu_run_noalloc(const rrtmg_lw_run_args* a, int32_t prec
     if (precision == RRTMG_LW_FP64) {
       Tables<double> t{v.kt64, v.tbl64, v.tbl64 + (NTBL + 1), v.tbl64 + 2 * (NTBL + 1)};
       e = launch_column_fp64(V, f.want_hlwb != 0, nullptr, 1, B, a->npts, f, v.cs, t, t, bits, scratch,
-                             scratch_bytes, nullptr, nullptr, v.num_sms, st, nullptr);
+                             scratch_bytes, nullptr, nullptr, v.num_sms, Shape(), st, nullptr);
     } else {
       Tables<float> t{v.kt32, v.tbl32, v.tbl32 + (NTBL + 1), v.tbl32 + 2 * (NTBL + 1)};
       Tables<double> t64{v.kt64, v.tbl64, v.tbl64 + (NTBL + 1), v.tbl64 + 2 * (NTBL + 1)};
       e = launch_column_fp32(V, f.want_hlwb != 0, nullptr, 1, B, a->npts, f, v.cs, t, t64, bits, scratch,
-                             scratch_bytes, nullptr, nullptr, v.num_sms, st, nullptr);
+                             scratch_bytes, nullptr, nullptr, v.num_sms, Shape(), st, nullptr);
     }
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);

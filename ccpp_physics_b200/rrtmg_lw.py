@@ -45,6 +45,11 @@ def lib():
             [C.c_char_p, C.c_int32]
         L.rrtmg_lw_gpu_gas_optics.argtypes = [C.POINTER(abi.RunArgs), C.c_int32, C.c_void_p, C.c_void_p,
                                               C.c_void_p, C.c_char_p, C.c_int32]
+        L.rrtmg_lw_gpu_run_blocks.argtypes = [C.POINTER(abi.RunArgs), C.c_int32, C.POINTER(abi.ExecArgs),
+                                              C.POINTER(abi.Tuning), C.c_char_p, C.c_int32]
+        L.rrtmg_lw_gpu_autotune.argtypes = [C.POINTER(abi.RunArgs), C.c_int32, C.c_int32, C.c_void_p,
+                                            C.c_int64, C.POINTER(abi.Tuning), C.POINTER(C.c_float),
+                                            C.c_char_p, C.c_int32]
         L.rrtmg_lw_gpu_finalize.argtypes = []
         _lib = L
     return _lib
@@ -143,6 +148,75 @@ def gas_optics(prof: dict, precision="fp64", stream=None):
     if rc:
         raise RRTMGLWError(msg.value.decode())
     return taug, fracs
+
+
+def block_args(prof: dict, out: dict, sizes, *, flags=None):
+    """RunArgs array describing consecutive physics blocks of ``sizes``
+    columns as views into one device-resident profile/output dict (each block
+    points at its first column and uses the full column count as ldim, the
+    way a host passes slices of larger arrays)."""
+    keep = []
+    base = abi.make_run_args(prof, out, flags=flags, keep=keep)
+    npts = prof["npts"]
+    if int(np.sum(sizes)) != npts:
+        raise ValueError("block sizes must add up to npts")
+    arr = (abi.RunArgs * len(sizes))()
+    col_fields = set(abi.INPUT_FIELDS + ("aeraod", "aerssa", "sfemis", "sfgtmp", "dzlyr", "delpin",
+                                         "de_lgth", "alpha", "cld_cf") + abi.OPTIONAL_CLOUD_FIELDS +
+                     ("hlwc", "cldtau", "hlw0", "hlwb"))
+    rec = {"topflx": 2, "sfcflx": 4, "flxprf": 4}
+    c0 = 0
+    for b, n in enumerate(sizes):
+        a = abi.RunArgs.from_buffer_copy(base)
+        a.npts, a.ldim = int(n), npts
+        for name, _ in abi.RunArgs._fields_:
+            p = getattr(a, name)
+            if not isinstance(p, C._Pointer) or not p:
+                continue
+            addr = C.cast(p, C.c_void_p).value
+            if name == "icseed":
+                off = 4 * c0
+            elif name in rec:
+                off = 8 * rec[name] * c0
+            elif name in col_fields:
+                off = 8 * c0
+            else:
+                continue
+            setattr(a, name, C.cast(C.c_void_p(addr + off), type(p)))
+        arr[b] = a
+        c0 += int(n)
+    return arr, keep
+
+
+def run_blocks(prof: dict, out: dict, sizes, *, precision="fp64", tuning=None, stream=None, sync=True,
+               kernel_ms=None):
+    """All physics blocks of ``sizes`` columns (views into one device-resident
+    profile) in one call of rrtmg_lw_gpu_run_blocks.  ``tuning``: an
+    abi.Tuning or dict (rt_warps, gas_per_sm, chunk_cols, use_graph).
+    Returns (errmsg, errflg)."""
+    arr, keep = block_args(prof, out, sizes)
+    x = abi.ExecArgs(precision=PRECISIONS[precision] if isinstance(precision, str) else precision,
+                     memory=abi.DEVICE, stream=None if stream is None else C.c_void_p(stream), sync=int(sync))
+    if kernel_ms is not None:
+        x.kernel_ms = kernel_ms
+    t = abi.Tuning(**tuning) if isinstance(tuning, dict) else tuning
+    msg = C.create_string_buffer(512)
+    rc = lib().rrtmg_lw_gpu_run_blocks(arr, len(arr), C.byref(x), C.byref(t) if t is not None else None, msg, 512)
+    return msg.value.decode(), rc
+
+
+def autotune(prof: dict, out: dict, sizes, *, precision="fp32", sample_cols=0, stream=None):
+    """Autotune the launch shape on the physics blocks of ``sizes`` columns;
+    returns (tuning dict, ms per call)."""
+    arr, keep = block_args(prof, out, sizes)
+    best = abi.Tuning()
+    ms = C.c_float(0.0)
+    msg = C.create_string_buffer(512)
+    rc = lib().rrtmg_lw_gpu_autotune(arr, len(arr), PRECISIONS[precision], None if stream is None else
+                                     C.c_void_p(stream), int(sample_cols), C.byref(best), C.byref(ms), msg, 512)
+    if rc:
+        raise RRTMGLWError(msg.value.decode())
+    return {n: getattr(best, n) for n, _ in abi.Tuning._fields_}, ms.value
 
 
 def to_device(prof: dict, device="cuda"):

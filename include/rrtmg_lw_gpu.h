@@ -164,6 +164,52 @@ int rrtmg_lw_gpu_gas_optics(const rrtmg_lw_run_args *args, int32_t precision,
 int rrtmg_lw_gpu_run_noalloc(const rrtmg_lw_run_args *args, int32_t precision,
                              void *stream, char *errmsg, int32_t errmsg_len);
 
+/* Launch shape of the column kernels.  Chosen by rrtmg_lw_gpu_autotune or
+ * given by the caller; zero fields take the defaults. */
+typedef struct rrtmg_lw_tuning {
+  int32_t rt_warps;        /* columns (one warp each) per CTA of the transfer
+                              kernel: 1, 2 or 4 (default 4) */
+  int32_t gas_per_sm;      /* resident gas-optics CTAs per SM to launch
+                              (0 = the occupancy limit) */
+  int32_t chunk_cols;      /* columns per gas-optics -> transfer hand-off
+                              (0 = as many as the scratch budget holds) */
+  int32_t use_graph;       /* run_blocks only: 1 = capture the call's launches
+                              in a CUDA graph on first use and replay it when
+                              the same block set (same pointers, sizes, flags
+                              and shape) is called again */
+} rrtmg_lw_tuning;
+
+/* UFS-style physics blocks in one call.  The reference host calls
+ * rrtmg_lw_run once per block of columns (radlw_main.F90:419, from OpenMP
+ * threads); here blocks[b] is the rrtmg_lw_run argument set of block b, all
+ * blocks with the same nlay and flags, every pointer device memory.  The
+ * columns of all blocks form one index space and run in one persistent
+ * launch of each kernel (McICA, gas optics, transfer; the last two repeat
+ * only when the scratch budget splits the columns into chunks), with no
+ * per-block launches.  exec: precision FP64 or FP32, memory must be
+ * RRTMG_LW_DEVICE, stream, sync; kernel_ms is filled only without a graph.
+ * tune: launch shape and graph use (NULL = the autotuned shape if
+ * rrtmg_lw_gpu_autotune ran for this layer count and precision, else the
+ * defaults, no graph).  A replayed graph reads the blocks' arrays through the
+ * same pointers, so inputs updated in place are picked up.  No counterpart
+ * in the reference.  Returns errflg. */
+int rrtmg_lw_gpu_run_blocks(const rrtmg_lw_run_args *blocks, int32_t nblocks,
+                            const rrtmg_lw_exec *exec,
+                            const rrtmg_lw_tuning *tune, char *errmsg,
+                            int32_t errmsg_len);
+
+/* Autotuner of the launch shape: runs the first blocks totalling at least
+ * sample_cols columns (0 = all blocks) with each candidate shape (transfer
+ * CTA of 1, 2 or 4 columns x chunk sizes), timing two runs of each with CUDA
+ * events, and keeps the fastest as the default shape of later calls with the
+ * same layer count and precision.  Writes the blocks' outputs.  best and
+ * best_ms (optional) receive the chosen shape and its time per call.  No
+ * counterpart in the reference.  Returns errflg. */
+int rrtmg_lw_gpu_autotune(const rrtmg_lw_run_args *blocks, int32_t nblocks,
+                          int32_t precision, void *stream,
+                          int64_t sample_cols, rrtmg_lw_tuning *best,
+                          float *best_ms, char *errmsg, int32_t errmsg_len);
+
 /* Release device tables and per-thread workspaces (call once at exit). */
 void rrtmg_lw_gpu_finalize(void);
 

@@ -8,7 +8,7 @@ import re
 
 import pytest
 
-from ccpp_physics_b200 import abi
+from ccpp_physics_b200 import abi, synthetic
 
 ROOT = os.path.join(os.path.dirname(__file__), "..")
 
@@ -70,3 +70,22 @@ def test_run_before_init_reports_error():
     assert err == 1 and "init" in msg
     rc, msg = lw.rlwinit()
     assert rc == 1 and "CUDA" in msg
+
+
+def test_block_args_offsets():
+    """Physics blocks as views into one profile: every pointer moves to the
+    block's first column; records move by their record size; ldim = npts."""
+    import ctypes as C
+    from ccpp_physics_b200 import rrtmg_lw as lw
+    npts, nlay = 40, 20
+    p = synthetic.make_profiles(npts, nlay, seed=1)
+    o = abi.alloc_outputs(npts, nlay, hlw0=True, hlwb=True, flxprf=True)
+    arr, keep = lw.block_args(p, o, [10, 25, 5])
+    addr = lambda a, n: C.cast(getattr(a, n), C.c_void_p).value
+    assert [a.npts for a in arr] == [10, 25, 5] and all(a.ldim == npts for a in arr)
+    for name, step in (("plyr", 8), ("aeraod", 8), ("hlwb", 8), ("icseed", 4), ("topflx", 16),
+                       ("sfcflx", 32), ("flxprf", 32)):
+        assert addr(arr[1], name) - addr(arr[0], name) == 10 * step, name
+        assert addr(arr[2], name) - addr(arr[0], name) == 35 * step, name
+    with pytest.raises(ValueError):
+        lw.block_args(p, o, [10, 10])
