@@ -296,8 +296,13 @@ int validate(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg, i
     for (const double* p : outs)
       if (!p) { set_msg(errmsg, errmsg_len, "rrtmg_lw_run: a required output array pointer is NULL"); return 1; }
   if (a->isubclw == 2 && !a->icseed) { set_msg(errmsg, errmsg_len, "rrtmg_lw_run: icseed is NULL"); return 1; }
-  if (x && x->precision != RRTMG_LW_FP64 && x->precision != RRTMG_LW_FP32) {
-    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: precision %d not available in this build", x->precision);
+  if (x && x->precision != RRTMG_LW_FP64 && x->precision != RRTMG_LW_FP32 && x->precision != RRTMG_LW_SURROGATE) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: unknown precision %d", x->precision);
+    return 1;
+  }
+  if (x && x->precision == RRTMG_LW_SURROGATE && !surrogate_norm()) {
+    set_msg(errmsg, errmsg_len,
+            "rrtmg_lw_gpu: RRTMG_LW_SURROGATE needs a network (rrtmg_lw_gpu_surrogate_init/_set and _train)");
     return 1;
   }
   return 0;
@@ -329,6 +334,16 @@ void fill_flags(const rrtmg_lw_run_args* a, Flags* f) {
   f->want_hlwb = a->hlwb != nullptr;
   f->want_flxprf = a->flxprf != nullptr;
   f->gas_only = 0;
+}
+
+// The learned gas optics runs the FP32 column kernels with the network
+// stage in front: turn the surrogate precision into FP32 + flags.
+int kernel_precision(int precision, Flags* f) {
+  if (precision != RRTMG_LW_SURROGATE) return precision;
+  f->surrogate = 1;
+  f->sg_norm = surrogate_norm();
+  f->sg_fallback = surrogate_fallback_counter();
+  return RRTMG_LW_FP32;
 }
 
 // Fill a block descriptor from (device) pointers of the argument struct.
@@ -563,8 +578,9 @@ extern "C" int rrtmg_lw_gpu_run_ex(const rrtmg_lw_run_args* a, const rrtmg_lw_ex
   if (x->memory == RRTMG_LW_DEVICE) {
     Block B;
     block_from_args(a, &B);
-    int r = launch(w, st, &B, 1, a->npts, f, x->precision, default_shape(x->precision, pick_v(f.nlay)),
-                   x->kernel_ms, errmsg, errmsg_len);
+    const int kp = kernel_precision(x->precision, &f);
+    int r = launch(w, st, &B, 1, a->npts, f, kp, default_shape(kp, pick_v(f.nlay)), x->kernel_ms, errmsg,
+                   errmsg_len);
     if (r) return r;
     if (x->sync) CK(cudaStreamSynchronize(st), "kernel execution");
     return 0;
@@ -617,8 +633,9 @@ extern "C" int rrtmg_lw_gpu_run_ex(const rrtmg_lw_run_args* a, const rrtmg_lw_ex
   }
   Block B;
   block_from_args(&d, &B);
-  int r = launch(w, st, &B, 1, a->npts, f, x->precision, default_shape(x->precision, pick_v(f.nlay)),
-                 x->kernel_ms, errmsg, errmsg_len);
+  const int kp = kernel_precision(x->precision, &f);
+  int r = launch(w, st, &B, 1, a->npts, f, kp, default_shape(kp, pick_v(f.nlay)), x->kernel_ms, errmsg,
+                 errmsg_len);
   if (r) return r;
   for (int k = 0; k < nout; ++k) {
     if (!host_out[k]) continue;
@@ -771,7 +788,8 @@ extern "C" int rrtmg_lw_gpu_run_blocks(const rrtmg_lw_run_args* blocks, int32_t 
   Workspace* w = workspace(errmsg, errmsg_len, &rc);
   if (!w) return rc;
   cudaStream_t st = x->stream ? (cudaStream_t)x->stream : w->stream;
-  Shape sh = default_shape(x->precision, pick_v(f.nlay));
+  const int kp = kernel_precision(x->precision, &f);
+  Shape sh = default_shape(kp, pick_v(f.nlay));
   bool graph = false;
   if (tune) {
     if (tune->rt_warps) sh.rt_warps = tune->rt_warps;
@@ -787,9 +805,8 @@ extern "C" int rrtmg_lw_gpu_run_blocks(const rrtmg_lw_run_args* blocks, int32_t 
     set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_blocks: negative tuning value");
     return 1;
   }
-  int r = graph ? launch_graph(w, st, hb, ncols, f, x->precision, sh, errmsg, errmsg_len)
-                : launch(w, st, hb.data(), (int)hb.size(), ncols, f, x->precision, sh, x->kernel_ms, errmsg,
-                         errmsg_len);
+  int r = graph ? launch_graph(w, st, hb, ncols, f, kp, sh, errmsg, errmsg_len)
+                : launch(w, st, hb.data(), (int)hb.size(), ncols, f, kp, sh, x->kernel_ms, errmsg, errmsg_len);
   if (r) return r;
   if (x->sync) CK(cudaStreamSynchronize(st), "kernel execution");
   return 0;
@@ -813,6 +830,7 @@ extern "C" int rrtmg_lw_gpu_autotune(const rrtmg_lw_run_args* blocks, int32_t nb
   if (!w) return rc;
   cudaStream_t st = stream ? (cudaStream_t)stream : w->stream;
   const int V = pick_v(f.nlay);
+  precision = kernel_precision(precision, &f);
   // candidates: transfer CTA of 1, 2, 4 columns x hand-off chunk (all, 1/2, 1/4 of the columns)
   std::vector<Shape> cands;
   for (int wv : {4, 2, 1})

@@ -3,6 +3,9 @@
 #include <algorithm>
 #include <cstdio>
 
+#include <type_traits>
+
+#include "lw_launch.h"
 #include "lw_rt.cuh"
 
 #define REAL double

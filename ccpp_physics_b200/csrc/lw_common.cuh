@@ -79,6 +79,22 @@ struct Flags {
   int ilwcliq, ilwcice, isubclw;
   int want_hlw0, want_hlwb, want_flxprf;
   int gas_only;        // 1: write taug/fracs only (training data / stage tests)
+  int surrogate = 0;   // 1: the learned gas optics wrote tau/frac; recompute only out-of-envelope layers
+  int pad_ = 0;
+  const float* sg_norm = nullptr;        // normalisation + envelope of the network (lw_features.cuh)
+  unsigned int* sg_fallback = nullptr;   // count of layers that fell back to taumol
+};
+
+// Device scratch of the gas-optics -> transfer hand-off (NLP = 32 V layers).
+template <typename R>
+struct Scratch {
+  R* tau;        // [nc][NGPT][NLP]
+  R* frac;       // [nc][NGPT][NLP]
+  R* band;       // [nc][3][NBANDS][NLP]
+  double* col;   // [nc][kColRec]
+  int c0;        // first global column of the chunk
+  int cap;       // columns the scratch holds
+  int ntot;      // columns of the whole call
 };
 
 // Launch shape of the column kernels (host side; chosen by the autotuner

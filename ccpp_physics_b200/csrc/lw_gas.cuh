@@ -21,6 +21,7 @@
 
 #include "lw_bands.cuh"
 #include "lw_common.cuh"
+#include "lw_features.cuh"
 
 namespace lw {
 
@@ -55,16 +56,6 @@ static __device__ __constant__ double c_a1[16] = {0.00, 0.25, 0.22, 0.00, 0.13, 
 static __device__ __constant__ double c_a2[16] = {0.00, -12.0, -11.7, 0.00, -0.72, -0.243, 0.19, -0.062,
                                                   0.414, 0.00, 0.00, 0.00, 0.00, 0.00, 0.00, 0.00};
 
-template <typename R>
-struct Scratch {
-  R* tau;        // [nc][NGPT][NLP]
-  R* frac;       // [nc][NGPT][NLP]
-  R* band;       // [nc][3][NBANDS][NLP]
-  double* col;   // [nc][kColRec]
-  int c0;        // first global column of the chunk
-  int cap;       // columns the scratch holds
-  int ntot;      // columns of the whole call
-};
 
 // checked read of the FP64 coefficient tables
 __device__ __forceinline__ double t64(const double* kt, long long o) {
@@ -162,6 +153,7 @@ lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int
     double tlyrfr = 0.0, tlvlfr = 0.0;
     int indlay = 1, indlev = 1, r = 0;
     bool lowerk = false, cldk = false;
+    bool sg_skip = false;   // learned gas optics already wrote this layer's tau/frac
     if (t < nlay) {
       const int kref = t + 1;
       r = top ? nlp1 - kref - 1 : t;                  // 0-based input row of the layer
@@ -191,6 +183,12 @@ lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int
       } else {
         colv[3] = colv[4] = colv[5] = colv[6] = 0.0;
         wxv[0] = wxv[1] = wxv[2] = wxv[3] = 0.0;
+      }
+      if (f.surrogate) {
+        float xf[SG_NFEAT];
+        layer_features(pavel, tavel, h2ovmr, o3vmr, IN(F_CO2, r), IN(F_CH4, r), IN(F_N2O, r), xf);
+        sg_skip = in_envelope(xf, f.sg_norm);
+        if (!sg_skip && f.sg_fallback) atomicAdd(f.sg_fallback, 1u);
       }
       double summol = 0.0;
       for (int m = 1; m < 7; ++m) summol = summol + colv[m];
@@ -331,7 +329,7 @@ lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int
         if (LW_OK(r < nlay && i < B.npts, 15, r)) tauaer = R(B.in[F_AERAOD][ab] * (1.0 - B.in[F_AERSSA][ab]));
         const int ns = ns_of(b);
         const size_t go = ((size_t)c * nlay + t) * NGPT + ns;
-        band_gas_optics<R>(b, kt, LR, [&](int g0, R tau, R frac) {
+        if (!sg_skip) band_gas_optics<R>(b, kt, LR, [&](int g0, R tau, R frac) {
           if (tcol && LW_OK(cc < sc.cap && ns + g0 < NGPT, 16, ns + g0)) {
             __stcs(tcol + (size_t)(ns + g0) * NLP, tau + tauaer);
             __stcs(fcol + (size_t)(ns + g0) * NLP, frac);

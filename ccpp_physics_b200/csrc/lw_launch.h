@@ -33,6 +33,14 @@ cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int 
                          int isubclw, int top_at_1, const double* cldf_dev, const int32_t* seed_dev, int dev_ld,
                          uint32_t* bits, int num_sms, cudaStream_t st);
 
+// learned gas optics (lw_mlp.cu): network stage of a chunk, its
+// normalisation/envelope (nullptr until a network is loaded) and the
+// fallback counter
+cudaError_t mlp_lw_launch(const Block* blocks, int nblocks, const Block& b0, int nc, const Flags& f,
+                          const Scratch<float>& sc, int num_sms, cudaStream_t st);
+const float* surrogate_norm();
+unsigned int* surrogate_fallback_counter();
+
 // layers per lane of the column kernels (NLP = 32 V padded layers)
 inline int pick_v(int nlay) { return nlay <= 63 ? 2 : nlay <= 127 ? 4 : 8; }
 

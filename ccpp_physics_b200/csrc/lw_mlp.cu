@@ -1,0 +1,1074 @@
+// lw_mlp.cu -- learned gas optics for the RRTMG-LW path: a BF16 MLP
+// 8 -> 128 -> 128 -> 288 (7 layer features + 1; 140 log(taug/coldry) and
+// 140 Planck fractions, padded to 288) on the 5th-generation tensor cores.
+//
+// Kernels (all hand-written, tcgen05 MMAs with FP32 accumulation in TMEM):
+//   mlp_fwd_kernel<MODE>  persistent; the three weight matrices stay in
+//                         shared memory; per 128-row tile: X -> MMA1 ->
+//                         SiLU -> MMA2 -> SiLU -> MMA3 (2 x N=144) -> epilogue.
+//                         MODE_FEATS: rows are feature vectors, writes the
+//                         normalised outputs.  MODE_TRAIN: rows are gathered
+//                         training samples; writes the activations the
+//                         backward pass needs, dL/dy and the loss.  MODE_LW:
+//                         rows are the layers of a chunk of columns; writes
+//                         tau = exp(y) * coldry + aerosol and the band-
+//                         normalised Planck fractions straight into the
+//                         gas-optics -> transfer scratch of the column path.
+//   gemm_tn_kernel<EPI>   C = A * B^T for the backward pass: dH = dZ W with
+//                         the activation derivative fused (EPI_DACT), and
+//                         split-K weight gradients dW = dZ^T H with FP32
+//                         atomics (EPI_ATOMIC).  Bias gradients come out as
+//                         the column of a constant-1 row appended to H.
+//   adam_kernel           Adam on FP32 master weights; rewrites the BF16
+//                         operand copies (W and W^T).
+//   features_kernel       layer features + coldry of a block (training data).
+//
+// The network replaces setcoef+taumol (radlw_main.F90:2151-2406, 3836-6840)
+// for layers inside the training envelope; the gas-optics kernel recomputes
+// every other layer with plain taumol (lw_gas.cuh).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <random>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/rrtmg_lw_gpu.h"
+#include "lw_common.cuh"
+#include "lw_features.cuh"
+#include "lw_launch.h"
+#include "lw_umma.cuh"
+
+namespace lw {
+
+typedef __nv_bfloat16 bf16;
+
+// ---------------------------------------------------------------------------
+// parameter / operand / gradient layouts
+constexpr int HID = SG_HID, NOP = SG_NOUTP, NIN = SG_NFEAT, KIN = 16;
+constexpr int P_W1 = 0;                      // [128][8]   (column 7: bias of layer 1)
+constexpr int P_W2 = P_W1 + HID * NIN;       // [128][128]
+constexpr int P_B2 = P_W2 + HID * HID;       // [128]
+constexpr int P_W3 = P_B2 + HID;             // [288][128] (pad rows 140..143, 284..287 stay 0)
+constexpr int P_B3 = P_W3 + NOP * HID;       // [288]
+constexpr int P_N = P_B3 + NOP;              // 54,688 (53,656 trainable)
+
+constexpr int O_W1 = 0;                      // bf16 [128][16]
+constexpr int O_W2 = O_W1 + HID * KIN;       // bf16 [128][128]
+constexpr int O_W2T = O_W2 + HID * HID;      // bf16 [128][128] = W2^T
+constexpr int O_W3 = O_W2T + HID * HID;      // bf16 [288][128]
+constexpr int O_W3T = O_W3 + NOP * HID;      // bf16 [128][288] = W3^T
+constexpr int O_N = O_W3T + HID * NOP;
+
+constexpr int GW2_LD = 144, GW3_ROWS = 384;  // gradients of [W | b] (column 128 = bias)
+constexpr int G_W1 = 0;                      // f32 [128][16]
+constexpr int G_W2 = G_W1 + HID * KIN;       // f32 [128][144]
+constexpr int G_W3 = G_W2 + HID * GW2_LD;    // f32 [384][144]
+constexpr int G_N = G_W3 + GW3_ROWS * GW2_LD;
+
+__host__ __device__ inline bool pad_out_row(int j) { return (j >= 140 && j < 144) || j >= 284; }
+
+__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float dsilu(float z) {
+  const float s = 1.0f / (1.0f + __expf(-z));
+  return s * (1.0f + z * (1.0f - s));
+}
+
+// ---------------------------------------------------------------------------
+// forward kernel
+enum { MODE_FEATS = 0, MODE_TRAIN = 1, MODE_LW = 2 };
+
+struct FwdArgs {
+  const bf16* ops;      // operand copies (O_*)
+  const float* params;  // FP32 master (biases)
+  const float* norm;    // SG_NORM_FLOATS
+  long nrows;
+  int* err;             // first error: 1 = MMA wait timed out
+  // MODE_FEATS / MODE_TRAIN
+  const float* feats;   // [*][8] raw features
+  float* y;             // MODE_FEATS: [nrows][288] normalised outputs
+  // MODE_TRAIN
+  const float* targets; // [*][288] normalised targets
+  long perm_a, perm_b, perm_n, perm_off;   // sample = (a * (perm_off + row) + b) mod n
+  float loss_scale;     // 2 / (batch * 280)
+  float* loss;          // += sum of squared errors
+  bf16 *xt, *z1, *h1t, *z2, *h2t, *dy, *dyt;   // activations, see the trainer
+  long ldt;             // leading dimension (batch) of the transposed arrays
+  // MODE_LW
+  const Block* blocks;
+  int nblocks;
+  Block b0;
+  Flags f;
+  Scratch<float> sc;
+  int nc;               // columns of this chunk
+};
+
+constexpr int FWD_THREADS = 128;
+constexpr uint32_t SM_W1 = 0;                               // canon [128][16]
+constexpr uint32_t SM_W2 = SM_W1 + HID * KIN * 2;           // canon [128][128]
+constexpr uint32_t SM_W3 = SM_W2 + HID * HID * 2;           // canon [288][128]
+constexpr uint32_t SM_X = SM_W3 + NOP * HID * 2;            // canon [128][16]
+constexpr uint32_t SM_H = SM_X + 128 * KIN * 2;             // canon [128][128]
+constexpr uint32_t SM_B2 = SM_H + 128 * HID * 2;            // f32 [128]
+constexpr uint32_t SM_B3 = SM_B2 + HID * 4;                 // f32 [288]
+constexpr uint32_t SM_NORM = SM_B3 + NOP * 4;               // f32 [608]
+constexpr uint32_t SM_BAR = (SM_NORM + SG_NORM_FLOATS * 4 + 15) & ~15u;
+constexpr uint32_t FWD_SMEM = SM_BAR + 32;
+static_assert(FWD_SMEM > 116 * 1024, "forward kernel must hold its SM alone (512 TMEM columns)");
+static_assert(FWD_SMEM <= 227 * 1024, "forward kernel shared memory");
+constexpr uint32_t W3_HALF = 144 * HID * 2;                 // second 144-row B operand of MMA3
+
+// band of each g-point (radlw_param.f:111-120 ngb)
+__device__ __forceinline__ int band_of_g(int g) {
+  return g < 10 ? 0 : g < 22 ? 1 : g < 38 ? 2 : g < 52 ? 3 : g < 68 ? 4 : g < 76 ? 5 : g < 88 ? 6 : g < 96 ? 7
+       : g < 108 ? 8 : g < 114 ? 9 : g < 122 ? 10 : g < 130 ? 11 : g < 134 ? 12 : g < 136 ? 13 : g < 138 ? 14 : 15;
+}
+
+__device__ __forceinline__ void copy_rows_canon(unsigned char* dst, const bf16* src, int rows, int K, int tid) {
+  const int chunks = rows * (K / 8);
+  for (int c = tid; c < chunks; c += FWD_THREADS) {
+    const int r = c / (K / 8), k = (c % (K / 8)) * 8;
+    *reinterpret_cast<uint4*>(dst + umma::canon_off(r, k, K)) =
+        __ldg(reinterpret_cast<const uint4*>(src + (size_t)r * K + k));
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  float* sb2 = reinterpret_cast<float*>(sm + SM_B2);
+  float* sb3 = reinterpret_cast<float*>(sm + SM_B3);
+  float* snorm = reinterpret_cast<float*>(sm + SM_NORM);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + SM_BAR);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SM_BAR + 8);
+  int* sfail = reinterpret_cast<int*>(sm + SM_BAR + 12);
+
+  copy_rows_canon(sm + SM_W1, a.ops + O_W1, HID, KIN, tid);
+  copy_rows_canon(sm + SM_W2, a.ops + O_W2, HID, HID, tid);
+  copy_rows_canon(sm + SM_W3, a.ops + O_W3, NOP, HID, tid);
+  for (int j = tid; j < HID; j += FWD_THREADS) sb2[j] = a.params[P_B2 + j];
+  for (int j = tid; j < NOP; j += FWD_THREADS) sb3[j] = a.params[P_B3 + j];
+  for (int j = tid; j < SG_NORM_FLOATS; j += FWD_THREADS) snorm[j] = a.norm[j];
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, 512);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    umma::mbar_init(mbar, 1);
+    *sfail = 0;
+  }
+  umma::fence_smem_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tb = *tslot;
+  const uint32_t sbase = umma::smem_u32(sm);
+  constexpr uint32_t ID128 = umma::idesc_bf16(128, 128), ID144 = umma::idesc_bf16(128, 144);
+  uint32_t phase = 0;
+  const long ntiles = (a.nrows + 127) / 128;
+
+  // wait for the MMAs committed last; on time-out every thread leaves the tile loop
+  bool failed = false;   // uniform across the CTA
+  auto wait_mma = [&]() -> bool {
+    const bool ok = umma::mbar_wait(mbar, phase);
+    phase ^= 1u;
+    umma::fence_after_sync();
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) *sfail = 1;
+      failed = true;
+      return false;
+    }
+    return true;
+  };
+
+  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long row = tile * 128 + tid;
+    const bool live = row < a.nrows;
+    // ---------------- layer inputs ----------------
+    float x[KIN];
+#pragma unroll
+    for (int j = 0; j < KIN; ++j) x[j] = 0.0f;
+    long sample = row;
+    double coldry = 0.0;
+    int lw_cc = 0, lw_t = 0;
+    const Block* LB = nullptr;
+    int lw_i = 0, lw_r = 0;
+    if (live) {
+      float raw[NIN];
+      if (MODE == MODE_LW) {
+        const int nlay = a.f.nlay, nlp1 = nlay + 1;
+        lw_cc = (int)(row / nlay);
+        lw_t = (int)(row - (long)lw_cc * nlay);
+        const int c = a.sc.c0 + lw_cc;
+        LB = (a.nblocks == 1) ? &a.b0 : &a.blocks[find_block(a.blocks, a.nblocks, c)];
+        lw_i = c - LB->col0;
+        lw_r = a.f.top_at_1 ? nlp1 - (lw_t + 1) - 1 : lw_t;
+        const size_t o = (size_t)lw_i + (size_t)LB->ld * lw_r;
+        const double pavel = LB->in[F_PLYR][o], tavel = LB->in[F_TLYR][o], q = LB->in[F_QLYR][o];
+        const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
+        const double h2ovmr = fmax(0.0, q * amdw / (1.0 - q));
+        const double o3vmr = fmax(0.0, LB->in[F_OLYR][o] * amdo3);
+        const double tem0 = (1.0 - h2ovmr) * 28.9644 + h2ovmr * 18.0154;
+        coldry = (1.0e-20 * 1.0e3 * 6.0221415e23) * LB->in[F_DELPIN][o] / (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr));
+        layer_features(pavel, tavel, h2ovmr, o3vmr, LB->in[F_CO2][o], LB->in[F_CH4][o], LB->in[F_N2O][o], raw);
+      } else {
+        if (MODE == MODE_TRAIN) sample = (long)(((unsigned long long)a.perm_a * (unsigned long long)(a.perm_off + row) +
+                                                 (unsigned long long)a.perm_b) % (unsigned long long)a.perm_n);
+        const float4* src = reinterpret_cast<const float4*>(a.feats + sample * NIN);
+        float4 u = __ldg(src), w = __ldg(src + 1);
+        raw[0] = u.x; raw[1] = u.y; raw[2] = u.z; raw[3] = u.w; raw[4] = w.x; raw[5] = w.y; raw[6] = w.z;
+        raw[7] = 1.0f;
+      }
+#pragma unroll
+      for (int j = 0; j < 7; ++j) x[j] = (raw[j] - snorm[SG_IN_MEAN + j]) / snorm[SG_IN_STD + j];
+      x[7] = 1.0f;
+    }
+    umma::st_canon8(sm + SM_X, tid, 0, KIN, x);
+    umma::st_canon8(sm + SM_X, tid, 8, KIN, x + 8);
+    if (MODE == MODE_TRAIN && live) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) a.xt[(size_t)j * a.ldt + row] = __float2bfloat16_rn(x[j]);
+    }
+    umma::fence_smem_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      umma::mma(tb, umma::tile_desc(sbase + SM_X, KIN, 0), umma::tile_desc(sbase + SM_W1, KIN, 0), ID128, 0u);
+      umma::commit(mbar);
+    }
+    if (!wait_mma()) break;
+
+    // ---------------- hidden layers ----------------
+#pragma unroll 1
+    for (int layer = 0; layer < 2; ++layer) {
+      const uint32_t dcol = layer == 0 ? 0u : 128u;
+#pragma unroll 1
+      for (int c0 = 0; c0 < HID; c0 += 16) {
+        float v[16], h[16];
+        umma::tmem_ld16(umma::tmem_addr(tb, warp, dcol + c0), v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const float z = v[j] + (layer == 1 ? sb2[c0 + j] : 0.0f);
+          v[j] = z;
+          h[j] = silu(z);
+        }
+        umma::st_canon8(sm + SM_H, tid, c0, HID, h);
+        umma::st_canon8(sm + SM_H, tid, c0 + 8, HID, h + 8);
+        if (MODE == MODE_TRAIN && live) {
+          bf16* z = (layer == 0 ? a.z1 : a.z2) + (size_t)row * HID + c0;
+          __nv_bfloat162 zp[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) zp[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+          reinterpret_cast<uint4*>(z)[0] = reinterpret_cast<uint4*>(zp)[0];
+          reinterpret_cast<uint4*>(z)[1] = reinterpret_cast<uint4*>(zp)[1];
+          bf16* ht = (layer == 0 ? a.h1t : a.h2t);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) ht[(size_t)(c0 + j) * a.ldt + row] = __float2bfloat16_rn(h[j]);
+        }
+      }
+      umma::fence_smem_async();
+      umma::fence_before_sync();
+      __syncthreads();
+      if (tid == 0) {
+        umma::fence_after_sync();
+        if (layer == 0) {
+#pragma unroll 1
+          for (int s = 0; s < HID / 16; ++s)
+            umma::mma(tb + 128, umma::tile_desc(sbase + SM_H, HID, s), umma::tile_desc(sbase + SM_W2, HID, s), ID128,
+                      s > 0 ? 1u : 0u);
+        } else {
+#pragma unroll 1
+          for (int s = 0; s < HID / 16; ++s)
+            umma::mma(tb + 256, umma::tile_desc(sbase + SM_H, HID, s), umma::tile_desc(sbase + SM_W3, HID, s), ID144,
+                      s > 0 ? 1u : 0u);
+#pragma unroll 1
+          for (int s = 0; s < HID / 16; ++s)
+            umma::mma(tb, umma::tile_desc(sbase + SM_H, HID, s), umma::tile_desc(sbase + SM_W3 + W3_HALF, HID, s),
+                      ID144, s > 0 ? 1u : 0u);
+        }
+        umma::commit(mbar);
+      }
+      if (!wait_mma()) break;
+    }
+    if (failed) break;
+
+    // ---------------- output epilogue ----------------
+    // outputs [0,144) in TMEM columns 256.., outputs [144,288) in columns 0..
+    auto out_addr = [&](int j) { return j < 144 ? umma::tmem_addr(tb, warp, 256 + j) : umma::tmem_addr(tb, warp, j - 144); };
+    if (MODE == MODE_FEATS) {
+#pragma unroll 1
+      for (int j0 = 0; j0 < NOP; j0 += 16) {
+        float v[16];
+        umma::tmem_ld16(out_addr(j0), v);
+        if (live) {
+          float4* dst = reinterpret_cast<float4*>(a.y + (size_t)row * NOP + j0);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            dst[q] = make_float4(v[4 * q] + sb3[j0 + 4 * q], v[4 * q + 1] + sb3[j0 + 4 * q + 1],
+                                 v[4 * q + 2] + sb3[j0 + 4 * q + 2], v[4 * q + 3] + sb3[j0 + 4 * q + 3]);
+        }
+      }
+    } else if (MODE == MODE_TRAIN) {
+      float sse = 0.0f;
+#pragma unroll 1
+      for (int j0 = 0; j0 < NOP; j0 += 16) {
+        float v[16], d[16];
+        umma::tmem_ld16(out_addr(j0), v);
+        if (live) {
+          const float4* tg = reinterpret_cast<const float4*>(a.targets + (size_t)sample * NOP + j0);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            float4 t4 = __ldg(tg + q);
+            float tt[4] = {t4.x, t4.y, t4.z, t4.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int j = j0 + 4 * q + u;
+              const float e = pad_out_row(j) ? 0.0f : v[4 * q + u] + sb3[j] - tt[u];
+              sse += e * e;
+              d[4 * q + u] = e * a.loss_scale;
+            }
+          }
+          __nv_bfloat162 dp[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) dp[u] = __floats2bfloat162_rn(d[2 * u], d[2 * u + 1]);
+          uint4* dst = reinterpret_cast<uint4*>(a.dy + (size_t)row * NOP + j0);
+          dst[0] = reinterpret_cast<uint4*>(dp)[0];
+          dst[1] = reinterpret_cast<uint4*>(dp)[1];
+#pragma unroll
+          for (int u = 0; u < 16; ++u) a.dyt[(size_t)(j0 + u) * a.ldt + row] = __float2bfloat16_rn(d[u]);
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sse += __shfl_xor_sync(0xffffffffu, sse, o);
+      if ((tid & 31) == 0) atomicAdd(a.loss, sse);
+    } else {   // MODE_LW
+      // pass 1: per-band sums of the Planck fractions
+      float bsum[NBANDS];
+#pragma unroll
+      for (int b = 0; b < NBANDS; ++b) bsum[b] = 0.0f;
+#pragma unroll 1
+      for (int j0 = 144; j0 < 284 + 4; j0 += 16) {
+        float v[16];
+        umma::tmem_ld16(out_addr(j0), v);
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const int j = j0 + u;
+          if (j < 284) {
+            const float fr = fminf(1.0f, fmaxf(0.0f, (v[u] + sb3[j]) * snorm[SG_OUT_STD + j] + snorm[SG_OUT_MEAN + j]));
+            bsum[band_of_g(j - 144)] += fr;
+          }
+        }
+      }
+      // scratch pitch NLP = 32 V padded layers of the column kernels
+      const size_t nlp = (size_t)a.f.nlay <= 63 ? 64 : (size_t)a.f.nlay <= 127 ? 128 : 256;
+      float* tcol = a.sc.tau + (size_t)lw_cc * NGPT * nlp + lw_t;
+      float* fcol = a.sc.frac + (size_t)lw_cc * NGPT * nlp + lw_t;
+      float aer[NBANDS];
+      if (live) {
+        const size_t ldl = (size_t)LB->ld;
+#pragma unroll
+        for (int b = 0; b < NBANDS; ++b) {
+          const size_t ab = (size_t)lw_i + ldl * ((size_t)lw_r + (size_t)a.f.nlay * b);
+          aer[b] = (float)(LB->in[F_AERAOD][ab] * (1.0 - LB->in[F_AERSSA][ab]));
+        }
+      }
+      const float cd = (float)coldry;
+      // pass 2: tau, then normalised fractions
+#pragma unroll 1
+      for (int j0 = 0; j0 < 144; j0 += 16) {
+        float v[16];
+        umma::tmem_ld16(out_addr(j0), v);
+        if (live) {
+#pragma unroll
+          for (int u = 0; u < 16; ++u) {
+            const int g = j0 + u;
+            if (g < NGPT) {
+              const float ly = (v[u] + sb3[g]) * snorm[SG_OUT_STD + g] + snorm[SG_OUT_MEAN + g];
+              __stcs(tcol + (size_t)g * nlp, __expf(ly) * cd + aer[band_of_g(g)]);
+            }
+          }
+        }
+      }
+#pragma unroll 1
+      for (int j0 = 144; j0 < 288; j0 += 16) {
+        float v[16];
+        umma::tmem_ld16(out_addr(j0), v);
+        if (live) {
+#pragma unroll
+          for (int u = 0; u < 16; ++u) {
+            const int j = j0 + u;
+            if (j < 284) {
+              const int g = j - 144;
+              const float fr = fminf(1.0f, fmaxf(0.0f, (v[u] + sb3[j]) * snorm[SG_OUT_STD + j] + snorm[SG_OUT_MEAN + j]));
+              const float s = bsum[band_of_g(g)];
+              __stcs(fcol + (size_t)g * nlp, s > 0.0f ? fr / s : fr);
+            }
+          }
+        }
+      }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+  }
+  // leave: every MMA this CTA issued has completed (or the wait timed out and
+  // the error is recorded); release tensor memory
+  umma::fence_before_sync();
+  __syncthreads();
+  if (tid == 0 && *sfail && a.err) atomicCAS(a.err, 0, 1);
+  if (warp == 0) umma::tmem_dealloc(tb, 512);
+}
+
+// ---------------------------------------------------------------------------
+// C[M x N] = A[M x K] * B[N x K]^T, BF16 in, FP32 accumulate (backward pass)
+enum { EPI_ATOMIC = 0, EPI_DACT = 1 };
+
+struct GemmArgs {
+  const bf16* A; long lda;
+  const bf16* B; long ldb;
+  int M, N, K, kslice;
+  float* C; long ldc;               // EPI_ATOMIC
+  const bf16* Z; long ldz;          // EPI_DACT
+  bf16* D; long ldd;                // EPI_DACT row-major out (nullable)
+  bf16* Dt; long lddt;              // EPI_DACT transposed out (nullable)
+  int* err;
+};
+
+constexpr int GK = 64;                                   // K per staged chunk
+constexpr uint32_t GSM_A = 0;                            // canon [128][64]
+constexpr uint32_t GSM_B = GSM_A + 128 * GK * 2;         // canon [288][64]
+constexpr uint32_t GSM_BAR = GSM_B + 288 * GK * 2;
+constexpr uint32_t GEMM_SMEM_MIN = GSM_BAR + 32;
+constexpr uint32_t GEMM_SMEM = 120 * 1024;               // > half an SM: one CTA per SM (512 TMEM columns)
+static_assert(GEMM_SMEM >= GEMM_SMEM_MIN, "gemm shared memory");
+
+template <int EPI>
+__global__ void __launch_bounds__(128, 1) gemm_tn_kernel(GemmArgs g) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + GSM_BAR);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + GSM_BAR + 8);
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, 512);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) umma::mbar_init(mbar, 1);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tb = *tslot;
+  const uint32_t sbase = umma::smem_u32(sm);
+  const int m0 = blockIdx.x * 128;
+  const int kb = blockIdx.y * g.kslice, ke = min(g.K, kb + g.kslice);
+  const int nsplit = g.N > 256 ? 2 : 1, nh = g.N / nsplit;
+  const uint32_t idesc = umma::idesc_bf16(128, nh);
+  uint32_t phase = 0;
+  bool ok = true, any = false;
+  for (int k0 = kb; k0 < ke; k0 += GK) {
+    const int kc = min(GK, ke - k0);   // multiple of 16
+    // stage A [128 x kc] and B [N x kc] (zero-fill the unused K of a short chunk)
+    for (int c = tid; c < 128 * (GK / 8); c += 128) {
+      const int r = c / (GK / 8), k = (c % (GK / 8)) * 8;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (k < kc && m0 + r < g.M) v = __ldg(reinterpret_cast<const uint4*>(g.A + (size_t)(m0 + r) * g.lda + k0 + k));
+      *reinterpret_cast<uint4*>(sm + GSM_A + umma::canon_off(r, k, GK)) = v;
+    }
+    for (int c = tid; c < g.N * (GK / 8); c += 128) {
+      const int r = c / (GK / 8), k = (c % (GK / 8)) * 8;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (k < kc) v = __ldg(reinterpret_cast<const uint4*>(g.B + (size_t)r * g.ldb + k0 + k));
+      *reinterpret_cast<uint4*>(sm + GSM_B + umma::canon_off(r, k, GK)) = v;
+    }
+    umma::fence_smem_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      for (int s = 0; s < kc / 16; ++s)
+        for (int h = 0; h < nsplit; ++h)
+          umma::mma(tb + (uint32_t)(h * nh), umma::tile_desc(sbase + GSM_A, GK, s),
+                    umma::tile_desc(sbase + GSM_B + (uint32_t)(h * nh * GK * 2), GK, s), idesc,
+                    (any || s > 0) ? 1u : 0u);
+      umma::commit(mbar);
+    }
+    any = true;
+    ok = umma::mbar_wait(mbar, phase);
+    phase ^= 1u;
+    umma::fence_after_sync();
+    if (__syncthreads_or(!ok)) { ok = false; break; }
+  }
+  if (ok && any) {
+    const int m = m0 + tid;
+    for (int n0 = 0; n0 < g.N; n0 += 16) {
+      float v[16];
+      umma::tmem_ld16(umma::tmem_addr(tb, warp, n0), v);
+      if (m >= g.M) continue;
+      if (EPI == EPI_ATOMIC) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) atomicAdd(g.C + (size_t)m * g.ldc + n0 + j, v[j]);
+      } else {
+        float d[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) d[j] = v[j] * dsilu(__bfloat162float(g.Z[(size_t)m * g.ldz + n0 + j]));
+        if (g.D) {
+          __nv_bfloat162 dp[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) dp[j] = __floats2bfloat162_rn(d[2 * j], d[2 * j + 1]);
+          uint4* dst = reinterpret_cast<uint4*>(g.D + (size_t)m * g.ldd + n0);
+          dst[0] = reinterpret_cast<uint4*>(dp)[0];
+          dst[1] = reinterpret_cast<uint4*>(dp)[1];
+        }
+        if (g.Dt) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) g.Dt[(size_t)(n0 + j) * g.lddt + m] = __float2bfloat16_rn(d[j]);
+        }
+      }
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (tid == 0 && !ok && g.err) atomicCAS(g.err, 0, 1);
+  if (warp == 0) umma::tmem_dealloc(tb, 512);
+}
+
+// ---------------------------------------------------------------------------
+// Adam on the FP32 master weights, then the BF16 operand copies
+__device__ inline void pack_param(int p, float w, bf16* ops) {
+  const bf16 b = __float2bfloat16_rn(w);
+  if (p < P_W2) {
+    const int r = p / NIN, c = p % NIN;
+    ops[O_W1 + r * KIN + c] = b;
+  } else if (p < P_B2) {
+    const int q = p - P_W2, r = q / HID, c = q % HID;
+    ops[O_W2 + r * HID + c] = b;
+    ops[O_W2T + c * HID + r] = b;
+  } else if (p >= P_W3 && p < P_B3) {
+    const int q = p - P_W3, r = q / HID, c = q % HID;
+    ops[O_W3 + r * HID + c] = b;
+    ops[O_W3T + c * NOP + r] = b;
+  }
+}
+
+__device__ inline float grad_of(int p, const float* G) {
+  if (p < P_W2) { const int r = p / NIN, c = p % NIN; return G[G_W1 + r * KIN + c]; }
+  if (p < P_B2) { const int q = p - P_W2; return G[G_W2 + (q / HID) * GW2_LD + q % HID]; }
+  if (p < P_W3) { return G[G_W2 + (p - P_B2) * GW2_LD + HID]; }
+  if (p < P_B3) { const int q = p - P_W3; return G[G_W3 + (q / HID) * GW2_LD + q % HID]; }
+  return G[G_W3 + (p - P_B3) * GW2_LD + HID];
+}
+
+__device__ inline bool frozen_param(int p) {   // padded output rows stay zero
+  if (p >= P_W3 && p < P_B3) return pad_out_row((p - P_W3) / HID);
+  if (p >= P_B3) return pad_out_row(p - P_B3);
+  return false;
+}
+
+__global__ void adam_kernel(float* P, float* M, float* V, const float* G, bf16* ops, float lr, float b1, float b2,
+                            float c1, float c2, float eps) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P_N; p += gridDim.x * blockDim.x) {
+    float w = P[p];
+    if (!frozen_param(p)) {
+      const float gr = grad_of(p, G);
+      const float m = b1 * M[p] + (1.0f - b1) * gr;
+      const float v = b2 * V[p] + (1.0f - b2) * gr * gr;
+      M[p] = m;
+      V[p] = v;
+      w -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+      P[p] = w;
+    }
+    pack_param(p, w, ops);
+  }
+}
+
+__global__ void pack_kernel(const float* P, bf16* ops) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P_N; p += gridDim.x * blockDim.x) pack_param(p, P[p], ops);
+}
+
+// export the gradients in parameter order (gradient check)
+__global__ void grads_kernel(const float* G, float* out) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P_N; p += gridDim.x * blockDim.x)
+    out[p] = frozen_param(p) ? 0.0f : grad_of(p, G);
+}
+
+// layer features and coldry of one block (internal layer order, surface first)
+__global__ void features_kernel(Block B, int nlay, int top_at_1, float* feats, float* coldry_out) {
+  const long n = (long)B.npts * nlay;
+  for (long row = blockIdx.x * (long)blockDim.x + threadIdx.x; row < n; row += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(row / nlay), t = (int)(row - (long)i * nlay);
+    const int r = top_at_1 ? nlay - t - 1 : t;
+    const size_t o = (size_t)i + (size_t)B.ld * r;
+    const double pavel = B.in[F_PLYR][o], tavel = B.in[F_TLYR][o], q = B.in[F_QLYR][o];
+    const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
+    const double h2ovmr = fmax(0.0, q * amdw / (1.0 - q));
+    const double o3vmr = fmax(0.0, B.in[F_OLYR][o] * amdo3);
+    const double tem0 = (1.0 - h2ovmr) * 28.9644 + h2ovmr * 18.0154;
+    float x[SG_NFEAT];
+    layer_features(pavel, tavel, h2ovmr, o3vmr, B.in[F_CO2][o], B.in[F_CH4][o], B.in[F_N2O][o], x);
+    for (int j = 0; j < SG_NFEAT; ++j) feats[row * SG_NFEAT + j] = x[j];
+    if (coldry_out)
+      coldry_out[row] = (float)((1.0e-20 * 1.0e3 * 6.0221415e23) * B.in[F_DELPIN][o] /
+                                (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr)));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+namespace {
+
+struct Net {
+  bool ready = false;     // weights present (init or set)
+  int device = -1;
+  float* P = nullptr;     // master weights
+  float* Madam = nullptr;
+  float* Vadam = nullptr;
+  float* G = nullptr;     // gradients
+  bf16* ops = nullptr;    // operand copies
+  float* norm = nullptr;  // SG_NORM_FLOATS
+  int* err = nullptr;
+  float* loss = nullptr;
+  unsigned int* fallback = nullptr;   // layers the gas-optics kernel recomputed with taumol
+  long adam_t = 0;
+  int num_sms = 0;
+  // training activations for batch `cap`
+  long cap = 0;
+  bf16 *xt = nullptr, *z1 = nullptr, *h1t = nullptr, *z2 = nullptr, *h2t = nullptr, *dy = nullptr, *dyt = nullptr,
+       *dz2 = nullptr, *dz1t = nullptr;
+  bool attrs = false;
+};
+Net net;
+std::mutex net_mu;
+
+void msg(char* e, int32_t n, const char* fmt, const char* what, cudaError_t c) {
+  if (e && n > 0) std::snprintf(e, (size_t)n, fmt, what, cudaGetErrorString(c));
+}
+#define SG_CK(call, what)                                                                 \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) {                                                              \
+      msg(errmsg, errmsg_len, "rrtmg_lw_gpu surrogate: %s failed: %s", what, e_);         \
+      return 1;                                                                           \
+    }                                                                                     \
+  } while (0)
+void smsg(char* e, int32_t n, const char* s) {
+  if (e && n > 0) std::snprintf(e, (size_t)n, "%s", s);
+}
+
+cudaError_t set_attrs() {
+  if (net.attrs) return cudaSuccess;
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(mlp_fwd_kernel<MODE_FEATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM)))
+    return e;
+  if ((e = cudaFuncSetAttribute(mlp_fwd_kernel<MODE_TRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM)))
+    return e;
+  if ((e = cudaFuncSetAttribute(mlp_fwd_kernel<MODE_LW>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM)))
+    return e;
+  if ((e = cudaFuncSetAttribute(gemm_tn_kernel<EPI_ATOMIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM)))
+    return e;
+  if ((e = cudaFuncSetAttribute(gemm_tn_kernel<EPI_DACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM)))
+    return e;
+  // one CTA per SM is what makes the 512-column TMEM allocations safe
+  int occ[5] = {0, 0, 0, 0, 0};
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], mlp_fwd_kernel<MODE_FEATS>, FWD_THREADS, FWD_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], mlp_fwd_kernel<MODE_TRAIN>, FWD_THREADS, FWD_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], mlp_fwd_kernel<MODE_LW>, FWD_THREADS, FWD_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], gemm_tn_kernel<EPI_ATOMIC>, 128, GEMM_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[4], gemm_tn_kernel<EPI_DACT>, 128, GEMM_SMEM);
+  for (int o : occ)
+    if (o != 1) return cudaErrorLaunchOutOfResources;
+  net.attrs = true;
+  return cudaSuccess;
+}
+
+cudaError_t ensure_net(int device, int num_sms) {
+  if (net.P && net.device == device) return cudaSuccess;
+  cudaError_t e;
+  net.device = device;
+  net.num_sms = num_sms;
+  if ((e = cudaMalloc(&net.P, sizeof(float) * P_N * 3))) return e;
+  net.Madam = net.P + P_N;
+  net.Vadam = net.P + 2 * P_N;
+  if ((e = cudaMemset(net.P, 0, sizeof(float) * P_N * 3))) return e;
+  if ((e = cudaMalloc(&net.G, sizeof(float) * G_N))) return e;
+  if ((e = cudaMemset(net.G, 0, sizeof(float) * G_N))) return e;
+  if ((e = cudaMalloc(&net.ops, sizeof(bf16) * O_N))) return e;
+  if ((e = cudaMemset(net.ops, 0, sizeof(bf16) * O_N))) return e;
+  if ((e = cudaMalloc(&net.norm, sizeof(float) * SG_NORM_FLOATS))) return e;
+  if ((e = cudaMalloc(&net.err, 4 * sizeof(int)))) return e;
+  net.loss = reinterpret_cast<float*>(net.err + 1);
+  net.fallback = reinterpret_cast<unsigned int*>(net.err + 2);
+  return cudaMemset(net.err, 0, 4 * sizeof(int));
+}
+
+cudaError_t ensure_batch(long batch) {
+  if (net.cap >= batch) return cudaSuccess;
+  bf16** bufs[] = {&net.xt, &net.z1, &net.h1t, &net.z2, &net.h2t, &net.dy, &net.dyt, &net.dz2, &net.dz1t};
+  for (bf16** b : bufs)
+    if (*b) { cudaFree(*b); *b = nullptr; }
+  net.cap = 0;
+  // rows: Xt 16, Z [B][128], H^T 144 (row 128 = 1), dY [B][288], dY^T 384, dZ2 [B][128], dZ1^T 128
+  const size_t B = (size_t)batch;
+  const size_t n[] = {16 * B, B * HID, 144 * B, B * HID, 144 * B, B * NOP, GW3_ROWS * B, B * HID, HID * B};
+  cudaError_t e;
+  for (int k = 0; k < 9; ++k) {
+    if ((e = cudaMalloc(bufs[k], n[k] * sizeof(bf16)))) return e;
+    if ((e = cudaMemset(*bufs[k], 0, n[k] * sizeof(bf16)))) return e;
+  }
+  // constant rows: the bias row of H1^T / H2^T and of X^T (feature 7 is written each step)
+  std::vector<bf16> ones(B, __float2bfloat16_rn(1.0f));
+  if ((e = cudaMemcpy(net.h1t + 128 * B, ones.data(), B * sizeof(bf16), cudaMemcpyHostToDevice))) return e;
+  if ((e = cudaMemcpy(net.h2t + 128 * B, ones.data(), B * sizeof(bf16), cudaMemcpyHostToDevice))) return e;
+  net.cap = batch;
+  return cudaSuccess;
+}
+
+FwdArgs base_args() {
+  FwdArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.ops = net.ops;
+  a.params = net.P;
+  a.norm = net.norm;
+  a.err = net.err;
+  return a;
+}
+
+cudaError_t launch_gemm(int epi, const GemmArgs& g, int ksplit, cudaStream_t st) {
+  dim3 grid((g.M + 127) / 128, ksplit);
+  if (epi == EPI_ATOMIC) gemm_tn_kernel<EPI_ATOMIC><<<grid, 128, GEMM_SMEM, st>>>(g);
+  else gemm_tn_kernel<EPI_DACT><<<grid, 128, GEMM_SMEM, st>>>(g);
+  return cudaGetLastError();
+}
+
+// forward (train mode) + backward of one batch: gradients accumulate in net.G
+cudaError_t train_batch(const float* feats, const float* targets, long nsamp, long batch, long pa, long pb,
+                        long off, cudaStream_t st) {
+  FwdArgs a = base_args();
+  a.nrows = batch;
+  a.feats = feats;
+  a.targets = targets;
+  a.perm_a = pa;
+  a.perm_b = pb;
+  a.perm_n = nsamp;
+  a.perm_off = off;
+  a.loss_scale = 2.0f / ((float)batch * (float)SG_NOUT);
+  a.loss = net.loss;
+  a.xt = net.xt; a.z1 = net.z1; a.h1t = net.h1t; a.z2 = net.z2; a.h2t = net.h2t; a.dy = net.dy; a.dyt = net.dyt;
+  const long ldt = net.cap;   // pitch of the transposed activations (their constant rows sit at this pitch)
+  a.ldt = ldt;
+  const int tiles = (int)((batch + 127) / 128);
+  mlp_fwd_kernel<MODE_TRAIN><<<std::min(tiles, net.num_sms), FWD_THREADS, FWD_SMEM, st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e) return e;
+  const int B = (int)batch;
+  // dZ2 = (dY W3) * silu'(Z2): row-major for dH1, transposed for dW2
+  GemmArgs g{};
+  g.err = net.err;
+  g.A = net.dy; g.lda = NOP; g.B = net.ops + O_W3T; g.ldb = NOP; g.M = B; g.N = HID; g.K = NOP; g.kslice = NOP;
+  g.Z = net.z2; g.ldz = HID; g.D = net.dz2; g.ldd = HID; g.Dt = nullptr; g.lddt = 0;
+  // dZ2^T (A operand of dW2) goes to the dZ1^T buffer: dW2 consumes it before dH1 overwrites it
+  g.Dt = net.dz1t;
+  g.lddt = ldt;
+  if ((e = launch_gemm(EPI_DACT, g, 1, st))) return e;
+  // dW3 += dY^T H2aug : [288 x B] x [144 x B]^T  (A rows 288..383 are zero)
+  GemmArgs w3{};
+  w3.err = net.err;
+  w3.A = net.dyt; w3.lda = ldt; w3.B = net.h2t; w3.ldb = ldt; w3.M = NOP; w3.N = 144; w3.K = B;
+  const int ks = std::max(1, std::min(32, B / 256));
+  w3.kslice = ((B / ks + 63) / 64) * 64;
+  w3.C = net.G + G_W3; w3.ldc = GW2_LD;
+  if ((e = launch_gemm(EPI_ATOMIC, w3, (B + w3.kslice - 1) / w3.kslice, st))) return e;
+  // dW2 += dZ2^T H1aug
+  GemmArgs w2 = w3;
+  w2.A = net.dz1t; w2.M = HID; w2.B = net.h1t; w2.C = net.G + G_W2;
+  if ((e = launch_gemm(EPI_ATOMIC, w2, (B + w2.kslice - 1) / w2.kslice, st))) return e;
+  // dZ1^T = ((dZ2 W2) * silu'(Z1))^T
+  GemmArgs d1{};
+  d1.err = net.err;
+  d1.A = net.dz2; d1.lda = HID; d1.B = net.ops + O_W2T; d1.ldb = HID; d1.M = B; d1.N = HID; d1.K = HID;
+  d1.kslice = HID;
+  d1.Z = net.z1; d1.ldz = HID; d1.D = nullptr; d1.Dt = net.dz1t; d1.lddt = ldt;
+  if ((e = launch_gemm(EPI_DACT, d1, 1, st))) return e;
+  // dW1 += dZ1^T X : [128 x B] x [16 x B]^T
+  GemmArgs w1 = w3;
+  w1.A = net.dz1t; w1.M = HID; w1.B = net.xt; w1.N = 16; w1.C = net.G + G_W1; w1.ldc = KIN;
+  return launch_gemm(EPI_ATOMIC, w1, (B + w1.kslice - 1) / w1.kslice, st);
+}
+
+int check_ready(char* errmsg, int32_t errmsg_len) {
+  if (!net.ready) {
+    smsg(errmsg, errmsg_len, "rrtmg_lw_gpu surrogate: no network (call rrtmg_lw_gpu_surrogate_init or _set)");
+    return 1;
+  }
+  return 0;
+}
+
+}  // namespace
+
+// MLP stage of the surrogate column path: writes tau/frac of every layer of
+// the chunk into the scratch (the gas-optics kernel then redoes the layers
+// outside the envelope).  Enqueue only.
+cudaError_t mlp_lw_launch(const Block* blocks, int nblocks, const Block& b0, int nc, const Flags& f,
+                          const Scratch<float>& sc, int num_sms, cudaStream_t st) {
+  if (!net.ready || !net.attrs) return cudaErrorNotReady;
+  FwdArgs a = base_args();
+  a.nrows = (long)nc * f.nlay;
+  a.blocks = blocks;
+  a.nblocks = nblocks;
+  a.b0 = b0;
+  a.f = f;
+  a.sc = sc;
+  a.nc = nc;
+  const long tiles = (a.nrows + 127) / 128;
+  const int grid = (int)std::min<long>(tiles, num_sms);
+  if (grid < 1) return cudaSuccess;
+  mlp_fwd_kernel<MODE_LW><<<grid, FWD_THREADS, FWD_SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+const float* surrogate_norm() { return net.ready ? net.norm : nullptr; }
+unsigned int* surrogate_fallback_counter() { return net.fallback; }
+
+}  // namespace lw
+
+using namespace lw;
+
+namespace {
+int dev_of_init(int* dev, int* sms) {
+  if (cudaGetDevice(dev) != cudaSuccess) return 1;
+  if (cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, *dev) != cudaSuccess) return 1;
+  return 0;
+}
+}  // namespace
+
+extern "C" int rrtmg_lw_gpu_surrogate_features(const rrtmg_lw_run_args* a, float* feats, float* coldry, void* stream,
+                                               char* errmsg, int32_t errmsg_len) {
+  smsg(errmsg, errmsg_len, "");
+  if (!a || !feats || a->npts < 0 || a->nlay < 1 || !a->plyr || !a->tlyr || !a->qlyr || !a->olyr || !a->delpin ||
+      !a->gasvmr_co2 || !a->gasvmr_ch4 || !a->gasvmr_n2o) {
+    smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_features: bad arguments");
+    return 1;
+  }
+  if (a->npts == 0) return 0;
+  Block B{};
+  const double* in[N_IN] = {a->plyr, a->plvl, a->tlyr, a->tlvl, a->qlyr, a->olyr, a->gasvmr_co2, a->gasvmr_n2o,
+                            a->gasvmr_ch4, a->gasvmr_o2, a->gasvmr_co, a->gasvmr_cfc11, a->gasvmr_cfc12,
+                            a->gasvmr_cfc22, a->gasvmr_ccl4, a->aeraod, a->aerssa, a->sfemis, a->sfgtmp,
+                            a->dzlyr, a->delpin, a->de_lgth, a->alpha, a->cld_cf, a->cld_lwp, a->cld_ref_liq,
+                            a->cld_iwp, a->cld_ref_ice, a->cld_rwp, a->cld_ref_rain, a->cld_swp,
+                            a->cld_ref_snow, a->cld_od};
+  std::memcpy(B.in, in, sizeof(in));
+  B.npts = a->npts;
+  B.ld = a->ldim > 0 ? a->ldim : a->npts;
+  cudaStream_t st = (cudaStream_t)stream;
+  features_kernel<<<1024, 256, 0, st>>>(B, a->nlay, a->top_at_1, feats, coldry);
+  SG_CK(cudaGetLastError(), "features kernel launch");
+  SG_CK(cudaStreamSynchronize(st), "features kernel");
+  return 0;
+}
+
+extern "C" int rrtmg_lw_gpu_surrogate_init(const float* norm, uint64_t seed, char* errmsg, int32_t errmsg_len) {
+  smsg(errmsg, errmsg_len, "");
+  if (!norm) { smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_init: NULL normalisation"); return 1; }
+  std::lock_guard<std::mutex> lk(net_mu);
+  int dev = 0, sms = 0;
+  if (dev_of_init(&dev, &sms)) { smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_init: no CUDA device"); return 1; }
+  SG_CK(set_attrs(), "kernel attributes (one CTA per SM)");
+  SG_CK(ensure_net(dev, sms), "cudaMalloc(network)");
+  // He-style uniform initialisation of the weights, zero biases
+  std::vector<float> P(P_N * 3, 0.0f);
+  std::mt19937_64 rng(seed);
+  auto fill = [&](int off, int rows, int cols, int fan_in) {
+    const float lim = std::sqrt(6.0f / (float)fan_in);
+    std::uniform_real_distribution<float> U(-lim, lim);
+    for (int r = 0; r < rows; ++r)
+      for (int c = 0; c < cols; ++c) P[off + r * cols + c] = U(rng);
+  };
+  fill(P_W1, HID, NIN, NIN);
+  for (int r = 0; r < HID; ++r) P[P_W1 + r * NIN + 7] = 0.0f;   // bias column
+  fill(P_W2, HID, HID, HID);
+  fill(P_W3, NOP, HID, HID);
+  for (int r = 0; r < NOP; ++r)
+    if (pad_out_row(r))
+      for (int c = 0; c < HID; ++c) P[P_W3 + r * HID + c] = 0.0f;
+  SG_CK(cudaMemcpy(net.P, P.data(), sizeof(float) * P.size(), cudaMemcpyHostToDevice), "cudaMemcpy(weights)");
+  SG_CK(cudaMemcpy(net.norm, norm, sizeof(float) * SG_NORM_FLOATS, cudaMemcpyHostToDevice), "cudaMemcpy(norm)");
+  SG_CK(cudaMemset(net.G, 0, sizeof(float) * G_N), "cudaMemset");
+  pack_kernel<<<64, 256>>>(net.P, net.ops);
+  SG_CK(cudaGetLastError(), "pack kernel");
+  SG_CK(cudaDeviceSynchronize(), "pack kernel");
+  net.adam_t = 0;
+  net.ready = true;
+  return 0;
+}
+
+// weights in natural shapes: W1 [128][8] (column 7 = bias of layer 1), W2 [128][128], b2 [128],
+// W3 [280][128], b3 [280]; norm float[SG_NORM_FLOATS]
+extern "C" int rrtmg_lw_gpu_surrogate_set(const float* w, const float* norm, char* errmsg, int32_t errmsg_len) {
+  smsg(errmsg, errmsg_len, "");
+  if (!w || !norm) { smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_set: NULL argument"); return 1; }
+  std::lock_guard<std::mutex> lk(net_mu);
+  int dev = 0, sms = 0;
+  if (dev_of_init(&dev, &sms)) { smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_set: no CUDA device"); return 1; }
+  SG_CK(set_attrs(), "kernel attributes (one CTA per SM)");
+  SG_CK(ensure_net(dev, sms), "cudaMalloc(network)");
+  std::vector<float> P(P_N * 3, 0.0f);
+  size_t k = 0;
+  for (int j = 0; j < HID * NIN + HID * HID + HID; ++j) P[j] = w[k++];
+  for (int r = 0; r < NOP; ++r) {
+    if (pad_out_row(r)) continue;
+    for (int c = 0; c < HID; ++c) P[P_W3 + r * HID + c] = w[k++];
+  }
+  for (int r = 0; r < NOP; ++r) {
+    if (pad_out_row(r)) continue;
+    P[P_B3 + r] = w[k++];
+  }
+  SG_CK(cudaMemcpy(net.P, P.data(), sizeof(float) * P.size(), cudaMemcpyHostToDevice), "cudaMemcpy(weights)");
+  SG_CK(cudaMemcpy(net.norm, norm, sizeof(float) * SG_NORM_FLOATS, cudaMemcpyHostToDevice), "cudaMemcpy(norm)");
+  pack_kernel<<<64, 256>>>(net.P, net.ops);
+  SG_CK(cudaGetLastError(), "pack kernel");
+  SG_CK(cudaDeviceSynchronize(), "pack kernel");
+  net.adam_t = 0;
+  net.ready = true;
+  return 0;
+}
+
+extern "C" int rrtmg_lw_gpu_surrogate_get(float* w, float* norm, char* errmsg, int32_t errmsg_len) {
+  smsg(errmsg, errmsg_len, "");
+  std::lock_guard<std::mutex> lk(net_mu);
+  if (check_ready(errmsg, errmsg_len)) return 1;
+  std::vector<float> P(P_N);
+  SG_CK(cudaMemcpy(P.data(), net.P, sizeof(float) * P_N, cudaMemcpyDeviceToHost), "cudaMemcpy(weights)");
+  if (w) {
+    size_t k = 0;
+    for (int j = 0; j < HID * NIN + HID * HID + HID; ++j) w[k++] = P[j];
+    for (int r = 0; r < NOP; ++r)
+      if (!pad_out_row(r))
+        for (int c = 0; c < HID; ++c) w[k++] = P[P_W3 + r * HID + c];
+    for (int r = 0; r < NOP; ++r)
+      if (!pad_out_row(r)) w[k++] = P[P_B3 + r];
+  }
+  if (norm) SG_CK(cudaMemcpy(norm, net.norm, sizeof(float) * SG_NORM_FLOATS, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  return 0;
+}
+
+extern "C" int rrtmg_lw_gpu_surrogate_forward(const float* feats, int64_t n, float* y, void* stream, char* errmsg,
+                                              int32_t errmsg_len) {
+  smsg(errmsg, errmsg_len, "");
+  std::lock_guard<std::mutex> lk(net_mu);
+  if (check_ready(errmsg, errmsg_len)) return 1;
+  if (n < 0 || (n > 0 && (!feats || !y))) { smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_forward: bad arguments"); return 1; }
+  if (n == 0) return 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  FwdArgs a = base_args();
+  a.nrows = n;
+  a.feats = feats;
+  a.y = y;
+  const long tiles = (n + 127) / 128;
+  SG_CK(cudaMemsetAsync(net.err, 0, sizeof(int), st), "cudaMemsetAsync");
+  mlp_fwd_kernel<MODE_FEATS><<<(int)std::min<long>(tiles, net.num_sms), FWD_THREADS, FWD_SMEM, st>>>(a);
+  SG_CK(cudaGetLastError(), "forward kernel launch");
+  int herr = 0;
+  SG_CK(cudaMemcpyAsync(&herr, net.err, sizeof(int), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  SG_CK(cudaStreamSynchronize(st), "forward kernel");
+  if (herr) { smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_forward: tensor-core wait timed out"); return 1; }
+  return 0;
+}
+
+// One forward + backward pass over the first `batch` samples (no update):
+// loss and the gradients in parameter order (float[54688], see the layout
+// comments) for gradient checks.
+extern "C" int rrtmg_lw_gpu_surrogate_grads(const float* feats, const float* targets, int32_t batch, float* grads,
+                                            float* loss, void* stream, char* errmsg, int32_t errmsg_len) {
+  smsg(errmsg, errmsg_len, "");
+  std::lock_guard<std::mutex> lk(net_mu);
+  if (check_ready(errmsg, errmsg_len)) return 1;
+  if (batch < 128 || batch % 128 || !feats || !targets) {
+    smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_grads: batch must be a positive multiple of 128");
+    return 1;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  SG_CK(ensure_batch(batch), "cudaMalloc(activations)");
+  SG_CK(cudaMemsetAsync(net.G, 0, sizeof(float) * G_N, st), "cudaMemsetAsync");
+  SG_CK(cudaMemsetAsync(net.err, 0, sizeof(int) + sizeof(float), st), "cudaMemsetAsync");
+  SG_CK(train_batch(feats, targets, batch, batch, 1, 0, 0, st), "training kernels launch");
+  float* dgr = nullptr;
+  SG_CK(cudaMallocAsync((void**)&dgr, sizeof(float) * P_N, st), "cudaMallocAsync");
+  grads_kernel<<<64, 256, 0, st>>>(net.G, dgr);
+  int herr[2] = {0, 0};
+  SG_CK(cudaMemcpyAsync(herr, net.err, sizeof(int) + sizeof(float), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  if (grads) SG_CK(cudaMemcpyAsync(grads, dgr, sizeof(float) * P_N, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  SG_CK(cudaFreeAsync(dgr, st), "cudaFreeAsync");
+  SG_CK(cudaStreamSynchronize(st), "training kernels");
+  SG_CK(cudaMemsetAsync(net.G, 0, sizeof(float) * G_N, st), "cudaMemsetAsync");
+  if (herr[0]) { smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_grads: tensor-core wait timed out"); return 1; }
+  if (loss) { float l; std::memcpy(&l, &herr[1], sizeof(float)); *loss = l / (float)((long)batch * SG_NOUT); }
+  return 0;
+}
+
+// Adam training on device-resident data: feats [n][8], targets [n][288]
+// (normalised, padded layout).  Each epoch visits floor(n / batch) batches
+// of an affine permutation of the samples.  loss_per_epoch (optional,
+// float[epochs]) receives the mean squared error of each epoch.
+extern "C" int rrtmg_lw_gpu_surrogate_train(const float* feats, const float* targets, int64_t n, int32_t epochs,
+                                            int32_t batch, float lr, float lr_final, uint64_t seed,
+                                            float* loss_per_epoch, void* stream, char* errmsg, int32_t errmsg_len) {
+  smsg(errmsg, errmsg_len, "");
+  std::lock_guard<std::mutex> lk(net_mu);
+  if (check_ready(errmsg, errmsg_len)) return 1;
+  if (batch < 128 || batch % 128 || n < batch || epochs < 1 || !feats || !targets) {
+    smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_train: need batch a multiple of 128, n >= batch, epochs >= 1");
+    return 1;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  SG_CK(ensure_batch(batch), "cudaMalloc(activations)");
+  SG_CK(cudaMemsetAsync(net.err, 0, sizeof(int), st), "cudaMemsetAsync");
+  std::mt19937_64 rng(seed);
+  const long steps = n / batch;
+  const long total = steps * (long)epochs;
+  long done = 0;
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  for (int ep = 0; ep < epochs; ++ep) {
+    SG_CK(cudaMemsetAsync(net.loss, 0, sizeof(float), st), "cudaMemsetAsync");
+    long pa;
+    do { pa = (long)(rng() % (uint64_t)n); } while (pa == 0 || std::gcd(pa, (long)n) != 1);
+    const long pb = (long)(rng() % (uint64_t)n);
+    for (long s = 0; s < steps; ++s, ++done) {
+      SG_CK(train_batch(feats, targets, n, batch, pa, pb, s * batch, st), "training kernels launch");
+      ++net.adam_t;
+      // cosine decay from lr to lr_final over the whole run
+      const double fr = (double)done / (double)std::max(1L, total - 1);
+      const float lr_t = (float)(lr_final + 0.5 * (lr - lr_final) * (1.0 + std::cos(3.14159265358979323846 * fr)));
+      const float c1 = 1.0f - std::pow(b1, (float)net.adam_t), c2 = 1.0f - std::pow(b2, (float)net.adam_t);
+      adam_kernel<<<64, 256, 0, st>>>(net.P, net.Madam, net.Vadam, net.G, net.ops, lr_t, b1, b2, c1, c2, eps);
+      SG_CK(cudaGetLastError(), "adam kernel launch");
+      SG_CK(cudaMemsetAsync(net.G, 0, sizeof(float) * G_N, st), "cudaMemsetAsync");
+    }
+    float l = 0.0f;
+    int herr = 0;
+    SG_CK(cudaMemcpyAsync(&l, net.loss, sizeof(float), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    SG_CK(cudaMemcpyAsync(&herr, net.err, sizeof(int), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    SG_CK(cudaStreamSynchronize(st), "training kernels");
+    if (herr) { smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_train: tensor-core wait timed out"); return 1; }
+    if (loss_per_epoch) loss_per_epoch[ep] = l / (float)(steps * batch * (long)SG_NOUT);
+  }
+  return 0;
+}
+
+// Layers of surrogate runs that fell outside the training envelope and were
+// recomputed with taumol, since the last reset; and the tensor-core error
+// flag of the last surrogate launches.
+extern "C" int rrtmg_lw_gpu_surrogate_stats(uint64_t* fallback_layers, int32_t* mma_error, int32_t reset) {
+  std::lock_guard<std::mutex> lk(net_mu);
+  if (!net.err) return 1;
+  int h[4] = {0, 0, 0, 0};
+  if (cudaMemcpy(h, net.err, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  if (fallback_layers) *fallback_layers = (uint64_t)(unsigned int)h[2];
+  if (mma_error) *mma_error = h[0];
+  if (reset && cudaMemset(net.err, 0, sizeof(h)) != cudaSuccess) return 1;
+  return 0;
+}

@@ -1,0 +1,141 @@
+// lw_umma.cuh -- thin wrappers over the sm_100a 5th-generation tensor-core
+// instructions (tcgen05.*) used by the learned gas-optics kernels.
+//
+// Conventions used by every caller:
+//   * cta_group::1, kind::f16 with BF16 A and B and an FP32 accumulator in
+//     tensor memory (TMEM); M = 128 (TMEM lane m = row m), N a multiple of 16
+//     up to 256.
+//   * Both operands are K-major (the contraction index is contiguous):
+//     D[m][n] = sum_k A[m][k] * B[n][k].
+//   * Shared-memory operands use the no-swizzle canonical layout: 8x8 BF16
+//     "core matrices" of 128 contiguous bytes (8 rows x 16 bytes); a tile of
+//     R rows x K columns stores core matrix (r/8, k/8) at byte
+//     ((r/8) * (K/8) + k/8) * 128.  Its descriptor has leading-dimension
+//     byte offset (between K-adjacent core matrices) 128 and stride byte
+//     offset (between 8-row groups) K/8 * 128.  One MMA consumes K = 16 (two
+//     core matrices), so K-step s starts 256 * s bytes into the tile.
+//   * One thread issues MMAs; completion is signalled through an mbarrier by
+//     tcgen05.commit.  Every wait is bounded: on time-out the caller records
+//     an error and skips the rest of its work (no spin without limit).
+#pragma once
+
+#include <cstdint>
+#include <cuda_bf16.h>
+
+namespace lw {
+namespace umma {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// byte offset of element (r, k) in a canonical no-swizzle K-major tile with K columns
+__host__ __device__ __forceinline__ uint32_t canon_off(int r, int k, int K) {
+  return (uint32_t)((((r >> 3) * (K >> 3) + (k >> 3)) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+// shared-memory matrix descriptor (no swizzle, sm100 descriptor version 1)
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1u << 46;
+  return d;
+}
+// descriptor of K-step s (16 columns) of a canonical tile with K columns at saddr
+__device__ __forceinline__ uint64_t tile_desc(uint32_t saddr, int K, int s) {
+  return sdesc(saddr + 256u * (uint32_t)s, 128u, (uint32_t)(K >> 3) * 128u);
+}
+
+// instruction descriptor: kind::f16, A = B = BF16, D = F32, both K-major
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {   // whole warp
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+               "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {   // whole warp
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {   // whole warp
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// D[tmem] (+)= A * B^T, one thread
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                    uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// arrive on mbar when every MMA issued so far by this thread has completed
+__device__ __forceinline__ void commit(uint64_t* mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// make this thread's generic-proxy shared-memory writes visible to the tensor core
+__device__ __forceinline__ void fence_smem_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* m, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* m, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(m)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for phase `parity` of mbar; false after ~max_iter polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity, uint32_t max_iter = 1u << 22) {
+  for (uint32_t it = 0; it < max_iter; ++it) {
+    if (mbar_try_wait(m, parity)) return true;
+    if (it > 64) __nanosleep(64);
+  }
+  return false;
+}
+
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// TMEM address of (lane 32*warp, column col) from the allocation base
+__device__ __forceinline__ uint32_t tmem_addr(uint32_t base, int warp, int col) {
+  return base + ((uint32_t)(32 * warp) << 16) + (uint32_t)col;
+}
+
+// store 8 consecutive BF16 values of row r, columns k..k+7 (k % 8 == 0) of a canonical tile
+__device__ __forceinline__ void st_canon8(unsigned char* tile, int r, int k, int K, const float* v) {
+  __nv_bfloat162 p[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) p[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+  *reinterpret_cast<uint4*>(tile + canon_off(r, k, K)) = *reinterpret_cast<uint4*>(p);
+}
+
+}  // namespace umma
+}  // namespace lw

@@ -210,6 +210,62 @@ int rrtmg_lw_gpu_autotune(const rrtmg_lw_run_args *blocks, int32_t nblocks,
                           int64_t sample_cols, rrtmg_lw_tuning *best,
                           float *best_ms, char *errmsg, int32_t errmsg_len);
 
+/* ---- Learned gas optics (no counterpart in the reference) -------------
+ * A BF16 MLP 8 -> 128 -> 128 -> 288 (SiLU) on the tensor cores replaces
+ * setcoef + taumol (radlw_main.F90:2151-2406, 3836-6840) for every layer
+ * whose features lie inside the training envelope; the gas-optics kernel
+ * recomputes the other layers with plain taumol.  Run it through
+ * rrtmg_lw_gpu_run_ex / _run_blocks with precision RRTMG_LW_SURROGATE (cloud
+ * optics, McICA and the transfer then run in FP32).
+ * Features per layer (float[8], internal order: row = column * nlay + layer,
+ * surface first): ln p[hPa], T[K], ln h2o vmr, ln o3 vmr, co2, ch4, n2o
+ * [ppmv], 1.  Outputs (float[288], normalised): [0,140) log(taug/coldry)
+ * for the 140 g-points, [144,284) Planck fractions, the rest padding.
+ * Normalisation, float[RRTMG_LW_SURROGATE_NORM]: input mean[8], std[8],
+ * envelope low[8], high[8], output mean[288], std[288].
+ * Weights, float[RRTMG_LW_SURROGATE_NPARAM]: W1[128][8] (column 7 = bias of
+ * layer 1), W2[128][128], b2[128], W3[280][128], b3[280]. */
+#define RRTMG_LW_SURROGATE_NORM 608
+#define RRTMG_LW_SURROGATE_NPARAM 53656
+#define RRTMG_LW_SURROGATE_NGRAD 54688   /* gradient export, padded output rows */
+
+/* Features and dry-air column amount (coldry of radlw_main.F90:835, in
+ * 1e20 molecules/cm^2) of every layer of one block, device pointers:
+ * feats[npts*nlay][8], coldry[npts*nlay] (may be NULL). */
+int rrtmg_lw_gpu_surrogate_features(const rrtmg_lw_run_args *args, float *feats,
+                                    float *coldry, void *stream, char *errmsg,
+                                    int32_t errmsg_len);
+/* Random initial weights (seeded) and the normalisation (host float[608]). */
+int rrtmg_lw_gpu_surrogate_init(const float *norm, uint64_t seed, char *errmsg,
+                                int32_t errmsg_len);
+/* Load / read trained weights and normalisation (host arrays). */
+int rrtmg_lw_gpu_surrogate_set(const float *weights, const float *norm,
+                               char *errmsg, int32_t errmsg_len);
+int rrtmg_lw_gpu_surrogate_get(float *weights, float *norm, char *errmsg,
+                               int32_t errmsg_len);
+/* Adam training on device data feats[n][8], targets[n][288] (normalised,
+ * padded), batch a multiple of 128, learning rate decaying from lr to
+ * lr_final (cosine); loss_per_epoch optional host float[epochs] (MSE). */
+int rrtmg_lw_gpu_surrogate_train(const float *feats, const float *targets,
+                                 int64_t n, int32_t epochs, int32_t batch,
+                                 float lr, float lr_final, uint64_t seed,
+                                 float *loss_per_epoch, void *stream,
+                                 char *errmsg, int32_t errmsg_len);
+/* Network outputs (normalised) for device features: y[n][288]. */
+int rrtmg_lw_gpu_surrogate_forward(const float *feats, int64_t n, float *y,
+                                   void *stream, char *errmsg,
+                                   int32_t errmsg_len);
+/* One forward + backward pass over the first `batch` samples without an
+ * update: host grads[RRTMG_LW_SURROGATE_NGRAD] in the padded parameter order
+ * (W1[128][8], W2[128][128], b2[128], W3[288][128], b3[288]) and the MSE. */
+int rrtmg_lw_gpu_surrogate_grads(const float *feats, const float *targets,
+                                 int32_t batch, float *grads, float *loss,
+                                 void *stream, char *errmsg, int32_t errmsg_len);
+/* Layers recomputed with taumol since the last reset, and the tensor-core
+ * wait-timeout flag of the surrogate kernels.  Returns 0 on success. */
+int rrtmg_lw_gpu_surrogate_stats(uint64_t *fallback_layers, int32_t *mma_error,
+                                 int32_t reset);
+
 /* Release device tables and per-thread workspaces (call once at exit). */
 void rrtmg_lw_gpu_finalize(void);
 
