@@ -96,6 +96,7 @@ struct FwdArgs {
   const float* targets; // [*][288] normalised targets
   long perm_a, perm_b, perm_n, perm_off;   // sample = (a * (perm_off + row) + b) mod n
   float loss_scale;     // 2 / (batch * 280)
+  int tau_weight;       // 1: weight optical-depth errors by 1 / (1 + 1.66 tau), coldry in feats[., 7]
   float* loss;          // += sum of squared errors
   bf16 *xt, *z1, *h1t, *z2, *h2t, *dy, *dyt;   // activations, see the trainer
   long ldt;             // leading dimension (batch) of the transposed arrays
@@ -108,7 +109,11 @@ struct FwdArgs {
   int nc;               // columns of this chunk
 };
 
-constexpr int FWD_THREADS = 128;
+// Thread layout: 4 warpgroups.  Thread tid serves tile row (tid & 127) -- the
+// TMEM lane its warp may read -- and column quarter q = tid >> 7 of every
+// stage, so four threads share the epilogue work of a row and 16 warps per SM
+// hide the load, TMEM and MMA latencies.
+constexpr int FWD_THREADS = 512;
 constexpr uint32_t SM_W1 = 0;                               // canon [128][16]
 constexpr uint32_t SM_W2 = SM_W1 + HID * KIN * 2;           // canon [128][128]
 constexpr uint32_t SM_W3 = SM_W2 + HID * HID * 2;           // canon [288][128]
@@ -117,7 +122,11 @@ constexpr uint32_t SM_H = SM_X + 128 * KIN * 2;             // canon [128][128]
 constexpr uint32_t SM_B2 = SM_H + 128 * HID * 2;            // f32 [128]
 constexpr uint32_t SM_B3 = SM_B2 + HID * 4;                 // f32 [288]
 constexpr uint32_t SM_NORM = SM_B3 + NOP * 4;               // f32 [608]
-constexpr uint32_t SM_BAR = (SM_NORM + SG_NORM_FLOATS * 4 + 15) & ~15u;
+constexpr uint32_t SM_AER = SM_NORM + SG_NORM_FLOATS * 4;   // f32 [2][16][128] aerosol tau of the tile's layers
+constexpr uint32_t SM_CD = SM_AER + 2 * NBANDS * 128 * 4;   // f32 [2][128] coldry of the tile's layers
+constexpr uint32_t SM_OSC = SM_CD + 2 * 128 * 4;            // f32 [288] output scale  (std)
+constexpr uint32_t SM_OSH = SM_OSC + NOP * 4;               // f32 [288] output shift (b3 * std + mean)
+constexpr uint32_t SM_BAR = (SM_OSH + NOP * 4 + 15) & ~15u;
 constexpr uint32_t FWD_SMEM = SM_BAR + 32;
 static_assert(FWD_SMEM > 116 * 1024, "forward kernel must hold its SM alone (512 TMEM columns)");
 static_assert(FWD_SMEM <= 227 * 1024, "forward kernel shared memory");
@@ -138,13 +147,73 @@ __device__ __forceinline__ void copy_rows_canon(unsigned char* dst, const bf16* 
   }
 }
 
+// TMEM column of network output j: outputs [0,144) sit at columns 256.., [144,288) at 0..
+__device__ __forceinline__ int out_col(int j) { return j < 144 ? 256 + j : j - 144; }
+
+// Where a tile row of MODE_LW lives: chunk column, layer, block, block column, input row
+struct LwRow {
+  int cc, t, i, r;
+  const Block* B;
+};
+__device__ __forceinline__ LwRow lw_row(const FwdArgs& a, long row) {
+  LwRow w;
+  const int nlay = a.f.nlay;
+  w.cc = (int)(row / nlay);
+  w.t = (int)(row - (long)w.cc * nlay);
+  const int c = a.sc.c0 + w.cc;
+  w.B = (a.nblocks == 1) ? &a.b0 : &a.blocks[find_block(a.blocks, a.nblocks, c)];
+  w.i = c - w.B->col0;
+  w.r = a.f.top_at_1 ? nlay - w.t - 1 : w.t;
+  return w;
+}
+
+// MODE_LW output stage of one quarter: g-points [GA, GB) (whole bands), their
+// optical depths and their band-normalised Planck fractions.  Ranges and bands
+// are compile-time, so the loops carry no per-element tests.
+template <int GA, int GB>
+__device__ __forceinline__ void lw_out_quarter(uint32_t tb, int wl, bool live, float* tcol, float* fcol, size_t nlp,
+                                               const float* osc, const float* osh, const float* aer_row, float cd) {
+  constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
+  float v[NCH * 16];
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, 256 + C0 + 16 * c), v + 16 * c);
+  if (live) {
+#pragma unroll
+    for (int g = GA; g < GB; ++g) {
+      const float ly = fmaf(v[g - C0], osc[g], osh[g]);
+      __stcs(tcol + (size_t)g * nlp, fmaf(__expf(ly), cd, aer_row[band_of_g(g) * 128]));
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, C0 + 16 * c), v + 16 * c);
+  if (live) {
+    float bsum[NBANDS];
+#pragma unroll
+    for (int b = 0; b < NBANDS; ++b) bsum[b] = 0.0f;
+#pragma unroll
+    for (int g = GA; g < GB; ++g) {
+      const float fr = __saturatef(fmaf(v[g - C0], osc[144 + g], osh[144 + g]));
+      v[g - C0] = fr;
+      bsum[band_of_g(g)] += fr;
+    }
+#pragma unroll
+    for (int b = 0; b < NBANDS; ++b) bsum[b] = bsum[b] > 0.0f ? 1.0f / bsum[b] : 1.0f;
+#pragma unroll
+    for (int g = GA; g < GB; ++g) __stcs(fcol + (size_t)g * nlp, v[g - C0] * bsum[band_of_g(g)]);
+  }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, wl = warp & 3, q = tid >> 7, tr = tid & 127;
   float* sb2 = reinterpret_cast<float*>(sm + SM_B2);
   float* sb3 = reinterpret_cast<float*>(sm + SM_B3);
   float* snorm = reinterpret_cast<float*>(sm + SM_NORM);
+  float* saer0 = reinterpret_cast<float*>(sm + SM_AER);
+  float* scd0 = reinterpret_cast<float*>(sm + SM_CD);
+  float* osc = reinterpret_cast<float*>(sm + SM_OSC);
+  float* osh = reinterpret_cast<float*>(sm + SM_OSH);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + SM_BAR);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SM_BAR + 8);
   int* sfail = reinterpret_cast<int*>(sm + SM_BAR + 12);
@@ -155,6 +224,11 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
   for (int j = tid; j < HID; j += FWD_THREADS) sb2[j] = a.params[P_B2 + j];
   for (int j = tid; j < NOP; j += FWD_THREADS) sb3[j] = a.params[P_B3 + j];
   for (int j = tid; j < SG_NORM_FLOATS; j += FWD_THREADS) snorm[j] = a.norm[j];
+  for (int j = tid; j < NOP; j += FWD_THREADS) {
+    const float sd = a.norm[SG_OUT_STD + j];
+    osc[j] = sd;
+    osh[j] = fmaf(a.params[P_B3 + j], sd, a.norm[SG_OUT_MEAN + j]);
+  }
   if (warp == 0) {
     umma::tmem_alloc(tslot, 512);
     umma::tmem_relinquish();
@@ -173,7 +247,6 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
   uint32_t phase = 0;
   const long ntiles = (a.nrows + 127) / 128;
 
-  // wait for the MMAs committed last; on time-out every thread leaves the tile loop
   bool failed = false;   // uniform across the CTA
   auto wait_mma = [&]() -> bool {
     const bool ok = umma::mbar_wait(mbar, phase);
@@ -186,58 +259,65 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
     }
     return true;
   };
-
-  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long row = tile * 128 + tid;
-    const bool live = row < a.nrows;
-    // ---------------- layer inputs ----------------
-    float x[KIN];
-#pragma unroll
-    for (int j = 0; j < KIN; ++j) x[j] = 0.0f;
-    long sample = row;
-    double coldry = 0.0;
-    int lw_cc = 0, lw_t = 0;
-    const Block* LB = nullptr;
-    int lw_i = 0, lw_r = 0;
-    if (live) {
-      float raw[NIN];
-      if (MODE == MODE_LW) {
-        const int nlay = a.f.nlay, nlp1 = nlay + 1;
-        lw_cc = (int)(row / nlay);
-        lw_t = (int)(row - (long)lw_cc * nlay);
-        const int c = a.sc.c0 + lw_cc;
-        LB = (a.nblocks == 1) ? &a.b0 : &a.blocks[find_block(a.blocks, a.nblocks, c)];
-        lw_i = c - LB->col0;
-        lw_r = a.f.top_at_1 ? nlp1 - (lw_t + 1) - 1 : lw_t;
-        const size_t o = (size_t)lw_i + (size_t)LB->ld * lw_r;
-        const double pavel = LB->in[F_PLYR][o], tavel = LB->in[F_TLYR][o], q = LB->in[F_QLYR][o];
-        const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
-        const double h2ovmr = fmax(0.0, q * amdw / (1.0 - q));
-        const double o3vmr = fmax(0.0, LB->in[F_OLYR][o] * amdo3);
-        const double tem0 = (1.0 - h2ovmr) * 28.9644 + h2ovmr * 18.0154;
-        coldry = (1.0e-20 * 1.0e3 * 6.0221415e23) * LB->in[F_DELPIN][o] / (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr));
-        layer_features(pavel, tavel, h2ovmr, o3vmr, LB->in[F_CO2][o], LB->in[F_CH4][o], LB->in[F_N2O][o], raw);
-      } else {
-        if (MODE == MODE_TRAIN) sample = (long)(((unsigned long long)a.perm_a * (unsigned long long)(a.perm_off + row) +
-                                                 (unsigned long long)a.perm_b) % (unsigned long long)a.perm_n);
-        const float4* src = reinterpret_cast<const float4*>(a.feats + sample * NIN);
-        float4 u = __ldg(src), w = __ldg(src + 1);
-        raw[0] = u.x; raw[1] = u.y; raw[2] = u.z; raw[3] = u.w; raw[4] = w.x; raw[5] = w.y; raw[6] = w.z;
-        raw[7] = 1.0f;
-      }
-#pragma unroll
-      for (int j = 0; j < 7; ++j) x[j] = (raw[j] - snorm[SG_IN_MEAN + j]) / snorm[SG_IN_STD + j];
-      x[7] = 1.0f;
-    }
-    umma::st_canon8(sm + SM_X, tid, 0, KIN, x);
-    umma::st_canon8(sm + SM_X, tid, 8, KIN, x + 8);
-    if (MODE == MODE_TRAIN && live) {
-#pragma unroll
-      for (int j = 0; j < 8; ++j) a.xt[(size_t)j * a.ldt + row] = __float2bfloat16_rn(x[j]);
-    }
+  auto sync_for_mma = [&]() {
     umma::fence_smem_async();
     umma::fence_before_sync();
     __syncthreads();
+  };
+
+  int parity = 0;   // double buffer of the per-tile aerosol / coldry rows
+  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, parity ^= 1) {
+    const long row = tile * 128 + tr;
+    const bool live = row < a.nrows;
+    float* saer = saer0 + parity * NBANDS * 128;
+    float* scd = scd0 + parity * 128;
+    long sample = row;
+    if (MODE == MODE_TRAIN && live)
+      sample = (long)(((unsigned long long)a.perm_a * (unsigned long long)(a.perm_off + row) +
+                       (unsigned long long)a.perm_b) % (unsigned long long)a.perm_n);
+    // ---------------- layer inputs (quarter 0: features; MODE_LW quarters 1-3: aerosol) ----
+    if (q == 0) {
+      float x[KIN];
+#pragma unroll
+      for (int j = 0; j < KIN; ++j) x[j] = 0.0f;
+      if (live) {
+        float raw[NIN];
+        if (MODE == MODE_LW) {
+          const LwRow w = lw_row(a, row);
+          const size_t o = (size_t)w.i + (size_t)w.B->ld * w.r;
+          const double pavel = w.B->in[F_PLYR][o], tavel = w.B->in[F_TLYR][o], qv = w.B->in[F_QLYR][o];
+          const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
+          const double h2ovmr = fmax(0.0, qv * amdw / (1.0 - qv));
+          const double o3vmr = fmax(0.0, w.B->in[F_OLYR][o] * amdo3);
+          const double tem0 = (1.0 - h2ovmr) * 28.9644 + h2ovmr * 18.0154;
+          scd[tr] = (float)((1.0e-20 * 1.0e3 * 6.0221415e23) * w.B->in[F_DELPIN][o] /
+                            (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr)));
+          layer_features(pavel, tavel, h2ovmr, o3vmr, w.B->in[F_CO2][o], w.B->in[F_CH4][o], w.B->in[F_N2O][o], raw);
+        } else {
+          const float4* src = reinterpret_cast<const float4*>(a.feats + sample * NIN);
+          const float4 u = __ldg(src), v = __ldg(src + 1);
+          raw[0] = u.x; raw[1] = u.y; raw[2] = u.z; raw[3] = u.w; raw[4] = v.x; raw[5] = v.y; raw[6] = v.z;
+        }
+#pragma unroll
+        for (int j = 0; j < 7; ++j) x[j] = (raw[j] - snorm[SG_IN_MEAN + j]) / snorm[SG_IN_STD + j];
+        x[7] = 1.0f;
+      }
+      umma::st_canon8(sm + SM_X, tr, 0, KIN, x);
+      umma::st_canon8(sm + SM_X, tr, 8, KIN, x + 8);
+      if (MODE == MODE_TRAIN && live) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a.xt[(size_t)j * a.ldt + row] = __float2bfloat16_rn(x[j]);
+      }
+    } else if (MODE == MODE_LW && live) {
+      const LwRow w = lw_row(a, row);
+      const size_t ldl = (size_t)w.B->ld;
+      const int b0 = q == 1 ? 0 : q == 2 ? 6 : 11, b1 = q == 1 ? 6 : q == 2 ? 11 : 16;
+      for (int b = b0; b < b1; ++b) {
+        const size_t ab = (size_t)w.i + ldl * ((size_t)w.r + (size_t)a.f.nlay * b);
+        saer[b * 128 + tr] = (float)(w.B->in[F_AERAOD][ab] * (1.0 - w.B->in[F_AERSSA][ab]));
+      }
+    }
+    sync_for_mma();
     if (tid == 0) {
       umma::fence_after_sync();
       umma::mma(tb, umma::tile_desc(sbase + SM_X, KIN, 0), umma::tile_desc(sbase + SM_W1, KIN, 0), ID128, 0u);
@@ -245,22 +325,23 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
     }
     if (!wait_mma()) break;
 
-    // ---------------- hidden layers ----------------
+    // ---------------- hidden layers: quarter q owns hidden units [32q, 32q+32) ----------------
 #pragma unroll 1
     for (int layer = 0; layer < 2; ++layer) {
-      const uint32_t dcol = layer == 0 ? 0u : 128u;
-#pragma unroll 1
-      for (int c0 = 0; c0 < HID; c0 += 16) {
+      const int dcol = layer == 0 ? 0 : 128;
+#pragma unroll
+      for (int h16 = 0; h16 < 2; ++h16) {
+        const int c0 = 32 * q + 16 * h16;
         float v[16], h[16];
-        umma::tmem_ld16(umma::tmem_addr(tb, warp, dcol + c0), v);
+        umma::tmem_ld16(umma::tmem_addr(tb, wl, dcol + c0), v);
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const float z = v[j] + (layer == 1 ? sb2[c0 + j] : 0.0f);
           v[j] = z;
           h[j] = silu(z);
         }
-        umma::st_canon8(sm + SM_H, tid, c0, HID, h);
-        umma::st_canon8(sm + SM_H, tid, c0 + 8, HID, h + 8);
+        umma::st_canon8(sm + SM_H, tr, c0, HID, h);
+        umma::st_canon8(sm + SM_H, tr, c0 + 8, HID, h + 8);
         if (MODE == MODE_TRAIN && live) {
           bf16* z = (layer == 0 ? a.z1 : a.z2) + (size_t)row * HID + c0;
           __nv_bfloat162 zp[8];
@@ -273,9 +354,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
           for (int j = 0; j < 16; ++j) ht[(size_t)(c0 + j) * a.ldt + row] = __float2bfloat16_rn(h[j]);
         }
       }
-      umma::fence_smem_async();
-      umma::fence_before_sync();
-      __syncthreads();
+      sync_for_mma();
       if (tid == 0) {
         umma::fence_after_sync();
         if (layer == 0) {
@@ -300,125 +379,84 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
     if (failed) break;
 
     // ---------------- output epilogue ----------------
-    // outputs [0,144) in TMEM columns 256.., outputs [144,288) in columns 0..
-    auto out_addr = [&](int j) { return j < 144 ? umma::tmem_addr(tb, warp, 256 + j) : umma::tmem_addr(tb, warp, j - 144); };
-    if (MODE == MODE_FEATS) {
-#pragma unroll 1
-      for (int j0 = 0; j0 < NOP; j0 += 16) {
-        float v[16];
-        umma::tmem_ld16(out_addr(j0), v);
-        if (live) {
-          float4* dst = reinterpret_cast<float4*>(a.y + (size_t)row * NOP + j0);
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            dst[q] = make_float4(v[4 * q] + sb3[j0 + 4 * q], v[4 * q + 1] + sb3[j0 + 4 * q + 1],
-                                 v[4 * q + 2] + sb3[j0 + 4 * q + 2], v[4 * q + 3] + sb3[j0 + 4 * q + 3]);
-        }
-      }
-    } else if (MODE == MODE_TRAIN) {
+    if (MODE == MODE_FEATS || MODE == MODE_TRAIN) {
+      // quarter q owns outputs [72q, 72q+72) (8-aligned; 16-column TMEM chunks never straddle 144)
+      const int ja = 72 * q, jb = ja + 72;
       float sse = 0.0f;
+      const float coldry_s = (MODE == MODE_TRAIN && a.tau_weight && q < 2 && live) ? __ldg(a.feats + sample * NIN + 7) : 0.0f;
 #pragma unroll 1
-      for (int j0 = 0; j0 < NOP; j0 += 16) {
-        float v[16], d[16];
-        umma::tmem_ld16(out_addr(j0), v);
-        if (live) {
-          const float4* tg = reinterpret_cast<const float4*>(a.targets + (size_t)sample * NOP + j0);
+      for (int j0 = ja & ~15; j0 < jb; j0 += 16) {
+        float v[16];
+        umma::tmem_ld16(umma::tmem_addr(tb, wl, out_col(j0)), v);
+        if (!live) continue;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            float4 t4 = __ldg(tg + q);
-            float tt[4] = {t4.x, t4.y, t4.z, t4.w};
+        for (int g8 = 0; g8 < 2; ++g8) {
+          const int jj = j0 + 8 * g8;
+          if (jj < ja || jj >= jb) continue;
+          float o[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int j = j0 + 4 * q + u;
-              const float e = pad_out_row(j) ? 0.0f : v[4 * q + u] + sb3[j] - tt[u];
-              sse += e * e;
-              d[4 * q + u] = e * a.loss_scale;
+          for (int u = 0; u < 8; ++u) o[u] = v[8 * g8 + u] + sb3[jj + u];
+          if (MODE == MODE_FEATS) {
+            float4* dst = reinterpret_cast<float4*>(a.y + (size_t)row * NOP + jj);
+            dst[0] = make_float4(o[0], o[1], o[2], o[3]);
+            dst[1] = make_float4(o[4], o[5], o[6], o[7]);
+          } else {
+            const float4* tg = reinterpret_cast<const float4*>(a.targets + (size_t)sample * NOP + jj);
+            const float4 t0 = __ldg(tg), t1 = __ldg(tg + 1);
+            const float tt[8] = {t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w};
+            float d[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const int j = jj + u;
+              float wgt = 1.0f;
+              if (a.tau_weight && j < 140) {
+                // the layer's diffuse optical depth from the target: thin and moderate
+                // layers set the fluxes, errors of opaque ones hardly matter
+                const float tau = 1.66f * __expf(tt[u] * snorm[SG_OUT_STD + j] + snorm[SG_OUT_MEAN + j]) * coldry_s;
+                wgt = 1.0f / (1.0f + tau);
+              }
+              const float e = pad_out_row(j) ? 0.0f : o[u] - tt[u];
+              sse += wgt * e * e;
+              d[u] = wgt * e * a.loss_scale;
             }
+            __nv_bfloat162 dp[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) dp[u] = __floats2bfloat162_rn(d[2 * u], d[2 * u + 1]);
+            *reinterpret_cast<uint4*>(a.dy + (size_t)row * NOP + jj) = *reinterpret_cast<uint4*>(dp);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) a.dyt[(size_t)(jj + u) * a.ldt + row] = __float2bfloat16_rn(d[u]);
           }
-          __nv_bfloat162 dp[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) dp[u] = __floats2bfloat162_rn(d[2 * u], d[2 * u + 1]);
-          uint4* dst = reinterpret_cast<uint4*>(a.dy + (size_t)row * NOP + j0);
-          dst[0] = reinterpret_cast<uint4*>(dp)[0];
-          dst[1] = reinterpret_cast<uint4*>(dp)[1];
-#pragma unroll
-          for (int u = 0; u < 16; ++u) a.dyt[(size_t)(j0 + u) * a.ldt + row] = __float2bfloat16_rn(d[u]);
         }
       }
+      if (MODE == MODE_TRAIN) {
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) sse += __shfl_xor_sync(0xffffffffu, sse, o);
-      if ((tid & 31) == 0) atomicAdd(a.loss, sse);
+        for (int o = 16; o > 0; o >>= 1) sse += __shfl_xor_sync(0xffffffffu, sse, o);
+        if ((tid & 31) == 0) atomicAdd(a.loss, sse);
+      }
     } else {   // MODE_LW
-      // pass 1: per-band sums of the Planck fractions
-      float bsum[NBANDS];
-#pragma unroll
-      for (int b = 0; b < NBANDS; ++b) bsum[b] = 0.0f;
-#pragma unroll 1
-      for (int j0 = 144; j0 < 284 + 4; j0 += 16) {
-        float v[16];
-        umma::tmem_ld16(out_addr(j0), v);
-#pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const int j = j0 + u;
-          if (j < 284) {
-            const float fr = fminf(1.0f, fmaxf(0.0f, (v[u] + sb3[j]) * snorm[SG_OUT_STD + j] + snorm[SG_OUT_MEAN + j]));
-            bsum[band_of_g(j - 144)] += fr;
-          }
-        }
-      }
-      // scratch pitch NLP = 32 V padded layers of the column kernels
-      const size_t nlp = (size_t)a.f.nlay <= 63 ? 64 : (size_t)a.f.nlay <= 127 ? 128 : 256;
-      float* tcol = a.sc.tau + (size_t)lw_cc * NGPT * nlp + lw_t;
-      float* fcol = a.sc.frac + (size_t)lw_cc * NGPT * nlp + lw_t;
-      float aer[NBANDS];
+      // quarters own whole bands: g-points [0,38), [38,68), [68,108), [108,140)
+      const size_t nlp = (size_t)a.f.nlay <= 63 ? 64 : (size_t)a.f.nlay <= 127 ? 128 : 256;   // 32 V
+      int cc = 0, t = 0;
       if (live) {
-        const size_t ldl = (size_t)LB->ld;
-#pragma unroll
-        for (int b = 0; b < NBANDS; ++b) {
-          const size_t ab = (size_t)lw_i + ldl * ((size_t)lw_r + (size_t)a.f.nlay * b);
-          aer[b] = (float)(LB->in[F_AERAOD][ab] * (1.0 - LB->in[F_AERSSA][ab]));
-        }
+        cc = (int)(row / a.f.nlay);
+        t = (int)(row - (long)cc * a.f.nlay);
       }
-      const float cd = (float)coldry;
-      // pass 2: tau, then normalised fractions
-#pragma unroll 1
-      for (int j0 = 0; j0 < 144; j0 += 16) {
-        float v[16];
-        umma::tmem_ld16(out_addr(j0), v);
-        if (live) {
-#pragma unroll
-          for (int u = 0; u < 16; ++u) {
-            const int g = j0 + u;
-            if (g < NGPT) {
-              const float ly = (v[u] + sb3[g]) * snorm[SG_OUT_STD + g] + snorm[SG_OUT_MEAN + g];
-              __stcs(tcol + (size_t)g * nlp, __expf(ly) * cd + aer[band_of_g(g)]);
-            }
-          }
-        }
-      }
-#pragma unroll 1
-      for (int j0 = 144; j0 < 288; j0 += 16) {
-        float v[16];
-        umma::tmem_ld16(out_addr(j0), v);
-        if (live) {
-#pragma unroll
-          for (int u = 0; u < 16; ++u) {
-            const int j = j0 + u;
-            if (j < 284) {
-              const int g = j - 144;
-              const float fr = fminf(1.0f, fmaxf(0.0f, (v[u] + sb3[j]) * snorm[SG_OUT_STD + j] + snorm[SG_OUT_MEAN + j]));
-              const float s = bsum[band_of_g(g)];
-              __stcs(fcol + (size_t)g * nlp, s > 0.0f ? fr / s : fr);
-            }
-          }
-        }
-      }
+      float* tcol = a.sc.tau + (size_t)cc * NGPT * nlp + t;
+      float* fcol = a.sc.frac + (size_t)cc * NGPT * nlp + t;
+      const float cd = scd[tr];
+      const float* ar = saer + tr;
+      if (q == 0) lw_out_quarter<0, 38>(tb, wl, live, tcol, fcol, nlp, osc, osh, ar, cd);
+      else if (q == 1) lw_out_quarter<38, 68>(tb, wl, live, tcol, fcol, nlp, osc, osh, ar, cd);
+      else if (q == 2) lw_out_quarter<68, 108>(tb, wl, live, tcol, fcol, nlp, osc, osh, ar, cd);
+      else lw_out_quarter<108, 140>(tb, wl, live, tcol, fcol, nlp, osc, osh, ar, cd);
     }
+    // The next tile's first barrier orders these TMEM reads before MMA1 overwrites
+    // the accumulators, and its per-tile rows use the other buffer.
     umma::fence_before_sync();
-    __syncthreads();
   }
   // leave: every MMA this CTA issued has completed (or the wait timed out and
   // the error is recorded); release tensor memory
+  if (failed) umma::mbar_wait(mbar, phase ^ 1u, 1u << 20);   // one more bounded wait for the MMA in flight
   umma::fence_before_sync();
   __syncthreads();
   if (tid == 0 && *sfail && a.err) atomicCAS(a.err, 0, 1);
@@ -746,8 +784,9 @@ cudaError_t launch_gemm(int epi, const GemmArgs& g, int ksplit, cudaStream_t st)
 
 // forward (train mode) + backward of one batch: gradients accumulate in net.G
 cudaError_t train_batch(const float* feats, const float* targets, long nsamp, long batch, long pa, long pb,
-                        long off, cudaStream_t st) {
+                        long off, int tau_weight, cudaStream_t st) {
   FwdArgs a = base_args();
+  a.tau_weight = tau_weight;
   a.nrows = batch;
   a.feats = feats;
   a.targets = targets;
@@ -995,7 +1034,7 @@ extern "C" int rrtmg_lw_gpu_surrogate_grads(const float* feats, const float* tar
   SG_CK(ensure_batch(batch), "cudaMalloc(activations)");
   SG_CK(cudaMemsetAsync(net.G, 0, sizeof(float) * G_N, st), "cudaMemsetAsync");
   SG_CK(cudaMemsetAsync(net.err, 0, sizeof(int) + sizeof(float), st), "cudaMemsetAsync");
-  SG_CK(train_batch(feats, targets, batch, batch, 1, 0, 0, st), "training kernels launch");
+  SG_CK(train_batch(feats, targets, batch, batch, 1, 0, 0, 0, st), "training kernels launch");
   float* dgr = nullptr;
   SG_CK(cudaMallocAsync((void**)&dgr, sizeof(float) * P_N, st), "cudaMallocAsync");
   grads_kernel<<<64, 256, 0, st>>>(net.G, dgr);
@@ -1011,11 +1050,12 @@ extern "C" int rrtmg_lw_gpu_surrogate_grads(const float* feats, const float* tar
 }
 
 // Adam training on device-resident data: feats [n][8], targets [n][288]
-// (normalised, padded layout).  Each epoch visits floor(n / batch) batches
+// (normalised, padded layout).  flags bit 0: weight each optical-depth error
+// by 1 / (1 + 1.66 tau) of its target, with the layer's coldry in feats[., 7].  Each epoch visits floor(n / batch) batches
 // of an affine permutation of the samples.  loss_per_epoch (optional,
 // float[epochs]) receives the mean squared error of each epoch.
 extern "C" int rrtmg_lw_gpu_surrogate_train(const float* feats, const float* targets, int64_t n, int32_t epochs,
-                                            int32_t batch, float lr, float lr_final, uint64_t seed,
+                                            int32_t batch, float lr, float lr_final, uint64_t seed, int32_t flags,
                                             float* loss_per_epoch, void* stream, char* errmsg, int32_t errmsg_len) {
   smsg(errmsg, errmsg_len, "");
   std::lock_guard<std::mutex> lk(net_mu);
@@ -1038,7 +1078,7 @@ extern "C" int rrtmg_lw_gpu_surrogate_train(const float* feats, const float* tar
     do { pa = (long)(rng() % (uint64_t)n); } while (pa == 0 || std::gcd(pa, (long)n) != 1);
     const long pb = (long)(rng() % (uint64_t)n);
     for (long s = 0; s < steps; ++s, ++done) {
-      SG_CK(train_batch(feats, targets, n, batch, pa, pb, s * batch, st), "training kernels launch");
+      SG_CK(train_batch(feats, targets, n, batch, pa, pb, s * batch, flags & 1, st), "training kernels launch");
       ++net.adam_t;
       // cosine decay from lr to lr_final over the whole run
       const double fr = (double)done / (double)std::max(1L, total - 1);

@@ -76,12 +76,26 @@ def _is_device(x):
         return False
 
 
+def torch_stream(stream, x):
+    """The CUDA stream to run on: `stream` if given, else torch's current
+    stream of device tensor `x` (so library work is ordered after the torch
+    work that produced its inputs), else None (host data)."""
+    if stream is not None:
+        return stream
+    if _is_device(x):
+        import torch
+        h = torch.cuda.current_stream(x.device).cuda_stream
+        return h or None
+    return None
+
+
 def run_profile(prof: dict, out: dict, *, precision="fp64", flags=None, stream=None, sync=True):
     """rrtmg_lw_run over a profile dict (field name -> array) into ``out``.
     Returns (errmsg, errflg) like the Fortran routine."""
     keep = []
     a = abi.make_run_args(prof, out, flags=flags, keep=keep)
     device = _is_device(prof["plyr"])
+    stream = torch_stream(stream, prof["plyr"])
     x = abi.ExecArgs(precision=PRECISIONS[precision] if isinstance(precision, str) else precision,
                      memory=abi.DEVICE if device else abi.HOST,
                      stream=None if stream is None else C.c_void_p(stream), sync=int(sync))
@@ -122,6 +136,7 @@ def mcica_bits(cldf, seed, iovr=1, stream=None):
     import torch
     nlay, npts = cldf.shape
     nw = (nlay + 31) // 32
+    stream = torch_stream(stream, cldf)
     bits = torch.zeros((npts, abi.NGPT, nw), dtype=torch.int32, device=cldf.device)
     msg = C.create_string_buffer(512)
     rc = lib().rrtmg_lw_gpu_mcica(npts, nlay, npts, iovr, C.c_void_p(seed.data_ptr()),
@@ -142,6 +157,7 @@ def gas_optics(prof: dict, precision="fp64", stream=None):
     fracs = torch.empty_like(taug)
     keep = []
     a = abi.make_run_args(prof, {}, keep=keep)
+    stream = torch_stream(stream, prof["plyr"])
     msg = C.create_string_buffer(512)
     rc = lib().rrtmg_lw_gpu_gas_optics(C.byref(a), PRECISIONS[precision], C.c_void_p(taug.data_ptr()),
                                        C.c_void_p(fracs.data_ptr()), stream, msg, 512)
@@ -195,6 +211,7 @@ def run_blocks(prof: dict, out: dict, sizes, *, precision="fp64", tuning=None, s
     abi.Tuning or dict (rt_warps, gas_per_sm, chunk_cols, use_graph).
     Returns (errmsg, errflg)."""
     arr, keep = block_args(prof, out, sizes)
+    stream = torch_stream(stream, prof["plyr"])
     x = abi.ExecArgs(precision=PRECISIONS[precision] if isinstance(precision, str) else precision,
                      memory=abi.DEVICE, stream=None if stream is None else C.c_void_p(stream), sync=int(sync))
     if kernel_ms is not None:
@@ -209,6 +226,7 @@ def autotune(prof: dict, out: dict, sizes, *, precision="fp32", sample_cols=0, s
     """Autotune the launch shape on the physics blocks of ``sizes`` columns;
     returns (tuning dict, ms per call)."""
     arr, keep = block_args(prof, out, sizes)
+    stream = torch_stream(stream, prof["plyr"])
     best = abi.Tuning()
     ms = C.c_float(0.0)
     msg = C.create_string_buffer(512)

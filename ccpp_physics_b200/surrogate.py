@@ -29,6 +29,11 @@ NOUTP = 288
 NGPT = 140
 TAU = slice(0, 140)
 FRAC = slice(144, 284)
+# Floor of the log(taug/coldry) targets: below it a layer's optical depth
+# (coldry is ~200 per hPa of layer thickness) is < 1e-8 and irrelevant, while
+# exact zeros (bands without an absorber above laytrop) would otherwise sit
+# at log(tiny) and dominate the output scaling of their g-points.
+LOG_TAU_FLOOR = -25.0
 
 WEIGHTS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "lw_surrogate_weights.npz")
 
@@ -43,8 +48,8 @@ def _lib():
         L.rrtmg_lw_gpu_surrogate_set.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int32]
         L.rrtmg_lw_gpu_surrogate_get.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int32]
         L.rrtmg_lw_gpu_surrogate_train.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32,
-                                                   C.c_float, C.c_float, C.c_uint64, C.c_void_p, C.c_void_p,
-                                                   C.c_char_p, C.c_int32]
+                                                   C.c_float, C.c_float, C.c_uint64, C.c_int32, C.c_void_p,
+                                                   C.c_void_p, C.c_char_p, C.c_int32]
         L.rrtmg_lw_gpu_surrogate_forward.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_char_p,
                                                      C.c_int32]
         L.rrtmg_lw_gpu_surrogate_grads.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
@@ -58,6 +63,11 @@ def _check(rc, msg):
     if rc:
         from .rrtmg_lw import RRTMGLWError
         raise RRTMGLWError(msg.value.decode())
+
+
+def _stream(stream, x):
+    from .rrtmg_lw import torch_stream
+    return torch_stream(stream, x)
 
 
 def _np_ptr(a):
@@ -75,6 +85,7 @@ def features(prof: dict, stream=None):
     coldry = torch.empty((n,), dtype=torch.float32, device=dev)
     keep = []
     a = abi.make_run_args(prof, {}, keep=keep)
+    stream = _stream(stream, prof["plyr"])
     msg = C.create_string_buffer(512)
     rc = _lib().rrtmg_lw_gpu_surrogate_features(C.byref(a), C.c_void_p(feats.data_ptr()),
                                                 C.c_void_p(coldry.data_ptr()), stream, msg, 512)
@@ -89,7 +100,8 @@ def targets_of(taug, fracs, coldry):
     n = coldry.numel()
     t = torch.zeros((n, NOUTP), dtype=torch.float32, device=coldry.device)
     tg = taug.reshape(n, NGPT)
-    t[:, TAU] = torch.log(torch.clamp(tg / coldry.double()[:, None], min=1e-30)).float()
+    t[:, TAU] = torch.clamp(torch.log(torch.clamp(tg / coldry.double()[:, None], min=1e-300)),
+                            min=LOG_TAU_FLOOR).float()
     t[:, FRAC] = fracs.reshape(n, NGPT).float()
     return t
 
@@ -97,8 +109,8 @@ def targets_of(taug, fracs, coldry):
 def make_dataset(nsamples: int, *, seed: int = 101, nlay: int = 127, chunk_cols: int = 8192, device="cuda"):
     """Training set from the synthetic profile generator (clear and cloudy
     columns alike: gas optics does not see clouds).  Returns feats [n, 8]
-    and raw targets [n, 288] (float32 CUDA tensors), n = whole columns
-    covering nsamples layers."""
+    (slot 7 holds the layer's coldry) and raw targets [n, 288] (float32 CUDA
+    tensors), n = whole columns covering nsamples layers."""
     import torch
     from . import rrtmg_lw as lw
     ncols = -(-nsamples // nlay)
@@ -110,6 +122,7 @@ def make_dataset(nsamples: int, *, seed: int = 101, nlay: int = 127, chunk_cols:
         f, cd = features(prof)
         taug, fracs = lw.gas_optics(prof, precision="fp64")
         r0, r1 = c0 * nlay, (c0 + nc) * nlay
+        f[:, 7] = cd          # the network ignores slot 7 (its bias input is a constant 1); training weights use it
         feats[r0:r1] = f
         targ[r0:r1] = targets_of(taug, fracs, cd)
         del prof, taug, fracs
@@ -176,12 +189,16 @@ def get_weights():
     return w, n
 
 
-def train(feats, ytarg, *, epochs=4, batch=8192, lr=2e-3, lr_final=1e-5, seed=7, stream=None):
-    """Adam training in the library; returns the per-epoch MSE."""
+def train(feats, ytarg, *, epochs=4, batch=8192, lr=2e-3, lr_final=1e-5, seed=7, tau_weight=False, stream=None):
+    """Adam training in the library; returns the per-epoch (weighted) MSE.
+    tau_weight: weight optical-depth errors by 1/(1+1.66 tau); needs the
+    layer coldry in feats[:, 7] (make_dataset stores it there)."""
     losses = np.zeros(epochs, dtype=np.float32)
+    stream = _stream(stream, feats)
     msg = C.create_string_buffer(512)
     rc = _lib().rrtmg_lw_gpu_surrogate_train(C.c_void_p(feats.data_ptr()), C.c_void_p(ytarg.data_ptr()),
-                                             feats.shape[0], epochs, batch, lr, lr_final, seed, _np_ptr(losses),
+                                             feats.shape[0], epochs, batch, lr, lr_final, seed, int(bool(tau_weight)),
+                                             _np_ptr(losses),
                                              stream, msg, 512)
     _check(rc, msg)
     return losses
@@ -190,6 +207,7 @@ def train(feats, ytarg, *, epochs=4, batch=8192, lr=2e-3, lr_final=1e-5, seed=7,
 def forward(feats, stream=None):
     import torch
     y = torch.empty((feats.shape[0], NOUTP), dtype=torch.float32, device=feats.device)
+    stream = _stream(stream, feats)
     msg = C.create_string_buffer(512)
     rc = _lib().rrtmg_lw_gpu_surrogate_forward(C.c_void_p(feats.data_ptr()), feats.shape[0],
                                                C.c_void_p(y.data_ptr()), stream, msg, 512)
@@ -202,7 +220,7 @@ def grads(feats, ytarg, batch):
     loss = np.zeros(1, dtype=np.float32)
     msg = C.create_string_buffer(512)
     rc = _lib().rrtmg_lw_gpu_surrogate_grads(C.c_void_p(feats.data_ptr()), C.c_void_p(ytarg.data_ptr()), batch,
-                                             _np_ptr(g), _np_ptr(loss), None, msg, 512)
+                                             _np_ptr(g), _np_ptr(loss), _stream(None, feats), msg, 512)
     _check(rc, msg)
     return g, float(loss[0])
 

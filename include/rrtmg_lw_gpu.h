@@ -245,11 +245,15 @@ int rrtmg_lw_gpu_surrogate_get(float *weights, float *norm, char *errmsg,
                                int32_t errmsg_len);
 /* Adam training on device data feats[n][8], targets[n][288] (normalised,
  * padded), batch a multiple of 128, learning rate decaying from lr to
- * lr_final (cosine); loss_per_epoch optional host float[epochs] (MSE). */
+ * lr_final (cosine); loss_per_epoch optional host float[epochs] (MSE).
+ * flags bit 0: weight every optical-depth error by 1 / (1 + 1.66 tau) of its
+ * target (opaque layers barely change the fluxes), with the layer's coldry
+ * stored in feats[., 7]. */
 int rrtmg_lw_gpu_surrogate_train(const float *feats, const float *targets,
                                  int64_t n, int32_t epochs, int32_t batch,
                                  float lr, float lr_final, uint64_t seed,
-                                 float *loss_per_epoch, void *stream,
+                                 int32_t flags, float *loss_per_epoch,
+                                 void *stream,
                                  char *errmsg, int32_t errmsg_len);
 /* Network outputs (normalised) for device features: y[n][288]. */
 int rrtmg_lw_gpu_surrogate_forward(const float *feats, int64_t n, float *y,

@@ -73,3 +73,102 @@ def test_training_reduces_loss(sg, small_set):
     losses = sg.train(feats, y, epochs=6, batch=1024, lr=3e-3, lr_final=1e-4)
     assert np.all(np.isfinite(losses))
     assert losses[-1] < 0.25 * losses[0], losses
+
+
+@pytest.fixture(scope="module")
+def trained(sg):
+    """The committed network, trained on the GPU by ccpp_physics_b200.train_surrogate."""
+    d = sg.load()
+    return d
+
+
+def _run(lw, prof, precision, n, nlay):
+    o = abi.alloc_outputs(n, nlay, hlw0=True, like="cuda")
+    msg, err = lw.run_profile(prof, o, precision=precision)
+    assert err == 0, msg
+    return o
+
+
+def _rmse(a, b):
+    import torch
+    return float(torch.sqrt(torch.mean((a - b) ** 2)).item())
+
+
+def test_surrogate_path_meets_accuracy_bounds(sg, trained):
+    """All-sky McICA columns the network never saw (generator seed 1): fluxes
+    within 0.5 W/m2 RMSE and heating rates within 0.1 K/day RMSE of the FP64 path."""
+    import torch
+    from ccpp_physics_b200 import rrtmg_lw as lw
+    n, nlay = 4096, 127
+    prof = lw.to_device(synthetic.make_profiles(n, nlay, seed=1))
+    sg.stats(reset=True)
+    s = _run(lw, prof, "surrogate", n, nlay)
+    fallback, mma_err = sg.stats()
+    r = _run(lw, prof, "fp64", n, nlay)
+    assert mma_err == 0
+    assert fallback < 0.01 * n * nlay
+    flux = _rmse(torch.cat([s["topflx"], s["sfcflx"]], 1), torch.cat([r["topflx"], r["sfcflx"]], 1))
+    hr = _rmse(s["hlwc"], r["hlwc"])
+    assert flux <= 0.5, flux
+    assert hr <= 0.1, hr
+    assert _rmse(s["hlw0"], r["hlw0"]) <= 0.1
+    assert torch.equal(s["cldtau"], r["cldtau"]) or _rmse(s["cldtau"], r["cldtau"]) < 1e-5
+
+
+def test_out_of_envelope_layers_fall_back_to_taumol(sg, trained):
+    """Doubled CO2 (the training set holds 400 ppmv) puts every layer outside
+    the envelope: the gas-optics kernel then recomputes all of them with plain
+    taumol and the result is the FP32 path's, bit for bit."""
+    import torch
+    from ccpp_physics_b200 import rrtmg_lw as lw
+    n, nlay = 512, 127
+    p = synthetic.make_profiles(n, nlay, seed=21)
+    p["gasvmr_co2"] = p["gasvmr_co2"] * 2.0
+    prof = lw.to_device(p)
+    sg.stats(reset=True)
+    s = _run(lw, prof, "surrogate", n, nlay)
+    fallback, _ = sg.stats()
+    assert fallback == n * nlay
+    f = _run(lw, prof, "fp32", n, nlay)
+    for k in s:
+        assert torch.equal(s[k], f[k]), k
+    # only the upper half of every column outside: exactly those layers fall back
+    p2 = synthetic.make_profiles(n, nlay, seed=21)
+    p2["gasvmr_co2"][64:] *= 2.0
+    sg.stats(reset=True)
+    _run(lw, lw.to_device(p2), "surrogate", n, nlay)
+    assert sg.stats()[0] == n * (nlay - 64)
+
+
+def test_trained_network_gain(sg, trained):
+    """What the trained network adds: against the same network untrained
+    (random initial weights, same normalisation) its fluxes are far closer to
+    FP64, and against plain taumol in FP32 (the path without it) it is faster."""
+    import torch
+    from ccpp_physics_b200 import rrtmg_lw as lw
+    n, nlay = 16384, 127
+    prof = lw.to_device(synthetic.make_profiles(n, nlay, seed=3))
+    r = _run(lw, prof, "fp64", n, nlay)
+    s = _run(lw, prof, "surrogate", n, nlay)
+    err_trained = _rmse(torch.cat([s["topflx"], s["sfcflx"]], 1), torch.cat([r["topflx"], r["sfcflx"]], 1))
+
+    def best_ms(precision):
+        o = abi.alloc_outputs(n, nlay, hlw0=True, like="cuda")
+        times = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            msg, err = lw.run_profile(prof, o, precision=precision)
+            e1.record()
+            torch.cuda.synchronize()
+            assert err == 0, msg
+            times.append(e0.elapsed_time(e1))
+        return min(times)
+    t_sg, t_fp32 = best_ms("surrogate"), best_ms("fp32")
+    w, norm = sg.get_weights()
+    sg.init(norm, seed=9)                       # untrained network
+    u = _run(lw, prof, "surrogate", n, nlay)
+    err_untrained = _rmse(torch.cat([u["topflx"], u["sfcflx"]], 1), torch.cat([r["topflx"], r["sfcflx"]], 1))
+    sg.set_weights(w, norm)
+    assert err_trained < 0.02 * err_untrained, (err_trained, err_untrained)
+    assert t_sg < 0.9 * t_fp32, (t_sg, t_fp32)
