@@ -173,8 +173,11 @@ def batched_leg(args, lw, abi, synthetic, torch, rank, world, sh, timed, rmse):
     res = {"workload": cfg["name"], "nblocks": int(len(sizes)), "block_sizes": "U{8..256}, seed 7"}
     outs = {}
     k = max(2, min(args.steps, 5))
-    for prec in ("fp32", "fp64"):
+    precs = ("fp32", "fp64", "surrogate") if args.surrogate_ready else ("fp32", "fp64")
+    for prec in precs:
         out = abi.alloc_outputs(n3, nlay, hlw0=True, like="cuda")
+        if prec == "surrogate":
+            from ccpp_physics_b200 import surrogate as sg
         t0 = time.time()
         best, tune_ms = lw.autotune(prof, out, sizes, precision=prec, sample_cols=65536, stream=sh)
         tune_s = time.time() - t0
@@ -188,17 +191,59 @@ def batched_leg(args, lw, abi, synthetic, torch, rank, world, sh, timed, rmse):
                 raise RuntimeError(buf.value.decode())
         for _ in range(2):
             call()
+        if prec == "surrogate":
+            sg.stats(reset=True)
         ms = timed(call, k)
         res[prec] = {"value": world * n3 * k / (ms / 1e3), "ms_per_step": ms / k, "steps": k,
                      "tuning": best, "autotune_s": round(tune_s, 2), "graph": True}
+        if prec == "surrogate":
+            fb, mma_err = sg.stats()
+            res[prec]["fallback_layer_fraction"] = fb / float(k * n3 * nlay)
+            res[prec]["mma_error"] = mma_err
         outs[prec] = out
-    a, b = outs["fp32"], outs["fp64"]
-    res["fp32"].update({
-        "flux_rmse_wm2": rmse(torch.cat([a["topflx"], a["sfcflx"]], 1), torch.cat([b["topflx"], b["sfcflx"]], 1)),
-        "hr_rmse_kday": rmse(a["hlwc"], b["hlwc"]), "hr0_rmse_kday": rmse(a["hlw0"], b["hlw0"])})
+    b = outs["fp64"]
+    for prec in precs:
+        if prec == "fp64":
+            continue
+        a = outs[prec]
+        res[prec].update({
+            "flux_rmse_wm2": rmse(torch.cat([a["topflx"], a["sfcflx"]], 1), torch.cat([b["topflx"], b["sfcflx"]], 1)),
+            "hr_rmse_kday": rmse(a["hlwc"], b["hlwc"]), "hr0_rmse_kday": rmse(a["hlw0"], b["hlw0"]),
+            "speedup_vs_fp64": res[prec]["value"] / res["fp64"]["value"]})
     del prof, outs, a, b
     torch.cuda.empty_cache()
     return res
+
+
+def training_leg(args, torch, sg):
+    """Learned gas optics training throughput on 20M layer samples labelled by
+    plain FP64 taumol: a fresh network, 2 epochs of the library's tcgen05
+    forward/backward kernels + Adam (batch 8,192).  The committed network
+    (trained the same way for 100 epochs) is reloaded afterwards."""
+    t0 = time.time()
+    feats, targ = sg.make_dataset(20_000_000, seed=101)
+    norm = sg.normalisation(feats, targ)
+    y = sg.normalise_targets(targ, norm)
+    del targ
+    torch.cuda.synchronize()
+    t_data = time.time() - t0
+    sg.init(norm, seed=1)
+    epochs = 2
+    t0 = time.time()
+    losses = sg.train(feats, y, epochs=epochs, batch=8192, lr=3e-3, lr_final=1e-5, tau_weight=True)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    n = feats.shape[0]
+    del feats, y
+    torch.cuda.empty_cache()
+    meta = sg.load()
+    flop = 2 * (16 * 128 + 128 * 128 + 128 * 288) + 2 * (2 * 288 * 128 + 2 * 128 * 128 + 128 * 16)   # padded fwd + bwd
+    return {"workload": "c4_surrogate_training_20M", "samples": int(n), "epochs": epochs, "batch": 8192,
+            "data_s": round(t_data, 2), "train_s": round(t_train, 2),
+            "samples_per_s": n * epochs / t_train, "tflops": n * epochs * flop / t_train / 1e12,
+            "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
+            "shipped_network": {"epochs": int(meta["epochs"]), "train_s": float(meta["train_seconds"]),
+                                "final_loss": float(meta["losses"][-1])}}
 
 
 def main():
@@ -212,6 +257,7 @@ def main():
     ap.add_argument("--ncols", type=int, default=0, help="override the column count (profiling runs)")
     ap.add_argument("--quick", action="store_true", help="FP64 device-resident loop only (profiling runs)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 884,736-column batched-block leg")
+    ap.add_argument("--no-train", action="store_true", help="skip the surrogate training-throughput leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = dict(CONFIGS[args.config])
@@ -323,8 +369,35 @@ def main():
                                        torch.cat([ref64["topflx"], ref64["sfcflx"]], 1)),
                  "hr_rmse_kday": rmse(out32["hlwc"], ref64["hlwc"]),
                  "hr0_rmse_kday": rmse(out32["hlw0"], ref64["hlw0"])},
-        "surrogate": {"value": None, "note": "learned gas optics not built yet"},
     }
+
+    # ---- learned gas optics: committed network (trained on this GPU by the library's kernels) ----
+    from ccpp_physics_b200 import surrogate as sg
+    args.surrogate_ready = False
+    try:
+        sg.load()
+        args.surrogate_ready = True
+    except Exception as exc:   # weights missing: report, do not fake
+        paths["surrogate"] = {"value": None, "note": f"no trained network: {exc}"}
+    if args.surrogate_ready:
+        outsg = abi.alloc_outputs(ncols, nlay, hlw0=True, like="cuda")
+        for _ in range(args.warmup):
+            step("surrogate", outsg)
+        sg.stats(reset=True)
+        mssg = timed(lambda: step("surrogate", outsg), args.steps)
+        fb, mma_err = sg.stats()
+        kms_sg = (C.c_float * 3)()
+        step("surrogate", outsg, kernel_ms=kms_sg)
+        paths["surrogate"] = {
+            "value": world * ncols * args.steps / (mssg / 1e3), "ms_per_step": mssg / args.steps,
+            "speedup_vs_fp64": (ms64 / mssg), "mcica_kernel_ms": kms_sg[0], "mlp_plus_gas_kernel_ms": kms_sg[1],
+            "rt_kernel_ms": kms_sg[2],
+            "flux_rmse_wm2": rmse(torch.cat([outsg["topflx"], outsg["sfcflx"]], 1),
+                                  torch.cat([ref64["topflx"], ref64["sfcflx"]], 1)),
+            "hr_rmse_kday": rmse(outsg["hlwc"], ref64["hlwc"]), "hr0_rmse_kday": rmse(outsg["hlw0"], ref64["hlw0"]),
+            "fallback_layer_fraction": fb / float(args.steps * ncols * nlay), "mma_error": mma_err}
+        if not args.no_train:
+            paths["c4_training"] = training_leg(args, torch, sg)
 
     # ---- batched production blocks (884,736 columns in uneven blocks of 8..256) ----
     if not args.no_batch:
