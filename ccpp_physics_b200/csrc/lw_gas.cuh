@@ -167,88 +167,93 @@ lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int
       const double tem1c = 100.0 * kConG, tem2c = 1.0e-20 * 1.0e3 * kConAvgd;
       double coldry = tem2c * delp / (tem1c * tem0 * (1.0 + h2ovmr));
       double temcol = 1.0e-12 * coldry;
-      double colv[7], wxv[4];
-      colv[0] = fmax(0.0, coldry * h2ovmr);
-      colv[1] = fmax(temcol, coldry * IN(F_CO2, r));
-      colv[2] = fmax(temcol, coldry * o3vmr);
-      if (f.inc_minor_gas) {
-        colv[3] = fmax(temcol, coldry * IN(F_N2O, r));
-        colv[4] = fmax(temcol, coldry * IN(F_CH4, r));
-        colv[5] = fmax(0.0, coldry * IN(F_O2, r));
-        colv[6] = fmax(0.0, coldry * IN(F_CO, r));
-        wxv[0] = fmax(0.0, coldry * IN(F_CCL4, r));
-        wxv[1] = fmax(0.0, coldry * IN(F_CFC11, r));
-        wxv[2] = fmax(0.0, coldry * IN(F_CFC12, r));
-        wxv[3] = fmax(0.0, coldry * IN(F_CFC22, r));
-      } else {
-        colv[3] = colv[4] = colv[5] = colv[6] = 0.0;
-        wxv[0] = wxv[1] = wxv[2] = wxv[3] = 0.0;
-      }
+      const double colh2o = fmax(0.0, coldry * h2ovmr);
+      // the learned gas optics already wrote tau/frac of layers inside its training
+      // envelope: they need no setcoef record and no taumol here
       if (f.surrogate) {
         float xf[SG_NFEAT];
         layer_features(pavel, tavel, h2ovmr, o3vmr, IN(F_CO2, r), IN(F_CH4, r), IN(F_N2O, r), xf);
         sg_skip = in_envelope(xf, f.sg_norm);
         if (!sg_skip && f.sg_fallback) atomicAdd(f.sg_fallback, 1u);
       }
-      double summol = 0.0;
-      for (int m = 1; m < 7; ++m) summol = summol + colv[m];
-      double colbrd = coldry - summol;
-
       indlay = min(180, max(1, (int)(tavel - 159.0)));
       tlyrfr = tavel - (int)tavel;
       indlev = min(180, max(1, (int)(tz - 159.0)));
       tlvlfr = tz - (int)tz;
       double plog = log(pavel);
-      int jp = max(1, min(58, (int)(36.0 - 5.0 * (plog + 0.04))));
-      int jp1 = jp + 1;
-      double fp = fmax(0.0, fmin(1.0, 5.0 * (t64(kt64, lwtab::preflog + jp - 1) - plog)));
-      double tem1 = (tavel - t64(kt64, lwtab::tref + jp - 1)) / 15.0;
-      double tem2 = (tavel - t64(kt64, lwtab::tref + jp1 - 1)) / 15.0;
-      int jt = max(1, min(4, (int)(3.0 + tem1)));
-      int jt1 = max(1, min(4, (int)(3.0 + tem2)));
-      double ft = fmax(-0.5, fmin(1.5, tem1 - (double)(jt - 3)));
-      double ft1 = fmax(-0.5, fmin(1.5, tem2 - (double)(jt1 - 3)));
-      tem1 = 1.0 - fp;
-      double fac10 = tem1 * ft, fac00 = tem1 * (1.0 - ft), fac11 = fp * ft1, fac01 = fp * (1.0 - ft1);
-      double forfac = pavel * kStpfac / (tavel * (1.0 + h2ovmr));
-      double selffac = h2ovmr * forfac;
-      double scaleminor = pavel / tavel;
-      double scaleminorn2 = (pavel / tavel) * (colbrd / (coldry + colv[0]));
-      tem1 = (tavel - 180.8) / 7.2;
-      int indminor = min(18, max(1, (int)tem1));
-      double minorfrac = tem1 - (double)indminor;
-      int indfor, indself;
-      double forfrac, selffrac;
       lowerk = plog > 4.56;
-      if (lowerk) {
-        tem1 = (332.0 - tavel) / 36.0;
-        indfor = min(2, max(1, (int)tem1));
-        forfrac = tem1 - (double)indfor;
-        tem1 = (tavel - 188.0) / 7.2;
-        indself = min(9, max(1, (int)tem1 - 7));
-        selffrac = tem1 - (double)(indself + 7);
-      } else {
-        tem1 = (tavel - 188.0) / 36.0;
-        indfor = 3;
-        forfrac = tem1 - 1.0;
-        indself = 0;
-        selffrac = 0.0;
-      }
-      selffac = colv[0] * selffac;
-      forfac = colv[0] * forfac;
+      if (!sg_skip) {
+        double colv[7], wxv[4];
+        colv[0] = colh2o;
+        colv[1] = fmax(temcol, coldry * IN(F_CO2, r));
+        colv[2] = fmax(temcol, coldry * o3vmr);
+        if (f.inc_minor_gas) {
+          colv[3] = fmax(temcol, coldry * IN(F_N2O, r));
+          colv[4] = fmax(temcol, coldry * IN(F_CH4, r));
+          colv[5] = fmax(0.0, coldry * IN(F_O2, r));
+          colv[6] = fmax(0.0, coldry * IN(F_CO, r));
+          wxv[0] = fmax(0.0, coldry * IN(F_CCL4, r));
+          wxv[1] = fmax(0.0, coldry * IN(F_CFC11, r));
+          wxv[2] = fmax(0.0, coldry * IN(F_CFC12, r));
+          wxv[3] = fmax(0.0, coldry * IN(F_CFC22, r));
+        } else {
+          colv[3] = colv[4] = colv[5] = colv[6] = 0.0;
+          wxv[0] = wxv[1] = wxv[2] = wxv[3] = 0.0;
+        }
+        double summol = 0.0;
+        for (int m = 1; m < 7; ++m) summol = summol + colv[m];
+        double colbrd = coldry - summol;
 
-      R* ls = s_lay + t;
-      ls[LF_FAC00 * NLP] = R(fac00); ls[LF_FAC01 * NLP] = R(fac01);
-      ls[LF_FAC10 * NLP] = R(fac10); ls[LF_FAC11 * NLP] = R(fac11);
-      ls[LF_SELFFAC * NLP] = R(selffac); ls[LF_SELFFRAC * NLP] = R(selffrac);
-      ls[LF_FORFAC * NLP] = R(forfac); ls[LF_FORFRAC * NLP] = R(forfrac);
-      ls[LF_MINORFRAC * NLP] = R(minorfrac);
-      ls[LF_SCALEMINOR * NLP] = R(scaleminor); ls[LF_SCALEMINORN2 * NLP] = R(scaleminorn2);
-      for (int m = 0; m < 7; ++m) ls[(LF_COL1 + m) * NLP] = R(colv[m]);
-      ls[LF_COLDRY * NLP] = R(coldry); ls[LF_COLBRD * NLP] = R(colbrd);
-      for (int m = 0; m < 4; ++m) ls[(LF_WX1 + m) * NLP] = R(wxv[m]);
-      ls[LF_PAVEL * NLP] = R(pavel);
-      s_li[t] = jp | (jt << 8) | (jt1 << 12) | (indself << 16) | (indfor << 20) | (indminor << 24);
+        int jp = max(1, min(58, (int)(36.0 - 5.0 * (plog + 0.04))));
+        int jp1 = jp + 1;
+        double fp = fmax(0.0, fmin(1.0, 5.0 * (t64(kt64, lwtab::preflog + jp - 1) - plog)));
+        double tem1 = (tavel - t64(kt64, lwtab::tref + jp - 1)) / 15.0;
+        double tem2 = (tavel - t64(kt64, lwtab::tref + jp1 - 1)) / 15.0;
+        int jt = max(1, min(4, (int)(3.0 + tem1)));
+        int jt1 = max(1, min(4, (int)(3.0 + tem2)));
+        double ft = fmax(-0.5, fmin(1.5, tem1 - (double)(jt - 3)));
+        double ft1 = fmax(-0.5, fmin(1.5, tem2 - (double)(jt1 - 3)));
+        tem1 = 1.0 - fp;
+        double fac10 = tem1 * ft, fac00 = tem1 * (1.0 - ft), fac11 = fp * ft1, fac01 = fp * (1.0 - ft1);
+        double forfac = pavel * kStpfac / (tavel * (1.0 + h2ovmr));
+        double selffac = h2ovmr * forfac;
+        double scaleminor = pavel / tavel;
+        double scaleminorn2 = (pavel / tavel) * (colbrd / (coldry + colv[0]));
+        tem1 = (tavel - 180.8) / 7.2;
+        int indminor = min(18, max(1, (int)tem1));
+        double minorfrac = tem1 - (double)indminor;
+        int indfor, indself;
+        double forfrac, selffrac;
+        if (lowerk) {
+          tem1 = (332.0 - tavel) / 36.0;
+          indfor = min(2, max(1, (int)tem1));
+          forfrac = tem1 - (double)indfor;
+          tem1 = (tavel - 188.0) / 7.2;
+          indself = min(9, max(1, (int)tem1 - 7));
+          selffrac = tem1 - (double)(indself + 7);
+        } else {
+          tem1 = (tavel - 188.0) / 36.0;
+          indfor = 3;
+          forfrac = tem1 - 1.0;
+          indself = 0;
+          selffrac = 0.0;
+        }
+        selffac = colv[0] * selffac;
+        forfac = colv[0] * forfac;
+
+        R* ls = s_lay + t;
+        ls[LF_FAC00 * NLP] = R(fac00); ls[LF_FAC01 * NLP] = R(fac01);
+        ls[LF_FAC10 * NLP] = R(fac10); ls[LF_FAC11 * NLP] = R(fac11);
+        ls[LF_SELFFAC * NLP] = R(selffac); ls[LF_SELFFRAC * NLP] = R(selffrac);
+        ls[LF_FORFAC * NLP] = R(forfac); ls[LF_FORFRAC * NLP] = R(forfrac);
+        ls[LF_MINORFRAC * NLP] = R(minorfrac);
+        ls[LF_SCALEMINOR * NLP] = R(scaleminor); ls[LF_SCALEMINORN2 * NLP] = R(scaleminorn2);
+        for (int m = 0; m < 7; ++m) ls[(LF_COL1 + m) * NLP] = R(colv[m]);
+        ls[LF_COLDRY * NLP] = R(coldry); ls[LF_COLBRD * NLP] = R(colbrd);
+        for (int m = 0; m < 4; ++m) ls[(LF_WX1 + m) * NLP] = R(wxv[m]);
+        ls[LF_PAVEL * NLP] = R(pavel);
+        s_li[t] = jp | (jt << 8) | (jt1 << 12) | (indself << 16) | (indfor << 20) | (indminor << 24);
+      }
       double cf = IN(F_CLDCF, r);
       cldk = cf > kEps;
       double* cl = s_cld + t;
@@ -261,7 +266,7 @@ lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int
         cl[5 * NLP] = IN(F_CLDOD, r);
       }
       s_red[t] = coldry;
-      s_red[NLP + t] = colv[0];
+      s_red[NLP + t] = colh2o;
     }
     const int laytrop = __syncthreads_count(lowerk);
     const int lcf1 = __syncthreads_or(cldk);
@@ -326,7 +331,7 @@ lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int
         }
         const size_t ab = i + ld * ((size_t)r + (size_t)nlay * b);
         R tauaer = R(0);
-        if (LW_OK(r < nlay && i < B.npts, 15, r)) tauaer = R(B.in[F_AERAOD][ab] * (1.0 - B.in[F_AERSSA][ab]));
+        if (!sg_skip && LW_OK(r < nlay && i < B.npts, 15, r)) tauaer = R(B.in[F_AERAOD][ab] * (1.0 - B.in[F_AERSSA][ab]));
         const int ns = ns_of(b);
         const size_t go = ((size_t)c * nlay + t) * NGPT + ns;
         if (!sg_skip) band_gas_optics<R>(b, kt, LR, [&](int g0, R tau, R frac) {

@@ -76,17 +76,42 @@ __device__ void twist(uint32_t* mt, int lane) {
   __syncwarp();
 }
 
+// u / (2^32 - 1), correctly rounded, without a division (the GFS twister's
+// harvest = real(y) / (2**32 - 1), mersenne_twister.f:362-369, for the
+// unsigned value u of y).  1/(2^32-1) = (2^32+1)/(2^64-1), so the quotient
+// is m * 2^-64 * (1 + 2^-64 + ...) with the 64-bit integer
+// m = u * (2^32 + 1) = (u << 32) | u.  One FMA gives RN(m * 2^-64) exactly;
+// the true quotient lies strictly above m * 2^-64 (for u > 0) but within one
+// unit of m's last bit, so the two round alike except when m's discarded
+// bits are exactly one half: then the quotient must round up, which ties-to-
+// even misses when the kept last bit is 0.  m has 32 + L significant bits
+// (L = bit length of u), so d = L - 21 bits are discarded, all from the low
+// word, i.e. the low d bits of u.
+__device__ __forceinline__ double u32_unit(uint32_t u) {
+  const double a = (double)u * 0x1p-32;   // exact
+  double r = fma(a, 0x1p-32, a);          // RN(m * 2^-64)
+  const int d = (32 - __clz(u)) - 21;
+  if (d >= 1) {
+    const uint32_t half = 1u << (d - 1);
+    if ((u & ((half << 1) - 1u)) == half && ((u >> d) & 1u) == 0u)
+      r = __longlong_as_double(__double_as_longlong(r) + 1);
+  }
+  return r;
+}
+
 struct McicaArgs {
   int nlay, nw, iovr, isubclw, top_at_1;
   int cap;        // ring capacity in words
 };
 
-// Per-warp shared memory: mt[624], cldf[nlay] (double), ring[cap].
+// Per-warp shared memory: mt[624], clear[nlay] = 1 - cldf (double), ring[cap].
 __host__ __device__ inline size_t mcica_warp_bytes(int nlay, int cap) {
   return 624 * 4 + ((nlay * 8 + 15) & ~15) + (size_t)cap * 4 + 16;
 }
 
-__global__ void __launch_bounds__(128)
+constexpr int kMcicaWarps = 5;   // 5 warps x 22 KB (127 layers): two CTAs, ten warps per SM
+
+__global__ void __launch_bounds__(32 * kMcicaWarps)
 lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int ncols, McicaArgs a,
                 const double* __restrict__ cldf_dev, const int32_t* __restrict__ seed_dev, int dev_ld,
                 uint32_t* __restrict__ bits) {
@@ -95,7 +120,7 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
   const size_t wbytes = mcica_warp_bytes(a.nlay, a.cap);
   char* my = smem_raw + wbytes * wib;
   uint32_t* mt = reinterpret_cast<uint32_t*>(my);
-  double* cldf = reinterpret_cast<double*>(my + 624 * 4);
+  double* clr = reinterpret_cast<double*>(my + 624 * 4);   // 1 - cldf(k), used by every test of the walk
   uint32_t* ring = reinterpret_cast<uint32_t*>(my + 624 * 4 + ((a.nlay * 8 + 15) & ~15));
   const int nlay = a.nlay, nlp1 = nlay + 1;
   const int warps_total = gridDim.x * (blockDim.x >> 5);
@@ -113,12 +138,12 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
         int r = a.top_at_1 ? nlp1 - (k + 1) - 1 : k;
         double cf = B.in[F_CLDCF][i + (size_t)B.ld * r];
         any |= cf > 1.0e-6;
-        cldf[k] = (cf < 2.2250738585072014e-308) ? 0.0 : cf;
+        clr[k] = 1.0 - ((cf < 2.2250738585072014e-308) ? 0.0 : cf);
       }
       seed = (a.isubclw == 1) ? 140 + (i + 1) : B.icseed[i];   // RLM:765-773
     } else {
       for (int k = lane; k < nlay; k += 32) {
-        cldf[k] = cldf_dev[c + (size_t)dev_ld * k];
+        clr[k] = 1.0 - cldf_dev[c + (size_t)dev_ld * k];
       }
       any = true;
       seed = seed_dev[c];
@@ -134,12 +159,12 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
       // maximum overlap: one draw per g-point, the same at every layer (RLM:1981-1993)
       twist(mt, lane);
       for (int n = lane; n < NGPT; n += 32) {
-        double r = (double)temper(mt[n]) / 4294967295.0;
+        double r = u32_unit(temper(mt[n]));
         for (int w = 0; w < a.nw; ++w) {
           uint32_t word = 0;
           for (int b = 0; b < 32; ++b) {
             int k = w * 32 + b;
-            if (k < nlay && r >= 1.0 - cldf[k]) word |= 1u << b;
+            if (k < nlay && r >= clr[k]) word |= 1u << b;
           }
           out[n * a.nw + w] = word;
         }
@@ -169,15 +194,15 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
         double cdf = 0.0;
         uint32_t word = 0;
         for (int k = 0; k < nlay; ++k) {
-          double r = (double)ring[q] / 4294967295.0;
+          double r = u32_unit(ring[q]);
           if (++q == cap) q = 0;
           if (k == 0 || a.iovr == 0) {
             cdf = r;
           } else {
-            double tem1 = 1.0 - cldf[k - 1];       // max-random walk (RLM:1949-1960)
+            double tem1 = clr[k - 1];              // max-random walk (RLM:1949-1960)
             cdf = (cdf > tem1) ? cdf : r * tem1;
           }
-          if (cdf >= 1.0 - cldf[k]) word |= 1u << (k & 31);   // RLM:2097-2103
+          if (cdf >= clr[k]) word |= 1u << (k & 31);   // RLM:2097-2103
           if ((k & 31) == 31 || k == nlay - 1) {
             out[n * a.nw + (k >> 5)] = word;
             word = 0;
@@ -214,7 +239,7 @@ cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int 
   a.isubclw = isubclw;
   a.top_at_1 = top_at_1;
   a.cap = mcica_ring_capacity(nlay);
-  const int wpb = 4;
+  const int wpb = kMcicaWarps;
   size_t smem = mcica_warp_bytes(nlay, a.cap) * wpb;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lw_mcica_kernel, wpb * 32, smem);

@@ -40,6 +40,8 @@ def lib():
         L.oracle_mcica.argtypes = [C.c_int, C.c_int32, C.c_int, C.c_void_p, C.c_void_p,
                                    C.c_double, C.c_void_p, C.c_void_p]
         L.oracle_tables.argtypes = [C.c_void_p] * 4
+        L.oracle_check_u32_unit.argtypes = [C.c_ulonglong, C.c_ulonglong]
+        L.oracle_check_u32_unit.restype = C.c_ulonglong
         _lib = L
     return _lib
 

@@ -1476,4 +1476,32 @@ void oracle_tables(double* tau, double* ex, double* tfn, double* fluxfac_heatfac
   fluxfac_heatfac[1] = heatfac;
 }
 
+// Exhaustive check of the division-free McICA draw conversion used by the GPU
+// kernel (csrc/lw_mcica.cu u32_unit): for every u in [start, start+count),
+// u / (2^32-1) as the reference computes it (mersenne_twister.f:362-369,
+// promoted reals) against fma(a, 2^-32, a) with a = u 2^-32 plus the
+// round-half-up fix of exact ties.  Returns the number of mismatches.
+unsigned long long oracle_check_u32_unit(unsigned long long start, unsigned long long count) {
+  unsigned long long bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+  for (long long j = 0; j < (long long)count; ++j) {
+    const uint32_t u = (uint32_t)(start + (unsigned long long)j);
+    const double ref = (double)u / 4294967295.0;
+    const double a = (double)u * 0x1p-32;
+    double r = std::fma(a, 0x1p-32, a);
+    const int d = (u ? 32 - __builtin_clz(u) : 0) - 21;
+    if (d >= 1) {
+      const uint32_t half = 1u << (d - 1);
+      if ((u & ((half << 1) - 1u)) == half && ((u >> d) & 1u) == 0u) {
+        uint64_t b;
+        std::memcpy(&b, &r, 8);
+        ++b;
+        std::memcpy(&r, &b, 8);
+      }
+    }
+    if (std::memcmp(&r, &ref, 8) != 0) ++bad;
+  }
+  return bad;
+}
+
 }  // extern "C"

@@ -180,3 +180,14 @@ def test_mcica_max_random_properties(oracle_lib):
     for k in range(1, 60):
         if cldf[k] >= cldf[k - 1] > 0:
             assert np.all(lc[k][lc[k - 1]])
+
+
+def test_mcica_draw_conversion_exhaustive(oracle_lib):
+    """The GPU McICA kernel converts each 32-bit draw u to u / (2^32 - 1)
+    without a division (one FMA and an exact-tie fix); that must equal the
+    reference's division for all 2^32 values of u."""
+    import time
+    t0 = time.time()
+    bad = oracle_lib.lib().oracle_check_u32_unit(0, 1 << 32)
+    assert bad == 0
+    assert time.time() - t0 < 120
