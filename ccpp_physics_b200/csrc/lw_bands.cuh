@@ -11,15 +11,23 @@
 
 #include "lw_common.cuh"
 
-// Unrolling of the per-band g-point loops: fully unrolled (the default), every
-// table gather of the band uses a constant offset from a per-layer row pointer.
+// Unrolling of the per-band g-point loops.  Full unrolling makes every table
+// gather a constant offset from a per-layer row pointer, but the sixteen
+// unrolled bands overflow the instruction cache: measured on B200 (16,384
+// columns x 127 layers) the rolled loops run the FP32 gas-optics kernel 25%
+// faster (6.4 -> 4.8 ms) and the FP64 one 3% faster, with identical results.
 #ifndef LW_GLOOP_FULL
-#define LW_GLOOP_FULL 1
+#define LW_GLOOP_FULL 0
 #endif
+#ifndef LW_GLOOP_N
+#define LW_GLOOP_N 1
+#endif
+#define LW_PRAGMA_(x) _Pragma(#x)
+#define LW_PRAGMA(x) LW_PRAGMA_(x)
 #if LW_GLOOP_FULL
 #define LW_GLOOP _Pragma("unroll")
 #else
-#define LW_GLOOP _Pragma("unroll 1")
+#define LW_GLOOP LW_PRAGMA(unroll LW_GLOOP_N)
 #endif
 
 namespace lw {

@@ -36,15 +36,29 @@ constexpr double kAbsrain = 0.33e-3, kAbssnow0 = 1.5;   // radlw_datatb.f:941,94
 constexpr int kColRec = 48;                     // doubles per column record
 
 // Minimum resident CTAs per SM requested from the register allocator
-// (measured on B200: FP64 gas optics 3, everything else 4).  The V = 8
+// (measured on B200, 16,384 columns x 127 layers: gas optics 3 in both
+// precisions, transfer 4, gas optics behind the network 5).  The V = 8
 // kernels (128..255 layers) are left uncapped: with the caps their
 // transfer kernel spilled ~1 KB per thread and an illegal address was
 // observed that reading the code did not explain.
 #ifndef LW_GAS_MINB
-#define LW_GAS_MINB (V > 4 ? 1 : (sizeof(R) == 8 ? 3 : 4))
+#ifdef LW_GAS_MINB_SMALL   // build-time override for V <= 4 (tuning builds)
+#define LW_GAS_MINB (V > 4 ? 1 : LW_GAS_MINB_SMALL)
+#else
+#define LW_GAS_MINB (V > 4 ? 1 : 3)
+#endif
+#endif
+// gas optics behind the learned gas optics (setcoef/taumol only for
+// out-of-envelope layers): light enough for more resident CTAs
+#ifndef LW_GAS_MINB_SG
+#define LW_GAS_MINB_SG (V > 4 ? 1 : 5)
 #endif
 #ifndef LW_RT_MINB
+#ifdef LW_RT_MINB_SMALL
+#define LW_RT_MINB (V > 4 ? 1 : LW_RT_MINB_SMALL)
+#else
 #define LW_RT_MINB (V > 4 ? 1 : 4)
+#endif
 #endif
 
 static __device__ __constant__ double c_delwave[16] = {340., 150., 130., 70., 120., 160., 100., 100.,
@@ -119,8 +133,8 @@ __host__ __device__ constexpr size_t gas_smem_bytes(int V) {
   return sizeof(double) * (2 * NLP + 24 + 8 * NLP) + sizeof(R) * N_LF * NLP + sizeof(int) * (NLP + 4);
 }
 
-template <typename R, int V>
-__global__ void __launch_bounds__(32 * V, LW_GAS_MINB)
+template <typename R, int V, bool SG>
+__global__ void __launch_bounds__(32 * V, SG ? LW_GAS_MINB_SG : LW_GAS_MINB)
 lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int ncols, Flags f,
               Tables<R> tab, Tables<double> tab64, Scratch<R> sc, double* __restrict__ gas_taug,
               double* __restrict__ gas_fracs) {
@@ -170,7 +184,7 @@ lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int
       const double colh2o = fmax(0.0, coldry * h2ovmr);
       // the learned gas optics already wrote tau/frac of layers inside its training
       // envelope: they need no setcoef record and no taumol here
-      if (f.surrogate) {
+      if (SG) {
         float xf[SG_NFEAT];
         layer_features(pavel, tavel, h2ovmr, o3vmr, IN(F_CO2, r), IN(F_CH4, r), IN(F_N2O, r), xf);
         sg_skip = in_envelope(xf, f.sg_norm);
