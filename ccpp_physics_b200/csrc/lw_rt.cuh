@@ -45,6 +45,15 @@ __device__ __forceinline__ void load_vec(const R* __restrict__ p, R (&o)[V]) {
   }
 }
 
+// Table-index quotient x / (bpade + x) and cloud transmittance exp(-x).  The
+// FP64 path keeps the exact operations (its table indices must match the
+// reference's); the FP32 path, already within its error bound of the FP64
+// result, uses the fast hardware approximations.
+__device__ __forceinline__ double tbl_quot(double x) { return x / (kBpade + x); }
+__device__ __forceinline__ float tbl_quot(float x) { return __fdividef(x, float(kBpade) + x); }
+__device__ __forceinline__ double exp_neg(double x) { return exp(-x); }
+__device__ __forceinline__ float exp_neg(float x) { return __expf(-x); }
+
 // Per-layer two-stream coefficients of one g-point (RLM:3598-3660).
 template <typename R>
 struct LayRT {
@@ -63,7 +72,7 @@ __device__ __forceinline__ void layer_rt(R tau, R frac, R secd, R blay, R plevu,
     trng = one - atrgas;
     gasfac = R(kRec6) * odepth;
   } else {
-    R tblind = odepth / (R(kBpade) + odepth);
+    R tblind = tbl_quot(odepth);
     int itgas = min(NTBL, max(0, (int)(R(kTblint) * tblind + R(0.5))));
     if (!LW_OK(itgas >= 0 && itgas <= NTBL, 22, itgas)) itgas = 0;
     const R* e = tab.exp_tbl + itgas;          // exp, tfn, tau tables are contiguous
@@ -81,14 +90,14 @@ __device__ __forceinline__ void layer_rt(R tau, R frac, R secd, R blay, R plevu,
   o.tr = trng;
   if (cloudy) {
     R odcld = secd * tcld;
-    o.ef = one - (one - exp(-odcld)) * one;   // clfm = 1 for a McICA cloudy sub-column
+    o.ef = one - (one - exp_neg(odcld)) * one;   // clfm = 1 for a McICA cloudy sub-column
     R odtot = odepth + odcld;
     R totfac, atrtot;
     if (odtot < R(0.06)) {
       totfac = R(kRec6) * odtot;
       atrtot = odtot - R(0.5) * odtot * odtot;
     } else {
-      R tblind = odtot / (R(kBpade) + odtot);
+      R tblind = tbl_quot(odtot);
       int ittot = min(NTBL, max(0, (int)(R(kTblint) * tblind + R(0.5))));
       const R* e = tab.exp_tbl + ittot;
       totfac = ldg(e + (NTBL + 1));
