@@ -258,6 +258,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="FP64 device-resident loop only (profiling runs)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 884,736-column batched-block leg")
     ap.add_argument("--no-train", action="store_true", help="skip the surrogate training-throughput leg")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "surrogate"],
+                    help="with --quick: the path to loop over (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     cfg = dict(CONFIGS[args.config])
@@ -326,6 +328,19 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         return ms
+
+    if args.quick and args.precision != "fp64":
+        # profiling runs of another path: the same loop, no other legs
+        if args.precision == "surrogate":
+            from ccpp_physics_b200 import surrogate as sg
+            sg.load()
+        for _ in range(args.warmup):
+            step(args.precision)
+        msq = timed(lambda: step(args.precision), args.steps)
+        if rank == 0:
+            print(json.dumps({"quick": True, "precision": args.precision, "value": world * ncols * args.steps / (msq / 1e3),
+                              "ms_per_step": msq / args.steps, "config": cfg["name"]}), flush=True)
+        return
 
     # ---- FP64 path, inputs resident in HBM (the headline value) ----
     for _ in range(args.warmup):
