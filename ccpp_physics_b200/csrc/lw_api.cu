@@ -281,8 +281,17 @@ int validate(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg, i
             "rrtmg_lw_gpu: isubclw=%d not supported (the McICA paths isubclw=1,2 with rtrnmc are)", a->isubclw);
     return 1;
   }
-  if (a->iovr < 0 || a->iovr > 2) {
-    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: McICA overlap iovr=%d not supported (0, 1, 2 are)", a->iovr);
+  if (a->iovr < 0 || a->iovr > 5) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: McICA overlap iovr=%d not supported (0..5 are)", a->iovr);
+    return 1;
+  }
+  // the decorrelation-length and exponential overlaps read these (RLM:796, 820, 933)
+  if (a->iovr == 3 && !a->de_lgth) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_run: iovr=3 (decorrelation length) needs de_lgth");
+    return 1;
+  }
+  if ((a->iovr == 4 || a->iovr == 5) && !a->alpha) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_run: iovr=%d (exponential overlap) needs alpha", a->iovr);
     return 1;
   }
   const double* req[] = {a->plyr, a->plvl, a->tlyr, a->tlvl, a->qlyr, a->olyr, a->gasvmr_co2, a->gasvmr_n2o,
@@ -428,7 +437,7 @@ cudaError_t enqueue(Workspace* w, cudaStream_t st, const Block* dblk, const Bloc
   cudaError_t e;
   if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return e;
   if (f.isubclw > 0 && !f.gas_only) {
-    e = mcica_launch(dblk, nblocks, b0, ncols, f.nlay, f.iovr, f.isubclw, f.top_at_1, nullptr, nullptr, 0, w->bits,
+    e = mcica_launch(dblk, nblocks, b0, ncols, f.nlay, f.iovr, f.isubclw, f.top_at_1, McicaStage(), w->bits,
                      g.num_sms, st);
     if (e != cudaSuccess) return e;
   }
@@ -654,15 +663,18 @@ extern "C" int rrtmg_lw_gpu_mcica(int32_t npts, int32_t nlay, int32_t ldim, int3
                                   const double* cldf, const double* dz, const double* de_lgth,
                                   const double* alpha, uint32_t* bits, void* stream, char* errmsg,
                                   int32_t errmsg_len) {
-  (void)dz; (void)de_lgth; (void)alpha;
   set_msg(errmsg, errmsg_len, "");
   if (!g.ready) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: rrtmg_lw_gpu_init has not been called"); return 1; }
   if (npts < 0 || nlay < 1 || nlay > 255 || (ldim != 0 && ldim < npts)) {
     set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_mcica: bad dimensions");
     return 1;
   }
-  if (iovr < 0 || iovr > 2) {
-    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_mcica: overlap iovr=%d not supported (0, 1, 2 are)", iovr);
+  if (iovr < 0 || iovr > 5) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_mcica: overlap iovr=%d not supported (0..5 are)", iovr);
+    return 1;
+  }
+  if ((iovr == 3 && (!dz || !de_lgth)) || (iovr >= 4 && !alpha)) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_mcica: iovr=%d needs %s", iovr, iovr == 3 ? "dz and de_lgth" : "alpha");
     return 1;
   }
   if (npts == 0) return 0;
@@ -673,7 +685,14 @@ extern "C" int rrtmg_lw_gpu_mcica(int32_t npts, int32_t nlay, int32_t ldim, int3
   if (!w) return rc;
   cudaStream_t st = stream ? (cudaStream_t)stream : w->stream;
   Block none{};
-  CK(mcica_launch(nullptr, 0, none, npts, nlay, iovr, 2, 0, cldf, seed, ldim > 0 ? ldim : npts, bits, g.num_sms, st),
+  McicaStage stg;
+  stg.cldf = cldf;
+  stg.seed = seed;
+  stg.dz = dz;
+  stg.delg = de_lgth;
+  stg.alpha = alpha;
+  stg.ld = ldim > 0 ? ldim : npts;
+  CK(mcica_launch(nullptr, 0, none, npts, nlay, iovr, 2, 0, stg, bits, g.num_sms, st),
      "McICA kernel launch");
   CK(cudaStreamSynchronize(st), "McICA kernel execution");
   return 0;

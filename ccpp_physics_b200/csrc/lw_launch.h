@@ -29,9 +29,18 @@ cudaError_t launch_column_fp32(int V, bool hlwb, const Block* blocks, int nblock
                                const Shape& sh, cudaStream_t st, cudaEvent_t ev_mid);
 cudaError_t mcica_upload_powers();
 cudaError_t mcica_prepare(int max_smem);
+// inputs of the McICA stage entry point (layer arrays [column + ld * layer], internal order)
+struct McicaStage {
+  const double* cldf = nullptr;
+  const int32_t* seed = nullptr;
+  const double* dz = nullptr;      // iovr 3
+  const double* delg = nullptr;    // iovr 3, per column
+  const double* alpha = nullptr;   // iovr 4, 5
+  int ld = 0;
+};
 cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int ncols, int nlay, int iovr,
-                         int isubclw, int top_at_1, const double* cldf_dev, const int32_t* seed_dev, int dev_ld,
-                         uint32_t* bits, int num_sms, cudaStream_t st);
+                         int isubclw, int top_at_1, const McicaStage& stage, uint32_t* bits, int num_sms,
+                         cudaStream_t st);
 
 // learned gas optics (lw_mlp.cu): network stage of a chunk, its
 // normalisation/envelope (nullptr until a network is loaded) and the

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include "lw_common.cuh"
+#include "lw_launch.h"
 
 namespace lw {
 
@@ -102,7 +103,112 @@ __device__ __forceinline__ double u32_unit(uint32_t u) {
 struct McicaArgs {
   int nlay, nw, iovr, isubclw, top_at_1;
   int cap;        // ring capacity in words
+  McicaStage st;  // stage entry point inputs (blocks == nullptr)
 };
+
+// Read the next 140 draws (one layer of a layer-major stream, RLM:2006-2024)
+// of a Mersenne-twister stream whose current twist is in mt[624] with read
+// position *pos; lane gets draws for g-points n = lane + 32 j (j < 5).  A
+// layer spans at most one twist boundary.
+__device__ __forceinline__ void layer_draws(uint32_t* mt, int* pos, int lane, double (&d)[5]) {
+  const int p = *pos;
+  uint32_t w[5] = {0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    const int n = lane + 32 * j;
+    if (n < NGPT && p + n < 624) w[j] = temper(mt[p + n]);
+  }
+  if (p + NGPT > 624) {
+    __syncwarp();
+    twist(mt, lane);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const int n = lane + 32 * j;
+      if (n < NGPT && p + n >= 624) w[j] = temper(mt[p + n - 624]);
+    }
+    *pos = p + NGPT - 624;
+  } else {
+    *pos = p + NGPT;
+  }
+#pragma unroll
+  for (int j = 0; j < 5; ++j) d[j] = u32_unit(w[j]);
+}
+
+// Overlaps built from two layer-major random sets (RLM:1995-2091):
+//   iovr = 3, decorrelation length: top-down, layer k keeps the value of layer
+//     k+1 when set2(k) <= fac_lcf(k+1), else its own set-1 draw;
+//   iovr = 4/5, exponential / exponential-random: bottom-up, layer k keeps the
+//     value of layer k-1 when set2(k) < alpha(k), else its own draw.
+// Set 1 is stream positions [0, 140 nlay), set 2 the next 140 nlay; two
+// twister states walk them in lockstep, layer by layer, surface first.  The
+// top-down rule is evaluated bottom-up: a layer's value is the set-1 draw of
+// the nearest layer at or above it whose link to the layer above is broken
+// (the top layer always is), so each g-point keeps the run of layers still
+// waiting for that draw and resolves it when the break arrives.
+// aux[k] is fac_lcf(k) (iovr 3, 0-based, aux[0] unused) or alpha(k).
+__device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const double* clr, const double* aux, int nlay, int iovr,
+                              uint32_t s0, int nw, uint32_t* out, int lane) {
+  for (int n = lane; n < 624; n += 32) {
+    const uint32_t v = s0 * c_pow69069[n];
+    mtA[n] = v;
+    mtB[n] = v;
+  }
+  __syncwarp();
+  // stream B starts at position 140 nlay: apply the twists up to and including
+  // the one that produces that position
+  const long P0 = (long)NGPT * nlay;
+  for (long t = 0; t <= P0 / 624; ++t) twist(mtB, lane);
+  int posB = (int)(P0 % 624);
+  twist(mtA, lane);
+  int posA = 0;
+  double cdf[5], c1[5], c2[5];
+  uint32_t word[5] = {0u, 0u, 0u, 0u, 0u};
+  int start[5] = {0, 0, 0, 0, 0}, wi[5] = {0, 0, 0, 0, 0};
+  for (int k = 0; k < nlay; ++k) {
+    layer_draws(mtA, &posA, lane, c1);
+    layer_draws(mtB, &posB, lane, c2);
+    if (iovr == 3) {
+      const bool top = (k == nlay - 1);
+      const double fk = top ? 0.0 : aux[k + 1];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        const int n = lane + 32 * j;
+        if (n >= NGPT) continue;
+        if (!top && c2[j] <= fk) continue;   // linked to the layer above: still waiting
+        const double v = c1[j];
+        for (int m = start[j]; m <= k; ++m) {
+          if ((m >> 5) != wi[j]) {
+            out[n * nw + wi[j]] = word[j];
+            word[j] = 0u;
+            wi[j] = m >> 5;
+          }
+          if (v >= clr[m]) word[j] |= 1u << (m & 31);   // RLM:2097-2103
+        }
+        start[j] = k + 1;
+      }
+    } else {
+      const double ak = aux[k];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        const int n = lane + 32 * j;
+        if (n >= NGPT) continue;
+        cdf[j] = (k > 0 && c2[j] < ak) ? cdf[j] : c1[j];
+        if (cdf[j] >= clr[k]) word[j] |= 1u << (k & 31);
+        if ((k & 31) == 31 || k == nlay - 1) {
+          out[n * nw + (k >> 5)] = word[j];
+          word[j] = 0u;
+        }
+      }
+    }
+  }
+  if (iovr == 3) {
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const int n = lane + 32 * j;
+      if (n < NGPT) out[n * nw + wi[j]] = word[j];
+    }
+  }
+}
 
 // Per-warp shared memory: mt[624], clear[nlay] = 1 - cldf (double), ring[cap].
 __host__ __device__ inline size_t mcica_warp_bytes(int nlay, int cap) {
@@ -113,7 +219,6 @@ constexpr int kMcicaWarps = 5;   // 5 warps x 22 KB (127 layers): two CTAs, ten 
 
 __global__ void __launch_bounds__(32 * kMcicaWarps)
 lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int ncols, McicaArgs a,
-                const double* __restrict__ cldf_dev, const int32_t* __restrict__ seed_dev, int dev_ld,
                 uint32_t* __restrict__ bits) {
   extern __shared__ __align__(16) char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -143,10 +248,10 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
       seed = (a.isubclw == 1) ? 140 + (i + 1) : B.icseed[i];   // RLM:765-773
     } else {
       for (int k = lane; k < nlay; k += 32) {
-        clr[k] = 1.0 - cldf_dev[c + (size_t)dev_ld * k];
+        clr[k] = 1.0 - a.st.cldf[c + (size_t)a.st.ld * k];
       }
       any = true;
-      seed = seed_dev[c];
+      seed = a.st.seed[c];
     }
     if (!__any_sync(0xffffffffu, any)) continue;   // clear column: no draws
     // random_setseed_t: mt(0)=seed (0 -> 4357), mt(i) = 69069*mt(i-1)
@@ -155,6 +260,36 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
     __syncwarp();
 
     uint32_t* out = bits + (size_t)c * NGPT * a.nw;
+    if (a.iovr >= 3) {
+      // second twister state and the per-layer overlap parameter live in the ring's space
+      uint32_t* mtB = ring;
+      double* aux = reinterpret_cast<double*>(ring + 624);
+      const Block* B = (nblocks > 0) ? ((nblocks == 1) ? &b0 : &blocks[find_block(blocks, nblocks, c)]) : nullptr;
+      const int i = B ? c - B->col0 : 0;
+      if (a.iovr == 3) {
+        // fac_lcf(k) = exp(-0.5 (dz(k) + dz(k-1)) / de_lgth), dz in the internal order (RLM:819, 2001)
+        const double dl = B ? B->in[F_DELGTH][i] : a.st.delg[c];
+        for (int k = 1 + lane; k < nlay; k += 32) {
+          double dz0, dz1;
+          if (B) {
+            const int r0 = a.top_at_1 ? nlp1 - (k + 1) - 1 : k, r1 = a.top_at_1 ? nlp1 - k - 1 : k - 1;
+            dz0 = B->in[F_DZLYR][i + (size_t)B->ld * r0];
+            dz1 = B->in[F_DZLYR][i + (size_t)B->ld * r1];
+          } else {
+            dz0 = a.st.dz[c + (size_t)a.st.ld * k];
+            dz1 = a.st.dz[c + (size_t)a.st.ld * (k - 1)];
+          }
+          aux[k] = exp(-0.5 * (dz0 + dz1) / dl);
+        }
+      } else {
+        // alpha is taken in the caller's row order, unflipped (RLM:820, 933)
+        for (int k = lane; k < nlay; k += 32)
+          aux[k] = B ? B->in[F_ALPHA][i + (size_t)B->ld * k] : a.st.alpha[c + (size_t)a.st.ld * k];
+      }
+      __syncwarp();
+      mcica_two_set(mt, mtB, clr, aux, nlay, a.iovr, (uint32_t)(seed == 0 ? 4357 : seed), a.nw, out, lane);
+      continue;
+    }
     if (a.iovr == 2) {
       // maximum overlap: one draw per g-point, the same at every layer (RLM:1981-1993)
       twist(mt, lane);
@@ -230,8 +365,7 @@ cudaError_t mcica_upload_powers() {
 }
 
 cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int ncols, int nlay, int iovr, int isubclw,
-                         int top_at_1, const double* cldf_dev, const int32_t* seed_dev, int dev_ld,
-                         uint32_t* bits, int num_sms, cudaStream_t st) {
+                         int top_at_1, const McicaStage& stage, uint32_t* bits, int num_sms, cudaStream_t st) {
   McicaArgs a;
   a.nlay = nlay;
   a.nw = (nlay + 31) / 32;
@@ -239,6 +373,7 @@ cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int 
   a.isubclw = isubclw;
   a.top_at_1 = top_at_1;
   a.cap = mcica_ring_capacity(nlay);
+  a.st = stage;
   const int wpb = kMcicaWarps;
   size_t smem = mcica_warp_bytes(nlay, a.cap) * wpb;
   int per_sm = 0;
@@ -246,7 +381,7 @@ cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int 
   if (per_sm < 1) per_sm = 1;
   int grid = min((ncols + wpb - 1) / wpb, num_sms * per_sm);
   if (grid < 1) return cudaSuccess;
-  lw_mcica_kernel<<<grid, wpb * 32, smem, st>>>(blocks, nblocks, b0, ncols, a, cldf_dev, seed_dev, dev_ld, bits);
+  lw_mcica_kernel<<<grid, wpb * 32, smem, st>>>(blocks, nblocks, b0, ncols, a, bits);
 #if LW_DEBUG_CHECKS
   {
     cudaError_t e = cudaStreamSynchronize(st);

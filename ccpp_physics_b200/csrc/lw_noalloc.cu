@@ -187,7 +187,7 @@ extern "C" int rrtmg_lw_gpu_run_noalloc(const rrtmg_lw_run_args* a, int32_t prec
   f.want_flxprf = a->flxprf != nullptr;
   f.gas_only = 0;
 
-  e = mcica_launch(nullptr, 1, B, a->npts, a->nlay, a->iovr, a->isubclw, f.top_at_1, nullptr, nullptr, 0, bits,
+  e = mcica_launch(nullptr, 1, B, a->npts, a->nlay, a->iovr, a->isubclw, f.top_at_1, McicaStage(), bits,
                    v.num_sms, st);
   if (e == cudaSuccess) {
     if (precision == RRTMG_LW_FP64) {

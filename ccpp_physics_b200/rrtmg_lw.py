@@ -129,18 +129,20 @@ def rrtmg_lw_run(plyr, plvl, tlyr, tlvl, qlyr, olyr, gasvmr_co2, gasvmr_n2o, gas
     return run_profile(prof, out, precision=precision, stream=stream)
 
 
-def mcica_bits(cldf, seed, iovr=1, stream=None):
+def mcica_bits(cldf, seed, iovr=1, dz=None, de_lgth=None, alpha=None, stream=None):
     """Sub-column cloud flags of ``mcica_subcol`` on the GPU for device
-    tensors cldf (nlay, npts) float64 and seed (npts,) int32.  Returns a
-    (npts, 140, nwords) int32 tensor of bit words (bit k&31 of word k>>5)."""
+    tensors cldf (nlay, npts) float64 and seed (npts,) int32; iovr 3 also
+    takes dz (nlay, npts) [km] and de_lgth (npts,) [km], iovr 4/5 alpha
+    (nlay, npts).  Returns a (npts, 140, nwords) int32 tensor of bit words
+    (bit k&31 of word k>>5)."""
     import torch
     nlay, npts = cldf.shape
     nw = (nlay + 31) // 32
     stream = torch_stream(stream, cldf)
     bits = torch.zeros((npts, abi.NGPT, nw), dtype=torch.int32, device=cldf.device)
+    ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
     msg = C.create_string_buffer(512)
-    rc = lib().rrtmg_lw_gpu_mcica(npts, nlay, npts, iovr, C.c_void_p(seed.data_ptr()),
-                                  C.c_void_p(cldf.data_ptr()), None, None, None,
+    rc = lib().rrtmg_lw_gpu_mcica(npts, nlay, npts, iovr, ptr(seed), ptr(cldf), ptr(dz), ptr(de_lgth), ptr(alpha),
                                   C.c_void_p(bits.data_ptr()), stream, msg, 512)
     if rc:
         raise RRTMGLWError(msg.value.decode())

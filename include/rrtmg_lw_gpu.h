@@ -126,8 +126,9 @@ int rrtmg_lw_gpu_run_ex(const rrtmg_lw_run_args *args,
 /* McICA sub-column generator alone (mcica_subcol, radlw_main.F90:1847-2107,
  * with the GFS Mersenne Twister, mersenne_twister.f:285-372), on the GPU.
  * For each column i: seed[i], cldf (ldim, nlay) layer cloud fraction already
- * floored as in cldprop (radlw_main.F90:1805-1811), dz (ldim, nlay) [km],
- * de_lgth (npts), alpha (ldim, nlay).  Writes lcloudy as bits:
+ * floored as in cldprop (radlw_main.F90:1805-1811), dz (ldim, nlay) [km]
+ * and de_lgth (npts) [km] for iovr 3, alpha (ldim, nlay) for iovr 4/5
+ * (NULL otherwise); every overlap 0..5 of mcica_subcol.  Writes lcloudy as bits:
  * bits[(i*RRTMG_LW_NGPT + ig) * nwords + (k >> 5)] bit (k & 31) for g-point
  * ig (0-based) and layer k (0-based, surface first), nwords = (nlay+31)/32.
  * Device pointers only.  Returns errflg. */

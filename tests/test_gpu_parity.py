@@ -98,9 +98,13 @@ def test_fp64_top_at_1(gpu, orc):
             flip[k] = np.ascontiguousarray(v[..., ::-1, :]) if v.ndim == 3 else np.ascontiguousarray(v[::-1])
     out, ref = _run_both(gpu, orc, flip, flags={"top_at_1": 1}, hlw0=True, hlwb=True, flxprf=True)
     _check_fp64(out, ref)
+    # dz is flipped with the other layer fields, alpha is read unflipped (RLM:819-820)
+    for iovr in (3, 4):
+        out, ref = _run_both(gpu, orc, flip, flags={"top_at_1": 1, "iovr": iovr}, hlw0=True)
+        _check_fp64(out, ref)
 
 
-@pytest.mark.parametrize("iovr,isubclw", [(0, 2), (1, 1), (2, 2)])
+@pytest.mark.parametrize("iovr,isubclw", [(0, 2), (1, 1), (2, 2), (3, 2), (3, 1), (4, 2), (5, 2)])
 def test_fp64_overlap_and_seeds(gpu, orc, iovr, isubclw):
     prof = synthetic.make_profiles(32, 127, seed=21)
     out, ref = _run_both(gpu, orc, prof, flags={"iovr": iovr, "isubclw": isubclw}, hlw0=True)
@@ -154,11 +158,17 @@ def test_mcica_bits_exact(gpu, orc):
     cldf[:, 0] = 1.0
     cldf[10:30, 1] = 1e-7
     seeds = np.array([0, 1, 2**31 - 1, -7] + list(range(100, 100 + npts - 4)), dtype=np.int32)
-    for iovr in (0, 1, 2):
-        bits = gpu.mcica_bits(torch.from_numpy(cldf).cuda(), torch.from_numpy(seeds).cuda(), iovr=iovr)
+    dz = rng.uniform(0.05, 1.5, (nlay, npts))
+    de_lgth = rng.uniform(0.5, 4.0, npts)
+    alpha = rng.uniform(0.0, 1.0, (nlay, npts))
+    alpha[:, 2] = 1.0                                 # exactly 1: always correlated
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    for iovr in (0, 1, 2, 3, 4, 5):
+        bits = gpu.mcica_bits(t(cldf), t(seeds), iovr=iovr, dz=t(dz), de_lgth=t(de_lgth), alpha=t(alpha))
         bits = bits.cpu().numpy().view(np.uint32)
         for i in range(npts):
-            ref = orc.mcica(cldf[:, i], int(seeds[i]), iovr=iovr)        # (nlay, 140) bool
+            ref = orc.mcica(cldf[:, i], int(seeds[i]), iovr=iovr, dz=dz[:, i], de_lgth=float(de_lgth[i]),
+                            alpha=alpha[:, i])                       # (nlay, 140) bool
             got = ((bits[i][:, np.arange(nlay) >> 5] >> (np.arange(nlay) & 31)) & 1).astype(bool).T
             assert np.array_equal(got, ref), (iovr, i)
 
