@@ -1049,102 +1049,76 @@ void taumol(Col& c) {
 }
 
 // ---- rtrnmc (RLM:3420-3785) ----------------------------------------------
-void rtrnmc(Col& c, bool lhlw0, bool lhlwb) {
-  const int nlay = c.nlay;
-  const double rec_6 = 0.166667;
-  std::vector<double> clrurad((size_t)(nlay + 1) * 16, 0.0), clrdrad(clrurad), toturad(clrurad), totdrad(clrurad);
-  auto R = [&](std::vector<double>& v, int k, int ib) -> double& { return v[k + (nlay + 1) * (ib - 1)]; };
-  std::vector<double> gassrcu(nlay + 1), totsrcu(nlay + 1), trngas(nlay + 1), efclrfr(nlay + 1), rfdelp(nlay + 1),
-      fnet(nlay + 1), fnetc(nlay + 1);
-  for (int k = 0; k <= nlay; ++k) c.totuflux[k] = c.totdflux[k] = c.totuclfl[k] = c.totdclfl[k] = f_zero;
+// Band radiances of a transfer routine, (0:nlay, nbands) each.
+struct BandRad {
+  int nlay;
+  std::vector<double> tu, td, cu, cd;   // total up/down, clear up/down
+  explicit BandRad(int n) : nlay(n), tu((size_t)(n + 1) * 16, 0.0), td(tu), cu(tu), cd(tu) {}
+  double& at(std::vector<double>& v, int k, int ib) { return v[k + (nlay + 1) * (ib - 1)]; }
+};
 
-  for (int ig = 1; ig <= NGPT; ++ig) {
-    int ib = ngb[ig - 1];
-    double radtotd = f_zero, radclrd = f_zero;
-    for (int k = nlay; k >= 1; --k) {
-      double odepth = std::max(f_zero, c.secdiff[ib - 1] * c.TAUTOT(ig, k));
-      double atrgas, trng, gasfac;
-      if (odepth <= 0.06) {
-        atrgas = odepth - 0.5 * odepth * odepth;
-        trng = f_one - atrgas;
-        gasfac = rec_6 * odepth;
-      } else {
-        double tblind = odepth / (bpade + odepth);
-        int itgas = (int)(tblint * tblind + 0.5);
-        trng = exp_tbl[itgas];
-        atrgas = f_one - trng;
-        gasfac = tfn_tbl[itgas];
-        odepth = tau_tbl[itgas];
-      }
-      double plfrac = c.FRACS(ig, k);
-      double blay = c.PKLAY(ib, k);
-      double dplnku = c.PKLEV(ib, k) - blay;
-      double dplnkd = c.PKLEV(ib, k - 1) - blay;
-      double bbdgas = plfrac * (blay + dplnkd * gasfac);
-      double bbugas = plfrac * (blay + dplnku * gasfac);
-      double gassrcd = bbdgas * atrgas;
-      gassrcu[k] = bbugas * atrgas;
-      trngas[k] = trng;
-      double clfm = c.CLDFMC(ig, k);
-      if (clfm >= eps) {
-        double odcld = c.secdiff[ib - 1] * c.TAUCLD(ib, k);
-        efclrfr[k] = f_one - (f_one - std::exp(-odcld)) * clfm;
-        double odtot = odepth + odcld;
-        double totfac, atrtot;
-        if (odtot < 0.06) {
-          totfac = rec_6 * odtot;
-          atrtot = odtot - 0.5 * odtot * odtot;
-        } else {
-          double tblind = odtot / (bpade + odtot);
-          int ittot = (int)(tblint * tblind + 0.5);
-          totfac = tfn_tbl[ittot];
-          atrtot = f_one - exp_tbl[ittot];
-        }
-        double bbdtot = plfrac * (blay + dplnkd * totfac);
-        double bbutot = plfrac * (blay + dplnku * totfac);
-        double totsrcd = bbdtot * atrtot;
-        totsrcu[k] = bbutot * atrtot;
-        radtotd = radtotd * trng * efclrfr[k] + gassrcd + clfm * (totsrcd - gassrcd);
-        R(totdrad, k - 1, ib) = R(totdrad, k - 1, ib) + radtotd;
-        radclrd = radclrd * trng + gassrcd;
-        R(clrdrad, k - 1, ib) = R(clrdrad, k - 1, ib) + radclrd;
-      } else {
-        radtotd = radtotd * trng + gassrcd;
-        R(totdrad, k - 1, ib) = R(totdrad, k - 1, ib) + radtotd;
-        radclrd = radclrd * trng + gassrcd;
-        R(clrdrad, k - 1, ib) = R(clrdrad, k - 1, ib) + radclrd;
-      }
-    }
-    double reflct = f_one - c.semiss[ib - 1];
-    double rad0 = c.semiss[ib - 1] * c.FRACS(ig, 1) * c.PKLAY(ib, 0);
-    double radtotu = rad0 + reflct * radtotd;
-    R(toturad, 0, ib) = R(toturad, 0, ib) + radtotu;
-    double radclru = rad0 + reflct * radclrd;
-    R(clrurad, 0, ib) = R(clrurad, 0, ib) + radclru;
-    for (int k = 1; k <= nlay; ++k) {
-      double clfm = c.CLDFMC(ig, k);
-      double trng = trngas[k];
-      double gasu = gassrcu[k];
-      if (clfm > eps) {
-        radtotu = radtotu * trng * efclrfr[k] + gasu + clfm * (totsrcu[k] - gasu);
-        R(toturad, k, ib) = R(toturad, k, ib) + radtotu;
-        radclru = radclru * trng + gasu;
-        R(clrurad, k, ib) = R(clrurad, k, ib) + radclru;
-      } else {
-        radtotu = radtotu * trng + gasu;
-        R(toturad, k, ib) = R(toturad, k, ib) + radtotu;
-        radclru = radclru * trng + gasu;
-        R(clrurad, k, ib) = R(clrurad, k, ib) + radclru;
-      }
-    }
+// Gas part of one layer of one g-point, shared by rtrnmc/rtrn/rtrnmr
+// (RLM:3598-3627, 2601-2627, 3174-3200): transmittance, down/up sources.
+struct GasLayer {
+  double trng, odepth, gassrcd, gassrcu, plfrac, blay, dplnku, dplnkd;
+};
+GasLayer gas_layer(Col& c, int ig, int ib, int k) {
+  const double rec_6 = 0.166667;
+  GasLayer g;
+  double odepth = std::max(f_zero, c.secdiff[ib - 1] * c.TAUTOT(ig, k));
+  double atrgas, gasfac;
+  if (odepth <= 0.06) {
+    atrgas = odepth - 0.5 * odepth * odepth;
+    g.trng = f_one - atrgas;
+    gasfac = rec_6 * odepth;
+  } else {
+    double tblind = odepth / (bpade + odepth);
+    int itgas = (int)(tblint * tblind + 0.5);
+    g.trng = exp_tbl[itgas];
+    atrgas = f_one - g.trng;
+    gasfac = tfn_tbl[itgas];
+    odepth = tau_tbl[itgas];
   }
+  g.odepth = odepth;
+  g.plfrac = c.FRACS(ig, k);
+  g.blay = c.PKLAY(ib, k);
+  g.dplnku = c.PKLEV(ib, k) - g.blay;
+  g.dplnkd = c.PKLEV(ib, k - 1) - g.blay;
+  const double bbdgas = g.plfrac * (g.blay + g.dplnkd * gasfac);
+  const double bbugas = g.plfrac * (g.blay + g.dplnku * gasfac);
+  g.gassrcd = bbdgas * atrgas;
+  g.gassrcu = bbugas * atrgas;
+  return g;
+}
+
+// Cloudy part: total optical depth table terms (RLM:3636-3650).
+void tot_layer(double odtot, double& totfac, double& atrtot, double& trnt) {
+  const double rec_6 = 0.166667;
+  if (odtot < 0.06) {
+    totfac = rec_6 * odtot;
+    atrtot = odtot - 0.5 * odtot * odtot;
+    trnt = f_one - atrtot;
+  } else {
+    double tblind = odtot / (bpade + odtot);
+    int ittot = (int)(tblint * tblind + 0.5);
+    totfac = tfn_tbl[ittot];
+    trnt = exp_tbl[ittot];
+    atrtot = f_one - trnt;
+  }
+}
+
+// Fluxes and heating rates from the band radiances (RLM:3737-3785).
+void finish_fluxes(Col& c, BandRad& br, bool lhlw0, bool lhlwb) {
+  const int nlay = c.nlay;
+  std::vector<double> rfdelp(nlay + 1), fnet(nlay + 1), fnetc(nlay + 1);
+  for (int k = 0; k <= nlay; ++k) c.totuflux[k] = c.totdflux[k] = c.totuclfl[k] = c.totdclfl[k] = f_zero;
   double flxfac = wtdiff * fluxfac;
   for (int k = 0; k <= nlay; ++k) {
     for (int ib = 1; ib <= NBANDS; ++ib) {
-      c.totuflux[k] = c.totuflux[k] + R(toturad, k, ib);
-      c.totdflux[k] = c.totdflux[k] + R(totdrad, k, ib);
-      c.totuclfl[k] = c.totuclfl[k] + R(clrurad, k, ib);
-      c.totdclfl[k] = c.totdclfl[k] + R(clrdrad, k, ib);
+      c.totuflux[k] = c.totuflux[k] + br.at(br.tu, k, ib);
+      c.totdflux[k] = c.totdflux[k] + br.at(br.td, k, ib);
+      c.totuclfl[k] = c.totuclfl[k] + br.at(br.cu, k, ib);
+      c.totdclfl[k] = c.totdclfl[k] + br.at(br.cd, k, ib);
     }
     c.totuflux[k] = c.totuflux[k] * flxfac;
     c.totdflux[k] = c.totdflux[k] * flxfac;
@@ -1166,13 +1140,226 @@ void rtrnmc(Col& c, bool lhlw0, bool lhlwb) {
   }
   if (lhlwb) {
     for (int ib = 1; ib <= NBANDS; ++ib) {
-      fnet[0] = (R(toturad, 0, ib) - R(totdrad, 0, ib)) * flxfac;
+      fnet[0] = (br.at(br.tu, 0, ib) - br.at(br.td, 0, ib)) * flxfac;
       for (int k = 1; k <= nlay; ++k) {
-        fnet[k] = (R(toturad, k, ib) - R(totdrad, k, ib)) * flxfac;
+        fnet[k] = (br.at(br.tu, k, ib) - br.at(br.td, k, ib)) * flxfac;
         c.HTRB(k, ib) = (fnet[k - 1] - fnet[k]) * rfdelp[k];
       }
     }
   }
+}
+
+// rtrnmc (RLM:3420-3785) and rtrn (RLM:2445-2800).  They differ only in the
+// cloud fraction of a layer -- McICA's 0/1 sub-column flag cldfmc(ig,k) or the
+// layer fraction cldfrc(k) -- and in the up-sweep cloud test (strict > eps in
+// rtrnmc, >= eps in rtrn).
+void rtrn_random(Col& c, bool lhlw0, bool lhlwb, bool mcica) {
+  const int nlay = c.nlay;
+  BandRad br(nlay);
+  std::vector<double> gassrcu(nlay + 1), totsrcu(nlay + 1), trngas(nlay + 1), efclrfr(nlay + 1);
+  auto clfr_of = [&](int ig, int k) { return mcica ? c.CLDFMC(ig, k) : c.cldfrc[k]; };
+  for (int ig = 1; ig <= NGPT; ++ig) {
+    int ib = ngb[ig - 1];
+    double radtotd = f_zero, radclrd = f_zero;
+    for (int k = nlay; k >= 1; --k) {
+      GasLayer g = gas_layer(c, ig, ib, k);
+      gassrcu[k] = g.gassrcu;
+      trngas[k] = g.trng;
+      double clfm = clfr_of(ig, k);
+      if (clfm >= eps) {
+        double odcld = c.secdiff[ib - 1] * c.TAUCLD(ib, k);
+        efclrfr[k] = f_one - (f_one - std::exp(-odcld)) * clfm;
+        double totfac, atrtot, trnt;
+        tot_layer(g.odepth + odcld, totfac, atrtot, trnt);
+        double bbdtot = g.plfrac * (g.blay + g.dplnkd * totfac);
+        double bbutot = g.plfrac * (g.blay + g.dplnku * totfac);
+        double totsrcd = bbdtot * atrtot;
+        totsrcu[k] = bbutot * atrtot;
+        radtotd = radtotd * g.trng * efclrfr[k] + g.gassrcd + clfm * (totsrcd - g.gassrcd);
+      } else {
+        radtotd = radtotd * g.trng + g.gassrcd;
+      }
+      br.at(br.td, k - 1, ib) = br.at(br.td, k - 1, ib) + radtotd;
+      radclrd = radclrd * g.trng + g.gassrcd;
+      br.at(br.cd, k - 1, ib) = br.at(br.cd, k - 1, ib) + radclrd;
+    }
+    double reflct = f_one - c.semiss[ib - 1];
+    double rad0 = c.semiss[ib - 1] * c.FRACS(ig, 1) * c.PKLAY(ib, 0);
+    double radtotu = rad0 + reflct * radtotd;
+    br.at(br.tu, 0, ib) = br.at(br.tu, 0, ib) + radtotu;
+    double radclru = rad0 + reflct * radclrd;
+    br.at(br.cu, 0, ib) = br.at(br.cu, 0, ib) + radclru;
+    for (int k = 1; k <= nlay; ++k) {
+      double clfm = clfr_of(ig, k);
+      double trng = trngas[k];
+      double gasu = gassrcu[k];
+      if (mcica ? (clfm > eps) : (clfm >= eps)) {
+        radtotu = radtotu * trng * efclrfr[k] + gasu + clfm * (totsrcu[k] - gasu);
+      } else {
+        radtotu = radtotu * trng + gasu;
+      }
+      br.at(br.tu, k, ib) = br.at(br.tu, k, ib) + radtotu;
+      radclru = radclru * trng + gasu;
+      br.at(br.cu, k, ib) = br.at(br.cu, k, ib) + radclru;
+    }
+  }
+  finish_fluxes(c, br, lhlw0, lhlwb);
+}
+
+void rtrnmc(Col& c, bool lhlw0, bool lhlwb) { rtrn_random(c, lhlw0, lhlwb, true); }
+
+// Maximum-random overlap coefficients of rtrnmr (RLM:2921-3092) in one
+// direction.  With dir = +1 (upward sweep) layer k pairs with k+1 and looks
+// back at k-1; with dir = -1 (downward) it pairs with k-1 and looks back at
+// k+1.  The factors of the pair (k, k+dir) are stored at index k+dir.
+struct MrFactors {
+  std::vector<double> clr1, clr2, cld1, cld2, cmb1, cmb2;
+  std::vector<char> lst;
+  explicit MrFactors(int n) : clr1(n + 2, 0.0), clr2(clr1), cld1(clr1), cld2(clr1), cmb1(clr1), cmb2(clr1), lst(n + 2, 0) {}
+};
+void mr_factors(const Col& c, int dir, MrFactors& f) {
+  const int nlay = c.nlay;
+  const std::vector<double>& cf = c.cldfrc;   // 0:nlp1, padded with 1 and 0
+  const int k0 = dir > 0 ? 1 : nlay, k1 = dir > 0 ? nlay - 1 : 2;
+  f.lst[k0] = cf[k0] > eps;
+  double rat1 = f_zero, rat2 = f_zero;
+  for (int k = k0; dir > 0 ? k <= k1 : k >= k1; k += dir) {
+    const int kn = k + dir, kb = k - dir;   // next layer in the sweep, the one behind
+    f.lst[kn] = cf[kn] > eps && cf[k] <= eps;
+    if (!(cf[k] > eps)) continue;
+    if (cf[kn] >= cf[k]) {
+      if (f.lst[k]) {
+        if (cf[k] < f_one) f.clr2[kn] = (cf[kn] - cf[k]) / (f_one - cf[k]);
+        f.clr2[k] = f_zero;
+        f.cld2[k] = f_zero;
+      } else {
+        double fmax = std::max(cf[k], cf[kb]);
+        if (cf[kn] > fmax) {
+          f.clr1[kn] = rat2;
+          f.clr2[kn] = (cf[kn] - fmax) / (f_one - fmax);
+        } else if (cf[kn] < fmax) {
+          f.clr1[kn] = (cf[kn] - cf[k]) / (cf[kb] - cf[k]);
+        } else {
+          f.clr1[kn] = rat2;
+        }
+      }
+      if (f.clr1[kn] > f_zero || f.clr2[kn] > f_zero) { rat1 = f_one; rat2 = f_zero; }
+      else { rat1 = f_zero; rat2 = f_zero; }
+    } else {
+      if (f.lst[k]) {
+        f.cld2[kn] = (cf[k] - cf[kn]) / cf[k];
+        f.clr2[k] = f_zero;
+        f.cld2[k] = f_zero;
+      } else {
+        double fmin = std::min(cf[k], cf[kb]);
+        if (cf[kn] <= fmin) {
+          f.cld1[kn] = rat1;
+          f.cld2[kn] = (fmin - cf[kn]) / fmin;
+        } else {
+          f.cld1[kn] = (cf[k] - cf[kn]) / (cf[k] - fmin);
+        }
+      }
+      if (f.cld1[kn] > f_zero || f.cld2[kn] > f_zero) { rat1 = f_zero; rat2 = f_one; }
+      else { rat1 = f_zero; rat2 = f_zero; }
+    }
+    f.cmb1[kn] = f.clr1[kn] * f.cld2[k] * cf[kb];
+    f.cmb2[kn] = f.cld1[kn] * f.clr2[k] * (f_one - cf[kb]);
+  }
+}
+
+// rtrnmr (RLM:2828-3392): maximum-random overlap of the layer cloud fractions.
+// The split radiances (totradd, clrradd, rad and their upward twins) are
+// reset at the first cloudy layer of every cloud block; a layer with a cloud
+// fraction of exactly eps is "cloudy" without starting a block, where the
+// Fortran reads the values left by the previous g-point -- here they start
+// from zero for every g-point.
+void rtrnmr(Col& c, bool lhlw0, bool lhlwb) {
+  const int nlay = c.nlay;
+  MrFactors up(nlay), dn(nlay);
+  mr_factors(c, +1, up);
+  mr_factors(c, -1, dn);
+  BandRad br(nlay);
+  std::vector<double> gassrcu(nlay + 1), totsrcu(nlay + 1), trngas(nlay + 1), trntot(nlay + 1);
+  for (int ig = 1; ig <= NGPT; ++ig) {
+    int ib = ngb[ig - 1];
+    double radtotd = f_zero, radclrd = f_zero;
+    double totradd = f_zero, clrradd = f_zero, rad = f_zero;
+    for (int k = nlay; k >= 1; --k) {
+      GasLayer g = gas_layer(c, ig, ib, k);
+      gassrcu[k] = g.gassrcu;
+      trngas[k] = g.trng;
+      double clfr = c.cldfrc[k];
+      if (dn.lst[k]) {
+        totradd = clfr * radtotd;
+        clrradd = radtotd - totradd;
+        rad = f_zero;
+      }
+      if (clfr >= eps) {
+        double odcld = c.secdiff[ib - 1] * c.TAUCLD(ib, k);
+        double totfac, atrtot, trnt;
+        tot_layer(g.odepth + odcld, totfac, atrtot, trnt);
+        double bbdtot = g.plfrac * (g.blay + g.dplnkd * totfac);
+        double bbutot = g.plfrac * (g.blay + g.dplnku * totfac);
+        double totsrcd = bbdtot * atrtot;
+        totsrcu[k] = bbutot * atrtot;
+        trntot[k] = trnt;
+        totradd = totradd * trnt + clfr * totsrcd;
+        clrradd = clrradd * g.trng + (f_one - clfr) * g.gassrcd;
+        radtotd = totradd + clrradd;
+        br.at(br.td, k - 1, ib) = br.at(br.td, k - 1, ib) + radtotd;
+        radclrd = radclrd * g.trng + g.gassrcd;
+        br.at(br.cd, k - 1, ib) = br.at(br.cd, k - 1, ib) + radclrd;
+        double radmod = rad * (dn.clr1[k - 1] * g.trng + dn.cld1[k - 1] * trnt) - dn.cmb1[k - 1] * g.gassrcd +
+                        dn.cmb2[k - 1] * totsrcd;
+        rad = -radmod + dn.clr2[k - 1] * (clrradd + radmod) - dn.cld2[k - 1] * (totradd - radmod);
+        totradd = totradd + rad;
+        clrradd = clrradd - rad;
+      } else {
+        radtotd = radtotd * g.trng + g.gassrcd;
+        br.at(br.td, k - 1, ib) = br.at(br.td, k - 1, ib) + radtotd;
+        radclrd = radclrd * g.trng + g.gassrcd;
+        br.at(br.cd, k - 1, ib) = br.at(br.cd, k - 1, ib) + radclrd;
+      }
+    }
+    double reflct = f_one - c.semiss[ib - 1];
+    double rad0 = c.semiss[ib - 1] * c.FRACS(ig, 1) * c.PKLAY(ib, 0);
+    double radtotu = rad0 + reflct * radtotd;
+    br.at(br.tu, 0, ib) = br.at(br.tu, 0, ib) + radtotu;
+    double radclru = rad0 + reflct * radclrd;
+    br.at(br.cu, 0, ib) = br.at(br.cu, 0, ib) + radclru;
+    double totradu = f_zero, clrradu = f_zero;
+    for (int k = 1; k <= nlay; ++k) {
+      double clfr = c.cldfrc[k];
+      double trng = trngas[k];
+      double gasu = gassrcu[k];
+      if (up.lst[k]) {
+        totradu = clfr * radtotu;
+        clrradu = radtotu - totradu;
+        rad = f_zero;
+      }
+      if (clfr >= eps) {
+        double trnt = trntot[k];
+        double totu = totsrcu[k];
+        totradu = totradu * trnt + clfr * totu;
+        clrradu = clrradu * trng + (f_one - clfr) * gasu;
+        radtotu = totradu + clrradu;
+        br.at(br.tu, k, ib) = br.at(br.tu, k, ib) + radtotu;
+        radclru = radclru * trng + gasu;
+        br.at(br.cu, k, ib) = br.at(br.cu, k, ib) + radclru;
+        double radmod = rad * (up.clr1[k + 1] * trng + up.cld1[k + 1] * trnt) - up.cmb1[k + 1] * gasu +
+                        up.cmb2[k + 1] * totu;
+        rad = -radmod + up.clr2[k + 1] * (clrradu + radmod) - up.cld2[k + 1] * (totradu - radmod);
+        totradu = totradu + rad;
+        clrradu = clrradu - rad;
+      } else {
+        radtotu = radtotu * trng + gasu;
+        br.at(br.tu, k, ib) = br.at(br.tu, k, ib) + radtotu;
+        radclru = radclru * trng + gasu;
+        br.at(br.cu, k, ib) = br.at(br.cu, k, ib) + radclru;
+      }
+    }
+  }
+  finish_fluxes(c, br, lhlw0, lhlwb);
 }
 
 inline void set_err(char* errmsg, int len, const std::string& s) {
@@ -1288,7 +1475,12 @@ void run_column(const rrtmg_lw_run_args& a, int iplon, int ipseed, Col& c) {
   }
   setcoef(c);
   taumol(c);
-  rtrnmc(c, a.hlw0 != nullptr, a.hlwb != nullptr);
+  if (a.isubclw <= 0) {   // RLM:1190-1224
+    if (a.iovr <= 0) rtrn_random(c, a.hlw0 != nullptr, a.hlwb != nullptr, false);
+    else rtrnmr(c, a.hlw0 != nullptr, a.hlwb != nullptr);
+  } else {
+    rtrnmc(c, a.hlw0 != nullptr, a.hlwb != nullptr);
+  }
   a.topflx[2 * (iplon - 1) + 0] = c.totuflux[nlay];
   a.topflx[2 * (iplon - 1) + 1] = c.totuclfl[nlay];
   a.sfcflx[4 * (iplon - 1) + 0] = c.totuflux[0];
@@ -1382,8 +1574,8 @@ int oracle_rrtmg_lw_run(const rrtmg_lw_run_args* a, int nthreads, char* errmsg, 
     set_err(errmsg, errmsg_len, "Logic error: ilwcliq<=0 requires the following optional argument to be present: cld_od");
     return 1;
   }
-  if (a->isubclw <= 0 || a->isubclw > 2) {
-    set_err(errmsg, errmsg_len, "oracle: only the McICA paths isubclw=1,2 (rtrnmc) are restated");
+  if (a->isubclw < 0 || a->isubclw > 2) {
+    set_err(errmsg, errmsg_len, "oracle: isubclw must be 0 (rtrn/rtrnmr), 1 or 2 (McICA, rtrnmc)");
     return 1;
   }
 #ifdef _OPENMP

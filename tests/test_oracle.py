@@ -191,3 +191,36 @@ def test_mcica_draw_conversion_exhaustive(oracle_lib):
     bad = oracle_lib.lib().oracle_check_u32_unit(0, 1 << 32)
     assert bad == 0
     assert time.time() - t0 < 120
+
+
+def test_grid_cloud_transfer_properties(oracle_lib):
+    """rtrn (random) and rtrnmr (maximum-random), the isubclw=0 transfer: with
+    overcast or clear layers only, rtrn gives McICA's fluxes (its sub-columns
+    are then all cloudy or all clear, same equations), and rtrnmr agrees to
+    the Pade-table quantisation (it takes the cloudy transmittance from the
+    total optical depth's table entry, RLM:3193-3202, not trng * exp(-odcld));
+    with partial clouds maximum-random overlap gives more OLR than random
+    overlap (fewer distinct cloud layers seen from above)."""
+    import numpy as np
+    prof = synthetic.make_profiles(24, 60, seed=12)
+    cf = prof["cld_cf"]
+    cf[:] = np.where(cf > 0, 1.0, 0.0)            # overcast or clear layers only
+    outs = {}
+    for name, flags in (("mc", dict(isubclw=2, iovr=1)), ("rand", dict(isubclw=0, iovr=0)),
+                        ("mr", dict(isubclw=0, iovr=1))):
+        rc, msg, o = oracle_lib.rrtmg_lw_run(prof, flags=flags, hlw0=True, hlwb=True)
+        assert rc == 0, msg
+        outs[name] = o
+    for k in ("topflx", "sfcflx", "hlwc", "hlw0", "hlwb"):
+        np.testing.assert_allclose(outs["rand"][k], outs["mc"][k], rtol=1e-12, atol=1e-12, err_msg=k)
+        np.testing.assert_allclose(outs["mr"][k], outs["mc"][k], rtol=2e-3, atol=2e-2, err_msg=k)
+    prof = synthetic.make_profiles(24, 60, seed=13)
+    prof["cld_cf"][:] = np.clip(prof["cld_cf"] * 0.7 + 0.2 * (prof["cld_cf"] > 0), 0, 1)
+    rc, msg, r = oracle_lib.rrtmg_lw_run(prof, flags=dict(isubclw=0, iovr=0))
+    rc2, msg2, m = oracle_lib.rrtmg_lw_run(prof, flags=dict(isubclw=0, iovr=1))
+    assert rc == 0 and rc2 == 0
+    assert np.all(np.isfinite(m["topflx"])) and np.all(np.isfinite(m["hlwc"]))
+    # (up to the table-vs-exp difference of the two routines' cloudy transmittance)
+    assert np.all(m["topflx"][:, 0] >= r["topflx"][:, 0] - 0.01)
+    assert np.mean(m["topflx"][:, 0]) > np.mean(r["topflx"][:, 0]) + 0.1
+    assert np.array_equal(m["topflx"][:, 1], r["topflx"][:, 1])   # clear-sky parts agree exactly
