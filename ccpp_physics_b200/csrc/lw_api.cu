@@ -276,9 +276,10 @@ int validate(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg, i
     set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: nlay=%d exceeds the supported maximum of 255 layers", a->nlay);
     return 1;
   }
-  if (a->isubclw != 1 && a->isubclw != 2) {
+  if (a->isubclw < 0 || a->isubclw > 2) {
     set_msg(errmsg, errmsg_len,
-            "rrtmg_lw_gpu: isubclw=%d not supported (the McICA paths isubclw=1,2 with rtrnmc are)", a->isubclw);
+            "rrtmg_lw_gpu: isubclw=%d not supported (0: grid-mean clouds with rtrn/rtrnmr; 1, 2: McICA with rtrnmc)",
+            a->isubclw);
     return 1;
   }
   if (a->iovr < 0 || a->iovr > 5) {

@@ -9,6 +9,7 @@
 
 #include "lw_launch.h"
 #include "lw_rt.cuh"
+#include "lw_rt_grid.cuh"
 
 #define REAL float
 #define LW_SCRATCH_FN scratch_per_column_fp32

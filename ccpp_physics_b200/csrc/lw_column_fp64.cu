@@ -11,6 +11,7 @@
 
 #include "lw_launch.h"
 #include "lw_rt.cuh"
+#include "lw_rt_grid.cuh"
 
 #define REAL double
 #define LW_SCRATCH_FN scratch_per_column_fp64

@@ -113,7 +113,10 @@ typedef struct rrtmg_lw_exec {
 int rrtmg_lw_gpu_init(const rrtmg_lw_init_args *args, char *errmsg,
                       int32_t errmsg_len);
 
-/* rrtmg_lw_run (radlw_main.F90:419) on the GPU, FP64, host pointers.
+/* rrtmg_lw_run (radlw_main.F90:419) on the GPU, FP64, host pointers.  Every
+ * cloud treatment of the reference: isubclw = 1, 2 (McICA with overlap iovr
+ * 0..5, transfer rtrnmc) and isubclw = 0 (grid-mean clouds, transfer rtrn for
+ * iovr <= 0 and rtrnmr otherwise, radlw_main.F90:1190-1224).
  * Returns errflg. */
 int rrtmg_lw_gpu_run(const rrtmg_lw_run_args *args, char *errmsg,
                      int32_t errmsg_len);

@@ -230,3 +230,28 @@ def test_fp32_error_bounds(gpu, orc):
     hr_rmse = np.sqrt(np.mean((out["hlwc"] - ref["hlwc"]) ** 2))
     assert flux_rmse < 0.05 and top_rmse < 0.05, (flux_rmse, top_rmse)   # W/m2
     assert hr_rmse < 0.05, hr_rmse                                      # K/day
+
+
+@pytest.mark.parametrize("iovr", [0, 1])
+def test_fp64_grid_cloud_transfer(gpu, orc, iovr):
+    """isubclw=0: grid-mean clouds through rtrn (iovr 0, random overlap) and
+    rtrnmr (iovr 1, maximum-random overlap), RLM:1190-1224, with partial
+    cloud fractions, cloud blocks and gaps, both vertical orders and every
+    optional output."""
+    prof = synthetic.make_profiles(40, 127, seed=31)
+    cf = prof["cld_cf"]
+    cf[:] = np.clip(cf * 0.8 + 0.15 * (cf > 0), 0.0, 1.0)
+    cf[40:50, 3] = 1.0                   # overcast block over partial layers
+    cf[60:62, 4] = 1e-6                  # exactly eps: cloudy in the transfer, not a block start
+    flags = {"isubclw": 0, "iovr": iovr}
+    out, ref = _run_both(gpu, orc, prof, flags=flags, hlw0=True, hlwb=True, flxprf=True)
+    _check_fp64(out, ref)
+    flip = dict(prof)
+    for k, v in prof.items():
+        if isinstance(v, np.ndarray) and v.ndim >= 2 and k != "alpha":
+            flip[k] = np.ascontiguousarray(v[..., ::-1, :]) if v.ndim == 3 else np.ascontiguousarray(v[::-1])
+    out, ref = _run_both(gpu, orc, flip, flags=dict(flags, top_at_1=1), hlw0=True)
+    _check_fp64(out, ref)
+    out32, ref = _run_both(gpu, orc, prof, precision="fp32", flags=flags, hlw0=True)
+    assert np.max(np.abs(out32["topflx"] - ref["topflx"])) < 0.05
+    assert np.max(np.abs(out32["hlwc"] - ref["hlwc"])) < 0.05
