@@ -75,6 +75,11 @@ struct Workspace {
   Block* hblocks = nullptr;   // pinned host copy of the descriptors
   size_t hblocks_n = 0;
   uint64_t gen = 0;           // bumped whenever bits/scratch move (graphs hold their addresses)
+  // pipelined host-memory calls: copy streams, double-buffered staging, events
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+  char* pbuf = nullptr;
+  size_t pbuf_bytes = 0;
   std::vector<GraphEntry*> graphs;
 };
 
@@ -371,7 +376,7 @@ void block_from_args(const rrtmg_lw_run_args* a, Block* B) {
   B->npts = a->npts;
   B->ld = a->ldim > 0 ? a->ldim : a->npts;
   B->col0 = 0;
-  B->pad = 0;
+  B->seed0 = 0;
 }
 
 // grow() for the buffers captured graphs refer to
@@ -559,6 +564,127 @@ int launch_graph(Workspace* w, cudaStream_t st, const std::vector<Block>& hb, in
 
 }  // namespace
 
+namespace {
+
+// Columns per chunk of a pipelined host-memory call (calls with fewer than two
+// chunks' worth of columns run unpipelined).
+constexpr int kHostChunk = 4096;
+
+// One field of the caller's Fortran arrays: `rows` rows of `width` elements
+// per column (1 = plain (ldim, rows) layout; 2 or 4 = the derived-type records
+// topflx/sfcflx/flxprf) at pitch `width * ldim`; rows == 0 means a 1-D
+// (npts) field.
+struct HostField {
+  const void* h;      // caller's array
+  void** dslot;       // where the staged device pointer goes (in the run_args copy)
+  int rows, width, elem;
+  bool out;
+};
+
+// rrtmg_lw_run on host memory with the copies overlapped with the kernels:
+// chunk j+1's inputs travel host -> device on one copy stream and chunk j-1's
+// outputs device -> host on another while chunk j computes.  Staging is
+// double-buffered; events order the reuse of each buffer.
+int run_host_pipelined(Workspace* w, const rrtmg_lw_run_args* a, const Flags& f0, int precision, cudaStream_t st,
+                       char* errmsg, int32_t errmsg_len) {
+  const int npts = a->npts, nlay = a->nlay, nlp1 = nlay + 1;
+  const size_t ld = a->ldim > 0 ? (size_t)a->ldim : (size_t)npts;
+  rrtmg_lw_run_args d = *a;
+  std::vector<HostField> fl;
+  auto in2 = [&](const double* const* p, int rows) {
+    if (*p) fl.push_back({*p, (void**)const_cast<const double**>(p), rows, 1, 8, false});
+  };
+  in2(&d.plyr, nlay); in2(&d.plvl, nlp1); in2(&d.tlyr, nlay); in2(&d.tlvl, nlp1); in2(&d.qlyr, nlay);
+  in2(&d.olyr, nlay); in2(&d.gasvmr_co2, nlay); in2(&d.gasvmr_n2o, nlay); in2(&d.gasvmr_ch4, nlay);
+  in2(&d.gasvmr_o2, nlay); in2(&d.gasvmr_co, nlay); in2(&d.gasvmr_cfc11, nlay); in2(&d.gasvmr_cfc12, nlay);
+  in2(&d.gasvmr_cfc22, nlay); in2(&d.gasvmr_ccl4, nlay); in2(&d.aeraod, nlay * NBANDS);
+  in2(&d.aerssa, nlay * NBANDS); in2(&d.sfemis, 0); in2(&d.sfgtmp, 0); in2(&d.dzlyr, nlay); in2(&d.delpin, nlay);
+  in2(&d.de_lgth, 0); in2(&d.alpha, nlay); in2(&d.cld_cf, nlay); in2(&d.cld_lwp, nlay); in2(&d.cld_ref_liq, nlay);
+  in2(&d.cld_iwp, nlay); in2(&d.cld_ref_ice, nlay); in2(&d.cld_rwp, nlay); in2(&d.cld_ref_rain, nlay);
+  in2(&d.cld_swp, nlay); in2(&d.cld_ref_snow, nlay); in2(&d.cld_od, nlay);
+  if (d.icseed) fl.push_back({d.icseed, (void**)const_cast<const int32_t**>(&d.icseed), 0, 1, 4, false});
+  auto out = [&](double** p, int rows, int width) {
+    if (*p) fl.push_back({*p, (void**)p, rows, width, 8, true});
+  };
+  out(&d.hlwc, nlay, 1); out(&d.topflx, 0, 2); out(&d.sfcflx, 0, 4); out(&d.cldtau, nlay, 1);
+  out(&d.hlw0, nlay, 1); out(&d.hlwb, nlay * NBANDS, 1); out(&d.flxprf, nlp1, 4);
+  // staging of one chunk (kHostChunk columns) and its layout
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  std::vector<size_t> off(fl.size());
+  size_t per = 0;
+  for (size_t k = 0; k < fl.size(); ++k) {
+    off[k] = per;
+    per += al((size_t)std::max(fl[k].rows, 1) * fl[k].width * kHostChunk * fl[k].elem);
+  }
+  CK(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  if (!w->h2d) {
+    CK(cudaStreamCreateWithFlags(&w->h2d, cudaStreamNonBlocking), "cudaStreamCreate");
+    CK(cudaStreamCreateWithFlags(&w->d2h, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (int k = 0; k < 2; ++k) {
+      CK(cudaEventCreateWithFlags(&w->ev_in[k], cudaEventDisableTiming), "cudaEventCreate");
+      CK(cudaEventCreateWithFlags(&w->ev_done[k], cudaEventDisableTiming), "cudaEventCreate");
+      CK(cudaEventCreateWithFlags(&w->ev_out[k], cudaEventDisableTiming), "cudaEventCreate");
+    }
+  }
+  CK(grow(&w->pbuf, &w->pbuf_bytes, 2 * per), "cudaMalloc(staging)");
+  const int kp = kernel_precision(precision, const_cast<Flags*>(&f0));
+  const Shape sh = default_shape(kp, pick_v(nlay));
+  const int nch = (npts + kHostChunk - 1) / kHostChunk;
+  for (int j = 0; j < nch; ++j) {
+    const int b = j & 1, c0 = j * kHostChunk, n = std::min(kHostChunk, npts - c0);
+    char* base = w->pbuf + (size_t)b * per;
+    // inputs: wait until chunk j-2 is done with this buffer
+    if (j >= 2) CK(cudaStreamWaitEvent(w->h2d, w->ev_done[b], 0), "cudaStreamWaitEvent");
+    for (size_t k = 0; k < fl.size(); ++k) {
+      char* dptr = base + off[k];
+      *fl[k].dslot = dptr;
+      if (fl[k].out) continue;
+      const size_t es = fl[k].elem, wdt = (size_t)fl[k].width;
+      const char* hp = static_cast<const char*>(fl[k].h) + (size_t)c0 * wdt * es;
+      if (fl[k].rows == 0)
+        CK(cudaMemcpyAsync(dptr, hp, (size_t)n * wdt * es, cudaMemcpyHostToDevice, w->h2d), "cudaMemcpyAsync(H2D)");
+      else
+        CK(cudaMemcpy2DAsync(dptr, (size_t)n * wdt * es, hp, ld * wdt * es, (size_t)n * wdt * es, fl[k].rows,
+                             cudaMemcpyHostToDevice, w->h2d),
+           "cudaMemcpy2DAsync(H2D)");
+    }
+    CK(cudaEventRecord(w->ev_in[b], w->h2d), "cudaEventRecord");
+    // kernels: after the inputs arrived and chunk j-2's outputs left this buffer
+    CK(cudaStreamWaitEvent(st, w->ev_in[b], 0), "cudaStreamWaitEvent");
+    if (j >= 2) CK(cudaStreamWaitEvent(st, w->ev_out[b], 0), "cudaStreamWaitEvent");
+    rrtmg_lw_run_args dc = d;
+    dc.npts = n;
+    dc.ldim = n;
+    Block B;
+    block_from_args(&dc, &B);
+    B.seed0 = c0;
+    Flags f = f0;
+    int r = launch(w, st, &B, 1, n, f, kp, sh, nullptr, errmsg, errmsg_len);
+    if (r) return r;
+    CK(cudaEventRecord(w->ev_done[b], st), "cudaEventRecord");
+    // outputs back to the caller's arrays
+    CK(cudaStreamWaitEvent(w->d2h, w->ev_done[b], 0), "cudaStreamWaitEvent");
+    for (size_t k = 0; k < fl.size(); ++k) {
+      if (!fl[k].out) continue;
+      const size_t es = fl[k].elem, wdt = (size_t)fl[k].width;
+      char* hp = static_cast<char*>(const_cast<void*>(fl[k].h)) + (size_t)c0 * wdt * es;
+      const char* dptr = base + off[k];
+      if (fl[k].rows == 0)
+        CK(cudaMemcpyAsync(hp, dptr, (size_t)n * wdt * es, cudaMemcpyDeviceToHost, w->d2h), "cudaMemcpyAsync(D2H)");
+      else
+        CK(cudaMemcpy2DAsync(hp, ld * wdt * es, dptr, (size_t)n * wdt * es, (size_t)n * wdt * es, fl[k].rows,
+                             cudaMemcpyDeviceToHost, w->d2h),
+           "cudaMemcpy2DAsync(D2H)");
+    }
+    CK(cudaEventRecord(w->ev_out[b], w->d2h), "cudaEventRecord");
+  }
+  CK(cudaStreamSynchronize(w->d2h), "kernel execution");
+  CK(cudaStreamSynchronize(st), "kernel execution");
+  return 0;
+}
+
+}  // namespace
+
 extern "C" int rrtmg_lw_gpu_run_ex(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg,
                                    int32_t errmsg_len) {
   set_msg(errmsg, errmsg_len, "");
@@ -595,6 +721,9 @@ extern "C" int rrtmg_lw_gpu_run_ex(const rrtmg_lw_run_args* a, const rrtmg_lw_ex
     if (x->sync) CK(cudaStreamSynchronize(st), "kernel execution");
     return 0;
   }
+
+  // host memory, large calls: copies overlapped with the kernels, chunk by chunk
+  if (a->npts >= 2 * kHostChunk && !x->kernel_ms) return run_host_pipelined(w, a, f, x->precision, st, errmsg, errmsg_len);
 
   // host memory: stage every array through the workspace
   FieldSizes fs = sizes_of(a);
@@ -907,6 +1036,14 @@ extern "C" void rrtmg_lw_gpu_finalize(void) {
     for (GraphEntry* e : w->graphs) drop_graph(e);
     w->graphs.clear();
     if (w->dbuf) cudaFree(w->dbuf);
+    if (w->pbuf) cudaFree(w->pbuf);
+    if (w->h2d) cudaStreamDestroy(w->h2d);
+    if (w->d2h) cudaStreamDestroy(w->d2h);
+    for (int k = 0; k < 2; ++k) {
+      if (w->ev_in[k]) cudaEventDestroy(w->ev_in[k]);
+      if (w->ev_done[k]) cudaEventDestroy(w->ev_done[k]);
+      if (w->ev_out[k]) cudaEventDestroy(w->ev_out[k]);
+    }
     if (w->bits) cudaFree(w->bits);
     if (w->scratch) cudaFree(w->scratch);
     if (w->dblocks) cudaFree(w->dblocks);

@@ -70,7 +70,7 @@ struct Block {
   int npts;   // columns in this block
   int ld;     // leading dimension of its (npts, ...) arrays
   int col0;   // global index of its first column (prefix sum)
-  int pad;
+  int seed0;  // index of its first column within the caller's block (isubclw=1 seeds 140+i, RLM:765-768)
 };
 
 // Flags common to every block of a launch.

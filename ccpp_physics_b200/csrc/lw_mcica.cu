@@ -245,7 +245,7 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
         any |= cf > 1.0e-6;
         clr[k] = 1.0 - ((cf < 2.2250738585072014e-308) ? 0.0 : cf);
       }
-      seed = (a.isubclw == 1) ? 140 + (i + 1) : B.icseed[i];   // RLM:765-773
+      seed = (a.isubclw == 1) ? 140 + (B.seed0 + i + 1) : B.icseed[i];   // RLM:765-773
     } else {
       for (int k = lane; k < nlay; k += 32) {
         clr[k] = 1.0 - a.st.cldf[c + (size_t)a.st.ld * k];

@@ -170,7 +170,7 @@ extern "C" int rrtmg_lw_gpu_run_noalloc(const rrtmg_lw_run_args* a, int32_t prec
   B.npts = a->npts;
   B.ld = a->ldim > 0 ? a->ldim : a->npts;
   B.col0 = 0;
-  B.pad = 0;
+  B.seed0 = 0;
   Flags f;
   f.nlay = a->nlay;
   f.top_at_1 = a->top_at_1 != 0;

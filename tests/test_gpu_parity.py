@@ -255,3 +255,32 @@ def test_fp64_grid_cloud_transfer(gpu, orc, iovr):
     out32, ref = _run_both(gpu, orc, prof, precision="fp32", flags=flags, hlw0=True)
     assert np.max(np.abs(out32["topflx"] - ref["topflx"])) < 0.05
     assert np.max(np.abs(out32["hlwc"] - ref["hlwc"])) < 0.05
+
+
+@pytest.mark.parametrize("isubclw", [1, 2])
+def test_pipelined_host_call_matches_device(gpu, isubclw):
+    """Host-memory calls of 8,192 columns or more are copied in chunks that
+    overlap the kernels; results must equal the device-memory call bit for
+    bit, with strided host arrays (ldim > npts), a partial last chunk, every
+    optional output, and block-relative McICA seeds (isubclw=1, RLM:765-768)."""
+    from ccpp_physics_b200 import rrtmg_lw as lw
+    ldim, npts, nlay = 9011, 9000, 64
+    prof = synthetic.make_profiles(ldim, nlay, seed=41)
+    prof["npts"] = npts
+    flags = {"ldim": ldim, "isubclw": isubclw}
+    out_h = abi.alloc_outputs(ldim, nlay, hlw0=True, hlwb=True, flxprf=True)
+    msg, err = lw.run_profile(prof, out_h, flags=flags)
+    assert err == 0, msg
+    dp = lw.to_device(prof)
+    dp["npts"] = npts
+    out_d = abi.alloc_outputs(ldim, nlay, hlw0=True, hlwb=True, flxprf=True, like="cuda")
+    msg, err = lw.run_profile(dp, out_d, flags=flags)
+    assert err == 0, msg
+    for k in out_h:
+        h, d = out_h[k], out_d[k].cpu().numpy()
+        sl = (slice(0, npts),) if k in ("topflx", "sfcflx") else (Ellipsis, slice(0, npts)) if k != "flxprf" \
+            else (slice(None), slice(0, npts))
+        assert np.array_equal(h[sl], d[sl]), k
+        assert np.all(np.isnan(h[(slice(npts, None),) if k in ("topflx", "sfcflx") else
+                                 (Ellipsis, slice(npts, None)) if k != "flxprf" else
+                                 (slice(None), slice(npts, None))])), k     # padding columns untouched
