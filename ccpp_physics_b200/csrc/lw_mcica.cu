@@ -329,15 +329,34 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
         double cdf = 0.0;
         uint32_t word = 0;
         for (int k = 0; k < nlay; ++k) {
-          double r = u32_unit(ring[q]);
+          const uint32_t u = ring[q];
           if (++q == cap) q = 0;
-          if (k == 0 || a.iovr == 0) {
-            cdf = r;
+          const double ck = clr[k];
+          if (ck == 1.0) {
+            // Clear layer (the same for every lane: lanes are g-points of one layer).
+            // Its flag is cdf >= 1, and every draw is <= 1 with equality only for
+            // u = 2^32 - 1, so the flag needs no conversion: a fresh draw is 1 only
+            // for that u, an inherited cdf only if it is 1, and r * tem1 < 1 when
+            // tem1 < 1.  The cdf of a clear layer is never read again: the next
+            // layer compares it with 1 - cldf = 1 and takes r * 1 = r instead.
+            bool bit;
+            if (k == 0 || a.iovr == 0) {
+              bit = (u == 0xFFFFFFFFu);
+            } else {
+              const double tem1 = clr[k - 1];
+              bit = (tem1 == 1.0) ? (u == 0xFFFFFFFFu) : (cdf > tem1 && cdf >= 1.0);
+            }
+            if (bit) word |= 1u << (k & 31);
           } else {
-            double tem1 = clr[k - 1];              // max-random walk (RLM:1949-1960)
-            cdf = (cdf > tem1) ? cdf : r * tem1;
+            const double r = u32_unit(u);
+            if (k == 0 || a.iovr == 0) {
+              cdf = r;
+            } else {
+              const double tem1 = clr[k - 1];        // max-random walk (RLM:1949-1960)
+              cdf = (cdf > tem1) ? cdf : r * tem1;
+            }
+            if (cdf >= ck) word |= 1u << (k & 31);   // RLM:2097-2103
           }
-          if (cdf >= clr[k]) word |= 1u << (k & 31);   // RLM:2097-2103
           if ((k & 31) == 31 || k == nlay - 1) {
             out[n * a.nw + (k >> 5)] = word;
             word = 0;
