@@ -73,9 +73,11 @@ constexpr int G_N = G_W3 + GW3_ROWS * GW2_LD;
 
 __host__ __device__ inline bool pad_out_row(int j) { return (j >= 140 && j < 144) || j >= 284; }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU and its derivative with the fast exp and division (the same functions
+// in training and inference)
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
+  const float s = __fdividef(1.0f, 1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
 }
 
@@ -329,11 +331,13 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
 #pragma unroll 1
     for (int layer = 0; layer < 2; ++layer) {
       const int dcol = layer == 0 ? 0 : 128;
+      float v32[32];
+      umma::tmem_ld32(umma::tmem_addr(tb, wl, dcol + 32 * q), v32);
 #pragma unroll
       for (int h16 = 0; h16 < 2; ++h16) {
         const int c0 = 32 * q + 16 * h16;
-        float v[16], h[16];
-        umma::tmem_ld16(umma::tmem_addr(tb, wl, dcol + c0), v);
+        float* v = v32 + 16 * h16;
+        float h[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const float z = v[j] + (layer == 1 ? sb2[c0 + j] : 0.0f);
