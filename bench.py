@@ -447,6 +447,7 @@ def main():
     peak, peak_kind = _peaks()
     achieved = BYTES_PER_COL * ncols / (col_ms / 1e3) / 1e9
     traffic = None
+    tr = {}
     tfile = os.path.join(ROOT, "profiles", "column_kernels_traffic.txt")
     if os.path.exists(tfile):
         # "dram_bytes_per_column_fp64: N" lines from the ncu summary
@@ -454,6 +455,22 @@ def main():
             tr = dict(l.split(":", 1) for l in fh if ":" in l and not l.startswith("#"))
         if "dram_bytes_per_column_fp64" in tr:
             traffic = float(tr["dram_bytes_per_column_fp64"]) * ncols
+    # FP-pipe side of the roofline: counted FP64 flops of the step's kernels (ncu instruction
+    # counts) against the FMA throughput measured on this GPU now
+    fp_pipe = None
+    try:
+        flop_col = sum(float(tr[k]) for k in ("fp64_flop_per_column_mcica", "fp64_flop_per_column_gas",
+                                              "fp64_flop_per_column_rt"))
+        p64, p32 = C.c_double(0.0), C.c_double(0.0)
+        lw.lib().rrtmg_lw_gpu_fma_peak.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        if lw.lib().rrtmg_lw_gpu_fma_peak(C.byref(p64), C.byref(p32)) == 0 and p64.value > 0:
+            ach = flop_col * value / world / 1e12
+            fp_pipe = {"flop_per_column": flop_col, "achieved_tflops": ach, "peak_tflops": p64.value,
+                       "peak_fp32_tflops": p32.value, "frac": ach / p64.value,
+                       "source": "flops: ncu FP64 dadd+dmul+2*dfma counts (profiles/column_kernels_traffic.txt); "
+                                 "peak: FMA-chain kernel (rrtmg_lw_gpu_fma_peak) in this run"}
+    except Exception as exc:   # report, never fake
+        fp_pipe = {"unavailable": str(exc)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -484,6 +501,7 @@ def main():
                      "kernel": "lw_gas_kernel<double,4> + lw_rt_kernel<double,4,0>",
                      "note": "compulsory bytes 61,052 B/column / (gas + transfer kernel time); the "
                              "kernels are FP64-issue and gather-latency bound, not HBM bound"},
+        "fp_pipe": fp_pipe,
         "cpu_baseline": cpu,
         "paths": paths,
     }

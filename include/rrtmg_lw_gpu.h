@@ -274,6 +274,12 @@ int rrtmg_lw_gpu_surrogate_grads(const float *feats, const float *targets,
 int rrtmg_lw_gpu_surrogate_stats(uint64_t *fallback_layers, int32_t *mma_error,
                                  int32_t reset);
 
+/* Measured FMA throughput of the current device in TFLOP/s (FP64 and FP32,
+ * either pointer may be NULL): independent FMA chains over every SM, timed
+ * with CUDA events.  The denominator of the FP-pipe roofline of the
+ * benchmark.  No counterpart in the reference.  Returns 0 on success. */
+int rrtmg_lw_gpu_fma_peak(double *fp64_tflops, double *fp32_tflops);
+
 /* Release device tables and per-thread workspaces (call once at exit). */
 void rrtmg_lw_gpu_finalize(void);
 
