@@ -128,7 +128,9 @@ constexpr uint32_t SM_AER = SM_NORM + SG_NORM_FLOATS * 4;   // f32 [2][16][128] 
 constexpr uint32_t SM_CD = SM_AER + 2 * NBANDS * 128 * 4;   // f32 [2][128] coldry of the tile's layers
 constexpr uint32_t SM_OSC = SM_CD + 2 * 128 * 4;            // f32 [288] output scale  (std)
 constexpr uint32_t SM_OSH = SM_OSC + NOP * 4;               // f32 [288] output shift (b3 * std + mean)
-constexpr uint32_t SM_BAR = (SM_OSH + NOP * 4 + 15) & ~15u;
+constexpr uint32_t SM_BLK = SM_OSH + NOP * 4;                // int [130] block of each column a tile spans
+constexpr int TILE_MAX_COLS = 130;                           // 128 rows of >= 1 layer, +2 partial columns
+constexpr uint32_t SM_BAR = (SM_BLK + TILE_MAX_COLS * 4 + 15) & ~15u;
 constexpr uint32_t FWD_SMEM = SM_BAR + 32;
 static_assert(FWD_SMEM > 116 * 1024, "forward kernel must hold its SM alone (512 TMEM columns)");
 static_assert(FWD_SMEM <= 227 * 1024, "forward kernel shared memory");
@@ -152,18 +154,20 @@ __device__ __forceinline__ void copy_rows_canon(unsigned char* dst, const bf16* 
 // TMEM column of network output j: outputs [0,144) sit at columns 256.., [144,288) at 0..
 __device__ __forceinline__ int out_col(int j) { return j < 144 ? 256 + j : j - 144; }
 
-// Where a tile row of MODE_LW lives: chunk column, layer, block, block column, input row
+// Where a tile row of MODE_LW lives: chunk column, layer, block, block column,
+// input row.  blk[] holds the block index of each column the tile spans
+// (resolved once per tile), cfirst the tile's first chunk column.
 struct LwRow {
   int cc, t, i, r;
   const Block* B;
 };
-__device__ __forceinline__ LwRow lw_row(const FwdArgs& a, long row) {
+__device__ __forceinline__ LwRow lw_row(const FwdArgs& a, long row, const int* blk, int cfirst) {
   LwRow w;
   const int nlay = a.f.nlay;
   w.cc = (int)(row / nlay);
   w.t = (int)(row - (long)w.cc * nlay);
   const int c = a.sc.c0 + w.cc;
-  w.B = (a.nblocks == 1) ? &a.b0 : &a.blocks[find_block(a.blocks, a.nblocks, c)];
+  w.B = (a.nblocks == 1) ? &a.b0 : &a.blocks[blk[w.cc - cfirst]];
   w.i = c - w.B->col0;
   w.r = a.f.top_at_1 ? nlay - w.t - 1 : w.t;
   return w;
@@ -219,6 +223,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + SM_BAR);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SM_BAR + 8);
   int* sfail = reinterpret_cast<int*>(sm + SM_BAR + 12);
+  int* sblk = reinterpret_cast<int*>(sm + SM_BLK);
 
   copy_rows_canon(sm + SM_W1, a.ops + O_W1, HID, KIN, tid);
   copy_rows_canon(sm + SM_W2, a.ops + O_W2, HID, HID, tid);
@@ -273,6 +278,17 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
     const bool live = row < a.nrows;
     float* saer = saer0 + parity * NBANDS * 128;
     float* scd = scd0 + parity * 128;
+    int cfirst = 0;
+    if (MODE == MODE_LW && a.nblocks > 1) {
+      // block of every column this tile touches, one binary search per column
+      const int nlay = a.f.nlay;
+      cfirst = (int)((tile * 128) / nlay);
+      const long rlast = min(tile * 128 + 127, a.nrows - 1);
+      const int ncol = (int)(rlast / nlay) - cfirst + 1;
+      __syncthreads();   // the previous tile's rows are done with sblk
+      for (int j = tid; j < ncol; j += FWD_THREADS) sblk[j] = find_block(a.blocks, a.nblocks, a.sc.c0 + cfirst + j);
+      __syncthreads();
+    }
     long sample = row;
     if (MODE == MODE_TRAIN && live)
       sample = (long)(((unsigned long long)a.perm_a * (unsigned long long)(a.perm_off + row) +
@@ -285,7 +301,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
       if (live) {
         float raw[NIN];
         if (MODE == MODE_LW) {
-          const LwRow w = lw_row(a, row);
+          const LwRow w = lw_row(a, row, sblk, cfirst);
           const size_t o = (size_t)w.i + (size_t)w.B->ld * w.r;
           const double pavel = w.B->in[F_PLYR][o], tavel = w.B->in[F_TLYR][o], qv = w.B->in[F_QLYR][o];
           const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
@@ -311,7 +327,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
         for (int j = 0; j < 8; ++j) a.xt[(size_t)j * a.ldt + row] = __float2bfloat16_rn(x[j]);
       }
     } else if (MODE == MODE_LW && live) {
-      const LwRow w = lw_row(a, row);
+      const LwRow w = lw_row(a, row, sblk, cfirst);
       const size_t ldl = (size_t)w.B->ld;
       const int b0 = q == 1 ? 0 : q == 2 ? 6 : 11, b1 = q == 1 ? 6 : q == 2 ? 11 : 16;
       for (int b = b0; b < b1; ++b) {

@@ -45,10 +45,14 @@ def _equal(a, b):
         assert torch.equal(a[k], b[k]), k
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "surrogate"])
 def test_blocks_equal_one_call(lw, case, precision):
-    """isubclw=2 seeds come from icseed, so the block split changes nothing."""
+    """isubclw=2 seeds come from icseed, so the block split changes nothing
+    (the learned gas optics included: its rows are independent)."""
     sizes, prof = case
+    if precision == "surrogate":
+        from ccpp_physics_b200 import surrogate
+        surrogate.load()
     one, many = _outs(), _outs()
     msg, err = lw.run_profile(prof, one, precision=precision)
     assert err == 0, msg
