@@ -585,7 +585,7 @@ struct HostField {
 // chunk j+1's inputs travel host -> device on one copy stream and chunk j-1's
 // outputs device -> host on another while chunk j computes.  Staging is
 // double-buffered; events order the reuse of each buffer.
-int run_host_pipelined(Workspace* w, const rrtmg_lw_run_args* a, const Flags& f0, int precision, cudaStream_t st,
+int run_host_pipelined(Workspace* w, const rrtmg_lw_run_args* a, Flags f0, int precision, cudaStream_t st,
                        char* errmsg, int32_t errmsg_len) {
   const int npts = a->npts, nlay = a->nlay, nlp1 = nlay + 1;
   const size_t ld = a->ldim > 0 ? (size_t)a->ldim : (size_t)npts;
@@ -627,7 +627,7 @@ int run_host_pipelined(Workspace* w, const rrtmg_lw_run_args* a, const Flags& f0
     }
   }
   CK(grow(&w->pbuf, &w->pbuf_bytes, 2 * per), "cudaMalloc(staging)");
-  const int kp = kernel_precision(precision, const_cast<Flags*>(&f0));
+  const int kp = kernel_precision(precision, &f0);
   const Shape sh = default_shape(kp, pick_v(nlay));
   const int nch = (npts + kHostChunk - 1) / kHostChunk;
   for (int j = 0; j < nch; ++j) {

@@ -10,7 +10,7 @@
  *                  CCPP metadata radlw_main.meta:1-444)
  *
  * A Fortran host reaches these through an ISO_C_BINDING shim that keeps the
- * original rlwinit / rrtmg_lw_run interfaces.  Every
+ * original rlwinit / rrtmg_lw_run interfaces (ccpp_physics_b200/fortran/).  Every
  * array is the caller's Fortran array, column-major, kind_phys = real(8):
  * element (i, k) of an (npts, nlay) array is at ptr[(i-1) + (k-1)*ldim],
  * element (i, k, b) of an (npts, nlay, nbands) array at

@@ -1,7 +1,7 @@
 """GPU parity tests: the CUDA path through the C ABI against the CPU
 restatement of rrtmg_lw_run on identical inputs.
 
-Bars (north star): the FP64 path reproduces the reference within 1e-10
+Bars: the FP64 path reproduces the reference within 1e-10
 relative on fluxes; McICA sub-columns are bit-exact; the FP32 path is held
 to flux/heating-rate error bounds stated below.
 """
@@ -12,7 +12,7 @@ from ccpp_physics_b200 import abi, synthetic
 
 pytestmark = pytest.mark.gpu
 
-FLUX_RTOL_FP64 = 1e-10      # fluxes, relative (north star)
+FLUX_RTOL_FP64 = 1e-10      # fluxes, relative
 # Heating rates are flux differences over the layer thickness, so the FP64
 # rounding of the g-point sums (summed in another order than the reference's)
 # is amplified in thin layers: 1.1e-10 was seen in the 0.002 hPa top layers of

@@ -1,4 +1,4 @@
-"""CPU checks of the network oracle (oracle/mlp_oracle.py) that judges the
+"""CPU checks of the network oracle (oracle/mlp_oracle.py) that checks the
 GPU training kernels: its backward pass against finite differences, and its
 BF16 rounding against the IEEE definition."""
 import numpy as np
