@@ -215,6 +215,114 @@ def batched_leg(args, lw, abi, synthetic, torch, rank, world, sh, timed, rmse):
     return res
 
 
+def caller_steps_leg(args, torch, timed, sh, peak_gbs):
+    """The steps either side of rrtmg_lw_run at 884,736 columns x 127 layers
+    (six C384 cubed-sphere faces of 384 x 384 columns):
+      * McICA seeds (GFS_rad_time_vary): one twister stream of 2 x 147,456
+        draws per face, then each column's pair; six calls, one per face;
+      * decorrelation length (Hogan) + alpha for exponential-random overlap;
+      * rrtmg_lw_post_run: heating rates (total and clear sky) onto 127 levels.
+    Device-resident, timed with CUDA events; the oracle times the same work on
+    a sample on one host core, and the GPU results are checked against it."""
+    import math
+    import numpy as np
+    from oracle import oracle
+    from ccpp_physics_b200 import cloud_overlap, rad_time_vary, rrtmg_lw_post
+    n, nlay, cn = 884_736, 127, 384
+    face = cn * cn
+    k = max(3, min(args.steps, 10))
+    g = torch.Generator(device="cuda").manual_seed(11)
+    res = {"workload": "c3_884736x127_as_6_c384_faces", "steps": k}
+
+    # seeds: every column of a face, rows of the tile in a shuffled order
+    perm = torch.randperm(face, generator=g, device="cuda").to(torch.int32)
+    imap, jmap = (perm % cn + 1).contiguous(), (perm // cn + 1).contiguous()
+    sw = torch.zeros(face, dtype=torch.int32, device="cuda")
+    lwseed = torch.zeros_like(sw)
+    sec, ipsd0, ipsdlim = 10800.0, 35000, 100_000_000
+
+    def seeds():
+        for _ in range(6):
+            m, e = rad_time_vary.gfs_rad_time_vary_seeds(False, None, True, True, 2, 2, sw, lwseed, cn, cn, 1, 1,
+                                                         imap, jmap, sec, ipsd0, ipsdlim, stream=sh, sync=False)
+            if e:
+                raise RuntimeError(m)
+    seeds()
+    ms = timed(seeds, k)
+    t0 = time.perf_counter()
+    _, sw_ref, lw_ref = oracle.seeds(sec=sec, ipsd0=ipsd0, ipsdlim=ipsdlim, cnx=cn, cny=cn, isc=1, jsc=1,
+                                     imap=imap.cpu().numpy(), jmap=jmap.cpu().numpy())
+    cpu_face_s = time.perf_counter() - t0
+    res["seeds"] = {"ms_per_step_6_faces": ms / k, "ms_per_face": ms / k / 6, "draws_per_face": 2 * face,
+                    "cpu_oracle_ms_per_face": cpu_face_s * 1e3, "cpu_cores": 1,
+                    "matches_oracle": bool(np.array_equal(sw.cpu().numpy(), sw_ref)
+                                           and np.array_equal(lwseed.cpu().numpy(), lw_ref))}
+
+    # overlap parameters (Hogan length, exponential-random alpha)
+    lat = (torch.rand(n, generator=g, device="cuda", dtype=torch.float64) - 0.5) * math.pi
+    dz = 0.02 + 2.0 * torch.rand((nlay, n), generator=g, device="cuda", dtype=torch.float64)
+    cf = torch.rand((nlay, n), generator=g, device="cuda", dtype=torch.float64)
+    cf = torch.where(cf < 0.5, torch.zeros_like(cf), cf)
+    dl = torch.zeros(n, dtype=torch.float64, device="cuda")
+    al = torch.zeros((nlay, n), dtype=torch.float64, device="cuda")
+
+    def overlap():
+        m, e = cloud_overlap.overlap_params(5, 1, dz, cf, dl, al, xlat=lat, stream=sh, sync=False)
+        if e:
+            raise RuntimeError(m)
+    overlap()
+    ms = timed(overlap, k)
+    ns = 65536
+    dz_s, cf_s, lat_s = (dz[:, :ns].cpu().numpy(), cf[:, :ns].cpu().numpy(), lat[:ns].cpu().numpy())
+    t0 = time.perf_counter()
+    dl_ref, al_ref = oracle.overlap_params(5, 1, dz_s, cf_s, xlat=lat_s)
+    cpu_s = time.perf_counter() - t0
+    al_g = al[:, :ns].cpu().numpy()
+    ulp = np.abs(al_g - al_ref) / np.maximum(np.spacing(np.abs(al_ref)), 5e-324)
+    obytes = (3 * nlay + 2) * 8 * n
+    res["overlap_params"] = {"ms_per_step": ms / k, "columns_per_s": n * k / (ms / 1e3),
+                             "achieved_gbs": obytes * k / (ms / 1e3) / 1e9, "bytes_per_step": obytes,
+                             "hbm_frac": obytes * k / (ms / 1e3) / 1e9 / peak_gbs,
+                             "cpu_oracle_columns_per_s": ns / cpu_s, "cpu_cores": 1,
+                             "cpu_sample": f"first {ns} columns",
+                             "de_lgth_matches_oracle": bool(np.array_equal(dl[:ns].cpu().numpy(), dl_ref)),
+                             "alpha_max_ulp_vs_oracle": float(ulp.max())}
+    del dz, cf, al, lat, dl
+
+    # rrtmg_lw_post_run
+    htlwc = torch.randn((nlay, n), generator=g, device="cuda", dtype=torch.float64)
+    htlw0 = torch.randn((nlay, n), generator=g, device="cuda", dtype=torch.float64)
+    sfc = torch.randn((n, 4), generator=g, device="cuda", dtype=torch.float64)
+    tsfa = torch.randn(n, generator=g, device="cuda", dtype=torch.float64)
+    outs = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(2)] + \
+           [torch.zeros((nlay, n), dtype=torch.float64, device="cuda") for _ in range(2)]
+
+    def post():
+        m, e = rrtmg_lw_post.rrtmg_lw_post_run(n, nlay, 0, nlay, 0, True, True, tsfa, htlwc, htlw0, sfc, *outs,
+                                               stream=sh, sync=False)
+        if e:
+            raise RuntimeError(m)
+    post()
+    ms = timed(post, k)
+    sl = [a[..., :ns].cpu().numpy().copy() if a.dim() == 2 else a[:ns].cpu().numpy().copy()
+          for a in (htlwc, htlw0)]
+    ref = [np.zeros(ns), np.zeros(ns), np.zeros((nlay, ns)), np.zeros((nlay, ns))]
+    t0 = time.perf_counter()
+    oracle.post(ns, nlay, 0, nlay, 0, 1, 1, tsfa[:ns].cpu().numpy(), sl[0], sl[1], sfc[:ns].cpu().numpy(), *ref)
+    cpu_s = time.perf_counter() - t0
+    pbytes = (4 * nlay + 3) * 8 * n
+    res["post"] = {"ms_per_step": ms / k, "columns_per_s": n * k / (ms / 1e3),
+                   "achieved_gbs": pbytes * k / (ms / 1e3) / 1e9, "bytes_per_step": pbytes,
+                   "hbm_frac": pbytes * k / (ms / 1e3) / 1e9 / peak_gbs,
+                   "cpu_oracle_columns_per_s": ns / cpu_s, "cpu_cores": 1, "cpu_sample": f"first {ns} columns",
+                   "matches_oracle": bool(np.array_equal(outs[2][:, :ns].cpu().numpy(), ref[2])
+                                          and np.array_equal(outs[3][:, :ns].cpu().numpy(), ref[3]))}
+    res["peak_gbs"] = peak_gbs
+    del htlwc, htlw0, sfc, tsfa, outs
+    torch.cuda.empty_cache()
+    return res
+
+
 def training_leg(args, torch, sg):
     """Learned gas optics training throughput on 20M layer samples labelled by
     plain FP64 taumol: a fresh network, 2 epochs of the library's tcgen05
@@ -257,6 +365,8 @@ def main():
     ap.add_argument("--ncols", type=int, default=0, help="override the column count (profiling runs)")
     ap.add_argument("--quick", action="store_true", help="FP64 device-resident loop only (profiling runs)")
     ap.add_argument("--no-batch", action="store_true", help="skip the 884,736-column batched-block leg")
+    ap.add_argument("--no-callers", action="store_true",
+                    help="skip the leg of the steps either side of rrtmg_lw_run (seeds, overlap, post)")
     ap.add_argument("--no-train", action="store_true", help="skip the surrogate training-throughput leg")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "surrogate"],
                     help="with --quick: the path to loop over (profiling runs)")
@@ -417,6 +527,10 @@ def main():
     # ---- batched production blocks (884,736 columns in uneven blocks of 8..256) ----
     if not args.no_batch:
         paths["c3_batched"] = batched_leg(args, lw, abi, synthetic, torch, rank, world, sh, timed, rmse)
+
+    # ---- the steps either side of rrtmg_lw_run (seeds, overlap parameters, post) ----
+    if not args.no_callers and world == 1 and not args.quick:
+        paths["caller_steps"] = caller_steps_leg(args, torch, timed, sh, _peaks()[0])
 
     # ---- end to end through the C ABI with pinned host buffers ----
     hprof = dict(npts=ncols, nlay=nlay, flags=dict(prof["flags"]))

@@ -66,6 +66,33 @@ class Tuning(C.Structure):
                 ("use_graph", C.c_int32)]
 
 
+class SeedArgs(C.Structure):
+    """rrtmg_lw_seed_args: seed part of GFS_rad_time_vary_timestep_init."""
+    _fields_ = ([("sec", C.c_double)]
+                + [(n, C.c_int32) for n in ("lslwr", "lsswr", "isubc_lw", "isubc_sw", "lrseeds", "ipsd0",
+                                             "ipsdlim", "cnx", "cny", "isc", "jsc", "n", "ld_rseeds")]
+                + [(n, _ip) for n in ("imap", "jmap", "rseeds", "icsdsw", "icsdlw")])
+
+
+class OverlapArgs(C.Structure):
+    """rrtmg_lw_overlap_args: decorrelation length and alpha (radiation_clouds.f:837-856)."""
+    _fields_ = ([(n, C.c_int32) for n in ("mode", "npts", "nlay", "ldim", "idcor", "idcor_con", "idcor_hogan",
+                                           "idcor_oreopoulos", "iovr", "iovr_dcorr", "iovr_exp",
+                                           "iovr_exprand", "yearlen")]
+                + [(n, C.c_double) for n in ("julian", "dcorr_con", "con_pi")]
+                + [(n, _dp) for n in ("xlat", "latdeg", "dzlay", "cld_frac", "de_lgth", "alpha")])
+
+
+class PostArgs(C.Structure):
+    """rrtmg_lw_post_args: rrtmg_lw_post_run (rrtmg_lw_post.F90:13-77)."""
+    _fields_ = ([(n, C.c_int32) for n in ("im", "levs", "ltp", "lm", "kd", "lslwr", "lwhtr")]
+                + [(n, _dp) for n in ("tsfa", "htlwc", "htlw0", "sfcflw", "tsflw", "sfcdlw", "htrlw", "lwhc")])
+
+
+OVERLAP_CLOUDS, OVERLAP_DCORR, OVERLAP_ALPHA = 0, 1, 2
+# Decorrelation-length flags (radiation_clouds.f:447-450).
+IDCOR_FLAGS = dict(idcor_con=0, idcor_hogan=1, idcor_oreopoulos=2)
+
 FP64, FP32, SURROGATE = 0, 1, 2
 HOST, DEVICE = 0, 1
 

@@ -1063,3 +1063,10 @@ lw::NoAllocView lw::noalloc_view() {
   std::lock_guard<std::mutex> lk(g_mu);
   return NoAllocView{g.ready ? 1 : 0, g.device, g.num_sms, g.kt64, g.kt32, g.tbl64, g.tbl32, g.cs};
 }
+
+// Device of the steps either side of the run (lw_prep.cu): the init device,
+// or -1 before init.
+int lw::selected_device() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return g.ready ? g.device : -1;
+}

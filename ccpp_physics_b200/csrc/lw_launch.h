@@ -41,6 +41,8 @@ struct McicaStage {
 cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int ncols, int nlay, int iovr,
                          int isubclw, int top_at_1, const McicaStage& stage, uint32_t* bits, int num_sms,
                          cudaStream_t st);
+// random_index of one twister stream (lw_mcica.cu): out[0..m) = max(ceiling(h * imax), 1)
+cudaError_t seed_index_launch(int32_t seed, int32_t imax, long long m, int32_t* out, cudaStream_t st);
 
 // learned gas optics (lw_mlp.cu): network stage of a chunk, its
 // normalisation/envelope (nullptr until a network is loaded) and the
@@ -49,6 +51,9 @@ cudaError_t mlp_lw_launch(const Block* blocks, int nblocks, const Block& b0, int
                           const Scratch<float>& sc, int num_sms, cudaStream_t st);
 const float* surrogate_norm();
 unsigned int* surrogate_fallback_counter();
+
+// device chosen by rrtmg_lw_gpu_init, -1 before init (lw_api.cu)
+int selected_device();
 
 // layers per lane of the column kernels (NLP = 32 V padded layers)
 inline int pick_v(int nlay) { return nlay <= 63 ? 2 : nlay <= 127 ? 4 : 8; }

@@ -368,7 +368,68 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
   }
 }
 
+// random_index_t (MT:489-503) of one stream: random_setseed_t(seed), then m
+// draws h, each giving max(ceiling(h * imax), 1).  One CTA walks the stream;
+// the 624-word state is double-buffered in shared memory, so a twist is its
+// three dependency phases (words 0..226 from the old state, 227..453 and
+// 454..622 from words 227 back in the new one, word 623 from new words 0 and
+// 396) with one barrier each and no read-before-write hazard.  Each word is
+// tempered, converted and stored as soon as its phase has produced it.
+constexpr int kSeedThreads = 256;
+
+__device__ __forceinline__ int32_t index_of(uint32_t w, double imax) {
+  const double c = ceil(u32_unit(temper(w)) * imax);   // h * imax rounds as in the Fortran
+  return c < 1.0 ? 1 : (int32_t)c;
+}
+
+__global__ void __launch_bounds__(kSeedThreads) lw_seed_index_kernel(uint32_t seed, int32_t imax, long long m,
+                                                                     int32_t* __restrict__ out) {
+  __shared__ uint32_t s[2][624];
+  const int t = threadIdx.x;
+  if (t == 0) {   // MT:290-296, signed wrap = unsigned multiply
+    uint32_t v = seed;
+    s[0][0] = v;
+    for (int i = 1; i < 624; ++i) { v *= 69069u; s[0][i] = v; }
+  }
+  __syncthreads();
+  const double dmax = (double)imax;
+  int cur = 0;
+  for (long long base = 0; base < m; base += 624) {
+    const uint32_t* o = s[cur];
+    uint32_t* w = s[cur ^ 1];
+    long long left = m - base;
+    if (t < 227) {   // words 0..226
+      w[t] = mt_word(o[t], o[t + 1], o[t + 397]);
+      if (t < left) out[base + t] = index_of(w[t], dmax);
+    }
+    __syncthreads();
+    if (t < 227) {   // words 227..453
+      const int kk = 227 + t;
+      w[kk] = mt_word(o[kk], o[kk + 1], w[kk - 227]);
+      if (kk < left) out[base + kk] = index_of(w[kk], dmax);
+    }
+    __syncthreads();
+    if (t < 169) {   // words 454..622
+      const int kk = 454 + t;
+      w[kk] = mt_word(o[kk], o[kk + 1], w[kk - 227]);
+      if (kk < left) out[base + kk] = index_of(w[kk], dmax);
+    } else if (t == 169) {   // word 623
+      w[623] = mt_word(o[623], w[0], w[396]);
+      if (623 < left) out[base + 623] = index_of(w[623], dmax);
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+}
+
 // host side ------------------------------------------------------------------
+
+cudaError_t seed_index_launch(int32_t seed, int32_t imax, long long m, int32_t* out, cudaStream_t st) {
+  if (m <= 0) return cudaSuccess;
+  const uint32_t s = (uint32_t)(seed == 0 ? 4357 : seed);   // MT:291
+  lw_seed_index_kernel<<<1, kSeedThreads, 0, st>>>(s, imax, m, out);
+  return cudaGetLastError();
+}
 
 int mcica_ring_capacity(int nlay) { return ((32 * nlay + 624 + 31) / 32) * 32; }
 

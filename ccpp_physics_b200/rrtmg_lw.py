@@ -50,6 +50,10 @@ def lib():
         L.rrtmg_lw_gpu_autotune.argtypes = [C.POINTER(abi.RunArgs), C.c_int32, C.c_int32, C.c_void_p,
                                             C.c_int64, C.POINTER(abi.Tuning), C.POINTER(C.c_float),
                                             C.c_char_p, C.c_int32]
+        L.rrtmg_lw_gpu_seeds.argtypes = [C.POINTER(abi.SeedArgs), C.POINTER(abi.ExecArgs), C.c_char_p, C.c_int32]
+        L.rrtmg_lw_gpu_overlap_params.argtypes = [C.POINTER(abi.OverlapArgs), C.POINTER(abi.ExecArgs),
+                                                  C.c_char_p, C.c_int32]
+        L.rrtmg_lw_gpu_post.argtypes = [C.POINTER(abi.PostArgs), C.POINTER(abi.ExecArgs), C.c_char_p, C.c_int32]
         L.rrtmg_lw_gpu_finalize.argtypes = []
         _lib = L
     return _lib

@@ -280,6 +280,94 @@ int rrtmg_lw_gpu_surrogate_stats(uint64_t *fallback_layers, int32_t *mma_error,
  * benchmark.  No counterpart in the reference.  Returns 0 on success. */
 int rrtmg_lw_gpu_fma_peak(double *fp64_tflops, double *fp32_tflops);
 
+/* ---- Steps either side of rrtmg_lw_run ------------------------------------
+ * They need no tables: they run on the device rrtmg_lw_gpu_init selected (the
+ * current device before init).  The exec struct gives memory, stream (NULL =
+ * the per-thread default stream) and sync; precision is ignored.  Host memory
+ * is staged through the device and always syncs.  Each returns 0, or 1 with
+ * a message. */
+
+/* Seed part of GFS_rad_time_vary_timestep_init
+ * (physics/Interstitials/UFS_SCM_NEPTUNE/GFS_rad_time_vary.fv3.F90:59-84).
+ * Only when (lsswr or lslwr) and (isubc_lw == 2 or isubc_sw == 2):
+ *   lrseeds: icsdsw(ix) = rseeds(ix,1), icsdlw(ix) = rseeds(ix,2);
+ *   else:    ipseed = mod(nint(100 sqrt(sec)), ipsdlim) + 1 + ipsd0 seeds one
+ *            twister stream, numrdm(1:2 cnx cny) = random_index(ipsdlim)
+ *            (mersenne_twister.f:489-503: max(ceiling(h ipsdlim), 1)), and
+ *            with (i, j) = (imap(ix), jmap(ix)), p = i+isc-1 + (j+jsc-2) cnx:
+ *            icsdsw(ix) = numrdm(p), icsdlw(ix) = numrdm(p + cnx cny).
+ * Otherwise the outputs are left as they are.  A p outside 1..cnx cny is an
+ * error (the Fortran would read out of bounds); the call syncs to report it. */
+typedef struct rrtmg_lw_seed_args {
+  double sec;                      /* seconds since the forecast start */
+  int32_t lslwr, lsswr, isubc_lw, isubc_sw;
+  int32_t lrseeds;                 /* logical: seeds supplied in rseeds */
+  int32_t ipsd0, ipsdlim;
+  int32_t cnx, cny, isc, jsc;
+  int32_t n;                       /* columns: size(jmap) */
+  int32_t ld_rseeds;               /* leading dimension of rseeds; 0 = n */
+  const int32_t *imap, *jmap;      /* (n), 1-based grid indices */
+  const int32_t *rseeds;           /* (ld_rseeds, 2) when lrseeds */
+  int32_t *icsdsw, *icsdlw;        /* (n) */
+} rrtmg_lw_seed_args;
+int rrtmg_lw_gpu_seeds(const rrtmg_lw_seed_args *args, const rrtmg_lw_exec *exec,
+                       char *errmsg, int32_t errmsg_len);
+
+/* Cloud-overlap parameters: the block of radiation_clouds.f:837-856 with the
+ * routines of physics/Radiation/radiation_cloud_overlap.F90.
+ *   de_lgth by idcor: idcor_hogan       max(0.6, 2.78 - 4.6 |xlat / con_pi|)
+ *                                       (cmp_dcorr_lgth_hogan, :28-50);
+ *                     idcor_oreopoulos  am1 + am2 exp(-(latdeg - am3)^2 / am4^2),
+ *                                       am3 by julian and yearlen (:58-93);
+ *                     idcor_con         dcorr_con;
+ *                     other             de_lgth left as it is.
+ *   alpha (get_alpha_exper, :99-145) when iovr is iovr_dcorr, iovr_exp or
+ *   iovr_exprand: alpha(:,1) = 0, alpha(:,k) = exp(-dzlay(:,k) / de_lgth), and
+ *   for iovr_exprand 0 where a clear layer follows a cloudy one (cld_frac);
+ *   for any other iovr de_lgth = 0 and alpha = 0.
+ * mode selects the block (both steps) or one routine alone. */
+enum rrtmg_lw_overlap_mode {
+  RRTMG_LW_OVERLAP_CLOUDS = 0,     /* the radiation_clouds.f block */
+  RRTMG_LW_OVERLAP_DCORR = 1,      /* cmp_dcorr_lgth by idcor only */
+  RRTMG_LW_OVERLAP_ALPHA = 2       /* get_alpha_exper only; de_lgth is an input */
+};
+typedef struct rrtmg_lw_overlap_args {
+  int32_t mode;                    /* enum rrtmg_lw_overlap_mode */
+  int32_t npts, nlay, ldim;        /* ldim: leading dimension of (npts, nlay); 0 = npts */
+  int32_t idcor, idcor_con, idcor_hogan, idcor_oreopoulos;
+  int32_t iovr, iovr_dcorr, iovr_exp, iovr_exprand;
+  int32_t yearlen;                 /* days in the year (Oreopoulos) */
+  double julian;                   /* julian day (Oreopoulos) */
+  double dcorr_con;                /* km (idcor_con) */
+  double con_pi;
+  const double *xlat;              /* (npts) radians (Hogan) */
+  const double *latdeg;            /* (npts) degrees (Oreopoulos) */
+  const double *dzlay;             /* (npts, nlay) km between layer centres */
+  const double *cld_frac;          /* (npts, nlay), read for iovr_exprand */
+  double *de_lgth;                 /* (npts) km */
+  double *alpha;                   /* (npts, nlay) */
+} rrtmg_lw_overlap_args;
+int rrtmg_lw_gpu_overlap_params(const rrtmg_lw_overlap_args *args, const rrtmg_lw_exec *exec,
+                                char *errmsg, int32_t errmsg_len);
+
+/* rrtmg_lw_post_run (physics/Radiation/RRTMG/rrtmg_lw_post.F90:13-77): when
+ * lslwr, tsflw = tsfa; htrlw(:,k) = htlwc(:,k+kd) for k = 1..lm and htrlw(:,lm)
+ * for k = lm+1..levs; the same from htlw0 into lwhc when lwhtr; sfcdlw =
+ * sfcflw%dnfxc.  On the device-resident outputs of a run this keeps the
+ * heating-rate arrays on the device (no host read-back).  Requires kd <= ltp,
+ * lm <= levs and lm >= 1 when levs > lm. */
+typedef struct rrtmg_lw_post_args {
+  int32_t im, levs, ltp, lm, kd;
+  int32_t lslwr, lwhtr;
+  const double *tsfa;              /* (im) */
+  const double *htlwc, *htlw0;     /* (im, lm+ltp) */
+  const double *sfcflw;            /* (im) records {upfxc, upfx0, dnfxc, dnfx0} */
+  double *tsflw, *sfcdlw;          /* (im) */
+  double *htrlw, *lwhc;            /* (im, levs); lwhc only when lwhtr */
+} rrtmg_lw_post_args;
+int rrtmg_lw_gpu_post(const rrtmg_lw_post_args *args, const rrtmg_lw_exec *exec,
+                      char *errmsg, int32_t errmsg_len);
+
 /* Release device tables and per-thread workspaces (call once at exit). */
 void rrtmg_lw_gpu_finalize(void);
 

@@ -40,6 +40,14 @@ def lib():
         L.oracle_mcica.argtypes = [C.c_int, C.c_int32, C.c_int, C.c_void_p, C.c_void_p,
                                    C.c_double, C.c_void_p, C.c_void_p]
         L.oracle_tables.argtypes = [C.c_void_p] * 4
+        L.oracle_random_index.argtypes = [C.c_int32, C.c_int32, C.c_longlong, C.c_void_p]
+        L.oracle_seeds.argtypes = [C.c_double] + [C.c_int32] * 13 + [C.c_void_p] * 5
+        L.oracle_dcorr_hogan.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_void_p]
+        L.oracle_dcorr_oreopoulos.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_void_p]
+        L.oracle_alpha_exper.argtypes = [C.c_int] * 5 + [C.c_void_p] * 4
+        L.oracle_overlap_params.argtypes = ([C.c_int] * 7 + [C.c_double, C.c_void_p, C.c_void_p, C.c_double,
+                                            C.c_int, C.c_double] + [C.c_int] * 4 + [C.c_void_p] * 4)
+        L.oracle_post.argtypes = [C.c_int] * 7 + [C.c_void_p] * 8
         L.oracle_check_u32_unit.argtypes = [C.c_ulonglong, C.c_ulonglong]
         L.oracle_check_u32_unit.restype = C.c_ulonglong
         _lib = L
@@ -123,3 +131,75 @@ def tables():
     fh = np.zeros(2)
     lib().oracle_tables(_vp(tau), _vp(ex), _vp(tfn), _vp(fh))
     return tau, ex, tfn, fh
+
+
+# ---- steps either side of rrtmg_lw_run ----------------------------------------
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def random_index(seed, imax, m):
+    """random_setseed_t(seed) then random_index_t(imax, out(m))."""
+    out = np.zeros(m, dtype=np.int32)
+    lib().oracle_random_index(seed, imax, m, _vp(out))
+    return out
+
+
+def seeds(*, sec, ipsd0, ipsdlim, cnx, cny, isc, jsc, imap, jmap, lslwr=1, lsswr=1, isubc_lw=2, isubc_sw=2,
+          lrseeds=0, rseeds=None, icsdsw=None, icsdlw=None):
+    """Seed part of GFS_rad_time_vary_timestep_init; returns (rc, icsdsw, icsdlw).
+    ``rseeds`` is the (n, 2) Fortran array as a C-contiguous (2, n) array."""
+    imap = np.ascontiguousarray(imap, dtype=np.int32)
+    jmap = np.ascontiguousarray(jmap, dtype=np.int32)
+    n = imap.size
+    sw = np.zeros(n, dtype=np.int32) if icsdsw is None else icsdsw
+    lw = np.zeros(n, dtype=np.int32) if icsdlw is None else icsdlw
+    rs = None if rseeds is None else np.ascontiguousarray(rseeds, dtype=np.int32)
+    ld = 0 if rs is None else rs.shape[-1]
+    rc = lib().oracle_seeds(float(sec), lslwr, lsswr, isubc_lw, isubc_sw, lrseeds, ipsd0, ipsdlim, cnx, cny, isc,
+                            jsc, n, ld, _vp(imap), _vp(jmap), _vp(rs), _vp(sw), _vp(lw))
+    return rc, sw, lw
+
+
+def dcorr_hogan(lat, con_pi=np.pi):
+    lat = _f64(lat)
+    out = np.zeros_like(lat)
+    lib().oracle_dcorr_hogan(lat.size, _vp(lat), con_pi, _vp(out))
+    return out
+
+
+def dcorr_oreopoulos(lat, juldat, yearlength):
+    lat = _f64(lat)
+    out = np.zeros_like(lat)
+    lib().oracle_dcorr_oreopoulos(lat.size, _vp(lat), float(juldat), int(yearlength), _vp(out))
+    return out
+
+
+def alpha_exper(iovr, iovr_exprand, dzlay, dcorr, cld_frac):
+    """(nlay, ncol) C-contiguous = Fortran (ncol, nlay)."""
+    dzlay, dcorr, cld_frac = _f64(dzlay), _f64(dcorr), _f64(cld_frac)
+    nlay, ncol = dzlay.shape
+    out = np.zeros_like(dzlay)
+    lib().oracle_alpha_exper(ncol, nlay, ncol, iovr, iovr_exprand, _vp(dzlay), _vp(dcorr), _vp(cld_frac), _vp(out))
+    return out
+
+
+def overlap_params(iovr, idcor, dzlay, cld_frac, *, xlat=None, latdeg=None, julian=0.0, yearlen=365,
+                   dcorr_con=2.5, con_pi=np.pi, de_lgth=None, idcor_flags=(0, 1, 2), iovr_flags=(3, 4, 5)):
+    """radiation_clouds.f:837-856; returns (de_lgth, alpha)."""
+    dzlay, cld_frac = _f64(dzlay), _f64(cld_frac)
+    nlay, ncol = dzlay.shape
+    dl = np.zeros(ncol) if de_lgth is None else _f64(de_lgth).copy()
+    al = np.zeros_like(dzlay)
+    c, h, o = idcor_flags
+    lib().oracle_overlap_params(ncol, nlay, ncol, idcor, c, h, o, float(dcorr_con), _vp(_f64(xlat)),
+                                _vp(_f64(latdeg)), float(julian), int(yearlen), float(con_pi), iovr, *iovr_flags,
+                                _vp(dzlay), _vp(cld_frac), _vp(dl), _vp(al))
+    return dl, al
+
+
+def post(im, levs, ltp, lm, kd, lslwr, lwhtr, tsfa, htlwc, htlw0, sfcflw, tsflw, sfcdlw, htrlw, lwhc):
+    """rrtmg_lw_post_run on numpy arrays (outputs in place)."""
+    lib().oracle_post(im, levs, ltp, lm, kd, int(lslwr), int(lwhtr), _vp(tsfa), _vp(htlwc), _vp(htlw0),
+                      _vp(sfcflw), _vp(tsflw), _vp(sfcdlw), _vp(htrlw), _vp(lwhc))

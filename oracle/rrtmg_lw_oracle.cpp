@@ -17,6 +17,11 @@
 //   physics/Radiation/mersenne_twister.f      random_setseed_t MT:285-299,
 //                                             random_number_t  MT:330-372
 //   physics/Radiation/RRTMG/radlw_param.f     band layout :103-142
+// and the steps either side of rrtmg_lw_run:
+//   physics/Radiation/mersenne_twister.f      random_index_t MT:489-503
+//   physics/Interstitials/UFS_SCM_NEPTUNE/GFS_rad_time_vary.fv3.F90:59-84
+//   physics/Radiation/radiation_cloud_overlap.F90:28-145, radiation_clouds.f:837-856
+//   physics/Radiation/RRTMG/rrtmg_lw_post.F90:13-77
 //   physics/hooks/physcons.F90                constants :52,66,107,110-112
 // Arithmetic is IEEE binary64 with FMA contraction disabled
 // (-ffp-contract=off), Fortran int() = truncation toward zero, mod(x,1.) =
@@ -1694,6 +1699,132 @@ unsigned long long oracle_check_u32_unit(unsigned long long start, unsigned long
     if (std::memcmp(&r, &ref, 8) != 0) ++bad;
   }
   return bad;
+}
+
+// ---- Steps either side of rrtmg_lw_run -------------------------------------
+
+// random_index_t (MT:489-503) after random_setseed_t(seed): m draws h of one
+// stream (random_number_t in chunks of 624 continues the same stream), each
+// max(ceiling(h * imax), 1).
+void oracle_random_index(int32_t seed, int32_t imax, long long m, int32_t* out) {
+  MTState st;
+  mt_setseed(st, seed);
+  for (long long j = 0; j < m; ++j) {
+    const double h = mt_u32_to_real(mt_next_u32(st));
+    const double c = std::ceil(h * (double)imax);
+    out[j] = c < 1.0 ? 1 : (int32_t)c;
+  }
+}
+
+// Seed part of GFS_rad_time_vary_timestep_init
+// (physics/Interstitials/UFS_SCM_NEPTUNE/GFS_rad_time_vary.fv3.F90:59-84).
+// rseeds is (ld_rseeds, 2) column-major when lrseeds.  Returns 1 for a grid
+// index outside the face (the Fortran would read out of bounds), else 0.
+int oracle_seeds(double sec, int32_t lslwr, int32_t lsswr, int32_t isubc_lw, int32_t isubc_sw, int32_t lrseeds,
+                 int32_t ipsd0, int32_t ipsdlim, int32_t cnx, int32_t cny, int32_t isc, int32_t jsc, int32_t n,
+                 int32_t ld_rseeds, const int32_t* imap, const int32_t* jmap, const int32_t* rseeds,
+                 int32_t* icsdsw, int32_t* icsdlw) {
+  if (!((lsswr || lslwr) && (isubc_lw == 2 || isubc_sw == 2))) return 0;
+  if (lrseeds) {
+    const int ld = ld_rseeds ? ld_rseeds : n;
+    for (int ix = 0; ix < n; ++ix) {
+      icsdsw[ix] = rseeds[ix];
+      icsdlw[ix] = rseeds[ix + ld];
+    }
+    return 0;
+  }
+  const long long nr = std::llround(100.0 * std::sqrt(sec));       // nint(con_100*sqrt(sec))
+  const int32_t ipseed = (int32_t)(uint32_t)((uint64_t)(nr % ipsdlim) + 1u + (uint64_t)(int64_t)ipsd0);
+  const long long face = (long long)cnx * cny;
+  std::vector<int32_t> numrdm((size_t)(2 * face));
+  oracle_random_index(ipseed, ipsdlim, 2 * face, numrdm.data());
+  for (int ix = 0; ix < n; ++ix) {
+    const long long p = (long long)imap[ix] + isc - 1 + ((long long)jmap[ix] + jsc - 2) * cnx;
+    if (p < 1 || p > face) return 1;
+    icsdsw[ix] = numrdm[(size_t)(p - 1)];
+    icsdlw[ix] = numrdm[(size_t)(p - 1 + face)];
+  }
+  return 0;
+}
+
+// cmp_dcorr_lgth_hogan (physics/Radiation/radiation_cloud_overlap.F90:28-50)
+void oracle_dcorr_hogan(int ncol, const double* lat, double con_pi, double* dcorr) {
+  const double min_dcorr = 0.6;
+  for (int i = 0; i < ncol; ++i) dcorr[i] = std::max(min_dcorr, 2.78 - 4.6 * std::fabs(lat[i] / con_pi));
+}
+
+// cmp_dcorr_lgth_oreopoulos (radiation_cloud_overlap.F90:58-93)
+void oracle_dcorr_oreopoulos(int ncol, const double* lat, double juldat, int yearlength, double* dcorr) {
+  const double am1 = 1.4315, am2 = 2.1219, am4 = -25.584, amr = 7.0;
+  for (int i = 0; i < ncol; ++i) {
+    double am3;
+    if (juldat > 181.0) am3 = -(4.0 * amr * (juldat - 272.0) / (double)yearlength);
+    else am3 = 4.0 * amr * (juldat - 91.0) / (double)yearlength;
+    const double d = lat[i] - am3;
+    dcorr[i] = am1 + am2 * std::exp(-(d * d) / (am4 * am4));
+  }
+}
+
+// get_alpha_exper (radiation_cloud_overlap.F90:99-145); (ncol, nlay) arrays
+// column-major with leading dimension ld.
+void oracle_alpha_exper(int ncol, int nlay, int ld, int iovr, int iovr_exprand, const double* dzlay,
+                        const double* dcorr, const double* cld_frac, double* alpha) {
+  for (int i = 0; i < ncol; ++i) {
+    alpha[i] = 0.0;
+    for (int k = 1; k < nlay; ++k) alpha[i + (size_t)ld * k] = std::exp(-dzlay[i + (size_t)ld * k] / dcorr[i]);
+  }
+  if (iovr == iovr_exprand) {
+    for (int k = 1; k < nlay; ++k)
+      for (int i = 0; i < ncol; ++i)
+        if (cld_frac[i + (size_t)ld * k] == 0.0 && cld_frac[i + (size_t)ld * (k - 1)] > 0.0)
+          alpha[i + (size_t)ld * k] = 0.0;
+  }
+}
+
+// The overlap block of radiation_clouds.f:837-856.
+void oracle_overlap_params(int ncol, int nlay, int ld, int idcor, int idcor_con, int idcor_hogan,
+                           int idcor_oreopoulos, double dcorr_con, const double* xlat, const double* latdeg,
+                           double julian, int yearlen, double con_pi, int iovr, int iovr_dcorr, int iovr_exp,
+                           int iovr_exprand, const double* dzlay, const double* cld_frac, double* de_lgth,
+                           double* alpha) {
+  if (idcor == idcor_hogan) oracle_dcorr_hogan(ncol, xlat, con_pi, de_lgth);
+  if (idcor == idcor_oreopoulos) oracle_dcorr_oreopoulos(ncol, latdeg, julian, yearlen, de_lgth);
+  if (idcor == idcor_con)
+    for (int i = 0; i < ncol; ++i) de_lgth[i] = dcorr_con;
+  if (iovr == iovr_dcorr || iovr == iovr_exp || iovr == iovr_exprand) {
+    oracle_alpha_exper(ncol, nlay, ld, iovr, iovr_exprand, dzlay, de_lgth, cld_frac, alpha);
+  } else {
+    for (int i = 0; i < ncol; ++i) de_lgth[i] = 0.0;
+    for (int k = 0; k < nlay; ++k)
+      for (int i = 0; i < ncol; ++i) alpha[i + (size_t)ld * k] = 0.0;
+  }
+}
+
+// rrtmg_lw_post_run (physics/Radiation/RRTMG/rrtmg_lw_post.F90:13-77);
+// (im, ...) arrays column-major with leading dimension im.
+void oracle_post(int im, int levs, int ltp, int lm, int kd, int lslwr, int lwhtr, const double* tsfa,
+                 const double* htlwc, const double* htlw0, const double* sfcflw, double* tsflw, double* sfcdlw,
+                 double* htrlw, double* lwhc) {
+  (void)ltp;
+  if (!lslwr) return;
+  for (int i = 0; i < im; ++i) tsflw[i] = tsfa[i];
+  for (int k = 1; k <= lm; ++k) {
+    const int k1 = k + kd;
+    for (int i = 0; i < im; ++i) htrlw[i + (size_t)im * (k - 1)] = htlwc[i + (size_t)im * (k1 - 1)];
+  }
+  if (lm < levs)
+    for (int k = lm + 1; k <= levs; ++k)
+      for (int i = 0; i < im; ++i) htrlw[i + (size_t)im * (k - 1)] = htrlw[i + (size_t)im * (lm - 1)];
+  if (lwhtr) {
+    for (int k = 1; k <= lm; ++k) {
+      const int k1 = k + kd;
+      for (int i = 0; i < im; ++i) lwhc[i + (size_t)im * (k - 1)] = htlw0[i + (size_t)im * (k1 - 1)];
+    }
+    if (lm < levs)
+      for (int k = lm + 1; k <= levs; ++k)
+        for (int i = 0; i < im; ++i) lwhc[i + (size_t)im * (k - 1)] = lwhc[i + (size_t)im * (lm - 1)];
+  }
+  for (int i = 0; i < im; ++i) sfcdlw[i] = sfcflw[4 * (size_t)i + 2];   // sfcflw%dnfxc
 }
 
 }  // extern "C"

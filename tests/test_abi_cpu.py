@@ -37,7 +37,9 @@ def test_struct_layout_matches_header(tmp_path):
     if not shutil.which("gcc"):
         pytest.skip("gcc not available")
     structs = {"rrtmg_lw_run_args": abi.RunArgs, "rrtmg_lw_init_args": abi.InitArgs,
-               "rrtmg_lw_exec": abi.ExecArgs}
+               "rrtmg_lw_exec": abi.ExecArgs, "rrtmg_lw_tuning": abi.Tuning,
+               "rrtmg_lw_seed_args": abi.SeedArgs, "rrtmg_lw_overlap_args": abi.OverlapArgs,
+               "rrtmg_lw_post_args": abi.PostArgs}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rrtmg_lw_gpu.h"', 'int main(void){']
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
