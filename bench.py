@@ -395,7 +395,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    rc, msg = lw.rlwinit(device=local, me=rank)
+    rc, msg = lw.rlwinit(device=local, me=1)   # me != 0: no banner, stdout carries only the JSON line
     assert rc == 0, msg
     ncols, nlay = cfg["ncols"], cfg["nlay"]
     # each rank owns its own shard of columns (weak scaling)

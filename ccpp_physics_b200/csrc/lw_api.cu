@@ -1028,6 +1028,7 @@ extern "C" int rrtmg_lw_gpu_autotune(const rrtmg_lw_run_args* blocks, int32_t nb
 }
 
 extern "C" void rrtmg_lw_gpu_finalize(void) {
+  lw::prep_release();
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g.ready) return;
   cudaSetDevice(g.device);

@@ -41,8 +41,14 @@ struct McicaStage {
 cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int ncols, int nlay, int iovr,
                          int isubclw, int top_at_1, const McicaStage& stage, uint32_t* bits, int num_sms,
                          cudaStream_t st);
-// random_index of one twister stream (lw_mcica.cu): out[0..m) = max(ceiling(h * imax), 1)
-cudaError_t seed_index_launch(int32_t seed, int32_t imax, long long m, int32_t* out, cudaStream_t st);
+// raw state words of one twister stream (lw_mcica.cu): raw[j] is what draw j tempers
+cudaError_t seed_stream_launch(int32_t seed, long long m, uint32_t* raw, cudaStream_t st);
+// icsdsw/icsdlw of n columns from the raw words of a face's stream
+// (lw_mcica.cu); *bad receives the smallest column whose grid index is outside
+// the face
+cudaError_t seed_gather_launch(const uint32_t* raw, const int32_t* imap, const int32_t* jmap, int n, int isc,
+                               int jsc, int cnx, long long face, int32_t imax, int32_t* icsdsw, int32_t* icsdlw,
+                               int* bad, cudaStream_t st);
 
 // learned gas optics (lw_mlp.cu): network stage of a chunk, its
 // normalisation/envelope (nullptr until a network is loaded) and the
@@ -54,6 +60,8 @@ unsigned int* surrogate_fallback_counter();
 
 // device chosen by rrtmg_lw_gpu_init, -1 before init (lw_api.cu)
 int selected_device();
+// frees the device scratch of the steps either side of the run (lw_prep.cu)
+void prep_release();
 
 // layers per lane of the column kernels (NLP = 32 V padded layers)
 inline int pick_v(int nlay) { return nlay <= 63 ? 2 : nlay <= 127 ? 4 : 8; }

@@ -368,22 +368,20 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
   }
 }
 
-// random_index_t (MT:489-503) of one stream: random_setseed_t(seed), then m
-// draws h, each giving max(ceiling(h * imax), 1).  One CTA walks the stream;
-// the 624-word state is double-buffered in shared memory, so a twist is its
+// The raw (untempered) words of one twister stream after
+// random_setseed_t(seed) (MT:285-299): out[j] is the state word that draw j
+// of random_number_t (MT:330-372) tempers.  One CTA walks the stream; the
+// 624-word state is double-buffered in shared memory, so a twist is its
 // three dependency phases (words 0..226 from the old state, 227..453 and
 // 454..622 from words 227 back in the new one, word 623 from new words 0 and
-// 396) with one barrier each and no read-before-write hazard.  Each word is
-// tempered, converted and stored as soon as its phase has produced it.
+// 396) with one barrier each and no read-before-write hazard.  Only integer
+// work sits on this serial path; tempering and the conversion to a random
+// index run later, in parallel, for the words that are used
+// (seed_index_of).
 constexpr int kSeedThreads = 256;
 
-__device__ __forceinline__ int32_t index_of(uint32_t w, double imax) {
-  const double c = ceil(u32_unit(temper(w)) * imax);   // h * imax rounds as in the Fortran
-  return c < 1.0 ? 1 : (int32_t)c;
-}
-
-__global__ void __launch_bounds__(kSeedThreads) lw_seed_index_kernel(uint32_t seed, int32_t imax, long long m,
-                                                                     int32_t* __restrict__ out) {
+__global__ void __launch_bounds__(kSeedThreads) lw_seed_stream_kernel(uint32_t seed, long long m,
+                                                                      uint32_t* __restrict__ out) {
   __shared__ uint32_t s[2][624];
   const int t = threadIdx.x;
   if (t == 0) {   // MT:290-296, signed wrap = unsigned multiply
@@ -392,42 +390,80 @@ __global__ void __launch_bounds__(kSeedThreads) lw_seed_index_kernel(uint32_t se
     for (int i = 1; i < 624; ++i) { v *= 69069u; s[0][i] = v; }
   }
   __syncthreads();
-  const double dmax = (double)imax;
   int cur = 0;
   for (long long base = 0; base < m; base += 624) {
     const uint32_t* o = s[cur];
     uint32_t* w = s[cur ^ 1];
-    long long left = m - base;
+    const long long left = m - base;
     if (t < 227) {   // words 0..226
-      w[t] = mt_word(o[t], o[t + 1], o[t + 397]);
-      if (t < left) out[base + t] = index_of(w[t], dmax);
+      const uint32_t v = mt_word(o[t], o[t + 1], o[t + 397]);
+      w[t] = v;
+      if (t < left) out[base + t] = v;
     }
     __syncthreads();
     if (t < 227) {   // words 227..453
       const int kk = 227 + t;
-      w[kk] = mt_word(o[kk], o[kk + 1], w[kk - 227]);
-      if (kk < left) out[base + kk] = index_of(w[kk], dmax);
+      const uint32_t v = mt_word(o[kk], o[kk + 1], w[kk - 227]);
+      w[kk] = v;
+      if (kk < left) out[base + kk] = v;
     }
     __syncthreads();
     if (t < 169) {   // words 454..622
       const int kk = 454 + t;
-      w[kk] = mt_word(o[kk], o[kk + 1], w[kk - 227]);
-      if (kk < left) out[base + kk] = index_of(w[kk], dmax);
+      const uint32_t v = mt_word(o[kk], o[kk + 1], w[kk - 227]);
+      w[kk] = v;
+      if (kk < left) out[base + kk] = v;
     } else if (t == 169) {   // word 623
-      w[623] = mt_word(o[623], w[0], w[396]);
-      if (623 < left) out[base + 623] = index_of(w[623], dmax);
+      const uint32_t v = mt_word(o[623], w[0], w[396]);
+      w[623] = v;
+      if (623 < left) out[base + 623] = v;
     }
     __syncthreads();
     cur ^= 1;
   }
 }
 
+// random_index_t (MT:489-503) of one raw word: max(ceiling(h * imax), 1)
+// with h = random_number_t's harvest of that word; h * imax rounds as in the
+// Fortran (FP64 product, no contraction).
+__device__ __forceinline__ int32_t seed_index_of(uint32_t raw, int32_t imax) {
+  const double c = ceil(__dmul_rn(u32_unit(temper(raw)), (double)imax));
+  return c < 1.0 ? 1 : (int32_t)c;
+}
+
+// icsdsw/icsdlw of column ix (GFS_rad_time_vary.fv3.F90:76-82): with
+// p = i+isc-1 + (j+jsc-2) cnx (1-based), numrdm(p) and numrdm(p + cnx cny),
+// numrdm = random_index(imax) of the face's stream.  A p outside the face
+// records the smallest such column in *bad and writes nothing for it.
+__global__ void lw_seed_gather_kernel(const uint32_t* __restrict__ raw, const int32_t* __restrict__ imap,
+                                      const int32_t* __restrict__ jmap, int n, int isc, int jsc, int cnx,
+                                      long long face, int32_t imax, int32_t* icsdsw, int32_t* icsdlw, int* bad) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ix >= n) return;
+  const long long p = (long long)imap[ix] + isc - 1 + ((long long)jmap[ix] + jsc - 2) * cnx;
+  if (p < 1 || p > face) {
+    atomicMin(bad, ix);
+    return;
+  }
+  icsdsw[ix] = seed_index_of(raw[p - 1], imax);
+  icsdlw[ix] = seed_index_of(raw[p - 1 + face], imax);
+}
+
 // host side ------------------------------------------------------------------
 
-cudaError_t seed_index_launch(int32_t seed, int32_t imax, long long m, int32_t* out, cudaStream_t st) {
+cudaError_t seed_stream_launch(int32_t seed, long long m, uint32_t* raw, cudaStream_t st) {
   if (m <= 0) return cudaSuccess;
   const uint32_t s = (uint32_t)(seed == 0 ? 4357 : seed);   // MT:291
-  lw_seed_index_kernel<<<1, kSeedThreads, 0, st>>>(s, imax, m, out);
+  lw_seed_stream_kernel<<<1, kSeedThreads, 0, st>>>(s, m, raw);
+  return cudaGetLastError();
+}
+
+cudaError_t seed_gather_launch(const uint32_t* raw, const int32_t* imap, const int32_t* jmap, int n, int isc,
+                               int jsc, int cnx, long long face, int32_t imax, int32_t* icsdsw, int32_t* icsdlw,
+                               int* bad, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  lw_seed_gather_kernel<<<(n + 255) / 256, 256, 0, st>>>(raw, imap, jmap, n, isc, jsc, cnx, face, imax, icsdsw,
+                                                         icsdlw, bad);
   return cudaGetLastError();
 }
 

@@ -12,8 +12,8 @@
 //                                rrtmg_lw_post.F90:13-77)
 //
 // The seed stream is one Mersenne-twister stream walked by one CTA
-// (lw_mcica.cu); the face's indices land in a device buffer and one thread
-// per column gathers its pair.  The overlap parameters run one thread per
+// (lw_mcica.cu) into a device buffer of raw words; one thread per column then
+// tempers and converts the two words it uses.  The overlap parameters run one thread per
 // column over its layers (coalesced across columns); the post step one
 // thread per (column, level) element.  This file is compiled without FMA
 // contraction, so every product and sum rounds as the Fortran's does.
@@ -23,6 +23,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -34,23 +35,6 @@
 namespace {
 
 // ---------------------------------------------------------------- kernels --
-
-// icsdsw/icsdlw of column ix from the face's indices numrdm[0, 2 cnx cny)
-// (GFS_rad_time_vary.fv3.F90:76-82); a grid index outside the face records
-// the smallest such column in *bad and writes nothing for it.
-__global__ void seed_gather_kernel(const int32_t* __restrict__ numrdm, const int32_t* __restrict__ imap,
-                                   const int32_t* __restrict__ jmap, int n, int isc, int jsc, int cnx,
-                                   long long face, int32_t* icsdsw, int32_t* icsdlw, int* bad) {
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ix >= n) return;
-  const long long p = (long long)imap[ix] + isc - 1 + ((long long)jmap[ix] + jsc - 2) * cnx;   // 1-based
-  if (p < 1 || p > face) {
-    atomicMin(bad, ix);
-    return;
-  }
-  icsdsw[ix] = numrdm[p - 1];
-  icsdlw[ix] = numrdm[p - 1 + face];
-}
 
 // lrseeds: seeds supplied by the host model (GFS_rad_time_vary.fv3.F90:66-70)
 __global__ void seed_copy_kernel(const int32_t* __restrict__ rseeds, int n, int ld, int32_t* icsdsw,
@@ -75,42 +59,72 @@ struct OverlapK {
   double *de_lgth, *alpha_out;
 };
 
-__global__ void overlap_kernel(OverlapK a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.npts) return;
-  if (a.zero) {
-    a.de_lgth[i] = 0.0;
-    for (int k = 0; k < a.nlay; ++k) a.alpha_out[i + (size_t)a.ld * k] = 0.0;
-    return;
-  }
+// Decorrelation length of column i by the selected routine, or the stored one.
+__device__ __forceinline__ double dcorr_of(const OverlapK& a, int i) {
   if (a.dcorr == kDcorrHogan) {
     // max(min_dcorr, 2.78 - 4.6 |lat / pi|), eq. 13 (radiation_cloud_overlap.F90:44-47)
-    a.de_lgth[i] = fmax(0.6, 2.78 - 4.6 * fabs(a.xlat[i] / a.con_pi));
-  } else if (a.dcorr == kDcorrOreopoulos) {
+    return fmax(0.6, 2.78 - 4.6 * fabs(a.xlat[i] / a.con_pi));
+  }
+  if (a.dcorr == kDcorrOreopoulos) {
     // eqs. 10-11 with am1, am2, am4, amr of Table 1 (radiation_cloud_overlap.F90:74-90)
     const double am1 = 1.4315, am2 = 2.1219, am4 = -25.584, amr = 7.0;
     const double am3 = (a.julian > 181.0) ? -(4.0 * amr * (a.julian - 272.0) / (double)a.yearlen)
                                           : 4.0 * amr * (a.julian - 91.0) / (double)a.yearlen;
     const double d = a.latdeg[i] - am3;
-    a.de_lgth[i] = am1 + am2 * exp(-(d * d) / (am4 * am4));
-  } else if (a.dcorr == kDcorrCon) {
-    a.de_lgth[i] = a.dcorr_con;
+    return am1 + am2 * exp(-(d * d) / (am4 * am4));
   }
-  if (!a.alpha) return;
-  // get_alpha_exper (radiation_cloud_overlap.F90:122-141); the exprand rule
-  // reads only cld_frac, so it is applied in the same pass
-  const double dl = a.de_lgth[i];
-  a.alpha_out[i] = 0.0;
-  double cf_prev = a.exprand ? a.cld_frac[i] : 0.0;
-  for (int k = 1; k < a.nlay; ++k) {
-    const size_t o = i + (size_t)a.ld * k;
-    double al = exp(-a.dzlay[o] / dl);
-    if (a.exprand) {
-      const double cf = a.cld_frac[o];
-      if (cf == 0.0 && cf_prev > 0.0) al = 0.0;
-      cf_prev = cf;
+  if (a.dcorr == kDcorrCon) return a.dcorr_con;
+  return a.de_lgth[i];
+}
+
+// One thread per column (coalesced across the warp for every layer): the
+// column's decorrelation length, then alpha of its layers
+// (get_alpha_exper, radiation_cloud_overlap.F90:122-141) kOverlapChunk at a
+// time, the chunk's loads issued together ahead of its stores; the
+// exponential-random rule keeps the layer below's cloud fraction in a
+// register.
+constexpr int kOverlapChunk = 8;
+
+__global__ void overlap_kernel(OverlapK a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.npts) return;
+  const size_t ld = (size_t)a.ld;
+  if (a.zero) {   // radiation_clouds.f:853-855
+    a.de_lgth[i] = 0.0;
+    for (int k = 0; k < a.nlay; ++k) a.alpha_out[i + ld * k] = 0.0;
+    return;
+  }
+  const double dl = dcorr_of(a, i);
+  if (a.dcorr != kDcorrNone) a.de_lgth[i] = dl;
+  if (!a.alpha || a.nlay == 0) return;
+  const double* __restrict__ dzp = a.dzlay + i;
+  const double* __restrict__ cfp = a.cld_frac + i;
+  double* __restrict__ out = a.alpha_out + i;
+  out[0] = 0.0;
+  double cf_prev = a.exprand ? cfp[0] : 0.0;
+  for (int k0 = 1; k0 < a.nlay; k0 += kOverlapChunk) {
+    double dz[kOverlapChunk], cf[kOverlapChunk];
+#pragma unroll
+    for (int u = 0; u < kOverlapChunk; ++u) {
+      const int k = k0 + u;
+      dz[u] = 1.0;
+      cf[u] = 1.0;
+      if (k < a.nlay) {
+        dz[u] = __ldcs(dzp + ld * k);
+        if (a.exprand) cf[u] = __ldcs(cfp + ld * k);
+      }
     }
-    a.alpha_out[o] = al;
+#pragma unroll
+    for (int u = 0; u < kOverlapChunk; ++u) {
+      const int k = k0 + u;
+      if (k >= a.nlay) break;
+      double al = exp(-dz[u] / dl);
+      if (a.exprand) {
+        if (cf[u] == 0.0 && cf_prev > 0.0) al = 0.0;
+        cf_prev = cf[u];
+      }
+      __stcs(out + ld * k, al);
+    }
   }
 }
 
@@ -120,27 +134,45 @@ struct PostK {
   double *tsflw, *sfcdlw, *htrlw, *lwhc;
 };
 
-// One thread per (column, level) element of htrlw/lwhc
-// (rrtmg_lw_post.F90:48-70); the level-0 threads also copy the per-column
-// fields (:46, :73).
+// rrtmg_lw_post_run (rrtmg_lw_post.F90:46-73).  Levels 1..lm of htrlw/lwhc
+// are one contiguous block of the source (levels kd+1..kd+lm), copied with
+// four loads in flight per thread; levels lm+1..levs repeat level lm; the
+// per-column fields last.
 __global__ void post_kernel(PostK a) {
-  const long long total = (long long)a.im * a.levs;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(e / a.im), i = (int)(e - (long long)k * a.im);
-    const int src = (k < a.lm ? k : a.lm - 1) + a.kd;
-    a.htrlw[e] = a.htlwc[i + (size_t)a.im * src];
-    if (a.lwhtr) a.lwhc[e] = a.htlw0[i + (size_t)a.im * src];
-    if (k == 0) {
-      a.tsflw[i] = a.tsfa[i];
-      a.sfcdlw[i] = a.sfcflw[4 * (size_t)i + 2];
+  const size_t stride = (size_t)gridDim.x * blockDim.x, t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t im = (size_t)a.im, nb = im * a.lm;
+  const double* s1 = a.htlwc + im * a.kd;
+  const double* s2 = a.htlw0 + im * a.kd;
+  for (size_t e = t0; e < nb; e += 4 * stride) {
+    double v[4], w[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const size_t q = e + u * stride;
+      if (q < nb) {
+        v[u] = __ldcs(s1 + q);
+        if (a.lwhtr) w[u] = __ldcs(s2 + q);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const size_t q = e + u * stride;
+      if (q < nb) {
+        __stcs(a.htrlw + q, v[u]);
+        if (a.lwhtr) __stcs(a.lwhc + q, w[u]);
+      }
     }
   }
-  if (a.levs == 0) {   // no levels: the per-column fields only
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.im; i += gridDim.x * blockDim.x) {
-      a.tsflw[i] = a.tsfa[i];
-      a.sfcdlw[i] = a.sfcflw[4 * (size_t)i + 2];
+  if (a.lm >= 1) {
+    for (int k = a.lm; k < a.levs; ++k) {
+      for (size_t i = t0; i < im; i += stride) {
+        a.htrlw[im * k + i] = s1[im * (a.lm - 1) + i];
+        if (a.lwhtr) a.lwhc[im * k + i] = s2[im * (a.lm - 1) + i];
+      }
     }
+  }
+  for (size_t i = t0; i < im; i += stride) {
+    a.tsflw[i] = a.tsfa[i];
+    a.sfcdlw[i] = a.sfcflw[4 * i + 2];
   }
 }
 
@@ -165,15 +197,51 @@ int fail(char* errmsg, int32_t len, const char* what, cudaError_t e) {
     if (e_ != cudaSuccess) return fail(errmsg, errmsg_len, what, e_); \
   } while (0)
 
-// Host-memory calls: the arrays of a call are staged through one device
-// buffer (stream-ordered allocation).  Outputs are copied in as well, so
-// elements a step leaves alone keep the caller's values.
+// Device scratch of the calling thread (seed stream, host-memory staging),
+// kept between calls.  Every call that uses it synchronises its stream before
+// returning, so a later call of the same thread may reuse or replace it.
+struct PrepScratch {
+  int device = -1;
+  char* p = nullptr;
+  size_t bytes = 0;
+};
+std::mutex g_scratch_mu;
+std::vector<PrepScratch*> g_scratch;   // every thread's scratch, released by prep_release
+thread_local PrepScratch* tl_scratch = nullptr;
+
+cudaError_t scratch(size_t need, char** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (!tl_scratch) {
+    tl_scratch = new PrepScratch();
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    g_scratch.push_back(tl_scratch);
+  }
+  PrepScratch& s = *tl_scratch;
+  if (s.p && (s.bytes < need || s.device != dev)) {
+    cudaFree(s.p);   // no queued work uses it (see above)
+    s.p = nullptr;
+    s.bytes = 0;
+  }
+  if (!s.p) {
+    const size_t n = std::max<size_t>(need, 1 << 20) * 5 / 4;
+    e = cudaMalloc((void**)&s.p, n);
+    if (e != cudaSuccess) return e;
+    s.bytes = n;
+    s.device = dev;
+  }
+  *out = s.p;
+  return cudaSuccess;
+}
+
+// Host-memory calls: the arrays of a call are staged through the thread's
+// scratch.  Outputs are copied in as well, so elements a step leaves alone
+// keep the caller's values.  upload() also reserves `extra` device bytes for
+// the call (returned in *extra_p), host memory or not.
 class Stager {
  public:
   Stager(bool host, cudaStream_t st) : host_(host), st_(st) {}
-  ~Stager() {
-    if (buf_) cudaFreeAsync(buf_, st_);
-  }
   template <typename T>
   void add(T*& field, size_t count, bool out) {
     if (!host_ || !field || count == 0) return;
@@ -181,10 +249,11 @@ class Stager {
                           (void*)field, count * sizeof(T), out, total_});
     total_ += (count * sizeof(T) + 255) / 256 * 256;
   }
-  cudaError_t upload() {
-    if (!host_ || total_ == 0) return cudaSuccess;
-    cudaError_t e = cudaMallocAsync((void**)&buf_, total_, st_);
+  cudaError_t upload(size_t extra = 0, char** extra_p = nullptr) {
+    if (total_ + extra == 0) return cudaSuccess;
+    cudaError_t e = scratch(total_ + extra, &buf_);
     if (e != cudaSuccess) return e;
+    if (extra_p) *extra_p = buf_ + total_;
     for (Item& it : items_) {
       e = cudaMemcpyAsync(buf_ + it.off, it.host, it.bytes, cudaMemcpyHostToDevice, st_);
       if (e != cudaSuccess) return e;
@@ -290,24 +359,18 @@ extern "C" int rrtmg_lw_gpu_seeds(const rrtmg_lw_seed_args* a, const rrtmg_lw_ex
   S.add(b.jmap, n, false);
   S.add(b.icsdsw, n, true);
   S.add(b.icsdlw, n, true);
-  CK(S.upload(), "staging");
-  char* tmp = nullptr;
-  const size_t nbytes = ((size_t)(2 * face) * sizeof(int32_t) + 255) / 256 * 256;
-  CK(cudaMallocAsync((void**)&tmp, nbytes + sizeof(int), st), "cudaMallocAsync(numrdm)");
-  int32_t* numrdm = (int32_t*)tmp;
-  int* bad = (int*)(tmp + nbytes);
+  char* extra = nullptr;
+  const size_t raw_bytes = ((size_t)(2 * face) * sizeof(uint32_t) + 255) / 256 * 256;
+  CK(S.upload(raw_bytes + 256, &extra), "staging");
+  uint32_t* raw = (uint32_t*)extra;
+  int* bad = (int*)(extra + raw_bytes);
   const int none = INT_MAX;
-  cudaError_t e = cudaMemcpyAsync(bad, &none, sizeof(int), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = lw::seed_index_launch(ipseed, a->ipsdlim, 2 * face, numrdm, st);
-  if (e == cudaSuccess) {
-    seed_gather_kernel<<<blocks_for(n, 256), 256, 0, st>>>(numrdm, b.imap, b.jmap, n, a->isc, a->jsc, a->cnx, face,
-                                                           b.icsdsw, b.icsdlw, bad);
-    e = cudaGetLastError();
-  }
   int first_bad = INT_MAX;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&first_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, st);
-  cudaFreeAsync(tmp, st);
-  if (e != cudaSuccess) return fail(errmsg, errmsg_len, "seed stream", e);
+  CK(cudaMemcpyAsync(bad, &none, sizeof(int), cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+  CK(lw::seed_stream_launch(ipseed, 2 * face, raw, st), "seed stream launch");
+  CK(lw::seed_gather_launch(raw, b.imap, b.jmap, n, a->isc, a->jsc, a->cnx, face, a->ipsdlim, b.icsdsw, b.icsdlw,
+                            bad, st), "seed gather launch");
+  CK(cudaMemcpyAsync(&first_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
   if (finish(S, true, true, st, errmsg, errmsg_len)) return 1;
   if (first_bad != INT_MAX) {
     set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_seeds: column %d: imap/jmap/isc/jsc give a grid index outside the "
@@ -371,7 +434,9 @@ extern "C" int rrtmg_lw_gpu_overlap_params(const rrtmg_lw_overlap_args* a, const
   CK(S.upload(), "staging");
   k.xlat = b.xlat; k.latdeg = b.latdeg; k.dzlay = b.dzlay; k.cld_frac = b.cld_frac;
   k.de_lgth = b.de_lgth; k.alpha_out = b.alpha;
-  if (k.dcorr || k.alpha || k.zero) overlap_kernel<<<blocks_for(npts, 128), 128, 0, st>>>(k);
+  if (k.dcorr || k.alpha || k.zero) {
+    overlap_kernel<<<blocks_for(npts, 128), 128, 0, st>>>(k);
+  }
   return finish(S, host, x->sync != 0, st, errmsg, errmsg_len);
 }
 
@@ -413,8 +478,21 @@ extern "C" int rrtmg_lw_gpu_post(const rrtmg_lw_post_args* a, const rrtmg_lw_exe
   }
   CK(S.upload(), "staging");
   PostK k{im, levs, lm, kd, a->lwhtr ? 1 : 0, b.tsfa, b.htlwc, b.htlw0, b.sfcflw, b.tsflw, b.sfcdlw, b.htrlw, b.lwhc};
-  const long long total = levs > 0 ? (long long)im * levs : im;
-  const int grid = (int)std::min<long long>(blocks_for(total, 256), 148LL * 16);
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long work = std::max<long long>((long long)im * lm / 4, im);
+  const int grid = (int)std::min<long long>(blocks_for(work, 256), 8LL * sms);
   post_kernel<<<grid, 256, 0, st>>>(k);
   return finish(S, host, x->sync != 0, st, errmsg, errmsg_len);
+}
+
+// Frees every thread's scratch (rrtmg_lw_gpu_finalize); the records stay, so a
+// later call regrows its buffer.
+void lw::prep_release() {
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  for (PrepScratch* sc : g_scratch) {
+    if (sc->p) cudaFree(sc->p);
+    sc->p = nullptr;
+    sc->bytes = 0;
+  }
 }
