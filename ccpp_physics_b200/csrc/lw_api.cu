@@ -50,7 +50,7 @@ struct DeviceState {
   int num_sms = 0;
   double* kt64 = nullptr;
   float* kt32 = nullptr;
-  double* tbl64 = nullptr;   // exp, tfn, tau (3 x (NTBL+1))
+  double* tbl64 = nullptr;   // records {exp, tfn, tau, 0} (4 x (NTBL+1))
   float* tbl32 = nullptr;
   Consts cs{};
   Shape tuned[2][9];         // autotuned launch shape per [fp32?][V]
@@ -214,7 +214,14 @@ extern "C" int rrtmg_lw_gpu_init(const rrtmg_lw_init_args* a, char* errmsg, int3
     ex[i] = (ta[i] >= explimit) ? expeps : std::exp(-ta[i]);
     tf[i] = (ta[i] < 0.06) ? ta[i] / 6.0 : 1.0 - 2.0 * ((1.0 / ta[i]) - (ex[i] / (1.0 - ex[i])));
   }
-  std::vector<float> tb32(tb.begin(), tb.end());
+  // interleave: record i = {exp_tbl(i), tfn_tbl(i), tau_tbl(i), 0}
+  std::vector<double> rec(4 * (NTBL + 1), 0.0);
+  for (int i = 0; i <= NTBL; ++i) {
+    rec[4 * i + 0] = ex[i];
+    rec[4 * i + 1] = tf[i];
+    rec[4 * i + 2] = ta[i];
+  }
+  std::vector<float> rec32(rec.begin(), rec.end());
 
   size_t nblob = (size_t)(rrtmg_lw_tables_blob_end - rrtmg_lw_tables_blob);
   if (nblob != sizeof(double) * RRTMG_LW_TABLES_NDOUBLE) {
@@ -229,13 +236,13 @@ extern "C" int rrtmg_lw_gpu_init(const rrtmg_lw_init_args* a, char* errmsg, int3
   if (!g.kt64) {
     CK(cudaMalloc(&g.kt64, kt.size() * sizeof(double)), "cudaMalloc(tables)");
     CK(cudaMalloc(&g.kt32, kt.size() * sizeof(float)), "cudaMalloc(tables)");
-    CK(cudaMalloc(&g.tbl64, tb.size() * sizeof(double)), "cudaMalloc(tables)");
-    CK(cudaMalloc(&g.tbl32, tb.size() * sizeof(float)), "cudaMalloc(tables)");
+    CK(cudaMalloc(&g.tbl64, rec.size() * sizeof(double)), "cudaMalloc(tables)");
+    CK(cudaMalloc(&g.tbl32, rec32.size() * sizeof(float)), "cudaMalloc(tables)");
   }
   CK(cudaMemcpy(g.kt64, kt.data(), kt.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
   CK(cudaMemcpy(g.kt32, kt32.data(), kt32.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
-  CK(cudaMemcpy(g.tbl64, tb.data(), tb.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
-  CK(cudaMemcpy(g.tbl32, tb32.data(), tb32.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
+  CK(cudaMemcpy(g.tbl64, rec.data(), rec.size() * sizeof(double), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
+  CK(cudaMemcpy(g.tbl32, rec32.data(), rec32.size() * sizeof(float), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
   CK(mcica_upload_powers(), "mcica powers upload");
   int optin = 0;
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, g.device), "cudaDeviceGetAttribute");
@@ -450,12 +457,12 @@ cudaError_t enqueue(Workspace* w, cudaStream_t st, const Block* dblk, const Bloc
   if (ev && (e = cudaEventRecord(ev[1], st)) != cudaSuccess) return e;
   const int V = pick_v(f.nlay);
   const bool hlwb = f.want_hlwb != 0;
-  Tables<double> t64{g.kt64, g.tbl64, g.tbl64 + (NTBL + 1), g.tbl64 + 2 * (NTBL + 1)};
+  Tables<double> t64{g.kt64, g.tbl64};
   if (precision == RRTMG_LW_FP64) {
     e = launch_column_fp64(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t64, t64, w->bits, w->scratch,
                            w->scratch_bytes, nullptr, nullptr, g.num_sms, sh, st, ev ? ev[3] : nullptr);
   } else {
-    Tables<float> t{g.kt32, g.tbl32, g.tbl32 + (NTBL + 1), g.tbl32 + 2 * (NTBL + 1)};
+    Tables<float> t{g.kt32, g.tbl32};
     e = launch_column_fp32(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t, t64, w->bits, w->scratch,
                            w->scratch_bytes, nullptr, nullptr, g.num_sms, sh, st, ev ? ev[3] : nullptr);
   }
@@ -851,13 +858,13 @@ extern "C" int rrtmg_lw_gpu_gas_optics(const rrtmg_lw_run_args* a, int32_t preci
   Block B;
   block_from_args(&a2, &B);
   const int V = pick_v(a2.nlay);
-  Tables<double> t64{g.kt64, g.tbl64, g.tbl64 + (NTBL + 1), g.tbl64 + 2 * (NTBL + 1)};
+  Tables<double> t64{g.kt64, g.tbl64};
   if (precision == RRTMG_LW_FP64) {
     CK(launch_column_fp64(V, false, nullptr, 1, B, a2.npts, f, g.cs, t64, t64, nullptr, nullptr, 0, taug, fracs,
                           g.num_sms, Shape(), st, nullptr),
        "gas optics launch");
   } else {
-    Tables<float> t{g.kt32, g.tbl32, g.tbl32 + (NTBL + 1), g.tbl32 + 2 * (NTBL + 1)};
+    Tables<float> t{g.kt32, g.tbl32};
     CK(launch_column_fp32(V, false, nullptr, 1, B, a2.npts, f, g.cs, t, t64, nullptr, nullptr, 0, taug, fracs,
                           g.num_sms, Shape(), st, nullptr),
        "gas optics launch");

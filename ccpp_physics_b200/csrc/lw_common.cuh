@@ -43,16 +43,28 @@ struct Consts {
 };
 
 // Coefficient tables in device memory, in the arithmetic precision R.
-// rlwinit tables (RLM:1474-1501) are one allocation: exp_tbl[0..NTBL], then
-// tfn_tbl, then tau_tbl, each NTBL+1 long (the kernels index them from
-// exp_tbl with constant offsets).
+// The rlwinit tables (RLM:1474-1501) are interleaved: record i is
+// {exp_tbl(i), tfn_tbl(i), tau_tbl(i), 0} at trec[4 i], so one lookup of the
+// transfer touches one 32-byte (FP64) or 16-byte (FP32) record.
 template <typename R>
 struct Tables {
   const R* kt;       // every radlw_datatb.f array (offsets lwtab::*)
-  const R* exp_tbl;
-  const R* tfn_tbl;  // = exp_tbl + NTBL + 1
-  const R* tau_tbl;  // = exp_tbl + 2 * (NTBL + 1)
+  const R* trec;     // (NTBL+1) records of 4
 };
+
+// exp_tbl(it), tfn_tbl(it), tau_tbl(it) of one record.
+__device__ __forceinline__ void tbl_rec(const double* trec, int it, double& ex, double& tf, double& ta) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(trec + 4 * it));
+  ex = v.x;
+  tf = v.y;
+  ta = __ldg(trec + 4 * it + 2);
+}
+__device__ __forceinline__ void tbl_rec(const float* trec, int it, float& ex, float& tf, float& ta) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(trec + 4 * it));
+  ex = v.x;
+  tf = v.y;
+  ta = v.z;
+}
 
 // Device-side view of one physics block (the arrays of one rrtmg_lw_run call).
 enum InField {

@@ -191,12 +191,12 @@ extern "C" int rrtmg_lw_gpu_run_noalloc(const rrtmg_lw_run_args* a, int32_t prec
                    v.num_sms, st);
   if (e == cudaSuccess) {
     if (precision == RRTMG_LW_FP64) {
-      Tables<double> t{v.kt64, v.tbl64, v.tbl64 + (NTBL + 1), v.tbl64 + 2 * (NTBL + 1)};
+      Tables<double> t{v.kt64, v.tbl64};
       e = launch_column_fp64(V, f.want_hlwb != 0, nullptr, 1, B, a->npts, f, v.cs, t, t, bits, scratch,
                              scratch_bytes, nullptr, nullptr, v.num_sms, Shape(), st, nullptr);
     } else {
-      Tables<float> t{v.kt32, v.tbl32, v.tbl32 + (NTBL + 1), v.tbl32 + 2 * (NTBL + 1)};
-      Tables<double> t64{v.kt64, v.tbl64, v.tbl64 + (NTBL + 1), v.tbl64 + 2 * (NTBL + 1)};
+      Tables<float> t{v.kt32, v.tbl32};
+      Tables<double> t64{v.kt64, v.tbl64};
       e = launch_column_fp32(V, f.want_hlwb != 0, nullptr, 1, B, a->npts, f, v.cs, t, t64, bits, scratch,
                              scratch_bytes, nullptr, nullptr, v.num_sms, Shape(), st, nullptr);
     }

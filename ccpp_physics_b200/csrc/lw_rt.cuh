@@ -45,6 +45,67 @@ __device__ __forceinline__ void load_vec(const R* __restrict__ p, R (&o)[V]) {
   }
 }
 
+// Shared-memory staging of the transfer kernel's inputs.  Each lane copies
+// only its own V values of a field (cp.async, 16- or 8-byte pieces) and reads
+// only them back, so no lane waits for another.  Per warp, in elements of R:
+// kRtDepth stages of {tau, frac} for the g-point pipeline, then two buffers
+// of the three band fields {pklay, pklev, taucld}; within a field, lane l's
+// values sit at [l V, l V + V).
+constexpr int kRtDepth = 3;
+template <typename R>
+__host__ __device__ constexpr bool rt_staged() { return sizeof(R) == 8; }
+template <int V>
+__host__ __device__ constexpr int rt_warp_elems() { return (2 * kRtDepth + 2 * 3) * 32 * V; }
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// V consecutive values (16-byte aligned for 16-byte pieces, 8-byte otherwise)
+template <typename R, int V>
+__device__ __forceinline__ void stage_vec(R* dst, const R* src) {
+  constexpr int B = V * (int)sizeof(R);
+  if constexpr (B % 16 == 0) {
+#pragma unroll
+    for (int o = 0; o < B; o += 16)
+      cp_async16(reinterpret_cast<char*>(dst) + o, reinterpret_cast<const char*>(src) + o);
+  } else {
+    static_assert(B == 8, "8- or 16k-byte lane vectors");
+    cp_async8(dst, src);
+  }
+}
+
+template <typename R, int V>
+__device__ __forceinline__ void lds_vec(const R* p, R (&o)[V]) {
+  if constexpr (sizeof(R) == 8) {
+#pragma unroll
+    for (int j = 0; j < V; j += 2) {
+      const double2 v = *reinterpret_cast<const double2*>(p + j);
+      o[j] = v.x; o[j + 1] = v.y;
+    }
+  } else if constexpr (V % 4 == 0) {
+#pragma unroll
+    for (int j = 0; j < V; j += 4) {
+      const float4 v = *reinterpret_cast<const float4*>(p + j);
+      o[j] = v.x; o[j + 1] = v.y; o[j + 2] = v.z; o[j + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; j += 2) {
+      const float2 v = *reinterpret_cast<const float2*>(p + j);
+      o[j] = v.x; o[j + 1] = v.y;
+    }
+  }
+}
+
 // Table-index quotient x / (bpade + x) and cloud transmittance exp(-x).  The
 // FP64 path keeps the exact operations (its table indices must match the
 // reference's); the FP32 path, already within its error bound of the FP64
@@ -75,11 +136,8 @@ __device__ __forceinline__ void layer_rt(R tau, R frac, R secd, R blay, R plevu,
     R tblind = tbl_quot(odepth);
     int itgas = min(NTBL, max(0, (int)(R(kTblint) * tblind + R(0.5))));
     if (!LW_OK(itgas >= 0 && itgas <= NTBL, 22, itgas)) itgas = 0;
-    const R* e = tab.exp_tbl + itgas;          // exp, tfn, tau tables are contiguous
-    trng = ldg(e);
+    tbl_rec(tab.trec, itgas, trng, gasfac, odepth);
     atrgas = one - trng;
-    gasfac = ldg(e + (NTBL + 1));
-    odepth = ldg(e + 2 * (NTBL + 1));
   }
   R dplnku = plevu - blay;
   R dplnkd = plevd - blay;
@@ -99,9 +157,9 @@ __device__ __forceinline__ void layer_rt(R tau, R frac, R secd, R blay, R plevu,
     } else {
       R tblind = tbl_quot(odtot);
       int ittot = min(NTBL, max(0, (int)(R(kTblint) * tblind + R(0.5))));
-      const R* e = tab.exp_tbl + ittot;
-      totfac = ldg(e + (NTBL + 1));
-      atrtot = one - ldg(e);
+      R ex, ta;
+      tbl_rec(tab.trec, ittot, ex, totfac, ta);
+      atrtot = one - ex;
     }
     R bbdtot = frac * (blay + dplnkd * totfac);
     R bbutot = frac * (blay + dplnku * totfac);
@@ -109,6 +167,8 @@ __device__ __forceinline__ void layer_rt(R tau, R frac, R secd, R blay, R plevu,
     o.tsu = bbutot * atrtot;
   }
 }
+
+extern __shared__ __align__(16) unsigned char lw_rt_smem[];
 
 template <typename R, int V, bool HLWB>
 __global__ void __launch_bounds__(128, LW_RT_MINB)
@@ -138,6 +198,12 @@ lw_rt_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int 
     const R* bcol = sc.band + (size_t)cc * 3 * NBANDS * NLP + k0;
     const uint32_t* cbw = bits_g + (size_t)c * NGPT * nw + (k0 >> 5);
     const uint32_t lmask = (k0 >= nlay) ? 0u : (nlay - k0 >= V ? (1u << V) - 1u : (1u << (nlay - k0)) - 1u);
+    // FP64: inputs staged through shared memory (the register budget at 4
+    // CTAs/SM cannot hold them); FP32: straight to registers.  This lane's
+    // slots: g-point stage s field q at sl + (2 s + q) 32 V, band buffer p
+    // field q at sl + (2 kRtDepth + 3 p + q) 32 V.
+    constexpr bool kStage = rt_staged<R>();
+    R* const sl = reinterpret_cast<R*>(lw_rt_smem) + (threadIdx.x >> 5) * rt_warp_elems<V>() + k0;
 
     double acc_tu[V], acc_td[V], acc_cu[V], acc_cd[V];
     double bnd_tu[HLWB ? V : 1], bnd_td[HLWB ? V : 1];
@@ -147,33 +213,76 @@ lw_rt_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int 
       if constexpr (HLWB) bnd_tu[j] = bnd_td[j] = 0.0;
     }
 
+    // copy groups (staged): group 0 = g-point 0 + band 0's fields, group 1 =
+    // g-point 1; the iteration of g-point g commits group g + 2 (g-point g + 2,
+    // and at a band's first g-point the next band's fields), then waits for
+    // group g
+    if constexpr (kStage) {
+      stage_vec<R, V>(sl, tcol);
+      stage_vec<R, V>(sl + 32 * V, fcol);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) stage_vec<R, V>(sl + (2 * kRtDepth + q) * 32 * V, bcol + (size_t)q * NBANDS * NLP);
+      cp_async_commit();
+      stage_vec<R, V>(sl + 2 * 32 * V, tcol + NLP);
+      stage_vec<R, V>(sl + 3 * 32 * V, fcol + NLP);
+      cp_async_commit();
+    }
+    uint32_t nbits = (mc && lmask && LW_OK((k0 >> 5) < nw, 27, k0)) ? __ldg(cbw) : 0u;
+
 #pragma unroll 1
     for (int b = 0; b < NBANDS; ++b) {
-      // band terms of the lane's layers: pklay(b,k+1), pklev(b,k..k+1), taucld(b,k+1)
-      R blay[V], plev[V], tcld[V];
-      load_vec<R, V>(bcol + (0 * NBANDS + b) * NLP, blay);
-      load_vec<R, V>(bcol + (1 * NBANDS + b) * NLP, plev);
-      load_vec<R, V>(bcol + (2 * NBANDS + b) * NLP, tcld);
-      const R plev_top = shdn(plev[0], 1);    // pklev of the level above the segment
       const R secd = R(crec[b]);
       const R pk0 = R(crec[16 + b]);          // pklay(b, 0): surface (RLM:2251-2262)
       const int ns = ns_of(b), ng = ng_of(b);
-      // inputs of the first g-point of the band; each iteration prefetches the next
-      R ntau[V], nfrac[V];
-      load_vec<R, V>(tcol + (size_t)ns * NLP, ntau);
-      load_vec<R, V>(fcol + (size_t)ns * NLP, nfrac);
-      uint32_t nbits = (mc && lmask && LW_OK((k0 >> 5) < nw, 27, k0)) ? __ldg(cbw + (size_t)ns * nw) : 0u;
+      const R* bsl = sl + (2 * kRtDepth + 3 * (b & 1)) * 32 * V;
+      // register path: the band's fields, and the band's first g-point (each
+      // iteration prefetches the next)
+      R rblay[kStage ? 1 : V], rplev[kStage ? 1 : V], rtcld[kStage ? 1 : V], ntau[kStage ? 1 : V],
+          nfrac[kStage ? 1 : V];
+      if constexpr (!kStage) {
+        load_vec<R, V>(bcol + (0 * NBANDS + b) * NLP, rblay);
+        load_vec<R, V>(bcol + (1 * NBANDS + b) * NLP, rplev);
+        load_vec<R, V>(bcol + (2 * NBANDS + b) * NLP, rtcld);
+        load_vec<R, V>(tcol + (size_t)ns * NLP, ntau);
+        load_vec<R, V>(fcol + (size_t)ns * NLP, nfrac);
+      }
 #pragma unroll 1
       for (int g = ns; g < ns + ng; ++g) {
-        R tau[V], frac[V];
+        // band terms of the lane's layers: pklay(b,k+1), pklev(b,k..k+1), taucld(b,k+1)
+        R tau[V], frac[V], blay[V], plev[V], tcld[V];
+        if constexpr (kStage) {
+          if (g + 2 < NGPT) {
+            const int s2 = (g + 2) % kRtDepth;
+            stage_vec<R, V>(sl + (2 * s2) * 32 * V, tcol + (size_t)(g + 2) * NLP);
+            stage_vec<R, V>(sl + (2 * s2 + 1) * 32 * V, fcol + (size_t)(g + 2) * NLP);
+          }
+          if (g == ns && b + 1 < NBANDS) {
+            R* nb = sl + (2 * kRtDepth + 3 * ((b + 1) & 1)) * 32 * V;
 #pragma unroll
-        for (int j = 0; j < V; ++j) { tau[j] = ntau[j]; frac[j] = nfrac[j]; }
-        const uint32_t cbits = (nbits >> (k0 & 31)) & lmask;
-        if (g + 1 < ns + ng && LW_OK(g + 1 < NGPT, 26, g)) {
-          load_vec<R, V>(tcol + (size_t)(g + 1) * NLP, ntau);
-          load_vec<R, V>(fcol + (size_t)(g + 1) * NLP, nfrac);
-          if (mc && lmask) nbits = __ldg(cbw + (size_t)(g + 1) * nw);
+            for (int q = 0; q < 3; ++q) stage_vec<R, V>(nb + q * 32 * V, bcol + (size_t)(q * NBANDS + b + 1) * NLP);
+          }
+          cp_async_commit();
+          cp_async_wait<2>();
+          const int s0 = g % kRtDepth;
+          lds_vec<R, V>(sl + (2 * s0) * 32 * V, tau);
+          lds_vec<R, V>(sl + (2 * s0 + 1) * 32 * V, frac);
+          lds_vec<R, V>(bsl, blay);
+          lds_vec<R, V>(bsl + 32 * V, plev);
+          lds_vec<R, V>(bsl + 2 * 32 * V, tcld);
+        } else {
+#pragma unroll
+          for (int j = 0; j < V; ++j) {
+            tau[j] = ntau[j]; frac[j] = nfrac[j];
+            blay[j] = rblay[j]; plev[j] = rplev[j]; tcld[j] = rtcld[j];
+          }
+          if (g + 1 < ns + ng) {
+            load_vec<R, V>(tcol + (size_t)(g + 1) * NLP, ntau);
+            load_vec<R, V>(fcol + (size_t)(g + 1) * NLP, nfrac);
+          }
         }
+        const R plev_top = shdn(plev[0], 1);    // pklev of the level above the segment
+        const uint32_t cbits = (nbits >> (k0 & 31)) & lmask;
+        if (g + 1 < NGPT && mc && lmask) nbits = __ldg(cbw + (size_t)(g + 1) * nw);
         LayRT<R> rt[V];
 #pragma unroll
         for (int j = 0; j < V; ++j) {

@@ -102,11 +102,8 @@ __device__ __forceinline__ GasL<R> grid_gas_layer(R tau, R frac, R secd, R blay,
   } else {
     const R tblind = tbl_quot(odepth);
     const int itgas = min(NTBL, max(0, (int)(R(kTblint) * tblind + R(0.5))));
-    const R* e = tab.exp_tbl + itgas;
-    o.trng = ldg(e);
+    tbl_rec(tab.trec, itgas, o.trng, gasfac, odepth);
     atrgas = R(1) - o.trng;
-    gasfac = ldg(e + (NTBL + 1));
-    odepth = ldg(e + 2 * (NTBL + 1));
   }
   o.odepth = odepth;
   o.frac = frac;
@@ -128,9 +125,8 @@ __device__ __forceinline__ void grid_tot_layer(R odtot, const Tables<R>& tab, R&
   } else {
     const R tblind = tbl_quot(odtot);
     const int ittot = min(NTBL, max(0, (int)(R(kTblint) * tblind + R(0.5))));
-    const R* e = tab.exp_tbl + ittot;
-    totfac = ldg(e + (NTBL + 1));
-    trnt = ldg(e);
+    R ta;
+    tbl_rec(tab.trec, ittot, trnt, totfac, ta);
     atrtot = R(1) - trnt;
   }
 }
