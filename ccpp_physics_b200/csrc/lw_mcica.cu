@@ -210,12 +210,52 @@ __device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const double* clr, c
   }
 }
 
-// Per-warp shared memory: mt[624], clear[nlay] = 1 - cldf (double), ring[cap].
-__host__ __device__ inline size_t mcica_warp_bytes(int nlay, int cap) {
-  return 624 * 4 + ((nlay * 8 + 15) & ~15) + (size_t)cap * 4 + 16;
+// The draws of random (iovr=0) and maximum-random (iovr=1) overlap come from
+// a ring that holds the raw (untempered) twister sequence itself: sequence
+// index s (x_0..x_623 = the seeding, draw p = tempered x_{624+p}) sits at
+// ring[s mod cap].  A twist appends the next 624 words in place,
+//   x_{j+t} = mt_word(x_{j+t-624}, x_{j+t-623}, x_{j+t-227}),
+// so there is no separate state array and no copy; cap is a multiple of
+// 624, so neither the block being written nor the one before it wraps.
+// Lanes walk g-points in rounds of kMcicaRound (5 x 28 = 140): the ring
+// holds one round's draws plus the twist history.
+constexpr int kMcicaRound = 28;
+
+// untempered word whose tempering is 2^32 - 1 (the only draw equal to 1)
+constexpr uint32_t kRawAllOnes = 0x12DD9BB3u;
+__host__ __device__ constexpr uint32_t temper_c(uint32_t y) {
+  return ((((y ^ (y >> 11)) ^ (((y ^ (y >> 11)) << 7) & kTmaskB)) ^
+           ((((y ^ (y >> 11)) ^ (((y ^ (y >> 11)) << 7) & kTmaskB)) << 15) & kTmaskC)) ^
+          (((((y ^ (y >> 11)) ^ (((y ^ (y >> 11)) << 7) & kTmaskB)) ^
+             ((((y ^ (y >> 11)) ^ (((y ^ (y >> 11)) << 7) & kTmaskB)) << 15) & kTmaskC)) >>
+            18)));
+}
+static_assert(temper_c(kRawAllOnes) == 0xFFFFFFFFu, "kRawAllOnes tempers to 2^32 - 1");
+
+// Appends sequence indices [j, j + 624) (j a multiple of 624) to the ring
+// (MT:341-356): words 0..226 of the block from the previous block, 227..453
+// and 454..622 from words 227 back in this block, 623 from x_{j-1}, x_j and
+// x_{j+396}; one barrier per dependency phase.
+__device__ void twist_ring(uint32_t* ring, int cap, long long j, int lane) {
+  const int jp = (int)(j % cap);
+  const uint32_t* o = ring + ((jp == 0 ? cap : jp) - 624);
+  uint32_t* w = ring + jp;
+  for (int t = lane; t < 227; t += 32) w[t] = mt_word(o[t], o[t + 1], o[t + 397]);
+  __syncwarp();
+  for (int t = 227 + lane; t < 454; t += 32) w[t] = mt_word(o[t], o[t + 1], w[t - 227]);
+  __syncwarp();
+  for (int t = 454 + lane; t < 624; t += 32) w[t] = mt_word(o[t], (t == 623) ? w[0] : o[t + 1], w[t - 227]);
+  __syncwarp();
 }
 
-constexpr int kMcicaWarps = 5;   // 5 warps x 22 KB (127 layers): two CTAs, ten warps per SM
+// Per-warp shared memory: clear[nlay] = 1 - cldf (double), ring[cap].  For
+// iovr 3..5 the ring's space holds the two twister states and the per-layer
+// overlap parameter instead.
+__host__ __device__ inline size_t mcica_warp_bytes(int nlay, int cap) {
+  return ((nlay * 8 + 15) & ~15) + (size_t)cap * 4;
+}
+
+constexpr int kMcicaWarps = 6;   // 6 warps x 18.5 KB (127 layers): two CTAs, twelve warps per SM
 
 __global__ void __launch_bounds__(32 * kMcicaWarps)
 lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int ncols, McicaArgs a,
@@ -224,10 +264,9 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const size_t wbytes = mcica_warp_bytes(a.nlay, a.cap);
   char* my = smem_raw + wbytes * wib;
-  uint32_t* mt = reinterpret_cast<uint32_t*>(my);
-  double* clr = reinterpret_cast<double*>(my + 624 * 4);   // 1 - cldf(k), used by every test of the walk
-  uint32_t* ring = reinterpret_cast<uint32_t*>(my + 624 * 4 + ((a.nlay * 8 + 15) & ~15));
-  const int nlay = a.nlay, nlp1 = nlay + 1;
+  double* clr = reinterpret_cast<double*>(my);   // 1 - cldf(k), used by every test of the walk
+  uint32_t* ring = reinterpret_cast<uint32_t*>(my + ((a.nlay * 8 + 15) & ~15));
+  const int nlay = a.nlay, nlp1 = nlay + 1, cap = a.cap;
   const int warps_total = gridDim.x * (blockDim.x >> 5);
 
   for (int c = blockIdx.x * (blockDim.x >> 5) + wib; c < ncols; c += warps_total) {
@@ -254,16 +293,14 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
       seed = a.st.seed[c];
     }
     if (!__any_sync(0xffffffffu, any)) continue;   // clear column: no draws
-    // random_setseed_t: mt(0)=seed (0 -> 4357), mt(i) = 69069*mt(i-1)
-    uint32_t s0 = (uint32_t)(seed == 0 ? 4357 : seed);
-    for (int n = lane; n < 624; n += 32) mt[n] = s0 * c_pow69069[n];
-    __syncwarp();
+    const uint32_t s0 = (uint32_t)(seed == 0 ? 4357 : seed);   // random_setseed_t (MT:285-299)
 
     uint32_t* out = bits + (size_t)c * NGPT * a.nw;
     if (a.iovr >= 3) {
-      // second twister state and the per-layer overlap parameter live in the ring's space
-      uint32_t* mtB = ring;
-      double* aux = reinterpret_cast<double*>(ring + 624);
+      // two twister states and the per-layer overlap parameter in the ring's space
+      uint32_t* mtA = ring;
+      uint32_t* mtB = ring + 624;
+      double* aux = reinterpret_cast<double*>(ring + 1248);
       const Block* B = (nblocks > 0) ? ((nblocks == 1) ? &b0 : &blocks[find_block(blocks, nblocks, c)]) : nullptr;
       const int i = B ? c - B->col0 : 0;
       if (a.iovr == 3) {
@@ -287,14 +324,17 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
           aux[k] = B ? B->in[F_ALPHA][i + (size_t)B->ld * k] : a.st.alpha[c + (size_t)a.st.ld * k];
       }
       __syncwarp();
-      mcica_two_set(mt, mtB, clr, aux, nlay, a.iovr, (uint32_t)(seed == 0 ? 4357 : seed), a.nw, out, lane);
+      mcica_two_set(mtA, mtB, clr, aux, nlay, a.iovr, s0, a.nw, out, lane);
       continue;
     }
+    // seeding x_0..x_623 at ring[0..623]: mt(i) = 69069^i seed
+    for (int n = lane; n < 624; n += 32) ring[n] = s0 * c_pow69069[n];
+    __syncwarp();
     if (a.iovr == 2) {
       // maximum overlap: one draw per g-point, the same at every layer (RLM:1981-1993)
-      twist(mt, lane);
+      twist_ring(ring, cap, 624, lane);
       for (int n = lane; n < NGPT; n += 32) {
-        double r = u32_unit(temper(mt[n]));
+        double r = u32_unit(temper(ring[624 + n]));
         for (int w = 0; w < a.nw; ++w) {
           uint32_t word = 0;
           for (int b = 0; b < 32; ++b) {
@@ -306,49 +346,41 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
       }
       continue;
     }
-    // random (iovr=0) and maximum-random (iovr=1): stream position n*nlay+k
-    const int cap = a.cap;
-    long gen_end = 0;          // stream positions generated so far
-    for (int n0 = 0; n0 < NGPT; n0 += 32) {
-      const int n1 = min(n0 + 32, NGPT);
-      const long need = (long)n1 * nlay;
-      while (gen_end < need) {
-        twist(mt, lane);
-        int p = (int)(gen_end % cap);
-        for (int j = lane; j < 624; j += 32) {
-          int q = p + j;
-          if (q >= cap) q -= cap;
-          ring[q] = temper(mt[j]);
-        }
-        gen_end += 624;
-        __syncwarp();
+    // random (iovr=0) and maximum-random (iovr=1): draw n*nlay+k (RLM:1920-1941)
+    long long gen = 624;       // sequence indices generated so far
+    for (int n0 = 0; n0 < NGPT; n0 += kMcicaRound) {
+      const long long need = 624 + (long long)(n0 + kMcicaRound) * nlay;
+      while (gen < need) {
+        twist_ring(ring, cap, gen, lane);
+        gen += 624;
       }
       const int n = n0 + lane;
-      if (n < n1) {
-        int q = (int)(((long)n * nlay) % cap);
+      if (lane < kMcicaRound) {
+        int q = (int)((624 + (long long)n * nlay) % cap);
         double cdf = 0.0;
         uint32_t word = 0;
         for (int k = 0; k < nlay; ++k) {
-          const uint32_t u = ring[q];
+          const uint32_t raw = ring[q];
           if (++q == cap) q = 0;
           const double ck = clr[k];
           if (ck == 1.0) {
             // Clear layer (the same for every lane: lanes are g-points of one layer).
             // Its flag is cdf >= 1, and every draw is <= 1 with equality only for
-            // u = 2^32 - 1, so the flag needs no conversion: a fresh draw is 1 only
-            // for that u, an inherited cdf only if it is 1, and r * tem1 < 1 when
-            // tem1 < 1.  The cdf of a clear layer is never read again: the next
-            // layer compares it with 1 - cldf = 1 and takes r * 1 = r instead.
+            // the word that tempers to 2^32 - 1, so the flag needs neither tempering
+            // nor conversion: a fresh draw is 1 only for that word, an inherited cdf
+            // only if it is 1, and r * tem1 < 1 when tem1 < 1.  The cdf of a clear
+            // layer is never read again: the next layer compares it with
+            // 1 - cldf = 1 and takes r * 1 = r instead.
             bool bit;
             if (k == 0 || a.iovr == 0) {
-              bit = (u == 0xFFFFFFFFu);
+              bit = (raw == kRawAllOnes);
             } else {
               const double tem1 = clr[k - 1];
-              bit = (tem1 == 1.0) ? (u == 0xFFFFFFFFu) : (cdf > tem1 && cdf >= 1.0);
+              bit = (tem1 == 1.0) ? (raw == kRawAllOnes) : (cdf > tem1 && cdf >= 1.0);
             }
             if (bit) word |= 1u << (k & 31);
           } else {
-            const double r = u32_unit(u);
+            const double r = u32_unit(temper(raw));
             if (k == 0 || a.iovr == 0) {
               cdf = r;
             } else {
@@ -467,7 +499,14 @@ cudaError_t seed_gather_launch(const uint32_t* raw, const int32_t* imap, const i
   return cudaGetLastError();
 }
 
-int mcica_ring_capacity(int nlay) { return ((32 * nlay + 624 + 31) / 32) * 32; }
+// ring words: one round's draws plus a twist block, and at least the two
+// states and the overlap parameter of iovr 3..5; a multiple of 624
+int mcica_ring_capacity(int nlay) {
+  const long round = (long)kMcicaRound * nlay + 623;
+  const long two_set = 1248 + 2L * nlay;
+  const long need = round > two_set ? round : two_set;
+  return (int)((need + 623) / 624 * 624);
+}
 
 cudaError_t mcica_prepare(int max_smem) {
   return cudaFuncSetAttribute(lw_mcica_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
