@@ -6,14 +6,14 @@
 // MT:330-372).  One warp owns one cloudy column:
 //   * seeding mt(i) = 69069^i * seed (mod 2^32) is one multiply per word
 //     with a table of powers of 69069 in constant memory;
-//   * each twist of the 624-word state runs in three dependency phases
-//     (words 0..226 from old words, 227..453 and 454..622 from words
-//     already updated, then word 623), 32 words per lane step;
+//   * the stream lives in shared memory as its raw (untempered) sequence; a
+//     twist appends the next 624 words in place in three dependency phases
+//     (words 0..226 from the previous block, 227..453 and 454..622 from
+//     words 227 back, then word 623), one barrier each;
 //   * for max-random overlap (iovr=1) the random array is g-point major
 //     (rand2d index (n-1)*nlay+k, RLM:1935-1941), so each g-point's walk
-//     reads a contiguous run of the stream.  Lanes own g-points, 32 at a
-//     time; the stream is generated into a per-warp ring buffer just ahead
-//     of the 32 walks that read it.
+//     reads a contiguous run of the stream.  Lanes own g-points, 28 at a
+//     time; the sequence ring holds one round's draws and the twist history.
 // Integer arithmetic is exact; the u32 -> real conversion (u/(2^32-1)) and
 // the FP64 comparisons/products of the walk are IEEE operations, so the
 // sub-column flags equal the Fortran's bit for bit.
@@ -43,40 +43,6 @@ __device__ __forceinline__ uint32_t temper(uint32_t y) {
   return y;
 }
 
-// One twist of the warp's state mt[624] (MT:341-356), parallel over lanes.
-__device__ void twist(uint32_t* mt, int lane) {
-  // phase A: kk = 0..226 reads mt[kk], mt[kk+1] (old), mt[kk+397] (old)
-  for (int base = 0; base < 227; base += 32) {
-    int kk = base + lane;
-    uint32_t v = 0;
-    if (kk < 227) v = mt_word(mt[kk], mt[kk + 1], mt[kk + 397]);
-    __syncwarp();
-    if (kk < 227) mt[kk] = v;
-    __syncwarp();
-  }
-  // phase B1: kk = 227..453 reads mt[kk-227] (new, from phase A)
-  for (int base = 227; base < 454; base += 32) {
-    int kk = base + lane;
-    uint32_t v = 0;
-    if (kk < 454) v = mt_word(mt[kk], mt[kk + 1], mt[kk - 227]);
-    __syncwarp();
-    if (kk < 454) mt[kk] = v;
-    __syncwarp();
-  }
-  // phase B2: kk = 454..622 reads mt[kk-227] (new, from phase B1)
-  for (int base = 454; base < 623; base += 32) {
-    int kk = base + lane;
-    uint32_t v = 0;
-    if (kk < 623) v = mt_word(mt[kk], mt[kk + 1], mt[kk - 227]);
-    __syncwarp();
-    if (kk < 623) mt[kk] = v;
-    __syncwarp();
-  }
-  // phase C: kk = 623 with mt[0] and mt[396] (both new)
-  if (lane == 0) mt[623] = mt_word(mt[623], mt[0], mt[396]);
-  __syncwarp();
-}
-
 // u / (2^32 - 1), correctly rounded, without a division (the GFS twister's
 // harvest = real(y) / (2**32 - 1), mersenne_twister.f:362-369, for the
 // unsigned value u of y).  1/(2^32-1) = (2^32+1)/(2^64-1), so the quotient
@@ -100,38 +66,52 @@ __device__ __forceinline__ double u32_unit(uint32_t u) {
   return r;
 }
 
+// Appends sequence indices [j, j + 624) (j a multiple of 624) to the ring
+// (MT:341-356): words 0..226 of the block from the previous block, 227..453
+// and 454..622 from words 227 back in this block, 623 from x_{j-1}, x_j and
+// x_{j+396}; one barrier per dependency phase.
+__device__ void twist_ring(uint32_t* ring, int cap, long long j, int lane) {
+  const int jp = (int)(j % cap);
+  const uint32_t* o = ring + ((jp == 0 ? cap : jp) - 624);
+  uint32_t* w = ring + jp;
+  for (int t = lane; t < 227; t += 32) w[t] = mt_word(o[t], o[t + 1], o[t + 397]);
+  __syncwarp();
+  for (int t = 227 + lane; t < 454; t += 32) w[t] = mt_word(o[t], o[t + 1], w[t - 227]);
+  __syncwarp();
+  for (int t = 454 + lane; t < 624; t += 32) w[t] = mt_word(o[t], (t == 623) ? w[0] : o[t + 1], w[t - 227]);
+  __syncwarp();
+}
+
 struct McicaArgs {
   int nlay, nw, iovr, isubclw, top_at_1;
   int cap;        // ring capacity in words
   McicaStage st;  // stage entry point inputs (blocks == nullptr)
 };
 
-// Read the next 140 draws (one layer of a layer-major stream, RLM:2006-2024)
-// of a Mersenne-twister stream whose current twist is in mt[624] with read
-// position *pos; lane gets draws for g-points n = lane + 32 j (j < 5).  A
-// layer spans at most one twist boundary.
-__device__ __forceinline__ void layer_draws(uint32_t* mt, int* pos, int lane, double (&d)[5]) {
-  const int p = *pos;
-  uint32_t w[5] = {0u, 0u, 0u, 0u, 0u};
+// The 140 draws p .. p+139 (one layer of a layer-major stream,
+// RLM:2006-2024) of a twister stream kept as a sequence ring of two blocks
+// (1248 words; sequence index s at ring[s mod 1248], draw p = tempered
+// x_{624+p}, *gen = sequence indices generated so far); lane gets the draws
+// of g-points n = lane + 32 j (j < 5).  Blocks are appended as the reads
+// advance; the block a new one overwrites was read before the barrier.
+constexpr int kTwoSetRing = 1248;
+__device__ __forceinline__ void layer_draws(uint32_t* ring, long long* gen, long long p, int lane, double (&d)[5]) {
+  const long long s = 624 + p;
+  if (*gen < s + NGPT) {
+    __syncwarp();
+    do {
+      twist_ring(ring, kTwoSetRing, *gen, lane);
+      *gen += 624;
+    } while (*gen < s + NGPT);
+  }
+  const int base = (int)(s % kTwoSetRing);
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
     const int n = lane + 32 * j;
-    if (n < NGPT && p + n < 624) w[j] = temper(mt[p + n]);
+    int q = base + n;
+    if (q >= kTwoSetRing) q -= kTwoSetRing;
+    d[j] = (n < NGPT) ? u32_unit(temper(ring[q])) : 0.0;
   }
-  if (p + NGPT > 624) {
-    __syncwarp();
-    twist(mt, lane);
-#pragma unroll
-    for (int j = 0; j < 5; ++j) {
-      const int n = lane + 32 * j;
-      if (n < NGPT && p + n >= 624) w[j] = temper(mt[p + n - 624]);
-    }
-    *pos = p + NGPT - 624;
-  } else {
-    *pos = p + NGPT;
-  }
-#pragma unroll
-  for (int j = 0; j < 5; ++j) d[j] = u32_unit(w[j]);
 }
 
 // Overlaps built from two layer-major random sets (RLM:1995-2091):
@@ -154,19 +134,16 @@ __device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const double* clr, c
     mtB[n] = v;
   }
   __syncwarp();
-  // stream B starts at position 140 nlay: apply the twists up to and including
-  // the one that produces that position
-  const long P0 = (long)NGPT * nlay;
-  for (long t = 0; t <= P0 / 624; ++t) twist(mtB, lane);
-  int posB = (int)(P0 % 624);
-  twist(mtA, lane);
-  int posA = 0;
+  // set 2 starts at draw 140 nlay of the same stream: its first layer_draws
+  // call appends blocks up to there
+  const long long P0 = (long long)NGPT * nlay;
+  long long genA = 624, genB = 624;
   double cdf[5], c1[5], c2[5];
   uint32_t word[5] = {0u, 0u, 0u, 0u, 0u};
   int start[5] = {0, 0, 0, 0, 0}, wi[5] = {0, 0, 0, 0, 0};
   for (int k = 0; k < nlay; ++k) {
-    layer_draws(mtA, &posA, lane, c1);
-    layer_draws(mtB, &posB, lane, c2);
+    layer_draws(mtA, &genA, (long long)NGPT * k, lane, c1);
+    layer_draws(mtB, &genB, P0 + (long long)NGPT * k, lane, c2);
     if (iovr == 3) {
       const bool top = (k == nlay - 1);
       const double fk = top ? 0.0 : aux[k + 1];
@@ -232,22 +209,6 @@ __host__ __device__ constexpr uint32_t temper_c(uint32_t y) {
 }
 static_assert(temper_c(kRawAllOnes) == 0xFFFFFFFFu, "kRawAllOnes tempers to 2^32 - 1");
 
-// Appends sequence indices [j, j + 624) (j a multiple of 624) to the ring
-// (MT:341-356): words 0..226 of the block from the previous block, 227..453
-// and 454..622 from words 227 back in this block, 623 from x_{j-1}, x_j and
-// x_{j+396}; one barrier per dependency phase.
-__device__ void twist_ring(uint32_t* ring, int cap, long long j, int lane) {
-  const int jp = (int)(j % cap);
-  const uint32_t* o = ring + ((jp == 0 ? cap : jp) - 624);
-  uint32_t* w = ring + jp;
-  for (int t = lane; t < 227; t += 32) w[t] = mt_word(o[t], o[t + 1], o[t + 397]);
-  __syncwarp();
-  for (int t = 227 + lane; t < 454; t += 32) w[t] = mt_word(o[t], o[t + 1], w[t - 227]);
-  __syncwarp();
-  for (int t = 454 + lane; t < 624; t += 32) w[t] = mt_word(o[t], (t == 623) ? w[0] : o[t + 1], w[t - 227]);
-  __syncwarp();
-}
-
 // Per-warp shared memory: clear[nlay] = 1 - cldf (double), ring[cap].  For
 // iovr 3..5 the ring's space holds the two twister states and the per-layer
 // overlap parameter instead.
@@ -297,10 +258,10 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
 
     uint32_t* out = bits + (size_t)c * NGPT * a.nw;
     if (a.iovr >= 3) {
-      // two twister states and the per-layer overlap parameter in the ring's space
+      // two sequence rings and the per-layer overlap parameter in the ring's space
       uint32_t* mtA = ring;
-      uint32_t* mtB = ring + 624;
-      double* aux = reinterpret_cast<double*>(ring + 1248);
+      uint32_t* mtB = ring + kTwoSetRing;
+      double* aux = reinterpret_cast<double*>(ring + 2 * kTwoSetRing);
       const Block* B = (nblocks > 0) ? ((nblocks == 1) ? &b0 : &blocks[find_block(blocks, nblocks, c)]) : nullptr;
       const int i = B ? c - B->col0 : 0;
       if (a.iovr == 3) {
@@ -503,7 +464,7 @@ cudaError_t seed_gather_launch(const uint32_t* raw, const int32_t* imap, const i
 // states and the overlap parameter of iovr 3..5; a multiple of 624
 int mcica_ring_capacity(int nlay) {
   const long round = (long)kMcicaRound * nlay + 623;
-  const long two_set = 1248 + 2L * nlay;
+  const long two_set = 2L * kTwoSetRing + 2L * nlay;
   const long need = round > two_set ? round : two_set;
   return (int)((need + 623) / 624 * 624);
 }
