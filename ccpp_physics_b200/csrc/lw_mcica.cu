@@ -91,11 +91,13 @@ struct McicaArgs {
 // The 140 draws p .. p+139 (one layer of a layer-major stream,
 // RLM:2006-2024) of a twister stream kept as a sequence ring of two blocks
 // (1248 words; sequence index s at ring[s mod 1248], draw p = tempered
-// x_{624+p}, *gen = sequence indices generated so far); lane gets the draws
-// of g-points n = lane + 32 j (j < 5).  Blocks are appended as the reads
-// advance; the block a new one overwrites was read before the barrier.
+// x_{624+p}, *gen = sequence indices generated so far); lane gets the
+// tempered words of g-points n = lane + 32 j (j < 5).  Blocks are appended
+// as the reads advance; the block a new one overwrites was read before the
+// barrier.
 constexpr int kTwoSetRing = 1248;
-__device__ __forceinline__ void layer_draws(uint32_t* ring, long long* gen, long long p, int lane, double (&d)[5]) {
+__device__ __forceinline__ void layer_draws(uint32_t* ring, long long* gen, long long p, int lane,
+                                            uint32_t (&d)[5]) {
   const long long s = 624 + p;
   if (*gen < s + NGPT) {
     __syncwarp();
@@ -110,8 +112,36 @@ __device__ __forceinline__ void layer_draws(uint32_t* ring, long long* gen, long
     const int n = lane + 32 * j;
     int q = base + n;
     if (q >= kTwoSetRing) q -= kTwoSetRing;
-    d[j] = (n < NGPT) ? u32_unit(temper(ring[q])) : 0.0;
+    d[j] = (n < NGPT) ? temper(ring[q]) : 0u;
   }
+}
+
+// The draw conversion h(u) = u / (2^32 - 1) (u32_unit) is strictly
+// increasing (consecutive u differ by 2^-32, far above a double's spacing),
+// so every comparison of a draw with a per-layer value x is a comparison of
+// the tempered word u with an exact integer threshold:
+//   h(u) >= x  <=>  u >= umin_ge(x),   h(u) < x  <=>  u < ulim_lt(x),
+//   h(u) <= x  <=>  u <= umax_le(x).
+// Thresholds are 64-bit: 2^32 / -1 / 0 mean that no word qualifies (x above
+// 1, below 0, or NaN, for which every comparison is false).  x (2^32 - 1) is
+// within one unit of the threshold, so a few exact steps settle it.
+__device__ long long umin_ge(double x) {
+  if (x <= 0.0) return 0;
+  if (!(x <= 1.0)) return 4294967296LL;
+  long long u = (long long)(x * 4294967295.0);
+  if (u > 4294967295LL) u = 4294967295LL;
+  for (int it = 0; it < 8 && u > 0 && u32_unit((uint32_t)(u - 1)) >= x; ++it) --u;
+  for (int it = 0; it < 8 && u <= 4294967295LL && u32_unit((uint32_t)u) < x; ++it) ++u;
+  return u;
+}
+__device__ long long ulim_lt(double x) { return (x != x) ? 0 : umin_ge(x); }
+__device__ long long umax_le(double x) {
+  if (!(x >= 0.0)) return -1;
+  if (x >= 1.0) return 4294967295LL;
+  long long u = (long long)(x * 4294967295.0);   // smallest u with h(u) > x, minus one
+  for (int it = 0; it < 8 && u > 0 && u32_unit((uint32_t)(u - 1)) > x; ++it) --u;
+  for (int it = 0; it < 8 && u32_unit((uint32_t)u) <= x; ++it) ++u;
+  return u - 1;
 }
 
 // Overlaps built from two layer-major random sets (RLM:1995-2091):
@@ -125,9 +155,12 @@ __device__ __forceinline__ void layer_draws(uint32_t* ring, long long* gen, long
 // the nearest layer at or above it whose link to the layer above is broken
 // (the top layer always is), so each g-point keeps the run of layers still
 // waiting for that draw and resolves it when the break arrives.
-// aux[k] is fac_lcf(k) (iovr 3, 0-based, aux[0] unused) or alpha(k).
-__device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const double* clr, const double* aux, int nlay, int iovr,
-                              uint32_t s0, int nw, uint32_t* out, int lane) {
+// The walk runs on tempered words against integer thresholds (above):
+// clr_t[k] = umin_ge(1 - cldf(k)) for the cloud test (RLM:2097-2103), and
+// aux_t[k] = umax_le(fac_lcf(k)) (iovr 3, 0-based, aux_t[0] unused) or
+// ulim_lt(alpha(k)) (iovr 4, 5).
+__device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const long long* clr_t, const long long* aux_t, int nlay,
+                              int iovr, uint32_t s0, int nw, uint32_t* out, int lane) {
   for (int n = lane; n < 624; n += 32) {
     const uint32_t v = s0 * c_pow69069[n];
     mtA[n] = v;
@@ -138,7 +171,7 @@ __device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const double* clr, c
   // call appends blocks up to there
   const long long P0 = (long long)NGPT * nlay;
   long long genA = 624, genB = 624;
-  double cdf[5], c1[5], c2[5];
+  uint32_t cdf[5], c1[5], c2[5];
   uint32_t word[5] = {0u, 0u, 0u, 0u, 0u};
   int start[5] = {0, 0, 0, 0, 0}, wi[5] = {0, 0, 0, 0, 0};
   for (int k = 0; k < nlay; ++k) {
@@ -146,31 +179,32 @@ __device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const double* clr, c
     layer_draws(mtB, &genB, P0 + (long long)NGPT * k, lane, c2);
     if (iovr == 3) {
       const bool top = (k == nlay - 1);
-      const double fk = top ? 0.0 : aux[k + 1];
+      const long long fk = top ? 0 : aux_t[k + 1];
 #pragma unroll
       for (int j = 0; j < 5; ++j) {
         const int n = lane + 32 * j;
         if (n >= NGPT) continue;
-        if (!top && c2[j] <= fk) continue;   // linked to the layer above: still waiting
-        const double v = c1[j];
+        if (!top && (long long)c2[j] <= fk) continue;   // linked to the layer above: still waiting
+        const long long v = c1[j];
         for (int m = start[j]; m <= k; ++m) {
           if ((m >> 5) != wi[j]) {
             out[n * nw + wi[j]] = word[j];
             word[j] = 0u;
             wi[j] = m >> 5;
           }
-          if (v >= clr[m]) word[j] |= 1u << (m & 31);   // RLM:2097-2103
+          if (v >= clr_t[m]) word[j] |= 1u << (m & 31);   // RLM:2097-2103
         }
         start[j] = k + 1;
       }
     } else {
-      const double ak = aux[k];
+      const long long ak = aux_t[k];
+      const long long ck = clr_t[k];
 #pragma unroll
       for (int j = 0; j < 5; ++j) {
         const int n = lane + 32 * j;
         if (n >= NGPT) continue;
-        cdf[j] = (k > 0 && c2[j] < ak) ? cdf[j] : c1[j];
-        if (cdf[j] >= clr[k]) word[j] |= 1u << (k & 31);
+        cdf[j] = (k > 0 && (long long)c2[j] < ak) ? cdf[j] : c1[j];
+        if ((long long)cdf[j] >= ck) word[j] |= 1u << (k & 31);
         if ((k & 31) == 31 || k == nlay - 1) {
           out[n * nw + (k >> 5)] = word[j];
           word[j] = 0u;
@@ -258,7 +292,8 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
 
     uint32_t* out = bits + (size_t)c * NGPT * a.nw;
     if (a.iovr >= 3) {
-      // two sequence rings and the per-layer overlap parameter in the ring's space
+      // two sequence rings, the per-layer overlap parameter and the walk's
+      // thresholds in the ring's space
       uint32_t* mtA = ring;
       uint32_t* mtB = ring + kTwoSetRing;
       double* aux = reinterpret_cast<double*>(ring + 2 * kTwoSetRing);
@@ -284,8 +319,17 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
         for (int k = lane; k < nlay; k += 32)
           aux[k] = B ? B->in[F_ALPHA][i + (size_t)B->ld * k] : a.st.alpha[c + (size_t)a.st.ld * k];
       }
+      // the walk's integer thresholds, after the rings and aux
+      long long* aux_t = reinterpret_cast<long long*>(aux + nlay);
+      long long* clr_t = aux_t + nlay;
       __syncwarp();
-      mcica_two_set(mtA, mtB, clr, aux, nlay, a.iovr, s0, a.nw, out, lane);
+      for (int k = lane; k < nlay; k += 32) {
+        clr_t[k] = umin_ge(clr[k]);
+        if (a.iovr == 3) aux_t[k] = (k > 0) ? umax_le(aux[k]) : 0;
+        else aux_t[k] = ulim_lt(aux[k]);
+      }
+      __syncwarp();
+      mcica_two_set(mtA, mtB, clr_t, aux_t, nlay, a.iovr, s0, a.nw, out, lane);
       continue;
     }
     // seeding x_0..x_623 at ring[0..623]: mt(i) = 69069^i seed
@@ -461,10 +505,11 @@ cudaError_t seed_gather_launch(const uint32_t* raw, const int32_t* imap, const i
 }
 
 // ring words: one round's draws plus a twist block, and at least the two
-// states and the overlap parameter of iovr 3..5; a multiple of 624
+// rings, the overlap parameter and the two threshold arrays of iovr 3..5; a
+// multiple of 624
 int mcica_ring_capacity(int nlay) {
   const long round = (long)kMcicaRound * nlay + 623;
-  const long two_set = 2L * kTwoSetRing + 2L * nlay;
+  const long two_set = 2L * kTwoSetRing + 6L * nlay;
   const long need = round > two_set ? round : two_set;
   return (int)((need + 623) / 624 * 624);
 }
