@@ -66,12 +66,12 @@ __device__ __forceinline__ double u32_unit(uint32_t u) {
   return r;
 }
 
-// Appends sequence indices [j, j + 624) (j a multiple of 624) to the ring
+// Appends the next 624 sequence words to the ring at position jp (a
+// multiple of 624; the previous block sits just before it, cyclically)
 // (MT:341-356): words 0..226 of the block from the previous block, 227..453
 // and 454..622 from words 227 back in this block, 623 from x_{j-1}, x_j and
 // x_{j+396}; one barrier per dependency phase.
-__device__ void twist_ring(uint32_t* ring, int cap, long long j, int lane) {
-  const int jp = (int)(j % cap);
+__device__ void twist_ring(uint32_t* ring, int cap, int jp, int lane) {
   const uint32_t* o = ring + ((jp == 0 ? cap : jp) - 624);
   uint32_t* w = ring + jp;
   for (int t = lane; t < 227; t += 32) w[t] = mt_word(o[t], o[t + 1], o[t + 397]);
@@ -88,32 +88,39 @@ struct McicaArgs {
   McicaStage st;  // stage entry point inputs (blocks == nullptr)
 };
 
-// The 140 draws p .. p+139 (one layer of a layer-major stream,
-// RLM:2006-2024) of a twister stream kept as a sequence ring of two blocks
-// (1248 words; sequence index s at ring[s mod 1248], draw p = tempered
-// x_{624+p}, *gen = sequence indices generated so far); lane gets the
-// tempered words of g-points n = lane + 32 j (j < 5).  Blocks are appended
-// as the reads advance; the block a new one overwrites was read before the
-// barrier.
+// One twister stream kept as a sequence ring of two blocks (1248 words;
+// sequence index s at ring[s mod 1248], draw p = tempered x_{624+p}).  The
+// reader tracks its next sequence index s, its ring position, and how far
+// the sequence has been generated.
 constexpr int kTwoSetRing = 1248;
-__device__ __forceinline__ void layer_draws(uint32_t* ring, long long* gen, long long p, int lane,
-                                            uint32_t (&d)[5]) {
-  const long long s = 624 + p;
-  if (*gen < s + NGPT) {
+struct TwoSetStream {
+  int s;      // sequence index of the next draw
+  int pos;    // s mod 1248
+  int gen;    // sequence indices generated so far (a multiple of 624)
+};
+
+// The next 140 draws (one layer of a layer-major stream, RLM:2006-2024);
+// lane gets the tempered words of g-points n = lane + 32 j (j < 5).  Blocks
+// are appended as the reads advance; the block a new one overwrites was read
+// before the barrier.
+__device__ __forceinline__ void layer_draws(uint32_t* ring, TwoSetStream& st, int lane, uint32_t (&d)[5]) {
+  if (st.gen < st.s + NGPT) {
     __syncwarp();
     do {
-      twist_ring(ring, kTwoSetRing, *gen, lane);
-      *gen += 624;
-    } while (*gen < s + NGPT);
+      twist_ring(ring, kTwoSetRing, (st.gen / 624) & 1 ? 624 : 0, lane);
+      st.gen += 624;
+    } while (st.gen < st.s + NGPT);
   }
-  const int base = (int)(s % kTwoSetRing);
 #pragma unroll
   for (int j = 0; j < 5; ++j) {
     const int n = lane + 32 * j;
-    int q = base + n;
+    int q = st.pos + n;
     if (q >= kTwoSetRing) q -= kTwoSetRing;
     d[j] = (n < NGPT) ? temper(ring[q]) : 0u;
   }
+  st.s += NGPT;
+  st.pos += NGPT;
+  if (st.pos >= kTwoSetRing) st.pos -= kTwoSetRing;
 }
 
 // The draw conversion h(u) = u / (2^32 - 1) (u32_unit) is strictly
@@ -169,14 +176,14 @@ __device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const long long* clr
   __syncwarp();
   // set 2 starts at draw 140 nlay of the same stream: its first layer_draws
   // call appends blocks up to there
-  const long long P0 = (long long)NGPT * nlay;
-  long long genA = 624, genB = 624;
+  const int P0 = NGPT * nlay;
+  TwoSetStream sa{624, 624, 624}, sb{624 + P0, (624 + P0) % kTwoSetRing, 624};
   uint32_t cdf[5], c1[5], c2[5];
   uint32_t word[5] = {0u, 0u, 0u, 0u, 0u};
   int start[5] = {0, 0, 0, 0, 0}, wi[5] = {0, 0, 0, 0, 0};
   for (int k = 0; k < nlay; ++k) {
-    layer_draws(mtA, &genA, (long long)NGPT * k, lane, c1);
-    layer_draws(mtB, &genB, P0 + (long long)NGPT * k, lane, c2);
+    layer_draws(mtA, sa, lane, c1);
+    layer_draws(mtB, sb, lane, c2);
     if (iovr == 3) {
       const bool top = (k == nlay - 1);
       const long long fk = top ? 0 : aux_t[k + 1];
@@ -337,7 +344,7 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
     __syncwarp();
     if (a.iovr == 2) {
       // maximum overlap: one draw per g-point, the same at every layer (RLM:1981-1993)
-      twist_ring(ring, cap, 624, lane);
+      twist_ring(ring, cap, 624, lane);   // sequence 624..1247 at ring[624..1247] (cap >= 1248)
       for (int n = lane; n < NGPT; n += 32) {
         double r = u32_unit(temper(ring[624 + n]));
         for (int w = 0; w < a.nw; ++w) {
@@ -353,11 +360,14 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
     }
     // random (iovr=0) and maximum-random (iovr=1): draw n*nlay+k (RLM:1920-1941)
     long long gen = 624;       // sequence indices generated so far
+    int jp = 624;              // gen mod cap
     for (int n0 = 0; n0 < NGPT; n0 += kMcicaRound) {
       const long long need = 624 + (long long)(n0 + kMcicaRound) * nlay;
       while (gen < need) {
-        twist_ring(ring, cap, gen, lane);
+        twist_ring(ring, cap, jp, lane);
         gen += 624;
+        jp += 624;
+        if (jp == cap) jp = 0;
       }
       const int n = n0 + lane;
       if (lane < kMcicaRound) {
