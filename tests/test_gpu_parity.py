@@ -193,6 +193,42 @@ def test_mcica_bits_exact(gpu, orc):
             assert np.array_equal(got, ref), (iovr, i)
 
 
+def test_mcica_comparison_boundaries(gpu, orc):
+    """The exponential overlaps compare draws with alpha and with 1 - cldf on
+    the GPU as integers against exact thresholds; put those values exactly on
+    draws of the stream (and at NaN, below 0, above 1) and check the flags
+    against the oracle's floating-point comparisons."""
+    import torch
+    nlay, npts = 64, 6
+    P0 = 140 * nlay
+    seeds = np.array([11, 12, 13, 14, 15, 16], dtype=np.int32)
+    cldf = np.zeros((nlay, npts))
+    alpha = np.full((nlay, npts), 0.5)
+    for i, sd in enumerate(seeds):
+        _, x, _ = orc.mt_stream(int(sd), 2 * P0)
+        for k in range(nlay):
+            n = (7 * k + i) % 140
+            alpha[k, i] = x[P0 + 140 * k + n]          # set-2 draw of g-point n: c2 < alpha is false
+            c1 = x[140 * k + ((n + 1) % 140)]           # a set-1 draw; 1 - (1 - c1) == c1 for c1 >= 0.5
+            cldf[k, i] = 1.0 - c1 if c1 >= 0.5 else 0.4
+    alpha[5::9, 3] = np.nan
+    alpha[6::9, 3] = 1.5
+    alpha[7::9, 3] = -0.5
+    alpha[8::9, 4] = 0.0
+    alpha[9::9, 4] = 1.0
+    dz = np.full((nlay, npts), 0.3)
+    de_lgth = np.full(npts, 2.0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    for iovr in (4, 5):
+        bits = gpu.mcica_bits(t(cldf), t(seeds), iovr=iovr, dz=t(dz), de_lgth=t(de_lgth), alpha=t(alpha))
+        bits = bits.cpu().numpy().view(np.uint32)
+        for i in range(npts):
+            ref = orc.mcica(cldf[:, i], int(seeds[i]), iovr=iovr, dz=dz[:, i], de_lgth=float(de_lgth[i]),
+                            alpha=alpha[:, i])
+            got = ((bits[i][:, np.arange(nlay) >> 5] >> (np.arange(nlay) & 31)) & 1).astype(bool).T
+            assert np.array_equal(got, ref), (iovr, i)
+
+
 def test_gas_optics_stage(gpu, orc):
     import torch
     from ccpp_physics_b200 import rrtmg_lw as lw
