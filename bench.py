@@ -170,12 +170,16 @@ def batched_leg(args, lw, abi, synthetic, torch, rank, world, sh, timed, rmse):
     n3, nlay = cfg["ncols"], cfg["nlay"]
     sizes = synthetic.physics_blocks(n3, seed=7)
     prof = synthetic.make_profiles(n3, nlay, seed=1, cloudy=True, col_offset=rank * n3, device="cuda")
-    res = {"workload": cfg["name"], "nblocks": int(len(sizes)), "block_sizes": "U{8..256}, seed 7"}
+    # each physics block is its own (n_b, nlay) array, as the GFS host allocates its blocks
+    lw.pack_blocks(prof, sizes, inplace=True)
+    torch.cuda.empty_cache()
+    res = {"workload": cfg["name"], "nblocks": int(len(sizes)), "block_sizes": "U{8..256}, seed 7",
+           "block_layout": "one contiguous (n_b, nlay) array per block (ldim = n_b)"}
     outs = {}
     k = max(2, min(args.steps, 5))
     precs = ("fp32", "fp64", "surrogate") if args.surrogate_ready else ("fp32", "fp64")
     for prec in precs:
-        out = abi.alloc_outputs(n3, nlay, hlw0=True, like="cuda")
+        out = lw.pack_blocks(abi.alloc_outputs(n3, nlay, hlw0=True, like="cuda"), sizes, inplace=True)
         if prec == "surrogate":
             from ccpp_physics_b200 import surrogate as sg
         t0 = time.time()

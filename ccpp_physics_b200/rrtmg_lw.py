@@ -172,31 +172,116 @@ def gas_optics(prof: dict, precision="fp64", stream=None):
     return taug, fracs
 
 
+# column axis of the fields whose columns are not the last axis (records)
+_COL_AXIS = {"topflx": 0, "sfcflx": 0, "flxprf": 1}
+
+
+def _block_index(sizes, A, R, device):
+    """Per column: first packed element of its block and its block size."""
+    import torch
+    sizes_t = torch.as_tensor(np.asarray(sizes, dtype=np.int64), device=device)
+    c0 = torch.cumsum(sizes_t, 0) - sizes_t
+    n_col = torch.repeat_interleave(sizes_t, sizes_t)
+    c0_col = torch.repeat_interleave(c0, sizes_t)
+    j = torch.arange(int(sizes_t.sum()), device=device) - c0_col
+    return (A * c0_col + j) * R, n_col * R
+
+
+def _pack_field(v, axis, sizes, unpack=False, full=None):
+    """Block-packed copy of field v (or, with unpack, v's columns scattered
+    back into ``full``): block b's columns become one contiguous
+    (n_b, ...) Fortran array."""
+    import torch
+    npts = v.shape[axis] if not unpack else full.shape[axis]
+    shape = (full if unpack else v).shape
+    A = int(np.prod(shape[:axis])) if axis > 0 else 1
+    R = int(np.prod(shape[axis + 1:])) if axis + 1 < len(shape) else 1
+    src = (full if unpack else v).reshape(A, npts, R)
+    base, step = _block_index(sizes, A, R, src.device)
+    dst = torch.empty_like(src) if not unpack else None
+    flat = (dst if not unpack else v).reshape(-1)
+    r = torch.arange(R, device=src.device)
+    rows = max(1, (1 << 27) // max(1, npts * R))       # index chunks of <= 128 M elements
+    for a0 in range(0, A, rows):
+        a = torch.arange(a0, min(A, a0 + rows), device=src.device)
+        idx = (base[None, :, None] + a[:, None, None] * step[None, :, None] + r[None, None, :]).reshape(-1)
+        if unpack:
+            src[a0:a0 + len(a)] = flat[idx].view(len(a), npts, R)
+        else:
+            flat.index_copy_(0, idx, src[a0:a0 + len(a)].reshape(-1))
+    return dst.view(shape) if not unpack else full
+
+
+def pack_blocks(d: dict, sizes, *, inplace=False) -> dict:
+    """A copy of a Fortran-ordered profile or output dict (device tensors) in
+    which every physics block of ``sizes`` columns is its own contiguous
+    (n_b, ...) array, the way a host that allocates each block separately
+    (ccpp-physics' GFS blocks) holds them.  Tensors keep their shapes; only
+    the element order changes.  block_args/run_blocks recognise the layout.
+    With inplace, d itself is converted field by field (one field's extra
+    memory at a time) and returned."""
+    import torch
+    out = d if inplace else {k: v for k, v in d.items() if not isinstance(v, torch.Tensor)}
+    for k in [k for k, v in d.items() if isinstance(v, torch.Tensor)]:
+        v = d[k]
+        packed = _pack_field(v, _COL_AXIS.get(k, v.dim() - 1), sizes)
+        if inplace:
+            d[k] = None
+            del v
+        out[k] = packed
+    out["_packed_sizes"] = np.asarray(sizes, dtype=np.int64)
+    return out
+
+
+def unpack_blocks(d: dict) -> dict:
+    """Inverse of pack_blocks: tensors in the ordinary column layout."""
+    import torch
+    sizes = d["_packed_sizes"]
+    out = {k: v for k, v in d.items() if not isinstance(v, torch.Tensor) and k != "_packed_sizes"}
+    for k, v in d.items():
+        if isinstance(v, torch.Tensor):
+            out[k] = _pack_field(v, _COL_AXIS.get(k, v.dim() - 1), sizes, unpack=True, full=torch.empty_like(v))
+    return out
+
+
 def block_args(prof: dict, out: dict, sizes, *, flags=None):
     """RunArgs array describing consecutive physics blocks of ``sizes``
-    columns as views into one device-resident profile/output dict (each block
-    points at its first column and uses the full column count as ldim, the
-    way a host passes slices of larger arrays)."""
+    columns.  For an ordinary profile/output dict each block is a view into
+    the full arrays (it points at its first column and uses the full column
+    count as ldim, the way a host passes slices of larger arrays); for a dict
+    from pack_blocks each block is its own contiguous array with ldim = its
+    column count."""
     keep = []
     base = abi.make_run_args(prof, out, flags=flags, keep=keep)
     npts = prof["npts"]
     if int(np.sum(sizes)) != npts:
         raise ValueError("block sizes must add up to npts")
+    packed = "_packed_sizes" in prof
+    if packed != ("_packed_sizes" in out) or (packed and not np.array_equal(prof["_packed_sizes"], sizes)):
+        raise ValueError("profile and outputs must share the block packing of sizes")
     arr = (abi.RunArgs * len(sizes))()
     col_fields = set(abi.INPUT_FIELDS + ("aeraod", "aerssa", "sfemis", "sfgtmp", "dzlyr", "delpin",
                                          "de_lgth", "alpha", "cld_cf") + abi.OPTIONAL_CLOUD_FIELDS +
                      ("hlwc", "cldtau", "hlw0", "hlwb"))
     rec = {"topflx": 2, "sfcflx": 4, "flxprf": 4}
+    per_col = {}          # bytes of one column of each field (packed layout)
+    if packed:
+        for name, _ in abi.RunArgs._fields_:
+            t = prof.get(name, out.get(name))
+            if t is not None and hasattr(t, "numel"):
+                per_col[name] = t.numel() // npts * t.element_size()
     c0 = 0
     for b, n in enumerate(sizes):
         a = abi.RunArgs.from_buffer_copy(base)
-        a.npts, a.ldim = int(n), npts
+        a.npts, a.ldim = int(n), (int(n) if packed else npts)
         for name, _ in abi.RunArgs._fields_:
             p = getattr(a, name)
             if not isinstance(p, C._Pointer) or not p:
                 continue
             addr = C.cast(p, C.c_void_p).value
-            if name == "icseed":
+            if packed:
+                off = per_col[name] * c0
+            elif name == "icseed":
                 off = 4 * c0
             elif name in rec:
                 off = 8 * rec[name] * c0

@@ -61,6 +61,21 @@ def test_blocks_equal_one_call(lw, case, precision):
     _equal(many, one)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_packed_blocks_equal_views(lw, case, precision):
+    """Blocks held as separate (n_b, nlay) arrays (ldim = n_b, as a host that
+    allocates each physics block separately passes them) give the results of
+    the same blocks as views into one array, bit for bit."""
+    sizes, prof = case
+    views = _outs()
+    assert lw.run_blocks(prof, views, sizes, precision=precision)[1] == 0
+    pp = lw.pack_blocks(prof, sizes)
+    po = lw.pack_blocks(_outs(), sizes)
+    msg, err = lw.run_blocks(pp, po, sizes, precision=precision)
+    assert err == 0, msg
+    _equal(lw.unpack_blocks(po), views)
+
+
 def test_blocks_equal_per_block_calls_isubclw1(lw, case):
     """isubclw=1 seeds are block-relative (140+i, radlw_main.F90:766-768):
     the batched call must equal one rrtmg_lw_run per block."""
