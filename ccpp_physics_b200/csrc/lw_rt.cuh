@@ -295,8 +295,13 @@ lw_rt_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int 
         }
         const bool any_cloud = __any_sync(0xffffffffu, cbits != 0);
 
-        // ---- down sweep (RLM:3598-3673): compose, suffix scan, replay ----
-        R Ac = R(1), Bc = R(0), At = R(1), Bt = R(0);
+        // ---- both sweeps' layer maps (down RLM:3598-3673, up RLM:3700-3730):
+        // each lane composes its V layers' affine maps.  The up maps do not
+        // depend on the down sweep (only the up replay needs the surface
+        // radiance), so the down suffix scan and the up prefix scan run
+        // interleaved, each in its own operation order. ----
+        R Ac = R(1), Bc = R(0), At = R(1), Bt = R(0);      // down
+        R Uc = R(1), Wc = R(0), Ut = R(1), Wt = R(0);      // up
 #pragma unroll
         for (int j = V - 1; j >= 0; --j) {
           Bc = rt[j].tr * Bc + rt[j].gsd; Ac = rt[j].tr * Ac;
@@ -310,15 +315,37 @@ lw_rt_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int 
           }
         }
 #pragma unroll
+        for (int j = 0; j < V; ++j) {
+          Wc = rt[j].tr * Wc + rt[j].gsu; Uc = rt[j].tr * Uc;
+          if (any_cloud) {
+            if ((cbits >> j) & 1u) {
+              const R a = rt[j].tr * rt[j].ef;
+              Wt = a * Wt + (rt[j].gsu + (rt[j].tsu - rt[j].gsu)); Ut = a * Ut;
+            } else {
+              Wt = rt[j].tr * Wt + rt[j].gsu; Ut = rt[j].tr * Ut;
+            }
+          }
+        }
+#pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-          const R ac = shdn(Ac, d), bc = shdn(Bc, d);
-          R at = R(0), bt = R(0);
-          if (any_cloud) { at = shdn(At, d); bt = shdn(Bt, d); }
+          const R ac = shdn(Ac, d), bc = shdn(Bc, d), uc = shup(Uc, d), wc = shup(Wc, d);
+          R at = R(0), bt = R(0), ut = R(0), wt = R(0);
+          if (any_cloud) { at = shdn(At, d); bt = shdn(Bt, d); ut = shup(Ut, d); wt = shup(Wt, d); }
           if (lane + d < 32) {
             Bc = Ac * bc + Bc; Ac = Ac * ac;
             if (any_cloud) { Bt = At * bt + Bt; At = At * at; }
           }
+          if (lane >= d) {
+            Wc = Uc * wc + Wc; Uc = Uc * uc;
+            if (any_cloud) { Wt = Ut * wt + Wt; Ut = Ut * ut; }
+          }
         }
+        // the up maps of the layers below each lane's segment (used once the
+        // surface radiance is known)
+        const R pac = shup(Uc, 1), pbc = shup(Wc, 1);
+        R pat = R(0), pbt = R(0);
+        if (any_cloud) { pat = shup(Ut, 1); pbt = shup(Wt, 1); }
+        // ---- down replay ----
         R xc = shdn(Bc, 1), xt = any_cloud ? shdn(Bt, 1) : R(0);
         if (lane == 31) { xc = R(0); xt = R(0); }
 #pragma unroll
@@ -338,38 +365,9 @@ lw_rt_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int 
         const R rad0 = semis * shidx(frac[0], 0) * pk0;
         const R r0c = rad0 + reflct * shidx(xc, 0);
         const R r0t = rad0 + reflct * shidx(xt, 0);
-        // ---- up sweep (RLM:3700-3730): compose, prefix scan, replay ----
-        Ac = R(1); Bc = R(0); At = R(1); Bt = R(0);
-#pragma unroll
-        for (int j = 0; j < V; ++j) {
-          Bc = rt[j].tr * Bc + rt[j].gsu; Ac = rt[j].tr * Ac;
-          if (any_cloud) {
-            if ((cbits >> j) & 1u) {
-              const R a = rt[j].tr * rt[j].ef;
-              Bt = a * Bt + (rt[j].gsu + (rt[j].tsu - rt[j].gsu)); At = a * At;
-            } else {
-              Bt = rt[j].tr * Bt + rt[j].gsu; At = rt[j].tr * At;
-            }
-          }
-        }
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const R ac = shup(Ac, d), bc = shup(Bc, d);
-          R at = R(0), bt = R(0);
-          if (any_cloud) { at = shup(At, d); bt = shup(Bt, d); }
-          if (lane >= d) {
-            Bc = Ac * bc + Bc; Ac = Ac * ac;
-            if (any_cloud) { Bt = At * bt + Bt; At = At * at; }
-          }
-        }
-        {
-          const R pac = shup(Ac, 1), pbc = shup(Bc, 1);
-          xc = (lane == 0) ? r0c : pac * r0c + pbc;
-          if (any_cloud) {
-            const R pat = shup(At, 1), pbt = shup(Bt, 1);
-            xt = (lane == 0) ? r0t : pat * r0t + pbt;
-          }
-        }
+        // ---- up replay from the surface ----
+        xc = (lane == 0) ? r0c : pac * r0c + pbc;
+        if (any_cloud) xt = (lane == 0) ? r0t : pat * r0t + pbt;
 #pragma unroll
         for (int j = 0; j < V; ++j) {
           acc_cu[j] += (double)xc;
