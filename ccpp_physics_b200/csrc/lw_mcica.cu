@@ -74,10 +74,14 @@ __device__ __forceinline__ double u32_unit(uint32_t u) {
 __device__ void twist_ring(uint32_t* ring, int cap, int jp, int lane) {
   const uint32_t* o = ring + ((jp == 0 ? cap : jp) - 624);
   uint32_t* w = ring + jp;
+  // fully unrolled, so each phase's shared-memory loads issue together
+#pragma unroll
   for (int t = lane; t < 227; t += 32) w[t] = mt_word(o[t], o[t + 1], o[t + 397]);
   __syncwarp();
+#pragma unroll
   for (int t = 227 + lane; t < 454; t += 32) w[t] = mt_word(o[t], o[t + 1], w[t - 227]);
   __syncwarp();
+#pragma unroll
   for (int t = 454 + lane; t < 624; t += 32) w[t] = mt_word(o[t], (t == 623) ? w[0] : o[t + 1], w[t - 227]);
   __syncwarp();
 }
@@ -374,6 +378,7 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
         int q = (int)((624 + (long long)n * nlay) % cap);
         double cdf = 0.0;
         uint32_t word = 0;
+#pragma unroll 4   // lets the ring and cloud-fraction loads of four layers issue ahead
         for (int k = 0; k < nlay; ++k) {
           const uint32_t raw = ring[q];
           if (++q == cap) q = 0;
