@@ -17,6 +17,7 @@
 // Integer arithmetic is exact; the u32 -> real conversion (u/(2^32-1)) and
 // the FP64 comparisons/products of the walk are IEEE operations, so the
 // sub-column flags equal the Fortran's bit for bit.
+#include <climits>
 #include <cstdint>
 #include <cstdio>
 #include <cuda_runtime.h>
@@ -170,8 +171,9 @@ __device__ long long umax_le(double x) {
 // clr_t[k] = umin_ge(1 - cldf(k)) for the cloud test (RLM:2097-2103), and
 // aux_t[k] = umax_le(fac_lcf(k)) (iovr 3, 0-based, aux_t[0] unused) or
 // ulim_lt(alpha(k)) (iovr 4, 5).
-__device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const long long* clr_t, const long long* aux_t, int nlay,
-                              int iovr, uint32_t s0, int nw, uint32_t* out, int lane) {
+__device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const long long* clr_t, const long long* aux_t,
+                              const long long* srt, const uint32_t* pm, int nlay, int iovr, uint32_t s0, int nw,
+                              uint32_t* out, int lane) {
   for (int n = lane; n < 624; n += 32) {
     const uint32_t v = s0 * c_pow69069[n];
     mtA[n] = v;
@@ -196,14 +198,25 @@ __device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const long long* clr
         const int n = lane + 32 * j;
         if (n >= NGPT) continue;
         if (!top && (long long)c2[j] <= fk) continue;   // linked to the layer above: still waiting
+        // the run start[j]..k takes this layer's set-1 draw: per 32-layer word,
+        // the layers whose threshold it reaches are a prefix of the word's
+        // sorted thresholds (RLM:2097-2103)
         const long long v = c1[j];
-        for (int m = start[j]; m <= k; ++m) {
-          if ((m >> 5) != wi[j]) {
+        for (int w = start[j] >> 5; w <= (k >> 5); ++w) {
+          const int lo = max(start[j], 32 * w) - 32 * w, hi = min(k, 32 * w + 31) - 32 * w;
+          const uint32_t rm = (hi == 31 ? 0xFFFFFFFFu : ((1u << (hi + 1)) - 1u)) & ~((1u << lo) - 1u);
+          const long long* sw = srt + 32 * w;
+          int cnt = 0;
+#pragma unroll
+          for (int st = 16; st >= 1; st >>= 1)
+            if (sw[cnt + st - 1] <= v) cnt += st;
+          cnt += (sw[31] <= v) ? 1 : 0;   // only when all 32 qualify (then cnt was 31)
+          if (w != wi[j]) {
             out[n * nw + wi[j]] = word[j];
             word[j] = 0u;
-            wi[j] = m >> 5;
+            wi[j] = w;
           }
-          if (v >= clr_t[m]) word[j] |= 1u << (m & 31);   // RLM:2097-2103
+          word[j] |= rm & pm[33 * w + cnt];
         }
         start[j] = k + 1;
       }
@@ -340,7 +353,29 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
         else aux_t[k] = ulim_lt(aux[k]);
       }
       __syncwarp();
-      mcica_two_set(mtA, mtB, clr_t, aux_t, nlay, a.iovr, s0, a.nw, out, lane);
+      // iovr 3: per 32-layer word, the cloud thresholds in ascending order and,
+      // for each count c, the mask of the word's layers with the c smallest
+      // (layers past nlay never qualify)
+      long long* srt = clr_t + nlay;
+      uint32_t* pm = reinterpret_cast<uint32_t*>(srt + 32 * a.nw);
+      if (a.iovr == 3) {
+        for (int w = 0; w < a.nw; ++w) {
+          const int m = 32 * w + lane;
+          const long long th = (m < nlay) ? clr_t[m] : LLONG_MAX;
+          int rank = 0;
+          for (int o = 0; o < 32; ++o) {
+            const long long t2 = __shfl_sync(0xffffffffu, th, o);
+            rank += (t2 < th || (t2 == th && o < lane)) ? 1 : 0;
+          }
+          srt[32 * w + rank] = th;
+          for (int c = 0; c <= 32; ++c) {
+            const uint32_t b = __ballot_sync(0xffffffffu, rank < c);
+            if (lane == 0) pm[33 * w + c] = b;
+          }
+        }
+        __syncwarp();
+      }
+      mcica_two_set(mtA, mtB, clr_t, aux_t, srt, pm, nlay, a.iovr, s0, a.nw, out, lane);
       continue;
     }
     // seeding x_0..x_623 at ring[0..623]: mt(i) = 69069^i seed
@@ -520,11 +555,12 @@ cudaError_t seed_gather_launch(const uint32_t* raw, const int32_t* imap, const i
 }
 
 // ring words: one round's draws plus a twist block, and at least the two
-// rings, the overlap parameter and the two threshold arrays of iovr 3..5; a
-// multiple of 624
+// rings, the overlap parameter, the two threshold arrays and the per-word
+// sorted thresholds and masks of iovr 3..5; a multiple of 624
 int mcica_ring_capacity(int nlay) {
   const long round = (long)kMcicaRound * nlay + 623;
-  const long two_set = 2L * kTwoSetRing + 6L * nlay;
+  const long nw = (nlay + 31) / 32;
+  const long two_set = 2L * kTwoSetRing + 6L * nlay + 97L * nw;   // + sorted thresholds, prefix masks
   const long need = round > two_set ? round : two_set;
   return (int)((need + 623) / 624 * 624);
 }
