@@ -170,13 +170,16 @@ def test_fp64_diagnostic_cloud_od(gpu, orc):
     _check_fp64(out, ref)
 
 
-def test_mcica_bits_exact(gpu, orc):
+@pytest.mark.parametrize("nlay", [127, 33, 255])
+def test_mcica_bits_exact(gpu, orc, nlay):
+    """Every overlap, bit for bit, at one word per g-point (33 layers), four
+    (127) and eight (255, the largest ring and threshold arrays)."""
     import torch
-    rng = np.random.default_rng(5)
-    nlay, npts = 127, 40
+    rng = np.random.default_rng(5 + nlay)
+    npts = 40
     cldf = np.where(rng.random((nlay, npts)) < 0.3, rng.random((nlay, npts)), 0.0)
     cldf[:, 0] = 1.0
-    cldf[10:30, 1] = 1e-7
+    cldf[10:min(30, nlay), 1] = 1e-7
     seeds = np.array([0, 1, 2**31 - 1, -7] + list(range(100, 100 + npts - 4)), dtype=np.int32)
     dz = rng.uniform(0.05, 1.5, (nlay, npts))
     de_lgth = rng.uniform(0.5, 4.0, npts)
