@@ -91,3 +91,40 @@ def test_block_args_offsets():
         assert addr(arr[2], name) - addr(arr[0], name) == 35 * step, name
     with pytest.raises(ValueError):
         lw.block_args(p, o, [10, 10])
+
+
+def test_packed_blocks_layout():
+    """Blocks held as separate arrays: pack/unpack round-trip, each block's
+    field is its own contiguous (n_b, ...) Fortran array, and block_args
+    points each block at its segment with ldim = its column count."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from ccpp_physics_b200 import rrtmg_lw as lw
+    npts, nlay, sizes = 40, 20, [10, 25, 5]
+    p = {k: (torch.from_numpy(v) if isinstance(v, np.ndarray) else v)
+         for k, v in synthetic.make_profiles(npts, nlay, seed=1).items()}
+    o = {k: torch.from_numpy(v) for k, v in abi.alloc_outputs(npts, nlay, hlw0=True, hlwb=True,
+                                                               flxprf=True).items()}
+    for k in o:
+        o[k].copy_(torch.arange(o[k].numel(), dtype=o[k].dtype).view(o[k].shape))
+    pp, po = lw.pack_blocks(p, sizes), lw.pack_blocks(o, sizes)
+    for src, packed in ((p, pp), (o, po)):
+        back = lw.unpack_blocks(packed)
+        for k, v in src.items():
+            if isinstance(v, torch.Tensor):
+                assert torch.equal(back[k], v), k
+    # block 1 (columns 10..34) of an (nlay, npts) field and of the (nlay+1, npts, 4) records
+    seg = pp["plyr"].reshape(-1)[nlay * 10: nlay * 35].view(nlay, 25)
+    assert torch.equal(seg, p["plyr"][:, 10:35])
+    seg = po["flxprf"].reshape(-1)[(nlay + 1) * 4 * 10: (nlay + 1) * 4 * 35].view(nlay + 1, 25, 4)
+    assert torch.equal(seg, o["flxprf"][:, 10:35])
+    arr, keep = lw.block_args(pp, po, sizes)
+    addr = lambda a, n: C.cast(getattr(a, n), C.c_void_p).value
+    assert [a.ldim for a in arr] == sizes
+    for name, per_col in (("plyr", 8 * nlay), ("aeraod", 8 * nlay * 16), ("icseed", 4), ("topflx", 16),
+                          ("flxprf", 32 * (nlay + 1)), ("hlwb", 8 * nlay * 16)):
+        assert addr(arr[1], name) - addr(arr[0], name) == 10 * per_col, name
+        assert addr(arr[2], name) - addr(arr[0], name) == 35 * per_col, name
+    with pytest.raises(ValueError):
+        lw.block_args(pp, o, sizes)          # profile packed, outputs not
