@@ -21,7 +21,8 @@ template <typename R> __device__ __forceinline__ R shup(R v, int d) { return __s
 template <typename R> __device__ __forceinline__ R shidx(R v, int s) { return __shfl_sync(0xffffffffu, v, s); }
 
 // V consecutive values starting at a 16-byte aligned address; the scratch
-// written by kernel A is read once, so it is loaded evict-first (.cs).
+// written by kernel A is read once, so it is loaded evict-first (.cs), and the
+// FP32 4-wide form without an L1 allocation.
 template <typename R, int V>
 __device__ __forceinline__ void load_vec(const R* __restrict__ p, R (&o)[V]) {
   if constexpr (sizeof(R) == 8) {
@@ -31,9 +32,12 @@ __device__ __forceinline__ void load_vec(const R* __restrict__ p, R (&o)[V]) {
       o[j] = v.x; o[j + 1] = v.y;
     }
   } else if constexpr (V % 4 == 0) {
+    // read once: not allocated in L1, which stays with the table records
 #pragma unroll
     for (int j = 0; j < V; j += 4) {
-      float4 v = __ldcs(reinterpret_cast<const float4*>(p + j));
+      float4 v;
+      asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+                   : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p + j));
       o[j] = v.x; o[j + 1] = v.y; o[j + 2] = v.z; o[j + 3] = v.w;
     }
   } else {
