@@ -52,19 +52,18 @@ __device__ __forceinline__ void load_vec(const R* __restrict__ p, R (&o)[V]) {
 // Shared-memory staging of the transfer kernel's inputs.  Each lane copies
 // only its own V values of a field (cp.async, 16- or 8-byte pieces) and reads
 // only them back, so no lane waits for another.  Per warp, in elements of R:
-// kRtDepth stages of {tau, frac} for the g-point pipeline, then two buffers
-// of the three band fields {pklay, pklev, taucld}; within a field, lane l's
-// values sit at [l V, l V + V).
-// Two stages (one g-point copied ahead) measured faster than three: the
-// staging then needs 40 instead of 48 KB per 4-warp CTA, which leaves the SM
-// a larger L1 for the table-record gathers (FP64 transfer 5.31 -> 5.19 ms at
-// 16,384 x 127).
+// kRtDepth stages of {tau, frac} for the g-point pipeline, then one buffer of
+// the three band fields {pklay, pklev, taucld}, refilled at each band's last
+// g-point; within a field, lane l's values sit at [l V, l V + V).
+// Less staging leaves the SM a larger L1 for the table-record gathers: two
+// stages (one g-point ahead) instead of three, 48 -> 40 KB per 4-warp CTA,
+// took the FP64 transfer kernel from 5.31 to 5.19 ms at 16,384 x 127.
 constexpr int kRtDepth = 2;
 constexpr int kRtAhead = kRtDepth - 1;   // g-points copied ahead of the one in use
 template <typename R>
 __host__ __device__ constexpr bool rt_staged() { return sizeof(R) == 8; }
 template <int V>
-__host__ __device__ constexpr int rt_warp_elems() { return (2 * kRtDepth + 2 * 3) * 32 * V; }
+__host__ __device__ constexpr int rt_warp_elems() { return (2 * kRtDepth + 3) * 32 * V; }
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
@@ -224,8 +223,8 @@ lw_rt_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int 
 
     // copy groups (staged), kRtAhead = kRtDepth - 1 g-points ahead: group i
     // (i < kRtAhead) = g-point i, group 0 also band 0's fields; the iteration
-    // of g-point g commits group g + kRtAhead (that g-point, and at a band's
-    // first g-point the next band's fields), then waits for group g
+    // of g-point g commits group g + kRtAhead (that g-point), then waits for
+    // group g; a band's last g-point adds a group with the next band's fields
     if constexpr (kStage) {
 #pragma unroll
       for (int q = 0; q < 3; ++q) stage_vec<R, V>(sl + (2 * kRtDepth + q) * 32 * V, bcol + (size_t)q * NBANDS * NLP);
@@ -243,7 +242,7 @@ lw_rt_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int 
       const R secd = R(crec[b]);
       const R pk0 = R(crec[16 + b]);          // pklay(b, 0): surface (RLM:2251-2262)
       const int ns = ns_of(b), ng = ng_of(b);
-      const R* bsl = sl + (2 * kRtDepth + 3 * (b & 1)) * 32 * V;
+      R* const bsl = sl + (2 * kRtDepth) * 32 * V;
       // register path: the band's fields, and the band's first g-point (each
       // iteration prefetches the next)
       R rblay[kStage ? 1 : V], rplev[kStage ? 1 : V], rtcld[kStage ? 1 : V], ntau[kStage ? 1 : V],
@@ -264,11 +263,6 @@ lw_rt_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int 
             const int s2 = (g + kRtAhead) % kRtDepth;
             stage_vec<R, V>(sl + (2 * s2) * 32 * V, tcol + (size_t)(g + kRtAhead) * NLP);
             stage_vec<R, V>(sl + (2 * s2 + 1) * 32 * V, fcol + (size_t)(g + kRtAhead) * NLP);
-          }
-          if (g == ns && b + 1 < NBANDS) {
-            R* nb = sl + (2 * kRtDepth + 3 * ((b + 1) & 1)) * 32 * V;
-#pragma unroll
-            for (int q = 0; q < 3; ++q) stage_vec<R, V>(nb + q * 32 * V, bcol + (size_t)(q * NBANDS + b + 1) * NLP);
           }
           cp_async_commit();
           cp_async_wait<kRtAhead>();
@@ -300,6 +294,17 @@ lw_rt_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int 
             layer_rt<R>(tau[j], frac[j], secd, blay[j], pu, plev[j], (cbits >> j) & 1u, tcld[j], tab, rt[j]);
           } else {
             rt[j].tr = R(1); rt[j].gsd = R(0); rt[j].gsu = R(0);
+          }
+        }
+        // single band buffer: at a band's last g-point, once this lane's band
+        // fields have been used, its slots take the next band's fields (a group
+        // of its own, complete by the next iteration's wait)
+        if constexpr (kStage) {
+          static_assert(kRtAhead == 1, "the band buffer's group must complete one iteration later");
+          if (g == ns + ng - 1 && b + 1 < NBANDS) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) stage_vec<R, V>(bsl + q * 32 * V, bcol + (size_t)(q * NBANDS + b + 1) * NLP);
+            cp_async_commit();
           }
         }
         const bool any_cloud = __any_sync(0xffffffffu, cbits != 0);
