@@ -1,0 +1,140 @@
+/*
+ * rrtmg_sw_gpu.h -- C ABI of the B200 RRTMG shortwave column path.
+ *
+ * The library (ccpp_physics_b200/librrtmg_lw_gpu.so, the same library as the
+ * longwave path) replaces the two public entry points of the Fortran module
+ * rrtmg_sw in ccpp-physics:
+ *
+ *   rswinit       physics/Radiation/RRTMG/radsw_main.F90:1388-1390
+ *   rrtmg_sw_run  physics/Radiation/RRTMG/radsw_main.F90:493-510
+ *                 (argument declarations radsw_main.F90:515-600)
+ *
+ * Array conventions are those of rrtmg_lw_gpu.h: the caller's Fortran arrays,
+ * column-major, real(8); element (i, k) of an (npts, nlay) array is at
+ * ptr[(i-1) + (k-1)*ldim], element (i, k, b) of an (npts, nlay, nbands)
+ * array at ptr[(i-1) + ldim*((k-1) + nlay*(b-1))].  Logicals are int32 0/1,
+ * absent optional arguments are NULL.  The derived-type outputs are arrays
+ * of records of doubles in the field order of radsw_param.f:
+ *   topfsw_type {upfxc, dnfxc, upfx0}
+ *   sfcfsw_type {upfxc, dnfxc, upfx0, dnfx0}
+ *   profsw_type {upfxc, dnfxc, upfx0, dnfx0}
+ *   cmpfsw_type {uvbfc, uvbf0, nirbm, nirdf, visbm, visdf}
+ * The functions return errflg (0 = success, 1 = error) and copy errmsg into
+ * the caller's buffer (NUL-terminated, truncated to errmsg_len).
+ *
+ * Built so far: McICA sub-columns (isubcsw = 1, 2) with random, maximum-random
+ * and maximum overlap (iovr 0, 1, 2), every cloud-optics option
+ * (iswcliq 0, 1, 2; iswcice 1, 2, 3), every two-stream option (iswmode 1, 2,
+ * 3) and every output of rrtmg_sw_run; FP64.  Calls asking for the
+ * grid-mean cloud transfer (isubcsw = 0, spcvrtc) or for the decorrelation-
+ * length / exponential overlaps (iovr 3, 4, 5) return errflg = 1 with a
+ * message saying so.
+ */
+#ifndef RRTMG_SW_GPU_H
+#define RRTMG_SW_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RRTMG_SW_NBANDS 14   /* radsw_param.f: NBANDS = NBHGH - NBLOW + 1 */
+#define RRTMG_SW_NGPT 112    /* radsw_param.f: NGPTSW */
+
+/* Arguments of rswinit (radsw_main.F90:1388-1390), plus the CUDA device. */
+typedef struct rrtmg_sw_init_args {
+  int32_t me;            /* print control: banner when me == 0 */
+  int32_t rad_hr_units;  /* 1: heating rates in K/day, otherwise K/s */
+  int32_t inc_minor_gas; /* logical; banner only (as in rswinit) */
+  int32_t iswcliq;
+  int32_t isubcsw;
+  int32_t iovr, iovr_rand, iovr_maxrand, iovr_max, iovr_dcorr, iovr_exp,
+      iovr_exprand;
+  int32_t iswmode;
+  int32_t device;        /* CUDA device ordinal (extension; 0 by default) */
+} rrtmg_sw_init_args;
+
+/* Arguments of rrtmg_sw_run (radsw_main.F90:493-510), same names. */
+typedef struct rrtmg_sw_run_args {
+  int32_t npts, nlay, nlp1;
+  int32_t ldim;          /* leading dimension of (npts,...) arrays; 0 = npts */
+  int32_t nday;          /* number of daytime points listed in idxday */
+  int32_t lprnt, lsswr, top_at_1, inc_minor_gas;
+  int32_t iovr, iovr_rand, iovr_maxrand, iovr_max, iovr_dcorr, iovr_exp,
+      iovr_exprand;
+  int32_t iswcliq, iswcice, isubcsw, iswmode;
+  double solcon;         /* solar constant [W/m2] */
+  /* inputs */
+  const double *plyr, *plvl, *tlyr, *tlvl, *qlyr, *olyr;
+  const double *gasvmr_co2, *gasvmr_n2o, *gasvmr_ch4, *gasvmr_o2, *gasvmr_co,
+      *gasvmr_cfc11, *gasvmr_cfc12, *gasvmr_cfc22, *gasvmr_ccl4;
+  const int32_t *icseed;                 /* (npts) */
+  const int32_t *idxday;                 /* (nday) 1-based daytime columns */
+  const double *aeraod, *aerssa, *aerasy;  /* (npts, nlay, nbands) */
+  const double *sfcalb_nir_dir, *sfcalb_nir_dif, *sfcalb_uvis_dir,
+      *sfcalb_uvis_dif;                  /* (npts) */
+  const double *dzlyr, *delpin;          /* (npts, nlay) */
+  const double *de_lgth;                 /* (npts) */
+  const double *alpha;                   /* (npts, nlay) */
+  const double *cosz;                    /* (npts) */
+  const double *cld_cf;                  /* (npts, nlay) */
+  /* optional cloud inputs (iswcliq > 0 needs the first eight, else the last three) */
+  const double *cld_lwp, *cld_ref_liq, *cld_iwp, *cld_ref_ice, *cld_rwp,
+      *cld_ref_rain, *cld_swp, *cld_ref_snow, *cld_od, *cld_ssa, *cld_asy;
+  /* outputs */
+  double *hswc;    /* (npts, nlay) total-sky heating rate */
+  double *topflx;  /* (npts) topfsw_type records */
+  double *sfcflx;  /* (npts) sfcfsw_type records */
+  double *cldtau;  /* (npts, nlay) layer cloud optical depth of band 25 (0.55 um) */
+  /* optional outputs (NULL = not present) */
+  double *hsw0;    /* (npts, nlay) clear-sky heating rate */
+  double *hswb;    /* (npts, nlay, nbands) spectral-band heating rates */
+  double *flxprf;  /* (npts, nlp1) profsw_type records */
+  double *fdncmp;  /* (npts) cmpfsw_type records */
+} rrtmg_sw_run_args;
+
+/* Execution options (extension): the same record as rrtmg_lw_exec;
+ * precision must be 0 (FP64).  memory 0 = host pointers, 1 = device. */
+typedef struct rrtmg_sw_exec {
+  int32_t precision;
+  int32_t memory;
+  void *stream;            /* cudaStream_t; NULL = the calling thread's stream */
+  int32_t sync;
+  int32_t reserved;
+  float *kernel_ms;        /* optional float[3]: device ms of the McICA, gas
+                              optics and transfer kernels (forces a sync) */
+} rrtmg_sw_exec;
+
+/* rswinit (radsw_main.F90:1388): validates iovr, sets heatfac, builds the
+ * exp_tbl transmittance table (radsw_main.F90:1516-1531) and uploads every
+ * coefficient table to the device.  Returns errflg. */
+int rrtmg_sw_gpu_init(const rrtmg_sw_init_args *args, char *errmsg,
+                      int32_t errmsg_len);
+
+/* rrtmg_sw_run (radsw_main.F90:493) on the GPU, FP64, host pointers,
+ * synchronous.  Returns errflg. */
+int rrtmg_sw_gpu_run(const rrtmg_sw_run_args *args, char *errmsg,
+                     int32_t errmsg_len);
+
+/* rrtmg_sw_run with an explicit memory space / stream. */
+int rrtmg_sw_gpu_run_ex(const rrtmg_sw_run_args *args,
+                        const rrtmg_sw_exec *exec, char *errmsg,
+                        int32_t errmsg_len);
+
+/* Gas optics alone (setcoef + taumol, radsw_main.F90:2242-2389, 4094-5573)
+ * for the daytime columns of `args`, device pointers: writes, for daytime
+ * point p (0-based, in idxday order) and internal (surface-first) layer k,
+ * taug[(p*nlay + k)*112 + ig], taur[(p*nlay + k)*112 + ig] and
+ * sfluxzen[p*112 + ig].  Stage entry point for parity tests. */
+int rrtmg_sw_gpu_gas_optics(const rrtmg_sw_run_args *args, double *taug,
+                            double *taur, double *sfluxzen, void *stream,
+                            char *errmsg, int32_t errmsg_len);
+
+/* Releases the device tables of rrtmg_sw_gpu_init. */
+void rrtmg_sw_gpu_finalize(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RRTMG_SW_GPU_H */
