@@ -15,6 +15,7 @@ namespace lw {
 
 constexpr int NBANDS = 16;
 constexpr int NGPT = 140;
+constexpr int kSwNgpt = 112;   // shortwave g-points (radsw_param.f NGPTSW)
 constexpr int NTBL = 10000;
 
 // g-points per band and first g-point of each band (radlw_param.f:111-120)

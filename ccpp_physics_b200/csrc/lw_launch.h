@@ -41,6 +41,10 @@ struct McicaStage {
 cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int ncols, int nlay, int iovr,
                          int isubclw, int top_at_1, const McicaStage& stage, uint32_t* bits, int num_sms,
                          cudaStream_t st);
+// shortwave McICA sub-columns (lw_mcica.cu), stage inputs, iovr 0..2:
+// bits[(c*112 + ig)*nw + (k >> 5)] bit (k & 31)
+cudaError_t mcica_sw_launch(int ncols, int nlay, int iovr, const McicaStage& stage, uint32_t* bits, int num_sms,
+                            cudaStream_t st);
 // raw state words of one twister stream (lw_mcica.cu): raw[j] is what draw j tempers
 cudaError_t seed_stream_launch(int32_t seed, long long m, uint32_t* raw, cudaStream_t st);
 // icsdsw/icsdlw of n columns from the raw words of a face's stream

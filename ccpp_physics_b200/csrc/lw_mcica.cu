@@ -276,6 +276,11 @@ __host__ __device__ inline size_t mcica_warp_bytes(int nlay, int cap) {
 
 constexpr int kMcicaWarps = 6;   // 6 warps x 18.5 KB (127 layers): two CTAs, twelve warps per SM
 
+// NG g-points per column: 140 for the longwave path (every overlap, block or
+// stage inputs), 112 for the shortwave path (stage inputs, iovr 0..2: the
+// shortwave decorrelation-length and exponential overlaps draw in another
+// order, radsw_main.F90:2104-2190, and are not built here).
+template <int NG>
 __global__ void __launch_bounds__(32 * kMcicaWarps)
 lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int ncols, McicaArgs a,
                 uint32_t* __restrict__ bits) {
@@ -314,7 +319,8 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
     if (!__any_sync(0xffffffffu, any)) continue;   // clear column: no draws
     const uint32_t s0 = (uint32_t)(seed == 0 ? 4357 : seed);   // random_setseed_t (MT:285-299)
 
-    uint32_t* out = bits + (size_t)c * NGPT * a.nw;
+    uint32_t* out = bits + (size_t)c * NG * a.nw;
+    if constexpr (NG == NGPT) {
     if (a.iovr >= 3) {
       // two sequence rings, the per-layer overlap parameter and the walk's
       // thresholds in the ring's space
@@ -378,13 +384,14 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
       mcica_two_set(mtA, mtB, clr_t, aux_t, srt, pm, nlay, a.iovr, s0, a.nw, out, lane);
       continue;
     }
+    }
     // seeding x_0..x_623 at ring[0..623]: mt(i) = 69069^i seed
     for (int n = lane; n < 624; n += 32) ring[n] = s0 * c_pow69069[n];
     __syncwarp();
     if (a.iovr == 2) {
       // maximum overlap: one draw per g-point, the same at every layer (RLM:1981-1993)
       twist_ring(ring, cap, 624, lane);   // sequence 624..1247 at ring[624..1247] (cap >= 1248)
-      for (int n = lane; n < NGPT; n += 32) {
+      for (int n = lane; n < NG; n += 32) {
         double r = u32_unit(temper(ring[624 + n]));
         for (int w = 0; w < a.nw; ++w) {
           uint32_t word = 0;
@@ -400,7 +407,8 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
     // random (iovr=0) and maximum-random (iovr=1): draw n*nlay+k (RLM:1920-1941)
     long long gen = 624;       // sequence indices generated so far
     int jp = 624;              // gen mod cap
-    for (int n0 = 0; n0 < NGPT; n0 += kMcicaRound) {
+    static_assert(NG % kMcicaRound == 0, "whole rounds of g-points");
+    for (int n0 = 0; n0 < NG; n0 += kMcicaRound) {
       const long long need = 624 + (long long)(n0 + kMcicaRound) * nlay;
       while (gen < need) {
         twist_ring(ring, cap, jp, lane);
@@ -566,7 +574,9 @@ int mcica_ring_capacity(int nlay) {
 }
 
 cudaError_t mcica_prepare(int max_smem) {
-  return cudaFuncSetAttribute(lw_mcica_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  cudaError_t e = cudaFuncSetAttribute(lw_mcica_kernel<NGPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(lw_mcica_kernel<kSwNgpt>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
 }
 
 cudaError_t mcica_upload_powers() {
@@ -589,17 +599,45 @@ cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int 
   const int wpb = kMcicaWarps;
   size_t smem = mcica_warp_bytes(nlay, a.cap) * wpb;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lw_mcica_kernel, wpb * 32, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lw_mcica_kernel<NGPT>, wpb * 32, smem);
   if (per_sm < 1) per_sm = 1;
   int grid = min((ncols + wpb - 1) / wpb, num_sms * per_sm);
   if (grid < 1) return cudaSuccess;
-  lw_mcica_kernel<<<grid, wpb * 32, smem, st>>>(blocks, nblocks, b0, ncols, a, bits);
+  lw_mcica_kernel<NGPT><<<grid, wpb * 32, smem, st>>>(blocks, nblocks, b0, ncols, a, bits);
 #if LW_DEBUG_CHECKS
   {
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { fprintf(stderr, "lw debug: mcica kernel failed\n"); return e; }
   }
 #endif
+  return cudaGetLastError();
+}
+
+// Shortwave sub-columns (mcica_subcol, radsw_main.F90:1952-2212) for iovr 0
+// (random), 1 (maximum-random) and 2 (maximum): the draws are g-major,
+// rand2d((n-1)*nlay + k) as in the longwave generator, over 112 g-points.
+// stage.cldf is the layer cloud fraction floored at ftiny = 1e-12
+// (radsw_main.F90:1900-1903), internal (surface-first) order.
+cudaError_t mcica_sw_launch(int ncols, int nlay, int iovr, const McicaStage& stage, uint32_t* bits, int num_sms,
+                            cudaStream_t st) {
+  if (iovr < 0 || iovr > 2) return cudaErrorInvalidValue;
+  McicaArgs a;
+  a.nlay = nlay;
+  a.nw = (nlay + 31) / 32;
+  a.iovr = iovr;
+  a.isubclw = 2;
+  a.top_at_1 = 0;
+  a.cap = mcica_ring_capacity(nlay);
+  a.st = stage;
+  const int wpb = kMcicaWarps;
+  size_t smem = mcica_warp_bytes(nlay, a.cap) * wpb;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lw_mcica_kernel<kSwNgpt>, wpb * 32, smem);
+  if (per_sm < 1) per_sm = 1;
+  int grid = min((ncols + wpb - 1) / wpb, num_sms * per_sm);
+  if (grid < 1) return cudaSuccess;
+  Block none{};
+  lw_mcica_kernel<kSwNgpt><<<grid, wpb * 32, smem, st>>>(nullptr, 0, none, ncols, a, bits);
   return cudaGetLastError();
 }
 

@@ -1,0 +1,472 @@
+// sw_api.cu -- C ABI of the B200 RRTMG-SW path (include/rrtmg_sw_gpu.h).
+//
+// rrtmg_sw_gpu_init   <- rswinit      (physics/Radiation/RRTMG/radsw_main.F90:1388-1536)
+// rrtmg_sw_gpu_run*   <- rrtmg_sw_run (radsw_main.F90:493-1379)
+//
+// The module state of the reference (heatfac, exp_tbl and the coefficient
+// DATA) becomes immutable device memory written once by init.  Each host
+// thread that calls run gets its own stream and device workspace.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/rrtmg_sw_gpu.h"
+#include "../data/rrtmg_sw_table_layout.h"
+#include "lw_common.cuh"
+#include "lw_launch.h"
+#include "sw_kernels.h"
+
+extern "C" const unsigned char rrtmg_sw_tables_blob[];
+extern "C" const unsigned char rrtmg_sw_tables_blob_end[];
+
+namespace {
+
+constexpr int kNtbmx = 10000;
+constexpr double kS0 = 1368.22;                  // RSM:332
+constexpr size_t kScratchBudget = (size_t)4 << 30;
+
+struct SwState {
+  bool ready = false;
+  int device = 0, num_sms = 0;
+  double* tab = nullptr;     // coefficient blob
+  double* etab = nullptr;    // exp_tbl(0:NTBMX)
+  double heatfac = 0.0;
+};
+SwState g;
+std::mutex g_mu;
+
+struct SwWorkspace {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  char* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  char* stage = nullptr;     // device copies of host arguments
+  size_t stage_bytes = 0;
+  int* bad = nullptr;
+};
+std::vector<SwWorkspace*> g_ws;
+thread_local SwWorkspace* tl_ws = nullptr;
+
+void set_msg(char* m, int32_t n, const char* fmt, ...) {
+  if (!m || n <= 0) return;
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(m, (size_t)n, fmt, ap);
+  va_end(ap);
+}
+int cuda_fail(char* m, int32_t n, const char* what, cudaError_t e) {
+  set_msg(m, n, "rrtmg_sw_gpu: %s failed: %s", what, cudaGetErrorString(e));
+  return 1;
+}
+#define CK(call, what)                                                      \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) return cuda_fail(errmsg, errmsg_len, what, e_);  \
+  } while (0)
+
+cudaError_t grow(char** p, size_t* have, size_t need) {
+  if (*have >= need && *p) return cudaSuccess;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  const size_t n = std::max<size_t>(need, 256) * 5 / 4;
+  cudaError_t e = cudaMalloc((void**)p, n);
+  if (e == cudaSuccess) *have = n;
+  return e;
+}
+
+SwWorkspace* workspace(char* errmsg, int32_t errmsg_len, int* rc) {
+  *rc = 0;
+  if (tl_ws && tl_ws->device == g.device) return tl_ws;
+  SwWorkspace* w = new SwWorkspace();
+  w->device = g.device;
+  cudaError_t e = cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&w->bad, sizeof(int));
+  if (e != cudaSuccess) {
+    *rc = cuda_fail(errmsg, errmsg_len, "workspace setup", e);
+    delete w;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_ws.push_back(w);
+  tl_ws = w;
+  return w;
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// per-column scratch bytes of the three kernels
+size_t scratch_per_col(int nlay) {
+  const int nw = (nlay + 31) / 32;
+  return align256(0) + (size_t)(2 * nlay * sw::kSwNg + sw::kSwNg + 3 * nlay * 14 + nlay + 1) * 8 + 4 +
+         (size_t)sw::kSwNg * nw * 4 + 64;
+}
+
+// carve one chunk's scratch out of the workspace
+sw::SwScratch carve(char* base, int nc, int nlay) {
+  sw::SwScratch s{};
+  const int nw = (nlay + 31) / 32;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { char* p = base + off; off += align256(bytes); return p; };
+  s.taug = (double*)take((size_t)nc * nlay * sw::kSwNg * 8);
+  s.taur = (double*)take((size_t)nc * nlay * sw::kSwNg * 8);
+  s.sflux = (double*)take((size_t)nc * sw::kSwNg * 8);
+  s.taucw = (double*)take((size_t)nc * nlay * 14 * 8);
+  s.ssacw = (double*)take((size_t)nc * nlay * 14 * 8);
+  s.asycw = (double*)take((size_t)nc * nlay * 14 * 8);
+  s.cldf = (double*)take((size_t)nc * nlay * 8);
+  s.zcf1 = (double*)take((size_t)nc * 8);
+  s.seed = (int32_t*)take((size_t)nc * 4);
+  s.bits = (uint32_t*)take((size_t)nc * sw::kSwNg * nw * 4);
+  s.nw = nw;
+  return s;
+}
+size_t carve_bytes(int nc, int nlay) {
+  const int nw = (nlay + 31) / 32;
+  const size_t parts[10] = {(size_t)nc * nlay * sw::kSwNg * 8, (size_t)nc * nlay * sw::kSwNg * 8,
+                            (size_t)nc * sw::kSwNg * 8,        (size_t)nc * nlay * 14 * 8,
+                            (size_t)nc * nlay * 14 * 8,        (size_t)nc * nlay * 14 * 8,
+                            (size_t)nc * nlay * 8,             (size_t)nc * 8,
+                            (size_t)nc * 4,                    (size_t)nc * sw::kSwNg * nw * 4};
+  size_t t = 0;
+  for (size_t p : parts) t += align256(p);
+  return t;
+}
+
+// Sizes (in elements) of the caller's arrays.
+struct Sizes { size_t n2, n3, nlev, np, nd; };
+Sizes sizes_of(const rrtmg_sw_run_args* a) {
+  const size_t ld = a->ldim > 0 ? (size_t)a->ldim : (size_t)a->npts;
+  return Sizes{ld * a->nlay, ld * a->nlay * RRTMG_SW_NBANDS, ld * (size_t)a->nlp1, (size_t)a->npts,
+               (size_t)std::max(a->nday, 0)};
+}
+
+// 0 = run, -1 = nothing to do, 1 = error
+int validate(const rrtmg_sw_run_args* a, const rrtmg_sw_exec* x, char* errmsg, int32_t errmsg_len) {
+  if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_run: null argument struct"); return 1; }
+  if (!a->lsswr || a->nday <= 0) return -1;                 // RSM:785-787
+  if (a->iswcliq > 0) {                                      // RSM:815-828
+    if (!a->cld_lwp || !a->cld_ref_liq || !a->cld_iwp || !a->cld_ref_ice || !a->cld_rwp || !a->cld_ref_rain ||
+        !a->cld_swp || !a->cld_ref_snow) {
+      set_msg(errmsg, errmsg_len,
+              "Logic error: iswcliq>0 requires the following optional arguments to be present: "
+              "cld_lwp, cld_ref_liq, cld_iwp, cld_ref_ice, cld_rwp, cld_ref_rain, cld_swp, cld_ref_snow");
+      return 1;
+    }
+  } else if (!a->cld_od || !a->cld_ssa || !a->cld_asy) {     // RSM:829-838
+    set_msg(errmsg, errmsg_len,
+            "Logic error: iswcliq<=0 requires the following optional arguments to be present: cld_od, cld_ssa, cld_asy");
+    return 1;
+  }
+  if (x->precision != 0) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: only FP64 (precision 0) is built"); return 1; }
+  if (x->memory != 0 && x->memory != 1) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: memory must be 0 or 1"); return 1; }
+  if (a->isubcsw != 1 && a->isubcsw != 2) {
+    set_msg(errmsg, errmsg_len,
+            "rrtmg_sw_gpu: isubcsw=%d: only the McICA transfer (isubcsw 1, 2: spcvrtm) is built; "
+            "the grid-mean cloud transfer spcvrtc (isubcsw 0) is not", a->isubcsw);
+    return 1;
+  }
+  if (a->iovr < 0 || a->iovr > 2) {
+    set_msg(errmsg, errmsg_len,
+            "rrtmg_sw_gpu: iovr=%d: the sub-column generator is built for iovr 0 (random), 1 (maximum-random) "
+            "and 2 (maximum) only", a->iovr);
+    return 1;
+  }
+  if (a->iswmode < 1 || a->iswmode > 3) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: iswmode must be 1, 2 or 3"); return 1; }
+  if (a->npts < 1 || a->nlay < 1 || a->nlp1 != a->nlay + 1 || a->nlay > sw::kSwMaxLay ||
+      (a->ldim != 0 && a->ldim < a->npts)) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: bad sizes npts=%d nlay=%d nlp1=%d ldim=%d (nlay <= %d)", a->npts,
+            a->nlay, a->nlp1, a->ldim, sw::kSwMaxLay);
+    return 1;
+  }
+  const void* req[] = {a->plyr, a->tlyr, a->qlyr, a->olyr, a->gasvmr_co2, a->gasvmr_n2o, a->gasvmr_ch4,
+                       a->gasvmr_o2, a->idxday, a->aeraod, a->aerssa, a->aerasy, a->sfcalb_nir_dir,
+                       a->sfcalb_nir_dif, a->sfcalb_uvis_dir, a->sfcalb_uvis_dif, a->delpin, a->cosz, a->cld_cf,
+                       a->hswc, a->topflx, a->sfcflx, a->cldtau};
+  for (const void* p : req)
+    if (!p) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: a required array is NULL"); return 1; }
+  if (a->isubcsw == 2 && !a->icseed) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: isubcsw=2 needs icseed"); return 1; }
+  if (x->memory == 0)
+    for (int p = 0; p < a->nday; ++p)
+      if (a->idxday[p] < 1 || a->idxday[p] > a->npts) {
+        set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: idxday(%d)=%d outside 1..npts", p + 1, a->idxday[p]);
+        return 1;
+      }
+  return 0;
+}
+
+sw::SwArgs device_args(const rrtmg_sw_run_args* a) {
+  sw::SwArgs d{};
+  d.plyr = a->plyr; d.tlyr = a->tlyr; d.qlyr = a->qlyr; d.olyr = a->olyr;
+  d.co2 = a->gasvmr_co2; d.n2o = a->gasvmr_n2o; d.ch4 = a->gasvmr_ch4; d.o2 = a->gasvmr_o2;
+  d.delp = a->delpin; d.cf = a->cld_cf;
+  d.aod = a->aeraod; d.ssa = a->aerssa; d.asy = a->aerasy; d.cosz = a->cosz;
+  d.alb_nir_dir = a->sfcalb_nir_dir; d.alb_nir_dif = a->sfcalb_nir_dif;
+  d.alb_uvis_dir = a->sfcalb_uvis_dir; d.alb_uvis_dif = a->sfcalb_uvis_dif;
+  d.lwp = a->cld_lwp; d.rel = a->cld_ref_liq; d.iwp = a->cld_iwp; d.rei = a->cld_ref_ice;
+  d.rwp = a->cld_rwp; d.rer = a->cld_ref_rain; d.swp = a->cld_swp; d.res = a->cld_ref_snow;
+  d.cod = a->cld_od; d.cssa = a->cld_ssa; d.casy = a->cld_asy;
+  d.icseed = a->icseed; d.idxday = a->idxday;
+  d.hswc = a->hswc; d.topflx = a->topflx; d.sfcflx = a->sfcflx; d.cldtau = a->cldtau;
+  d.hsw0 = a->hsw0; d.hswb = a->hswb; d.flxprf = a->flxprf; d.fdncmp = a->fdncmp;
+  d.npts = a->npts; d.nlay = a->nlay; d.ld = a->ldim > 0 ? a->ldim : a->npts;
+  d.top_at_1 = a->top_at_1; d.inc_minor = a->inc_minor_gas; d.iovr = a->iovr;
+  d.iovr_rand = a->iovr_rand; d.iovr_maxrand = a->iovr_maxrand;
+  d.iswcliq = a->iswcliq; d.iswcice = a->iswcice; d.isubcsw = a->isubcsw; d.iswmode = a->iswmode;
+  d.s0fac = a->solcon / kS0;   // RSM:793
+  d.heatfac = g.heatfac;
+  return d;
+}
+
+// zero every output of every column (RSM:795-813); device pointers
+cudaError_t zero_outputs(const sw::SwArgs& d, const Sizes& z, int nlay, cudaStream_t st) {
+  const size_t pitch = (size_t)d.ld * 8, width = (size_t)d.npts * 8;
+  cudaError_t e = cudaMemset2DAsync(d.hswc, pitch, 0, width, nlay, st);
+  if (e == cudaSuccess) e = cudaMemset2DAsync(d.cldtau, pitch, 0, width, nlay, st);
+  if (e == cudaSuccess && d.hsw0) e = cudaMemset2DAsync(d.hsw0, pitch, 0, width, nlay, st);
+  if (e == cudaSuccess && d.hswb) e = cudaMemset2DAsync(d.hswb, pitch, 0, width, (size_t)nlay * 14, st);
+  if (e == cudaSuccess && d.flxprf) e = cudaMemset2DAsync(d.flxprf, pitch * 4, 0, width * 4, nlay + 1, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d.topflx, 0, z.np * 3 * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d.sfcflx, 0, z.np * 4 * 8, st);
+  if (e == cudaSuccess && d.fdncmp) e = cudaMemsetAsync(d.fdncmp, 0, z.np * 6 * 8, st);
+  return e;
+}
+
+// all kernels of one call on device arguments
+int run_device(SwWorkspace* w, const sw::SwArgs& d, int nday, cudaStream_t st, float* kernel_ms, char* errmsg,
+               int32_t errmsg_len, const Sizes& z) {
+  CK(zero_outputs(d, z, d.nlay, st), "zeroing the outputs");
+  const size_t per = scratch_per_col(d.nlay);
+  int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nday, kScratchBudget / per));
+  CK(grow(&w->scratch, &w->scratch_bytes, carve_bytes(chunk, d.nlay)), "scratch allocation");
+  CK(cudaMemsetAsync(w->bad, 0, sizeof(int), st), "cudaMemsetAsync");
+  cudaEvent_t ev[4] = {};
+  if (kernel_ms) {
+    for (auto& e : ev) CK(cudaEventCreate(&e), "cudaEventCreate");
+  }
+  for (int p0 = 0; p0 < nday; p0 += chunk) {
+    const int nc = std::min(chunk, nday - p0);
+    sw::SwScratch s = carve(w->scratch, nc, d.nlay);
+    s.bad = w->bad;
+    const bool first = kernel_ms && p0 == 0;
+    if (first) CK(cudaEventRecord(ev[0], st), "cudaEventRecord");
+    CK(sw::optics_launch(d, s, p0, nc, g.tab, st), "optics kernel launch");
+    if (first) CK(cudaEventRecord(ev[1], st), "cudaEventRecord");
+    lw::McicaStage ms;
+    ms.cldf = s.cldf;
+    ms.seed = s.seed;
+    ms.ld = nc;
+    CK(lw::mcica_sw_launch(nc, d.nlay, d.iovr, ms, s.bits, g.num_sms, st), "McICA kernel launch");
+    if (first) CK(cudaEventRecord(ev[2], st), "cudaEventRecord");
+    CK(sw::rt_launch(d, s, p0, nc, g.etab, st), "transfer kernel launch");
+    if (first) CK(cudaEventRecord(ev[3], st), "cudaEventRecord");
+  }
+  if (kernel_ms) {
+    CK(cudaEventSynchronize(ev[3]), "kernel execution");
+    // [McICA, optics, transfer], the order of the longwave timings
+    cudaEventElapsedTime(&kernel_ms[0], ev[1], ev[2]);
+    cudaEventElapsedTime(&kernel_ms[1], ev[0], ev[1]);
+    cudaEventElapsedTime(&kernel_ms[2], ev[2], ev[3]);
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  return 0;
+}
+
+int check_bad(SwWorkspace* w, cudaStream_t st, char* errmsg, int32_t errmsg_len) {
+  int bad = 0;
+  CK(cudaMemcpyAsync(&bad, w->bad, sizeof(int), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  CK(cudaStreamSynchronize(st), "kernel execution");
+  if (bad) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: idxday names a column outside 1..npts (those points were skipped)");
+    return 1;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int rrtmg_sw_gpu_init(const rrtmg_sw_init_args* a, char* errmsg, int32_t errmsg_len) {
+  set_msg(errmsg, errmsg_len, "");
+  if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_init: null argument struct"); return 1; }
+  int errflg = 0;
+  if (a->iovr != a->iovr_rand && a->iovr != a->iovr_maxrand && a->iovr != a->iovr_max &&
+      a->iovr != a->iovr_dcorr && a->iovr != a->iovr_exp && a->iovr != a->iovr_exprand) {   // RSM:1450-1455
+    errflg = 1;
+    set_msg(errmsg, errmsg_len, "ERROR(rswinit): Error in specification of cloud overlap flag");
+  }
+  if (a->me == 0) {   // RSM:1457-1487
+    std::printf(" - Using AER Shortwave Radiation, Version: NCEP SW v5.1  Nov 2012 -RRTMG-SW v3.8   \n");
+    if (a->iswmode == 1) std::printf("   --- Delta-eddington 2-stream transfer scheme\n");
+    else if (a->iswmode == 2) std::printf("   --- PIFM 2-stream transfer scheme\n");
+    else if (a->iswmode == 3) std::printf("   --- Discrete ordinates 2-stream transfer scheme\n");
+    if (!a->inc_minor_gas) std::printf("   --- Rare gases absorption is NOT included in SW\n");
+    else std::printf("   --- Include rare gases N2O, CH4, O2, absorptions in SW\n");
+    if (a->isubcsw == 0) std::printf("   --- Using standard grid average clouds, no sub-column clouds approximation applied\n");
+    else if (a->isubcsw == 1) std::printf("   --- Using MCICA sub-colum clouds approximation with a prescribed sequence of permutation seeds\n");
+    else if (a->isubcsw == 2) std::printf("   --- Using MCICA sub-colum clouds approximation with provided input array of permutation seeds\n");
+  }
+  std::lock_guard<std::mutex> lk(g_mu);
+  g.heatfac = (a->rad_hr_units == 1) ? 9.80665 * 864.0 / 1.0046e+3 : 9.80665 * 1.0e-2 / 1.0046e+3;   // RSM:1491-1495
+  // exp_tbl (RSM:1516-1531), on the host with the C library's exp
+  std::vector<double> et(kNtbmx + 1);
+  const double bpade = 1.0 / 0.278;
+  et[0] = 1.0;
+  et[kNtbmx] = 1.e-20;
+  for (int i = 1; i <= kNtbmx - 1; ++i) {
+    const double tfn = (double)i / (double)(kNtbmx - i);
+    et[i] = std::exp(-(bpade * tfn));
+  }
+  CK(cudaSetDevice(a->device), "cudaSetDevice");
+  if (!g.ready || g.device != a->device) {
+    g.device = a->device;
+    CK(cudaDeviceGetAttribute(&g.num_sms, cudaDevAttrMultiProcessorCount, g.device), "cudaDeviceGetAttribute");
+    const size_t nb = (size_t)(rrtmg_sw_tables_blob_end - rrtmg_sw_tables_blob);
+    if (nb != (size_t)RRTMG_SW_TABLES_NDOUBLE * 8) {
+      set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_init: embedded table blob has %zu bytes, expected %zu", nb,
+              (size_t)RRTMG_SW_TABLES_NDOUBLE * 8);
+      return 1;
+    }
+    CK(cudaMalloc((void**)&g.tab, nb), "cudaMalloc tables");
+    CK(cudaMemcpy(g.tab, rrtmg_sw_tables_blob, nb, cudaMemcpyHostToDevice), "table upload");
+    CK(cudaMalloc((void**)&g.etab, (kNtbmx + 1) * 8), "cudaMalloc exp_tbl");
+    int max_smem = 0;
+    CK(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, g.device), "cudaDeviceGetAttribute");
+    CK(lw::mcica_upload_powers(), "mcica powers upload");
+    CK(lw::mcica_prepare(max_smem), "mcica kernel attributes");
+    CK(sw::rt_prepare(max_smem), "transfer kernel attributes");
+  }
+  CK(cudaMemcpy(g.etab, et.data(), (kNtbmx + 1) * 8, cudaMemcpyHostToDevice), "exp_tbl upload");
+  g.ready = true;
+  return errflg;
+}
+
+extern "C" int rrtmg_sw_gpu_run_ex(const rrtmg_sw_run_args* a, const rrtmg_sw_exec* x, char* errmsg,
+                                   int32_t errmsg_len) {
+  set_msg(errmsg, errmsg_len, "");
+  if (!g.ready) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: rrtmg_sw_gpu_init has not been called"); return 1; }
+  rrtmg_sw_exec dflt{0, 0, nullptr, 1, 0, nullptr};
+  if (!x) x = &dflt;
+  const int v = validate(a, x, errmsg, errmsg_len);
+  if (v == -1) return 0;
+  if (v) return 1;
+  CK(cudaSetDevice(g.device), "cudaSetDevice");
+  int rc = 0;
+  SwWorkspace* w = workspace(errmsg, errmsg_len, &rc);
+  if (!w) return rc;
+  cudaStream_t st = x->stream ? (cudaStream_t)x->stream : w->stream;
+  const Sizes z = sizes_of(a);
+  if (x->memory == 1) {
+    sw::SwArgs d = device_args(a);
+    int r = run_device(w, d, a->nday, st, x->kernel_ms, errmsg, errmsg_len, z);
+    if (r) return r;
+    if (x->sync || x->kernel_ms) return check_bad(w, st, errmsg, errmsg_len);
+    return 0;
+  }
+  // host arrays: stage every argument in one device buffer
+  rrtmg_sw_run_args da = *a;
+  std::vector<std::pair<const double**, size_t>> ins = {
+      {&da.plyr, z.n2}, {&da.tlyr, z.n2}, {&da.qlyr, z.n2}, {&da.olyr, z.n2},
+      {&da.gasvmr_co2, z.n2}, {&da.gasvmr_n2o, z.n2}, {&da.gasvmr_ch4, z.n2}, {&da.gasvmr_o2, z.n2},
+      {&da.aeraod, z.n3}, {&da.aerssa, z.n3}, {&da.aerasy, z.n3},
+      {&da.sfcalb_nir_dir, z.np}, {&da.sfcalb_nir_dif, z.np}, {&da.sfcalb_uvis_dir, z.np},
+      {&da.sfcalb_uvis_dif, z.np}, {&da.delpin, z.n2}, {&da.cosz, z.np}, {&da.cld_cf, z.n2},
+      {&da.cld_lwp, z.n2}, {&da.cld_ref_liq, z.n2}, {&da.cld_iwp, z.n2}, {&da.cld_ref_ice, z.n2},
+      {&da.cld_rwp, z.n2}, {&da.cld_ref_rain, z.n2}, {&da.cld_swp, z.n2}, {&da.cld_ref_snow, z.n2},
+      {&da.cld_od, z.n2}, {&da.cld_ssa, z.n2}, {&da.cld_asy, z.n2}};
+  std::vector<std::pair<double**, size_t>> outs = {
+      {&da.hswc, z.n2}, {&da.topflx, z.np * 3}, {&da.sfcflx, z.np * 4}, {&da.cldtau, z.n2},
+      {&da.hsw0, z.n2}, {&da.hswb, z.n3}, {&da.flxprf, z.nlev * 4}, {&da.fdncmp, z.np * 6}};
+  size_t total = align256(z.np * 4) + align256(z.nd * 4);
+  for (auto& p : ins) if (*p.first) total += align256(p.second * 8);
+  for (auto& p : outs) if (*p.first) total += align256(p.second * 8);
+  CK(grow(&w->stage, &w->stage_bytes, total), "staging allocation");
+  size_t off = 0;
+  auto place = [&](size_t bytes) { char* p = w->stage + off; off += align256(bytes); return p; };
+  if (a->icseed) {
+    int32_t* p = (int32_t*)place(z.np * 4);
+    CK(cudaMemcpyAsync(p, a->icseed, z.np * 4, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+    da.icseed = p;
+  }
+  {
+    int32_t* p = (int32_t*)place(z.nd * 4);
+    CK(cudaMemcpyAsync(p, a->idxday, z.nd * 4, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+    da.idxday = p;
+  }
+  for (auto& p : ins) {
+    if (!*p.first) continue;
+    double* d = (double*)place(p.second * 8);
+    CK(cudaMemcpyAsync(d, *p.first, p.second * 8, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+    *p.first = d;
+  }
+  struct Back { double* host; double* dev; size_t n; };
+  std::vector<Back> back;
+  for (auto& p : outs) {
+    if (!*p.first) continue;
+    double* d = (double*)place(p.second * 8);
+    back.push_back({*p.first, d, p.second});
+    *p.first = d;
+  }
+  sw::SwArgs d = device_args(&da);
+  int r = run_device(w, d, a->nday, st, x->kernel_ms, errmsg, errmsg_len, z);
+  if (r) return r;
+  for (const Back& b : back)
+    CK(cudaMemcpyAsync(b.host, b.dev, b.n * 8, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  return check_bad(w, st, errmsg, errmsg_len);
+}
+
+extern "C" int rrtmg_sw_gpu_run(const rrtmg_sw_run_args* a, char* errmsg, int32_t errmsg_len) {
+  return rrtmg_sw_gpu_run_ex(a, nullptr, errmsg, errmsg_len);
+}
+
+extern "C" int rrtmg_sw_gpu_gas_optics(const rrtmg_sw_run_args* a, double* taug, double* taur, double* sfluxzen,
+                                       void* stream, char* errmsg, int32_t errmsg_len) {
+  set_msg(errmsg, errmsg_len, "");
+  if (!g.ready) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: rrtmg_sw_gpu_init has not been called"); return 1; }
+  if (!a || a->nday <= 0 || a->nlay < 1 || a->nlay > sw::kSwMaxLay || !taug || !taur || !sfluxzen) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_gas_optics: bad arguments");
+    return 1;
+  }
+  CK(cudaSetDevice(g.device), "cudaSetDevice");
+  int rc = 0;
+  SwWorkspace* w = workspace(errmsg, errmsg_len, &rc);
+  if (!w) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : w->stream;
+  sw::SwArgs d = device_args(a);
+  d.cldtau = nullptr;
+  const int nday = a->nday, nlay = a->nlay;
+  CK(grow(&w->scratch, &w->scratch_bytes, carve_bytes(nday, nlay)), "scratch allocation");
+  sw::SwScratch s = carve(w->scratch, nday, nlay);
+  s.bad = w->bad;
+  d.gas_only = 1;
+  CK(cudaMemsetAsync(w->bad, 0, sizeof(int), st), "cudaMemsetAsync");
+  CK(sw::optics_launch(d, s, 0, nday, g.tab, st), "optics kernel launch");
+  const size_t n = (size_t)nday * nlay * sw::kSwNg;
+  CK(cudaMemcpyAsync(taug, s.taug, n * 8, cudaMemcpyDeviceToDevice, st), "cudaMemcpyAsync");
+  CK(cudaMemcpyAsync(taur, s.taur, n * 8, cudaMemcpyDeviceToDevice, st), "cudaMemcpyAsync");
+  CK(cudaMemcpyAsync(sfluxzen, s.sflux, (size_t)nday * sw::kSwNg * 8, cudaMemcpyDeviceToDevice, st), "cudaMemcpyAsync");
+  return check_bad(w, st, errmsg, errmsg_len);
+}
+
+extern "C" void rrtmg_sw_gpu_finalize(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (SwWorkspace* w : g_ws) {
+    if (w->stream) cudaStreamSynchronize(w->stream);
+    cudaFree(w->scratch);
+    cudaFree(w->stage);
+    cudaFree(w->bad);
+    if (w->stream) cudaStreamDestroy(w->stream);
+    delete w;
+  }
+  g_ws.clear();
+  tl_ws = nullptr;
+  if (g.tab) cudaFree(g.tab);
+  if (g.etab) cudaFree(g.etab);
+  g = SwState{};
+}

@@ -17,7 +17,7 @@ def _declared():
     names = set()
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         txt = open(h).read()
-        names |= set(re.findall(r"^\s*(?:int|void)\s+(rrtmg_lw_gpu_\w+)\s*\(", txt, re.M))
+        names |= set(re.findall(r"^\s*(?:int|void)\s+(rrtmg_[ls]w_gpu_\w+)\s*\(", txt, re.M))
     return names
 
 
@@ -25,7 +25,8 @@ def test_library_exports_header_symbols():
     from ccpp_physics_b200 import rrtmg_lw as lw
     L = lw.lib()
     declared = _declared()
-    assert {"rrtmg_lw_gpu_init", "rrtmg_lw_gpu_run", "rrtmg_lw_gpu_run_ex"} <= declared
+    assert {"rrtmg_lw_gpu_init", "rrtmg_lw_gpu_run", "rrtmg_lw_gpu_run_ex", "rrtmg_sw_gpu_init",
+            "rrtmg_sw_gpu_run", "rrtmg_sw_gpu_run_ex"} <= declared
     for n in sorted(declared):
         assert hasattr(L, n), n
 

@@ -1,0 +1,170 @@
+"""GPU parity tests of the RRTMG-SW path: the CUDA kernels through the C ABI
+(rrtmg_sw_gpu_run_ex) against the CPU restatement of rrtmg_sw_run
+(physics/Radiation/RRTMG/radsw_main.F90:493-1379) on identical inputs.
+
+Bars (those of the longwave path): fluxes within 1e-10 relative; heating
+rates within 1e-9 * max(|ref|, 1 K/day), since the GPU sums the g-point
+fluxes in another order than the reference and heating rates difference
+nearly equal fluxes; McICA flags are bit-exact, which the cloudy-column
+fluxes expose (one flipped sub-column moves fluxes by far more than 1e-10).
+"""
+import numpy as np
+import pytest
+
+from ccpp_physics_b200 import rrtmg_sw as sw, synthetic
+
+pytestmark = pytest.mark.gpu
+
+FLUX_RTOL = 1e-10
+HR_TOL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    sw.rswinit(device=0)
+    return sw
+
+
+@pytest.fixture(scope="module")
+def osw():
+    from oracle import oracle_sw
+    rc, msg = oracle_sw.rswinit()
+    assert rc == 0, msg
+    return oracle_sw
+
+
+def _profile(npts, nlay, seed, **kw):
+    prof = synthetic.make_profiles(npts, nlay, seed=seed, cloudy=kw.pop("cloudy", True))
+    return sw.add_sw_inputs(prof, seed=seed, **kw)
+
+
+def _flip(prof):
+    """The same columns with the layer order reversed (top_at_1 input)."""
+    f = dict(prof)
+    for k, v in prof.items():
+        if isinstance(v, np.ndarray) and v.ndim == 2 and v.shape[0] == prof["nlay"]:
+            f[k] = np.ascontiguousarray(v[::-1])
+        elif isinstance(v, np.ndarray) and v.ndim == 3 and v.shape[1] == prof["nlay"]:
+            f[k] = np.ascontiguousarray(v[:, ::-1])
+    return f
+
+
+def _rel(a, b, floor=0.0):
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor))) if a.size else 0.0
+
+
+def _both(gpu, osw, prof, flags=None, **opt):
+    ref = sw.alloc_outputs(prof["npts"], prof["nlay"], **opt)
+    rc, msg = osw.run(prof, ref, flags=flags)
+    assert rc == 0, msg
+    out = sw.alloc_outputs(prof["npts"], prof["nlay"], **opt)
+    gpu.rrtmg_sw_run(prof, out, flags=flags)
+    return out, ref
+
+
+def _check(out, ref):
+    for k in ("topflx", "sfcflx", "fdncmp", "flxprf"):
+        if k in out:
+            assert np.isfinite(out[k]).all(), k
+            assert _rel(out[k], ref[k], 1e-300) <= FLUX_RTOL, (k, _rel(out[k], ref[k], 1e-300))
+    for k in ("hswc", "hsw0", "hswb"):
+        if k in out:
+            assert _rel(out[k], ref[k], 1.0) <= HR_TOL, (k, _rel(out[k], ref[k], 1.0))
+    assert _rel(out["cldtau"], ref["cldtau"], 1.0) <= 1e-14
+
+
+def test_sw_allsky_127(gpu, osw):
+    prof = _profile(96, 127, 21, night_fraction=0.2, precip=True)
+    out, ref = _both(gpu, osw, prof, hswb=True, flxprf=True)
+    _check(out, ref)
+    assert (ref["topflx"][:, 0] != ref["topflx"][:, 2]).any()   # cloudy columns present
+
+
+def test_sw_top_at_1(gpu, osw):
+    prof = _profile(40, 64, 22, precip=True)
+    out, ref = _both(gpu, osw, _flip(prof), flags=dict(top_at_1=1), hswb=True, flxprf=True)
+    _check(out, ref)
+
+
+@pytest.mark.parametrize("flags", [
+    dict(iovr=0), dict(iovr=2), dict(iswmode=1), dict(iswmode=3), dict(iswcice=1), dict(iswcice=2),
+    dict(iswcliq=2), dict(isubcsw=1), dict(inc_minor_gas=0),
+])
+def test_sw_options(gpu, osw, flags):
+    prof = _profile(48, 72, 23, night_fraction=0.1, precip=True)
+    out, ref = _both(gpu, osw, prof, flags=flags, flxprf=True)
+    _check(out, ref)
+
+
+def test_sw_diagnostic_clouds(gpu, osw):
+    prof = _profile(32, 50, 24)
+    cf = prof["cld_cf"]
+    rng = np.random.default_rng(3)
+    prof["cld_od"] = np.where(cf > 0, rng.uniform(0.5, 30, cf.shape), 0.0)
+    prof["cld_ssa"] = rng.uniform(0.9, 1.0, cf.shape)
+    prof["cld_asy"] = rng.uniform(0.7, 0.9, cf.shape)
+    out, ref = _both(gpu, osw, prof, flags=dict(iswcliq=0), hswb=True)
+    _check(out, ref)
+
+
+def test_sw_clear_and_one_column(gpu, osw):
+    prof = _profile(20, 40, 25, cloudy=False, aerosol=False)
+    out, ref = _both(gpu, osw, prof, flxprf=True)
+    _check(out, ref)
+    prof = _profile(1, 127, 26)
+    out, ref = _both(gpu, osw, prof)
+    _check(out, ref)
+
+
+def test_sw_device_memory(gpu, osw):
+    import torch
+    prof = _profile(64, 127, 27, night_fraction=0.3, precip=True)
+    ref = sw.alloc_outputs(64, 127, hswb=True, flxprf=True)
+    assert osw.run(prof, ref)[0] == 0
+    dev = {k: (torch.as_tensor(np.ascontiguousarray(v)).cuda() if isinstance(v, np.ndarray) else v)
+           for k, v in prof.items()}
+    like = torch.zeros(1, device="cuda")
+    out = sw.alloc_outputs(64, 127, hswb=True, flxprf=True, like=like)
+    kms = [0.0, 0.0, 0.0]
+    gpu.rrtmg_sw_run(dev, out, device_memory=True, kernel_ms=kms)
+    torch.cuda.synchronize()
+    _check({k: v.cpu().numpy() for k, v in out.items()}, ref)
+    assert all(t > 0 for t in kms)
+
+
+def test_sw_gas_optics_stage(gpu, osw):
+    """taug, taur, sfluxzen of the optics kernel against setcoef + taumol."""
+    import ctypes as C
+    import torch
+    prof = _profile(12, 90, 28, night_fraction=0.3)
+    nday, nl = len(prof["idxday"]), 90
+    keep = []
+    dev = {k: torch.as_tensor(np.ascontiguousarray(v)).cuda() for k, v in prof.items() if isinstance(v, np.ndarray)}
+    ad = sw.make_run_args(dict(prof, **dev), sw.alloc_outputs(12, nl, like=dev["plyr"]), keep=keep)
+    tg = torch.zeros(nday, nl, 112, dtype=torch.float64, device="cuda")
+    tr, sf = torch.zeros_like(tg), torch.zeros(nday, 112, dtype=torch.float64, device="cuda")
+    msg = C.create_string_buffer(256)
+    rc = sw.lib().rrtmg_sw_gpu_gas_optics(C.byref(ad), tg.data_ptr(), tr.data_ptr(), sf.data_ptr(), None, msg, 256)
+    assert rc == 0, msg.value
+    for p in range(nday):
+        g0, r0, s0, _ = osw.gas_optics(prof, p + 1)
+        assert _rel(tg[p].cpu().numpy(), g0, 1e-300) <= 1e-13
+        assert _rel(tr[p].cpu().numpy(), r0, 1e-300) <= 1e-13
+        assert np.array_equal(sf[p].cpu().numpy(), s0)
+
+
+def test_sw_refusals_and_noops(gpu):
+    prof = _profile(4, 20, 29)
+    for flags, word in ((dict(isubcsw=0), "spcvrtc"), (dict(iovr=3), "iovr=3")):
+        with pytest.raises(sw.RrtmgSwError, match=word):
+            gpu.rrtmg_sw_run(prof, sw.alloc_outputs(4, 20), flags=flags)
+    out = sw.alloc_outputs(4, 20)
+    out["hswc"][:] = 7.0
+    gpu.rrtmg_sw_run(prof, out, flags=dict(lsswr=0))     # radsw_main.F90:785: no-op
+    assert (out["hswc"] == 7.0).all()
+    p2 = dict(prof, idxday=np.array([1, 9], np.int32))
+    with pytest.raises(sw.RrtmgSwError, match="idxday"):
+        gpu.rrtmg_sw_run(p2, sw.alloc_outputs(4, 20))
