@@ -327,6 +327,68 @@ def caller_steps_leg(args, torch, timed, sh, peak_gbs):
     return res
 
 
+def sw_leg(args, torch, timed, sh):
+    """rrtmg_sw_run (radsw_main.F90:493) at 16,384 columns x 127 layers, every
+    column daylit, McICA with maximum-random overlap, PIFM two-stream, the
+    C2 cloud fields plus aerosols and rain/snow: device-resident inputs timed
+    with CUDA events, the host-array call timed end to end, the per-kernel
+    split from one call, and the oracle on all host threads as the CPU
+    baseline; the GPU fluxes are checked against the oracle's."""
+    import ctypes as C
+    import numpy as np
+    from ccpp_physics_b200 import rrtmg_sw as swm, synthetic
+    from oracle import oracle_sw
+    n, nlay = args.sw_ncols, 127
+    swm.rswinit(device=torch.cuda.current_device())
+    prof = swm.add_sw_inputs(synthetic.make_profiles(n, nlay, seed=1), seed=1, precip=True)
+    dev = {k: (torch.as_tensor(np.ascontiguousarray(v)).cuda() if isinstance(v, np.ndarray) else v)
+           for k, v in prof.items()}
+    like = dev["plyr"]
+    out = swm.alloc_outputs(n, nlay, like=like)
+    keep = []
+    a = swm.make_run_args(dev, out, keep=keep)
+    x = swm.SwExec(precision=0, memory=1, stream=sh, sync=0)
+    buf = C.create_string_buffer(256)
+
+    def step():
+        if swm.lib().rrtmg_sw_gpu_run_ex(C.byref(a), C.byref(x), buf, 256):
+            raise RuntimeError(buf.value.decode())
+    k = max(3, min(args.steps, 10))
+    for _ in range(args.warmup):
+        step()
+    ms = timed(step, k)
+    km = (C.c_float * 3)()
+    xk = swm.SwExec(precision=0, memory=1, stream=sh, sync=1, kernel_ms=C.cast(km, C.POINTER(C.c_float)))
+    if swm.lib().rrtmg_sw_gpu_run_ex(C.byref(a), C.byref(xk), buf, 256):
+        raise RuntimeError(buf.value.decode())
+    torch.cuda.synchronize()
+    got = {kk: v.cpu().numpy() for kk, v in out.items()}
+    # host arrays through the public call (copies in and out inside the timing)
+    hout = swm.alloc_outputs(n, nlay)
+    swm.rrtmg_sw_run(prof, hout)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        swm.rrtmg_sw_run(prof, hout)
+    e2e_s = (time.perf_counter() - t0) / 3
+    # CPU baseline + parity: the oracle on every column, all host threads
+    oracle_sw.rswinit()
+    ref = swm.alloc_outputs(n, nlay)
+    t0 = time.perf_counter()
+    rc, msg = oracle_sw.run(prof, ref)
+    cpu_s = time.perf_counter() - t0
+    assert rc == 0, msg
+    rel = lambda u, v, f: float(np.max(np.abs(u - v) / np.maximum(np.abs(v), f)))
+    return {"workload": f"sw_c2_allsky_mcica_{n}x127", "steps": k, "value": n * k / (ms / 1e3),
+            "unit": "columns/s", "ms_per_step": ms / k,
+            "kernel_ms": {"optics": km[1], "mcica": km[0], "transfer": km[2]},
+            "e2e_columns_per_s": n / e2e_s,
+            "flux_max_rel_vs_oracle": max(rel(got[kk], ref[kk], 1e-300) for kk in ("topflx", "sfcflx", "fdncmp")),
+            "hr_max_rel_vs_oracle": max(rel(got[kk], ref[kk], 1.0) for kk in ("hswc", "hsw0")),
+            "cpu_oracle_columns_per_s": n / cpu_s, "cpu_cores": os.cpu_count(),
+            "cpu_sample": f"all {n} columns, OpenMP over columns",
+            "flags": "iovr=1 isubcsw=2 iswcliq=1 iswcice=3 iswmode=2, aerosols, rain+snow, all columns daylit"}
+
+
 def training_leg(args, torch, sg):
     """Learned gas optics training throughput on 20M layer samples labelled by
     plain FP64 taumol: a fresh network, 2 epochs of the library's tcgen05
@@ -372,6 +434,9 @@ def main():
     ap.add_argument("--no-callers", action="store_true",
                     help="skip the leg of the steps either side of rrtmg_lw_run (seeds, overlap, post)")
     ap.add_argument("--no-train", action="store_true", help="skip the surrogate training-throughput leg")
+    ap.add_argument("--no-sw", action="store_true", help="skip the shortwave (rrtmg_sw_run) leg")
+    ap.add_argument("--sw-only", action="store_true", help="run the shortwave leg alone (profiling runs)")
+    ap.add_argument("--sw-ncols", type=int, default=16384, help="columns of the shortwave leg")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "surrogate"],
                     help="with --quick: the path to loop over (profiling runs)")
     args = ap.parse_args()
@@ -442,6 +507,11 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         return ms
+
+    if args.sw_only:
+        if rank == 0:
+            print(json.dumps({"rrtmg_sw": sw_leg(args, torch, timed, sh)}), flush=True)
+        return
 
     if args.quick and args.precision != "fp64":
         # profiling runs of another path: the same loop, no other legs
@@ -548,6 +618,9 @@ def main():
     # ---- the steps either side of rrtmg_lw_run (seeds, overlap parameters, post) ----
     if not args.no_callers and world == 1 and not args.quick:
         paths["caller_steps"] = caller_steps_leg(args, torch, timed, sh, _peaks()[0])
+    # ---- the shortwave scheme (rrtmg_sw_run) at 16,384 x 127 ----
+    if not args.no_sw and world == 1 and not args.quick:
+        paths["rrtmg_sw"] = sw_leg(args, torch, timed, sh)
 
     # ---- end to end through the C ABI with pinned host buffers ----
     hprof = dict(npts=ncols, nlay=nlay, flags=dict(prof["flags"]))

@@ -13,11 +13,12 @@
 //   sw_rt_kernel      one warp per column, lanes over g-points: spcvrtm
 //                     (RSM:3228-3942) with vrtqdr (RSM:3959-4051) and the
 //                     flux / heating-rate outputs (RSM:1180-1376).
-// The transfer keeps only the upward adding recurrence (zrupb, zrupd) per
-// lane; the downward sweep recomputes each layer's two-stream optics (the
-// same arithmetic, so the same bits) and produces the fluxes level by level,
-// instead of holding six per-level arrays per g-point.  Fluxes are summed
-// over g-points with warp butterflies in a fixed order.
+// Per lane (g-point) the clear pass evaluates each layer's two-stream optics
+// once and keeps them in local memory with the upward adding recurrence
+// (zrupb, zrupd); the downward sweep reads them back and produces the fluxes
+// level by level.  The cloudy pass re-evaluates only the layers whose McICA
+// flag is set.  Fluxes are summed over g-points with warp butterflies in a
+// fixed order.
 //
 // Built with -fmad=false: every statement keeps the reference's evaluation
 // order and rounding.
@@ -652,6 +653,8 @@ struct ColIn {
   int iswmode;
 };
 
+__device__ __forceinline__ bool cloud_bit(const ColIn& c, int k) { return (c.bits[k >> 5] >> (k & 31)) & 1u; }
+
 // layer k of g-point g (band b) in the clear (cloudy = false) or cloudy pass
 __device__ __forceinline__ void layer_opt(const ColIn& c, int g, int b, int k, bool cloudy_pass,
                                           const double* __restrict__ ET, LayOpt& o) {
@@ -714,6 +717,7 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
   double sfc[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
 
   double zrupb[kSwMaxLay + 1], zrupd[kSwMaxLay + 1];
+  double lrb[kSwMaxLay], lrd[kSwMaxLay], ltb[kSwMaxLay], ltd[kSwMaxLay], le3[kSwMaxLay], le4[kSwMaxLay];
   for (int r0 = 0; r0 < kSwNg; r0 += 32) {
     const int g = r0 + lane;
     const bool valid = g < kSwNg;
@@ -729,13 +733,23 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
       if (pass == 1 && !cloudy) break;
       const bool cp = pass == 1;
       const bool total = cp || !cloudy;   // these fluxes are the total-sky ones
-      // upward adding (vrtqdr, RSM:3990-3999)
+      // upward adding (vrtqdr, RSM:3990-3999).  The clear pass stores each
+      // layer's optics; the cloudy pass recomputes only the layers its
+      // sub-column flags cloudy and takes the stored clear values elsewhere,
+      // as spcvrtm keeps the clear-pass arrays for clear layers (RSM:3755-3760).
       double ub = refb1, ud = refd1;
       zrupb[0] = ub;
       zrupd[0] = ud;
       for (int k = 0; k < nlay; ++k) {
         LayOpt o;
-        layer_opt(c, gg, b, k, cp, ET, o);
+        if (!cp) {
+          layer_opt(c, gg, b, k, false, ET, o);
+          lrb[k] = o.rb; lrd[k] = o.rd; ltb[k] = o.tb; ltd[k] = o.td; le3[k] = o.e3; le4[k] = o.e4;
+        } else if (cloud_bit(c, k)) {
+          layer_opt(c, gg, b, k, true, ET, o);
+        } else {
+          o.rb = lrb[k]; o.rd = lrd[k]; o.tb = ltb[k]; o.td = ltd[k]; o.e3 = le3[k]; o.e4 = le4[k];
+        }
         const double zden1 = 1.0 / (1.0 - ud * o.rd);
         const double nb = o.rb + (o.td * ((o.tb - o.e3) * ud + o.e3 * ub)) * zden1;
         const double nd = o.rd + o.td * o.td * ud * zden1;
@@ -749,7 +763,11 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
       for (int m = nlay; m >= 0; --m) {
         if (m < nlay) {
           LayOpt o;
-          layer_opt(c, gg, b, m, cp, ET, o);
+          if (cp && cloud_bit(c, m)) {
+            layer_opt(c, gg, b, m, true, ET, o);
+          } else {
+            o.rb = lrb[m]; o.rd = lrd[m]; o.tb = ltb[m]; o.td = ltd[m]; o.e3 = le3[m]; o.e4 = le4[m];
+          }
           double tdn_m, rdnd_m;
           if (m == nlay - 1) {
             tdn_m = o.tb;
