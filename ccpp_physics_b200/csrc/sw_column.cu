@@ -14,7 +14,7 @@
 //                     (RSM:3228-3942) with vrtqdr (RSM:3959-4051) and the
 //                     flux / heating-rate outputs (RSM:1180-1376).
 // Per lane (g-point) the clear pass evaluates each layer's two-stream optics
-// once and keeps them in local memory with the upward adding recurrence
+// once and keeps them in global scratch with the upward adding recurrence
 // (zrupb, zrupd); the downward sweep reads them back and produces the fluxes
 // level by level.  The cloudy pass re-evaluates only the layers whose McICA
 // flag is set.  Fluxes are summed over g-points with warp butterflies in a
@@ -418,7 +418,7 @@ __device__ void cloud_layer(const SwArgs& a, size_t x, const double* __restrict_
 // ---- kernel 1: optics ------------------------------------------------------
 constexpr int kOptWarps = 4;
 
-__global__ void __launch_bounds__(32 * kOptWarps)
+__global__ void __launch_bounds__(32 * kOptWarps, 3)   // 168 registers: twelve warps per SM hide the table gathers better than eight
 sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ T) {
   __shared__ int s_jp[kOptWarps][kSwMaxLay];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -655,20 +655,36 @@ struct ColIn {
 
 __device__ __forceinline__ bool cloud_bit(const ColIn& c, int k) { return (c.bits[k >> 5] >> (k & 31)) & 1u; }
 
-// layer k of g-point g (band b) in the clear (cloudy = false) or cloudy pass
-__device__ __forceinline__ void layer_opt(const ColIn& c, int g, int b, int k, bool cloudy_pass,
-                                          const double* __restrict__ ET, LayOpt& o) {
+// the inputs of layer k of g-point g (band b): gas, Rayleigh and aerosol
+// optics, plus the cloud optics when the cloudy pass flags the layer
+struct LayIn {
+  double tr, tg, tae, sae, gae, tcw, scw, gcw;
+  bool cld;
+};
+__device__ __forceinline__ void layer_in(const ColIn& c, int g, int b, int k, bool cloudy_pass, LayIn& v) {
   const int r = c.top_at_1 ? c.nlay - 1 - k : k;
   const size_t xa = c.i + (size_t)c.ld * ((size_t)r + (size_t)c.nlay * b);
-  const double tr = c.taur[(size_t)k * kSwNg + g], tg = c.taug[(size_t)k * kSwNg + g];
-  const double tae = __ldg(c.aod + xa), sae = __ldg(c.ssa + xa), gae = __ldg(c.asy + xa);
-  double ztau0 = fmax(kFtiny, tr + tg + tae);
-  double zssa0 = tr + tae * sae;
-  double zasy0 = gae * sae * tae;
-  if (cloudy_pass && ((c.bits[k >> 5] >> (k & 31)) & 1u)) {
-    ztau0 = ztau0 + c.tcw[(size_t)k * 14 + b];
-    zssa0 = zssa0 + c.scw[(size_t)k * 14 + b];
-    zasy0 = zasy0 + c.gcw[(size_t)k * 14 + b];
+  v.tr = c.taur[(size_t)k * kSwNg + g];
+  v.tg = c.taug[(size_t)k * kSwNg + g];
+  v.tae = __ldg(c.aod + xa);
+  v.sae = __ldg(c.ssa + xa);
+  v.gae = __ldg(c.asy + xa);
+  v.cld = cloudy_pass && cloud_bit(c, k);
+  if (v.cld) {
+    v.tcw = c.tcw[(size_t)k * 14 + b];
+    v.scw = c.scw[(size_t)k * 14 + b];
+    v.gcw = c.gcw[(size_t)k * 14 + b];
+  }
+}
+// the layer's two-stream optics (RSM:3330-3336 clear, 3495-3501 cloudy)
+__device__ __forceinline__ void layer_opt(const ColIn& c, const LayIn& v, const double* __restrict__ ET, LayOpt& o) {
+  double ztau0 = fmax(kFtiny, v.tr + v.tg + v.tae);
+  double zssa0 = v.tr + v.tae * v.sae;
+  double zasy0 = v.gae * v.sae * v.tae;
+  if (v.cld) {
+    ztau0 = ztau0 + v.tcw;
+    zssa0 = zssa0 + v.scw;
+    zasy0 = zasy0 + v.gcw;
   }
   two_stream(ztau0, zssa0, zasy0, c.cosz, c.sntz, c.iswmode, ET, o);
 }
@@ -681,7 +697,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 constexpr int kRtWarps = 4;
 
-__global__ void __launch_bounds__(32 * kRtWarps)
+__global__ void __launch_bounds__(32 * kRtWarps, 4)   // 128 registers: sixteen warps per SM
 sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ ET) {
   extern __shared__ double sm[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -716,8 +732,12 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
   // surface partition and UV-B sums of lane 0: [pass][bm1, bm2, df1, df2, uvb]
   double sfc[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
 
-  double zrupb[kSwMaxLay + 1], zrupd[kSwMaxLay + 1];
-  double lrb[kSwMaxLay], lrd[kSwMaxLay], ltb[kSwMaxLay], ltd[kSwMaxLay], le3[kSwMaxLay], le4[kSwMaxLay];
+  // per-lane storage in global scratch, [layer][value][lane] per column: a
+  // warp touches 256 contiguous bytes per value, and the L2-only (.cg)
+  // accesses keep L1 for exp_tbl and the streamed optical depths
+  double* lst = s.lane_store + (size_t)pl * (size_t)(nlay + 1) * 8 * 32 + lane;
+  auto st8 = [&](int k, int q, double v) { __stcg(lst + ((size_t)k * 8 + q) * 32, v); };
+  auto ld8 = [&](int k, int q) { return __ldcg(lst + ((size_t)k * 8 + q) * 32); };
   for (int r0 = 0; r0 < kSwNg; r0 += 32) {
     const int g = r0 + lane;
     const bool valid = g < kSwNg;
@@ -738,36 +758,47 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
       // sub-column flags cloudy and takes the stored clear values elsewhere,
       // as spcvrtm keeps the clear-pass arrays for clear layers (RSM:3755-3760).
       double ub = refb1, ud = refd1;
-      zrupb[0] = ub;
-      zrupd[0] = ud;
+      st8(0, 6, ub);
+      st8(0, 7, ud);
+      LayIn vin;
+      layer_in(c, gg, b, 0, cp, vin);
       for (int k = 0; k < nlay; ++k) {
+        const LayIn cur = vin;
+        if (k + 1 < nlay) layer_in(c, gg, b, k + 1, cp, vin);   // issued ahead of this layer's arithmetic
         LayOpt o;
         if (!cp) {
-          layer_opt(c, gg, b, k, false, ET, o);
-          lrb[k] = o.rb; lrd[k] = o.rd; ltb[k] = o.tb; ltd[k] = o.td; le3[k] = o.e3; le4[k] = o.e4;
-        } else if (cloud_bit(c, k)) {
-          layer_opt(c, gg, b, k, true, ET, o);
+          layer_opt(c, cur, ET, o);
+          st8(k, 0, o.rb); st8(k, 1, o.rd); st8(k, 2, o.tb); st8(k, 3, o.td); st8(k, 4, o.e3); st8(k, 5, o.e4);
+        } else if (cur.cld) {
+          layer_opt(c, cur, ET, o);
         } else {
-          o.rb = lrb[k]; o.rd = lrd[k]; o.tb = ltb[k]; o.td = ltd[k]; o.e3 = le3[k]; o.e4 = le4[k];
+          o.rb = ld8(k, 0); o.rd = ld8(k, 1); o.tb = ld8(k, 2); o.td = ld8(k, 3); o.e3 = ld8(k, 4); o.e4 = ld8(k, 5);
         }
         const double zden1 = 1.0 / (1.0 - ud * o.rd);
         const double nb = o.rb + (o.td * ((o.tb - o.e3) * ud + o.e3 * ub)) * zden1;
         const double nd = o.rd + o.td * o.td * ud * zden1;
         ub = nb;
         ud = nd;
-        zrupb[k + 1] = ub;
-        zrupd[k + 1] = ud;
+        st8(k + 1, 6, ub);
+        st8(k + 1, 7, ud);
       }
       // downward sweep (RSM:4001-4017) with the fluxes of each level (RSM:4019-4026)
       double tdbt = 1.0, tdn = 1.0, rdnd = 0.0, tdbt0 = 1.0, fd0 = 0.0;
+      auto fetch = [&](int m, LayOpt& o) {
+        LayIn v;
+        if (cp && cloud_bit(c, m)) {
+          layer_in(c, gg, b, m, true, v);
+          layer_opt(c, v, ET, o);
+        } else {
+          o.rb = ld8(m, 0); o.rd = ld8(m, 1); o.tb = ld8(m, 2); o.td = ld8(m, 3); o.e3 = ld8(m, 4); o.e4 = ld8(m, 5);
+        }
+      };
+      LayOpt nx;
+      fetch(nlay - 1, nx);
       for (int m = nlay; m >= 0; --m) {
         if (m < nlay) {
-          LayOpt o;
-          if (cp && cloud_bit(c, m)) {
-            layer_opt(c, gg, b, m, true, ET, o);
-          } else {
-            o.rb = lrb[m]; o.rd = lrd[m]; o.tb = ltb[m]; o.td = ltd[m]; o.e3 = le3[m]; o.e4 = le4[m];
-          }
+          const LayOpt o = nx;
+          if (m > 0) fetch(m - 1, nx);   // the next layer's loads overlap this layer's recurrence
           double tdn_m, rdnd_m;
           if (m == nlay - 1) {
             tdn_m = o.tb;
@@ -782,9 +813,10 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
           tdn = tdn_m;
           rdnd = rdnd_m;
         }
-        const double zden1 = 1.0 / (1.0 - rdnd * zrupd[m]);
-        const double fu = (tdbt * zrupb[m] + (tdn - tdbt) * zrupd[m]) * zden1;
-        const double fd = tdbt + (tdn - tdbt + tdbt * zrupb[m] * rdnd) * zden1;
+        const double rub = ld8(m, 6), rud = ld8(m, 7);
+        const double zden1 = 1.0 / (1.0 - rdnd * rud);
+        const double fu = (tdbt * rub + (tdn - tdbt) * rud) * zden1;
+        const double fd = tdbt + (tdn - tdbt + tdbt * rub * rdnd) * zden1;
         if (m == 0) fd0 = fd;
         const double su = warp_sum(wgt * fu), sd = warp_sum(wgt * fd);
         if (lane == 0) {
