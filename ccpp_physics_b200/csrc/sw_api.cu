@@ -30,7 +30,7 @@ namespace {
 
 constexpr int kNtbmx = 10000;
 constexpr double kS0 = 1368.22;                  // RSM:332
-constexpr size_t kScratchBudget = (size_t)4 << 30;
+constexpr size_t kScratchBudget = (size_t)12 << 30;   // 16,384 columns of 127 layers in one chunk
 
 struct SwState {
   bool ready = false;
@@ -105,7 +105,7 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 // per-column scratch bytes of the three kernels
 size_t scratch_per_col(int nlay) {
   const int nw = (nlay + 31) / 32;
-  return (size_t)(2 * nlay * sw::kSwNg + sw::kSwNg + 3 * nlay * 14 + nlay + 1 + (nlay + 1) * 8 * 32) * 8 + 4 +
+  return (size_t)(2 * nlay * sw::kSwNg + sw::kSwNg + 3 * nlay * 14 + nlay + 1 + (nlay + 1) * 10 * 32) * 8 + 4 +
          (size_t)sw::kSwNg * nw * 4 + 64;
 }
 
@@ -125,13 +125,13 @@ sw::SwScratch carve(char* base, int nc, int nlay) {
   s.zcf1 = (double*)take((size_t)nc * 8);
   s.seed = (int32_t*)take((size_t)nc * 4);
   s.bits = (uint32_t*)take((size_t)nc * sw::kSwNg * nw * 4);
-  s.lane_store = (double*)take((size_t)nc * (nlay + 1) * 8 * 32 * 8);
+  s.lane_store = (double*)take((size_t)nc * (nlay + 1) * 10 * 32 * 8);
   s.nw = nw;
   return s;
 }
 size_t carve_bytes(int nc, int nlay) {
   const int nw = (nlay + 31) / 32;
-  const size_t parts[11] = {(size_t)nc * (nlay + 1) * 8 * 32 * 8, (size_t)nc * nlay * sw::kSwNg * 8, (size_t)nc * nlay * sw::kSwNg * 8,
+  const size_t parts[11] = {(size_t)nc * (nlay + 1) * 10 * 32 * 8, (size_t)nc * nlay * sw::kSwNg * 8, (size_t)nc * nlay * sw::kSwNg * 8,
                             (size_t)nc * sw::kSwNg * 8,        (size_t)nc * nlay * 14 * 8,
                             (size_t)nc * nlay * 14 * 8,        (size_t)nc * nlay * 14 * 8,
                             (size_t)nc * nlay * 8,             (size_t)nc * 8,

@@ -13,12 +13,13 @@
 //   sw_rt_kernel      one warp per column, lanes over g-points: spcvrtm
 //                     (RSM:3228-3942) with vrtqdr (RSM:3959-4051) and the
 //                     flux / heating-rate outputs (RSM:1180-1376).
-// Per lane (g-point) the clear pass evaluates each layer's two-stream optics
-// once and keeps them in global scratch with the upward adding recurrence
-// (zrupb, zrupd); the downward sweep reads them back and produces the fluxes
-// level by level.  The cloudy pass re-evaluates only the layers whose McICA
-// flag is set.  Fluxes are summed over g-points with warp butterflies in a
-// fixed order.
+// Per lane (g-point) the clear-sky and all-sky sweeps run side by side: the
+// upward sweep evaluates each layer's clear two-stream optics once (the
+// all-sky sweep re-evaluates only the layers whose McICA flag is set) and
+// keeps them, with both adding recurrences (zrupb, zrupd), in global
+// scratch; the downward sweep reads them back and produces both sweeps'
+// fluxes level by level.  Fluxes are summed over g-points with warp
+// butterflies in a fixed order.
 //
 // Built with -fmad=false: every statement keeps the reference's evaluation
 // order and rounding.
@@ -696,6 +697,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 constexpr int kRtWarps = 4;
+constexpr int kLaneVals = 10;   // per-lane stored values per level
 
 __global__ void __launch_bounds__(32 * kRtWarps, 4)   // 128 registers: sixteen warps per SM
 sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ ET) {
@@ -732,12 +734,14 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
   // surface partition and UV-B sums of lane 0: [pass][bm1, bm2, df1, df2, uvb]
   double sfc[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
 
-  // per-lane storage in global scratch, [layer][value][lane] per column: a
-  // warp touches 256 contiguous bytes per value, and the L2-only (.cg)
-  // accesses keep L1 for exp_tbl and the streamed optical depths
-  double* lst = s.lane_store + (size_t)pl * (size_t)(nlay + 1) * 8 * 32 + lane;
-  auto st8 = [&](int k, int q, double v) { __stcg(lst + ((size_t)k * 8 + q) * 32, v); };
-  auto ld8 = [&](int k, int q) { return __ldcg(lst + ((size_t)k * 8 + q) * 32); };
+  // per-lane storage in global scratch, [level][value][lane] per column
+  // (values: 6 clear-sky layer optics, clear zrupb/zrupd, cloudy
+  // zrupb/zrupd): a warp touches 256 contiguous bytes per value, and the
+  // L2-only (.cg) accesses keep L1 for exp_tbl and the streamed optical depths
+  double* lst = s.lane_store + (size_t)pl * (size_t)(nlay + 1) * kLaneVals * 32 + lane;
+  auto st8 = [&](int k, int q, double v) { __stcg(lst + ((size_t)k * kLaneVals + q) * 32, v); };
+  auto ld8 = [&](int k, int q) { return __ldcg(lst + ((size_t)k * kLaneVals + q) * 32); };
+
   for (int r0 = 0; r0 < kSwNg; r0 += 32) {
     const int g = r0 + lane;
     const bool valid = g < kSwNg;
@@ -749,31 +753,30 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
     c.bits = s.bits + ((size_t)pl * kSwNg + gg) * s.nw;
     const double refb1 = ibd ? albbm[ibd - 1] : 0.5 * (albbm[0] + albbm[1]);
     const double refd1 = ibd ? albdf[ibd - 1] : 0.5 * (albdf[0] + albdf[1]);
-    for (int pass = 0; pass < 2; ++pass) {
-      if (pass == 1 && !cloudy) break;
-      const bool cp = pass == 1;
-      const bool total = cp || !cloudy;   // these fluxes are the total-sky ones
-      // upward adding (vrtqdr, RSM:3990-3999).  The clear pass stores each
-      // layer's optics; the cloudy pass recomputes only the layers its
-      // sub-column flags cloudy and takes the stored clear values elsewhere,
-      // as spcvrtm keeps the clear-pass arrays for clear layers (RSM:3755-3760).
-      double ub = refb1, ud = refd1;
-      st8(0, 6, ub);
-      st8(0, 7, ud);
-      LayIn vin;
-      layer_in(c, gg, b, 0, cp, vin);
-      for (int k = 0; k < nlay; ++k) {
-        const LayIn cur = vin;
-        if (k + 1 < nlay) layer_in(c, gg, b, k + 1, cp, vin);   // issued ahead of this layer's arithmetic
-        LayOpt o;
-        if (!cp) {
-          layer_opt(c, cur, ET, o);
-          st8(k, 0, o.rb); st8(k, 1, o.rd); st8(k, 2, o.tb); st8(k, 3, o.td); st8(k, 4, o.e3); st8(k, 5, o.e4);
-        } else if (cur.cld) {
-          layer_opt(c, cur, ET, o);
-        } else {
-          o.rb = ld8(k, 0); o.rd = ld8(k, 1); o.tb = ld8(k, 2); o.td = ld8(k, 3); o.e3 = ld8(k, 4); o.e4 = ld8(k, 5);
-        }
+    // The clear-sky sweep and, in a cloudy column, the all-sky sweep of
+    // spcvrtm (RSM:3318-3668, 3680-3920) run side by side: a layer's clear
+    // optics are evaluated once and serve both, and the all-sky sweep
+    // re-evaluates only the layers its sub-column flags cloudy, as spcvrtm
+    // keeps the clear-pass arrays for clear layers (RSM:3755-3760).
+    // upward adding (vrtqdr, RSM:3990-3999)
+    double ub = refb1, ud = refd1, ubw = refb1, udw = refd1;
+    st8(0, 6, ub);
+    st8(0, 7, ud);
+    if (cloudy) {
+      st8(0, 8, ubw);
+      st8(0, 9, udw);
+    }
+    LayIn vin;
+    layer_in(c, gg, b, 0, cloudy, vin);
+    for (int k = 0; k < nlay; ++k) {
+      const LayIn cur = vin;
+      if (k + 1 < nlay) layer_in(c, gg, b, k + 1, cloudy, vin);   // issued ahead of this layer's arithmetic
+      LayIn clr = cur;
+      clr.cld = false;
+      LayOpt o;
+      layer_opt(c, clr, ET, o);
+      st8(k, 0, o.rb); st8(k, 1, o.rd); st8(k, 2, o.tb); st8(k, 3, o.td); st8(k, 4, o.e3); st8(k, 5, o.e4);
+      {
         const double zden1 = 1.0 / (1.0 - ud * o.rd);
         const double nb = o.rb + (o.td * ((o.tb - o.e3) * ud + o.e3 * ub)) * zden1;
         const double nd = o.rd + o.td * o.td * ud * zden1;
@@ -782,64 +785,99 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
         st8(k + 1, 6, ub);
         st8(k + 1, 7, ud);
       }
-      // downward sweep (RSM:4001-4017) with the fluxes of each level (RSM:4019-4026)
-      double tdbt = 1.0, tdn = 1.0, rdnd = 0.0, tdbt0 = 1.0, fd0 = 0.0;
-      auto fetch = [&](int m, LayOpt& o) {
+      if (cloudy) {
+        LayOpt w = o;
+        if (cur.cld) layer_opt(c, cur, ET, w);
+        const double zden1 = 1.0 / (1.0 - udw * w.rd);
+        const double nb = w.rb + (w.td * ((w.tb - w.e3) * udw + w.e3 * ubw)) * zden1;
+        const double nd = w.rd + w.td * w.td * udw * zden1;
+        ubw = nb;
+        udw = nd;
+        st8(k + 1, 8, ubw);
+        st8(k + 1, 9, udw);
+      }
+    }
+    // downward sweep (RSM:4001-4017) with the fluxes of each level (RSM:4019-4026)
+    auto fetch = [&](int m, LayOpt& o, LayOpt& w) {
+      o.rb = ld8(m, 0); o.rd = ld8(m, 1); o.tb = ld8(m, 2); o.td = ld8(m, 3); o.e3 = ld8(m, 4); o.e4 = ld8(m, 5);
+      w = o;
+      if (cloudy && cloud_bit(c, m)) {
         LayIn v;
-        if (cp && cloud_bit(c, m)) {
-          layer_in(c, gg, b, m, true, v);
-          layer_opt(c, v, ET, o);
-        } else {
-          o.rb = ld8(m, 0); o.rd = ld8(m, 1); o.tb = ld8(m, 2); o.td = ld8(m, 3); o.e3 = ld8(m, 4); o.e4 = ld8(m, 5);
-        }
-      };
-      LayOpt nx;
-      fetch(nlay - 1, nx);
-      for (int m = nlay; m >= 0; --m) {
-        if (m < nlay) {
-          const LayOpt o = nx;
-          if (m > 0) fetch(m - 1, nx);   // the next layer's loads overlap this layer's recurrence
-          double tdn_m, rdnd_m;
-          if (m == nlay - 1) {
-            tdn_m = o.tb;
-            rdnd_m = o.rd;
-          } else {
-            const double zden1 = 1.0 / (1.0 - o.rd * rdnd);
-            tdn_m = tdbt * o.tb + (o.td * ((tdn - tdbt) + tdbt * o.rb * rdnd)) * zden1;
-            rdnd_m = o.rd + o.td * o.td * rdnd * zden1;
-          }
-          tdbt = o.e3 * tdbt;
-          tdbt0 = o.e4 * tdbt0;
-          tdn = tdn_m;
-          rdnd = rdnd_m;
-        }
-        const double rub = ld8(m, 6), rud = ld8(m, 7);
-        const double zden1 = 1.0 / (1.0 - rdnd * rud);
-        const double fu = (tdbt * rub + (tdn - tdbt) * rud) * zden1;
-        const double fd = tdbt + (tdn - tdbt + tdbt * rub * rdnd) * zden1;
-        if (m == 0) fd0 = fd;
-        const double su = warp_sum(wgt * fu), sd = warp_sum(wgt * fd);
+        layer_in(c, gg, b, m, true, v);
+        layer_opt(c, v, ET, w);
+      }
+    };
+    // one downward step of a sweep: layer optics o, state (tdbt, tdn, rdnd, tdbt0)
+    auto down = [&](int m, const LayOpt& o, double& tdbt, double& tdn, double& rdnd, double& tdbt0) {
+      double tdn_m, rdnd_m;
+      if (m == nlay - 1) {
+        tdn_m = o.tb;
+        rdnd_m = o.rd;
+      } else {
+        const double zden1 = 1.0 / (1.0 - o.rd * rdnd);
+        tdn_m = tdbt * o.tb + (o.td * ((tdn - tdbt) + tdbt * o.rb * rdnd)) * zden1;
+        rdnd_m = o.rd + o.td * o.td * rdnd * zden1;
+      }
+      tdbt = o.e3 * tdbt;
+      tdbt0 = o.e4 * tdbt0;
+      tdn = tdn_m;
+      rdnd = rdnd_m;
+    };
+    auto flux = [&](double tdbt, double tdn, double rdnd, double rub, double rud, double& fu, double& fd) {
+      const double zden1 = 1.0 / (1.0 - rdnd * rud);
+      fu = (tdbt * rub + (tdn - tdbt) * rud) * zden1;
+      fd = tdbt + (tdn - tdbt + tdbt * rub * rdnd) * zden1;
+    };
+    double tdbt = 1.0, tdn = 1.0, rdnd = 0.0, tdbt0 = 1.0, fd0 = 0.0;
+    double tdbtw = 1.0, tdnw = 1.0, rdndw = 0.0, tdbt0w = 1.0, fd0w = 0.0;
+    LayOpt nx, nxw;
+    fetch(nlay - 1, nx, nxw);
+    for (int m = nlay; m >= 0; --m) {
+      if (m < nlay) {
+        const LayOpt o = nx, w = nxw;
+        if (m > 0) fetch(m - 1, nx, nxw);   // the next layer's loads overlap this layer's recurrences
+        down(m, o, tdbt, tdn, rdnd, tdbt0);
+        if (cloudy) down(m, w, tdbtw, tdnw, rdndw, tdbt0w);
+      }
+      double fu, fd, fuw = 0.0, fdw = 0.0;
+      flux(tdbt, tdn, rdnd, ld8(m, 6), ld8(m, 7), fu, fd);
+      if (cloudy) flux(tdbtw, tdnw, rdndw, ld8(m, 8), ld8(m, 9), fuw, fdw);
+      if (m == 0) {
+        fd0 = fd;
+        fd0w = fdw;
+      }
+      const double su = warp_sum(wgt * fu), sd = warp_sum(wgt * fd);
+      if (lane == 0) {
+        up0[m] += su;
+        dn0[m] += sd;
+      }
+      if (cloudy) {
+        const double suw = warp_sum(wgt * fuw), sdw = warp_sum(wgt * fdw);
         if (lane == 0) {
-          (cp ? upc : up0)[m] += su;
-          (cp ? dnc : dn0)[m] += sd;
+          upc[m] += suw;
+          dnc[m] += sdw;
         }
-        if (want_b && total) {
-          for (int bb = blo; bb <= bhi; ++bb) {
-            const double mu = warp_sum(b == bb ? wgt * fu : 0.0), md = warp_sum(b == bb ? wgt * fd : 0.0);
-            if (lane == 0) {
-              accb[(size_t)(2 * bb) * nlp1 + m] += mu;
-              accb[(size_t)(2 * bb + 1) * nlp1 + m] += md;
-            }
+      }
+      if (want_b) {   // total-sky band fluxes
+        const double tu = cloudy ? fuw : fu, td = cloudy ? fdw : fd;
+        for (int bb = blo; bb <= bhi; ++bb) {
+          const double mu = warp_sum(b == bb ? wgt * tu : 0.0), md = warp_sum(b == bb ? wgt * td : 0.0);
+          if (lane == 0) {
+            accb[(size_t)(2 * bb) * nlp1 + m] += mu;
+            accb[(size_t)(2 * bb + 1) * nlp1 + m] += md;
           }
         }
       }
-      // surface direct / diffuse partition (RSM:3625-3640) and UV-B (RSM:3925)
-      const double zb1 = wgt * tdbt0, zb2 = wgt * (fd0 - tdbt0);
+    }
+    // surface direct / diffuse partition (RSM:3625-3640) and UV-B (RSM:3925)
+    for (int pass = 0; pass < (cloudy ? 2 : 1); ++pass) {
+      const double t0 = pass ? tdbt0w : tdbt0, f0 = pass ? fd0w : fd0;
+      const double zb1 = wgt * t0, zb2 = wgt * (f0 - t0);
       const double bm1 = (ibd == 1) ? zb1 : (ibd == 0 ? 0.5 * zb1 : 0.0);
       const double bm2 = (ibd == 2) ? zb1 : (ibd == 0 ? 0.5 * zb1 : 0.0);
       const double df1 = (ibd == 1) ? zb2 : (ibd == 0 ? 0.5 * zb2 : 0.0);
       const double df2 = (ibd == 2) ? zb2 : (ibd == 0 ? 0.5 * zb2 : 0.0);
-      const double uv = (b == 27 - 16) ? wgt * fd0 : 0.0;
+      const double uv = (b == 27 - 16) ? wgt * f0 : 0.0;
       const double v[5] = {warp_sum(bm1), warp_sum(bm2), warp_sum(df1), warp_sum(df2), warp_sum(uv)};
       if (lane == 0)
         for (int q = 0; q < 5; ++q) sfc[pass][q] += v[q];

@@ -32,7 +32,7 @@ struct SwScratch {
   int32_t* seed;                     // [pl]
   double* zcf1;                      // [pl] cloudy-column fraction indicator
   uint32_t* bits;                    // [pl][112][nw] McICA cloudy flags
-  double* lane_store;                // [pl][k][8][32] the transfer's per-lane layer optics and recurrence
+  double* lane_store;                // [pl][k][10][32] the transfer's per-lane layer optics and recurrences
   int nw;
   int* bad;                          // set when idxday names a column outside 1..npts
 };
