@@ -363,6 +363,23 @@ def sw_leg(args, torch, timed, sh):
         raise RuntimeError(buf.value.decode())
     torch.cuda.synchronize()
     got = {kk: v.cpu().numpy() for kk, v in out.items()}
+    # the decorrelation-length overlap of GFS v16 (iovr=3, de_lgth 2 km)
+    out3 = swm.alloc_outputs(n, nlay, like=like)
+    a3 = swm.make_run_args(dev, out3, flags=dict(iovr=3), keep=keep)
+
+    def step3():
+        if swm.lib().rrtmg_sw_gpu_run_ex(C.byref(a3), C.byref(x), buf, 256):
+            raise RuntimeError(buf.value.decode())
+    for _ in range(args.warmup):
+        step3()
+    ms3 = timed(step3, k)
+    km3 = (C.c_float * 3)()
+    xk3 = swm.SwExec(precision=0, memory=1, stream=sh, sync=1, kernel_ms=C.cast(km3, C.POINTER(C.c_float)))
+    if swm.lib().rrtmg_sw_gpu_run_ex(C.byref(a3), C.byref(xk3), buf, 256):
+        raise RuntimeError(buf.value.decode())
+    torch.cuda.synchronize()
+    got3 = {kk: v.cpu().numpy() for kk, v in out3.items()}
+    del out3
     # host arrays through the public call (copies in and out inside the timing)
     hout = swm.alloc_outputs(n, nlay)
     swm.rrtmg_sw_run(prof, hout)
@@ -377,6 +394,9 @@ def sw_leg(args, torch, timed, sh):
     rc, msg = oracle_sw.run(prof, ref)
     cpu_s = time.perf_counter() - t0
     assert rc == 0, msg
+    ref3 = swm.alloc_outputs(n, nlay)
+    rc, msg = oracle_sw.run(prof, ref3, flags=dict(iovr=3))
+    assert rc == 0, msg
     rel = lambda u, v, f: float(np.max(np.abs(u - v) / np.maximum(np.abs(v), f)))
     return {"workload": f"sw_c2_allsky_mcica_{n}x127", "steps": k, "value": n * k / (ms / 1e3),
             "unit": "columns/s", "ms_per_step": ms / k,
@@ -384,6 +404,10 @@ def sw_leg(args, torch, timed, sh):
             "e2e_columns_per_s": n / e2e_s,
             "flux_max_rel_vs_oracle": max(rel(got[kk], ref[kk], 1e-300) for kk in ("topflx", "sfcflx", "fdncmp")),
             "hr_max_rel_vs_oracle": max(rel(got[kk], ref[kk], 1.0) for kk in ("hswc", "hsw0")),
+            "iovr3": {"value": n * k / (ms3 / 1e3), "ms_per_step": ms3 / k,
+                      "kernel_ms": {"optics": km3[1], "mcica": km3[0], "transfer": km3[2]},
+                      "flux_max_rel_vs_oracle": max(rel(got3[kk], ref3[kk], 1e-300) for kk in ("topflx", "sfcflx")),
+                      "overlap": "decorrelation length (iovr=3), de_lgth 2 km"},
             "cpu_oracle_columns_per_s": n / cpu_s, "cpu_cores": os.cpu_count(),
             "cpu_sample": f"all {n} columns, OpenMP over columns",
             "flags": "iovr=1 isubcsw=2 iswcliq=1 iswcice=3 iswmode=2, aerosols, rain+snow, all columns daylit"}

@@ -45,6 +45,10 @@ cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int 
 // bits[(c*112 + ig)*nw + (k >> 5)] bit (k & 31)
 cudaError_t mcica_sw_launch(int ncols, int nlay, int iovr, const McicaStage& stage, uint32_t* bits, int num_sms,
                             cudaStream_t st);
+// the same for iovr 3..5 (two g-major sets); stage.alpha = fac_lcf (iovr 3) or alpha (4, 5) per layer
+cudaError_t mcica_sw_two_set_prepare(int max_smem);
+cudaError_t mcica_sw_two_set_launch(int ncols, int nlay, int iovr, const McicaStage& stage, uint32_t* bits,
+                                    int num_sms, cudaStream_t st);
 // raw state words of one twister stream (lw_mcica.cu): raw[j] is what draw j tempers
 cudaError_t seed_stream_launch(int32_t seed, long long m, uint32_t* raw, cudaStream_t st);
 // icsdsw/icsdlw of n columns from the raw words of a face's stream

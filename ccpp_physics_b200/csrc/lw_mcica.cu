@@ -613,6 +613,128 @@ cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int 
   return cudaGetLastError();
 }
 
+// Shortwave sub-columns with decorrelation-length (iovr 3) or exponential /
+// exponential-random (iovr 4, 5) overlap (radsw_main.F90:2104-2190).  Both
+// random sets are g-major, set 1 = draws [0, 112 nlay) and set 2 = draws
+// [112 nlay, 224 nlay) of one stream, cdfunc(k, n) = draw (n-1) nlay + k.
+// Set 2 is read from a second sequence ring that runs 112 nlay draws ahead
+// of the first; each ring holds one round's draws plus the twist history,
+// as in the iovr 0/1 walk.  Each lane walks its g-point: top-down for iovr
+// 3 (cdfunc(k) = cdfunc(k+1) when cdfun2(k) <= fac_lcf(k+1)), bottom-up for
+// 4, 5 (cdfunc(k) = cdfunc(k-1) when cdfun2(k) < alpha(k)), flagging
+// cdfunc(k) >= 1 - cldf(k).  stage.alpha holds fac_lcf (iovr 3, entry k is
+// the factor between layers k-1 and k) or alpha (iovr 4, 5), per layer in
+// internal order.
+constexpr int kSwTwoSetWarps = 4;
+
+__host__ __device__ inline size_t sw_two_set_warp_bytes(int nlay, int cap) {
+  return 2 * (((size_t)nlay * 8 + 15) & ~(size_t)15) + 2 * (size_t)cap * 4;
+}
+
+__global__ void __launch_bounds__(32 * kSwTwoSetWarps)
+sw_mcica_two_set_kernel(int ncols, McicaArgs a, uint32_t* __restrict__ bits) {
+  extern __shared__ __align__(16) char smem_raw[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int nlay = a.nlay, cap = a.cap, nw = a.nw;
+  const size_t lb = ((size_t)nlay * 8 + 15) & ~(size_t)15;
+  char* my = smem_raw + sw_two_set_warp_bytes(nlay, cap) * wib;
+  double* clr = reinterpret_cast<double*>(my);         // 1 - cldf(k)
+  double* aux = reinterpret_cast<double*>(my + lb);    // fac_lcf or alpha
+  uint32_t* ra = reinterpret_cast<uint32_t*>(my + 2 * lb);
+  uint32_t* rb = ra + cap;
+  const int warps_total = gridDim.x * kSwTwoSetWarps;
+  const long long P0 = (long long)kSwNgpt * nlay;   // set 2 starts here
+  for (int c = blockIdx.x * kSwTwoSetWarps + wib; c < ncols; c += warps_total) {
+    __syncwarp();
+    for (int k = lane; k < nlay; k += 32) {
+      clr[k] = 1.0 - a.st.cldf[c + (size_t)a.st.ld * k];
+      aux[k] = a.st.alpha[c + (size_t)a.st.ld * k];
+    }
+    const int32_t seed = a.st.seed[c];
+    const uint32_t s0 = (uint32_t)(seed == 0 ? 4357 : seed);   // random_setseed_t (MT:285-299)
+    for (int n = lane; n < 624; n += 32) ra[n] = rb[n] = s0 * c_pow69069[n];
+    __syncwarp();
+    long long ga = 624, gb = 624;    // sequence words generated in each ring
+    int ja = 624 % cap, jb = 624 % cap;
+    uint32_t* out = bits + (size_t)c * kSwNgpt * nw;
+    for (int n0 = 0; n0 < kSwNgpt; n0 += kMcicaRound) {
+      const long long need_a = 624 + (long long)(n0 + kMcicaRound) * nlay;
+      while (ga < need_a) {
+        twist_ring(ra, cap, ja, lane);
+        ga += 624;
+        ja += 624;
+        if (ja == cap) ja = 0;
+      }
+      const long long need_b = need_a + P0;
+      while (gb < need_b) {
+        twist_ring(rb, cap, jb, lane);
+        gb += 624;
+        jb += 624;
+        if (jb == cap) jb = 0;
+      }
+      const int n = n0 + lane;
+      if (lane < kMcicaRound) {
+        const int qa = (int)((624 + (long long)n * nlay) % cap);
+        const int qb = (int)((624 + P0 + (long long)n * nlay) % cap);
+        auto at = [&](const uint32_t* r, int q0, int k) {
+          int q = q0 + k;
+          if (q >= cap) q -= cap;
+          return u32_unit(temper(r[q]));
+        };
+        uint32_t word = 0;
+        if (a.iovr == 3) {
+          double cur = at(ra, qa, nlay - 1);
+          for (int k = nlay - 1; k >= 0; --k) {
+            if (k < nlay - 1 && !(at(rb, qb, k) <= aux[k + 1])) cur = at(ra, qa, k);
+            if (cur >= clr[k]) word |= 1u << (k & 31);
+            if ((k & 31) == 0) {
+              out[n * nw + (k >> 5)] = word;
+              word = 0;
+            }
+          }
+        } else {
+          double cur = 0.0;
+          for (int k = 0; k < nlay; ++k) {
+            if (k == 0 || !(at(rb, qb, k) < aux[k])) cur = at(ra, qa, k);
+            if (cur >= clr[k]) word |= 1u << (k & 31);
+            if ((k & 31) == 31 || k == nlay - 1) {
+              out[n * nw + (k >> 5)] = word;
+              word = 0;
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+cudaError_t mcica_sw_two_set_prepare(int max_smem) {
+  return cudaFuncSetAttribute(sw_mcica_two_set_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+}
+
+cudaError_t mcica_sw_two_set_launch(int ncols, int nlay, int iovr, const McicaStage& stage, uint32_t* bits,
+                                    int num_sms, cudaStream_t st) {
+  if (iovr < 3 || iovr > 5) return cudaErrorInvalidValue;
+  McicaArgs a;
+  a.nlay = nlay;
+  a.nw = (nlay + 31) / 32;
+  a.iovr = iovr;
+  a.isubclw = 2;
+  a.top_at_1 = 0;
+  const long round = (long)kMcicaRound * nlay + 623;
+  a.cap = (int)((round + 623) / 624 * 624);
+  a.st = stage;
+  const size_t smem = sw_two_set_warp_bytes(nlay, a.cap) * kSwTwoSetWarps;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sw_mcica_two_set_kernel, 32 * kSwTwoSetWarps, smem);
+  if (per_sm < 1) per_sm = 1;
+  const int grid = min((ncols + kSwTwoSetWarps - 1) / kSwTwoSetWarps, num_sms * per_sm);
+  if (grid < 1) return cudaSuccess;
+  sw_mcica_two_set_kernel<<<grid, 32 * kSwTwoSetWarps, smem, st>>>(ncols, a, bits);
+  return cudaGetLastError();
+}
+
 // Shortwave sub-columns (mcica_subcol, radsw_main.F90:1952-2212) for iovr 0
 // (random), 1 (maximum-random) and 2 (maximum): the draws are g-major,
 // rand2d((n-1)*nlay + k) as in the longwave generator, over 112 g-points.

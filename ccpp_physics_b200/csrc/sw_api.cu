@@ -105,7 +105,7 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 // per-column scratch bytes of the three kernels
 size_t scratch_per_col(int nlay) {
   const int nw = (nlay + 31) / 32;
-  return (size_t)(2 * nlay * sw::kSwNg + sw::kSwNg + 3 * nlay * 14 + nlay + 1 + (nlay + 1) * 10 * 32) * 8 + 4 +
+  return (size_t)(2 * nlay * sw::kSwNg + sw::kSwNg + 3 * nlay * 14 + 2 * nlay + 1 + (nlay + 1) * 10 * 32) * 8 + 4 +
          (size_t)sw::kSwNg * nw * 4 + 64;
 }
 
@@ -122,6 +122,7 @@ sw::SwScratch carve(char* base, int nc, int nlay) {
   s.ssacw = (double*)take((size_t)nc * nlay * 14 * 8);
   s.asycw = (double*)take((size_t)nc * nlay * 14 * 8);
   s.cldf = (double*)take((size_t)nc * nlay * 8);
+  s.aux = (double*)take((size_t)nc * nlay * 8);
   s.zcf1 = (double*)take((size_t)nc * 8);
   s.seed = (int32_t*)take((size_t)nc * 4);
   s.bits = (uint32_t*)take((size_t)nc * sw::kSwNg * nw * 4);
@@ -131,7 +132,7 @@ sw::SwScratch carve(char* base, int nc, int nlay) {
 }
 size_t carve_bytes(int nc, int nlay) {
   const int nw = (nlay + 31) / 32;
-  const size_t parts[11] = {(size_t)nc * (nlay + 1) * 10 * 32 * 8, (size_t)nc * nlay * sw::kSwNg * 8, (size_t)nc * nlay * sw::kSwNg * 8,
+  const size_t parts[12] = {(size_t)nc * nlay * 8, (size_t)nc * (nlay + 1) * 10 * 32 * 8, (size_t)nc * nlay * sw::kSwNg * 8, (size_t)nc * nlay * sw::kSwNg * 8,
                             (size_t)nc * sw::kSwNg * 8,        (size_t)nc * nlay * 14 * 8,
                             (size_t)nc * nlay * 14 * 8,        (size_t)nc * nlay * 14 * 8,
                             (size_t)nc * nlay * 8,             (size_t)nc * 8,
@@ -174,10 +175,16 @@ int validate(const rrtmg_sw_run_args* a, const rrtmg_sw_exec* x, char* errmsg, i
             "the grid-mean cloud transfer spcvrtc (isubcsw 0) is not", a->isubcsw);
     return 1;
   }
-  if (a->iovr < 0 || a->iovr > 2) {
-    set_msg(errmsg, errmsg_len,
-            "rrtmg_sw_gpu: iovr=%d: the sub-column generator is built for iovr 0 (random), 1 (maximum-random) "
-            "and 2 (maximum) only", a->iovr);
+  if (a->iovr < 0 || a->iovr > 5) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: iovr=%d: mcica_subcol takes iovr 0..5", a->iovr);
+    return 1;
+  }
+  if (a->iovr == 3 && (!a->dzlyr || !a->de_lgth)) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: iovr=3 needs dzlyr and de_lgth");
+    return 1;
+  }
+  if ((a->iovr == 4 || a->iovr == 5) && !a->alpha) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: iovr=%d needs alpha", a->iovr);
     return 1;
   }
   if (a->iswmode < 1 || a->iswmode > 3) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: iswmode must be 1, 2 or 3"); return 1; }
@@ -214,6 +221,7 @@ sw::SwArgs device_args(const rrtmg_sw_run_args* a) {
   d.lwp = a->cld_lwp; d.rel = a->cld_ref_liq; d.iwp = a->cld_iwp; d.rei = a->cld_ref_ice;
   d.rwp = a->cld_rwp; d.rer = a->cld_ref_rain; d.swp = a->cld_swp; d.res = a->cld_ref_snow;
   d.cod = a->cld_od; d.cssa = a->cld_ssa; d.casy = a->cld_asy;
+  d.dz = a->dzlyr; d.alpha = a->alpha; d.delg = a->de_lgth;
   d.icseed = a->icseed; d.idxday = a->idxday;
   d.hswc = a->hswc; d.topflx = a->topflx; d.sfcflx = a->sfcflx; d.cldtau = a->cldtau;
   d.hsw0 = a->hsw0; d.hswb = a->hswb; d.flxprf = a->flxprf; d.fdncmp = a->fdncmp;
@@ -263,8 +271,10 @@ int run_device(SwWorkspace* w, const sw::SwArgs& d, int nday, cudaStream_t st, f
     lw::McicaStage ms;
     ms.cldf = s.cldf;
     ms.seed = s.seed;
+    ms.alpha = s.aux;
     ms.ld = nc;
-    CK(lw::mcica_sw_launch(nc, d.nlay, d.iovr, ms, s.bits, g.num_sms, st), "McICA kernel launch");
+    if (d.iovr <= 2) CK(lw::mcica_sw_launch(nc, d.nlay, d.iovr, ms, s.bits, g.num_sms, st), "McICA kernel launch");
+    else CK(lw::mcica_sw_two_set_launch(nc, d.nlay, d.iovr, ms, s.bits, g.num_sms, st), "McICA kernel launch");
     if (first) CK(cudaEventRecord(ev[2], st), "cudaEventRecord");
     CK(sw::rt_launch(d, s, p0, nc, g.etab, st), "transfer kernel launch");
     if (first) CK(cudaEventRecord(ev[3], st), "cudaEventRecord");
@@ -342,6 +352,7 @@ extern "C" int rrtmg_sw_gpu_init(const rrtmg_sw_init_args* a, char* errmsg, int3
     CK(lw::mcica_upload_powers(), "mcica powers upload");
     CK(lw::mcica_prepare(max_smem), "mcica kernel attributes");
     CK(sw::rt_prepare(max_smem), "transfer kernel attributes");
+    CK(lw::mcica_sw_two_set_prepare(max_smem), "two-set McICA kernel attributes");
   }
   CK(cudaMemcpy(g.etab, et.data(), (kNtbmx + 1) * 8, cudaMemcpyHostToDevice), "exp_tbl upload");
   g.ready = true;
@@ -378,6 +389,7 @@ extern "C" int rrtmg_sw_gpu_run_ex(const rrtmg_sw_run_args* a, const rrtmg_sw_ex
       {&da.aeraod, z.n3}, {&da.aerssa, z.n3}, {&da.aerasy, z.n3},
       {&da.sfcalb_nir_dir, z.np}, {&da.sfcalb_nir_dif, z.np}, {&da.sfcalb_uvis_dir, z.np},
       {&da.sfcalb_uvis_dif, z.np}, {&da.delpin, z.n2}, {&da.cosz, z.np}, {&da.cld_cf, z.n2},
+      {&da.dzlyr, z.n2}, {&da.de_lgth, z.np}, {&da.alpha, z.n2},
       {&da.cld_lwp, z.n2}, {&da.cld_ref_liq, z.n2}, {&da.cld_iwp, z.n2}, {&da.cld_ref_ice, z.n2},
       {&da.cld_rwp, z.n2}, {&da.cld_ref_rain, z.n2}, {&da.cld_swp, z.n2}, {&da.cld_ref_snow, z.n2},
       {&da.cld_od, z.n2}, {&da.cld_ssa, z.n2}, {&da.cld_asy, z.n2}};

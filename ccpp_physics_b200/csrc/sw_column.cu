@@ -537,6 +537,16 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
     const size_t x = (size_t)i + (size_t)a.ld * r;
     const double cf = a.cf[x];
     s.cldf[(size_t)pl + (size_t)nc * k] = (cf < kFtiny) ? 0.0 : cf;   // mcica_subcol input (RSM:1900-1903)
+    if (a.iovr == 3) {   // fac_lcf between layers k-1 and k (RSM:2106-2108), dz in internal order
+      double f = 0.0;
+      if (k > 0) {
+        const int r1 = a.top_at_1 ? nlay - k : k - 1;
+        f = exp(-0.5 * (a.dz[x] + a.dz[(size_t)i + (size_t)a.ld * r1]) / a.delg[i]);
+      }
+      s.aux[(size_t)pl + (size_t)nc * k] = f;
+    } else if (a.iovr == 4 || a.iovr == 5) {   // alpha, in the caller's row order (RSM:889, 990)
+      s.aux[(size_t)pl + (size_t)nc * k] = a.alpha[(size_t)i + (size_t)a.ld * k];
+    }
     if (zcf1 > 0.0) {
       double* tw = s.taucw + ((size_t)pl * nlay + k) * 14;
       double* sw = s.ssacw + ((size_t)pl * nlay + k) * 14;

@@ -16,6 +16,7 @@ struct SwArgs {
   const double *plyr, *tlyr, *qlyr, *olyr, *co2, *n2o, *ch4, *o2, *delp, *cf;
   const double *aod, *ssa, *asy, *cosz, *alb_nir_dir, *alb_nir_dif, *alb_uvis_dir, *alb_uvis_dif;
   const double *lwp, *rel, *iwp, *rei, *rwp, *rer, *swp, *res, *cod, *cssa, *casy;
+  const double *dz, *alpha, *delg;   // layer thickness, alpha, de_lgth: sub-column overlaps 3..5
   const int32_t *icseed, *idxday;
   double *hswc, *topflx, *sfcflx, *cldtau, *hsw0, *hswb, *flxprf, *fdncmp;
   int npts, nlay, ld, top_at_1, inc_minor, iovr, iovr_rand, iovr_maxrand, iswcliq, iswcice, isubcsw, iswmode;
@@ -29,6 +30,7 @@ struct SwScratch {
   double* sflux;                     // [pl][112]
   double *taucw, *ssacw, *asycw;     // [pl][k][14]
   double* cldf;                      // [pl + nc*k], floored cloud fraction (McICA input)
+  double* aux;                       // [pl + nc*k], fac_lcf (iovr 3) or alpha (iovr 4, 5)
   int32_t* seed;                     // [pl]
   double* zcf1;                      // [pl] cloudy-column fraction indicator
   uint32_t* bits;                    // [pl][112][nw] McICA cloudy flags

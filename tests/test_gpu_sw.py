@@ -83,14 +83,15 @@ def test_sw_allsky_127(gpu, osw):
     assert (ref["topflx"][:, 0] != ref["topflx"][:, 2]).any()   # cloudy columns present
 
 
-def test_sw_top_at_1(gpu, osw):
+@pytest.mark.parametrize("iovr", [1, 3, 5])
+def test_sw_top_at_1(gpu, osw, iovr):
     prof = _profile(40, 64, 22, precip=True)
-    out, ref = _both(gpu, osw, _flip(prof), flags=dict(top_at_1=1), hswb=True, flxprf=True)
+    out, ref = _both(gpu, osw, _flip(prof), flags=dict(top_at_1=1, iovr=iovr), hswb=True, flxprf=True)
     _check(out, ref)
 
 
 @pytest.mark.parametrize("flags", [
-    dict(iovr=0), dict(iovr=2), dict(iswmode=1), dict(iswmode=3), dict(iswcice=1), dict(iswcice=2),
+    dict(iovr=0), dict(iovr=2), dict(iovr=3), dict(iovr=4), dict(iovr=5), dict(iswmode=1), dict(iswmode=3), dict(iswcice=1), dict(iswcice=2),
     dict(iswcliq=2), dict(isubcsw=1), dict(inc_minor_gas=0),
 ])
 def test_sw_options(gpu, osw, flags):
@@ -158,7 +159,7 @@ def test_sw_gas_optics_stage(gpu, osw):
 
 def test_sw_refusals_and_noops(gpu):
     prof = _profile(4, 20, 29)
-    for flags, word in ((dict(isubcsw=0), "spcvrtc"), (dict(iovr=3), "iovr=3")):
+    for flags, word in ((dict(isubcsw=0), "spcvrtc"), (dict(iovr=6), "iovr=6")):
         with pytest.raises(sw.RrtmgSwError, match=word):
             gpu.rrtmg_sw_run(prof, sw.alloc_outputs(4, 20), flags=flags)
     out = sw.alloc_outputs(4, 20)

@@ -128,15 +128,29 @@ def _gfs_stream(seed, m):
     return bg.random_raw(m).astype(np.float64) / 4294967295.0
 
 
-@pytest.mark.parametrize("iovr", [0, 1, 2])
+@pytest.mark.parametrize("iovr", [0, 1, 2, 3, 4, 5])
 def test_oracle_mcica_against_numpy_twister(osw, iovr):
     """mcica_subcol (radsw_main.F90:1952-2212), g-major draws, on numpy's MT19937."""
     nlay, seed = 37, 1234567
     rng = np.random.default_rng(4)
     cldf = rng.uniform(0, 1, nlay) * (rng.uniform(0, 1, nlay) > 0.3)
-    bits = osw.mcica_bits(nlay, seed, iovr, cldf)
+    dz = rng.uniform(0.05, 1.5, nlay)
+    alpha = rng.uniform(0, 1, nlay)
+    bits = osw.mcica_bits(nlay, seed, iovr, cldf, dz=dz, de_lgth=2.0, alpha=alpha)
     if iovr == 2:
         cdf = np.repeat(_gfs_stream(seed, 112)[:, None], nlay, 1)
+    elif iovr >= 3:
+        st = _gfs_stream(seed, 2 * 112 * nlay)
+        cdf = st[:112 * nlay].reshape(112, nlay).copy()
+        cd2 = st[112 * nlay:].reshape(112, nlay)
+        if iovr == 3:
+            fac = np.zeros(nlay)
+            fac[1:] = np.exp(-0.5 * (dz[1:] + dz[:-1]) / 2.0)
+            for k in range(nlay - 2, -1, -1):
+                cdf[:, k] = np.where(cd2[:, k] <= fac[k + 1], cdf[:, k + 1], cdf[:, k])
+        else:
+            for k in range(1, nlay):
+                cdf[:, k] = np.where(cd2[:, k] < alpha[k], cdf[:, k - 1], cdf[:, k])
     else:
         cdf = _gfs_stream(seed, 112 * nlay).reshape(112, nlay)
         if iovr == 1:
