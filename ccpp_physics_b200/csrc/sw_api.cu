@@ -105,7 +105,7 @@ size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 // per-column scratch bytes of the three kernels
 size_t scratch_per_col(int nlay) {
   const int nw = (nlay + 31) / 32;
-  return (size_t)(2 * nlay * sw::kSwNg + sw::kSwNg + 3 * nlay * 14 + 2 * nlay + 1 + (nlay + 1) * 10 * 32) * 8 + 4 +
+  return (size_t)(2 * nlay * sw::kSwNg + sw::kSwNg + 3 * nlay * 14 + 2 * nlay + 2 + (nlay + 1) * 10 * 32) * 8 + 4 +
          (size_t)sw::kSwNg * nw * 4 + 64;
 }
 
@@ -124,6 +124,7 @@ sw::SwScratch carve(char* base, int nc, int nlay) {
   s.cldf = (double*)take((size_t)nc * nlay * 8);
   s.aux = (double*)take((size_t)nc * nlay * 8);
   s.zcf1 = (double*)take((size_t)nc * 8);
+  s.zcf0 = (double*)take((size_t)nc * 8);
   s.seed = (int32_t*)take((size_t)nc * 4);
   s.bits = (uint32_t*)take((size_t)nc * sw::kSwNg * nw * 4);
   s.lane_store = (double*)take((size_t)nc * (nlay + 1) * 10 * 32 * 8);
@@ -132,7 +133,7 @@ sw::SwScratch carve(char* base, int nc, int nlay) {
 }
 size_t carve_bytes(int nc, int nlay) {
   const int nw = (nlay + 31) / 32;
-  const size_t parts[12] = {(size_t)nc * nlay * 8, (size_t)nc * (nlay + 1) * 10 * 32 * 8, (size_t)nc * nlay * sw::kSwNg * 8, (size_t)nc * nlay * sw::kSwNg * 8,
+  const size_t parts[13] = {(size_t)nc * 8, (size_t)nc * nlay * 8, (size_t)nc * (nlay + 1) * 10 * 32 * 8, (size_t)nc * nlay * sw::kSwNg * 8, (size_t)nc * nlay * sw::kSwNg * 8,
                             (size_t)nc * sw::kSwNg * 8,        (size_t)nc * nlay * 14 * 8,
                             (size_t)nc * nlay * 14 * 8,        (size_t)nc * nlay * 14 * 8,
                             (size_t)nc * nlay * 8,             (size_t)nc * 8,
@@ -169,21 +170,19 @@ int validate(const rrtmg_sw_run_args* a, const rrtmg_sw_exec* x, char* errmsg, i
   }
   if (x->precision != 0) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: only FP64 (precision 0) is built"); return 1; }
   if (x->memory != 0 && x->memory != 1) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: memory must be 0 or 1"); return 1; }
-  if (a->isubcsw != 1 && a->isubcsw != 2) {
-    set_msg(errmsg, errmsg_len,
-            "rrtmg_sw_gpu: isubcsw=%d: only the McICA transfer (isubcsw 1, 2: spcvrtm) is built; "
-            "the grid-mean cloud transfer spcvrtc (isubcsw 0) is not", a->isubcsw);
+  if (a->isubcsw > 2) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: isubcsw=%d: 0 (spcvrtc), 1 or 2 (McICA, spcvrtm)", a->isubcsw);
     return 1;
   }
   if (a->iovr < 0 || a->iovr > 5) {
     set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: iovr=%d: mcica_subcol takes iovr 0..5", a->iovr);
     return 1;
   }
-  if (a->iovr == 3 && (!a->dzlyr || !a->de_lgth)) {
+  if (a->isubcsw > 0 && a->iovr == 3 && (!a->dzlyr || !a->de_lgth)) {
     set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: iovr=3 needs dzlyr and de_lgth");
     return 1;
   }
-  if ((a->iovr == 4 || a->iovr == 5) && !a->alpha) {
+  if (a->isubcsw > 0 && (a->iovr == 4 || a->iovr == 5) && !a->alpha) {
     set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: iovr=%d needs alpha", a->iovr);
     return 1;
   }
@@ -273,8 +272,13 @@ int run_device(SwWorkspace* w, const sw::SwArgs& d, int nday, cudaStream_t st, f
     ms.seed = s.seed;
     ms.alpha = s.aux;
     ms.ld = nc;
-    if (d.iovr <= 2) CK(lw::mcica_sw_launch(nc, d.nlay, d.iovr, ms, s.bits, g.num_sms, st), "McICA kernel launch");
-    else CK(lw::mcica_sw_two_set_launch(nc, d.nlay, d.iovr, ms, s.bits, g.num_sms, st), "McICA kernel launch");
+    if (d.isubcsw <= 0) {
+      // grid-mean clouds (spcvrtc): no sub-columns
+    } else if (d.iovr <= 2) {
+      CK(lw::mcica_sw_launch(nc, d.nlay, d.iovr, ms, s.bits, g.num_sms, st), "McICA kernel launch");
+    } else {
+      CK(lw::mcica_sw_two_set_launch(nc, d.nlay, d.iovr, ms, s.bits, g.num_sms, st), "McICA kernel launch");
+    }
     if (first) CK(cudaEventRecord(ev[2], st), "cudaEventRecord");
     CK(sw::rt_launch(d, s, p0, nc, g.etab, st), "transfer kernel launch");
     if (first) CK(cudaEventRecord(ev[3], st), "cudaEventRecord");

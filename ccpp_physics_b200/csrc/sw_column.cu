@@ -529,7 +529,9 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
     if (zcf0 > kOneMinus) zcf0 = 1.0;
     zcf1 = 1.0 - zcf0;
     s.zcf1[pl] = zcf1;
-    s.seed[pl] = (a.isubcsw == 1) ? 1 + j1 : a.icseed[i];   // ipsdsw0 + i (RSM:849-857)
+    s.zcf0[pl] = zcf0;
+    // McICA seed: ipsdsw0 + i or icseed(i) (RSM:849-857); grid-mean clouds draw none
+    s.seed[pl] = (a.isubcsw == 2) ? a.icseed[i] : 1 + j1;
   }
   zcf1 = __shfl_sync(0xffffffffu, zcf1, 0);
   for (int k = lane; k < nlay; k += 32) {
@@ -537,7 +539,9 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
     const size_t x = (size_t)i + (size_t)a.ld * r;
     const double cf = a.cf[x];
     s.cldf[(size_t)pl + (size_t)nc * k] = (cf < kFtiny) ? 0.0 : cf;   // mcica_subcol input (RSM:1900-1903)
-    if (a.iovr == 3) {   // fac_lcf between layers k-1 and k (RSM:2106-2108), dz in internal order
+    if (a.isubcsw <= 0) {   // grid-mean clouds: cldfrc = cfrac / cf1 (RSM:1930-1934)
+      s.aux[(size_t)pl + (size_t)nc * k] = (zcf1 > 0.0) ? cf / zcf1 : 0.0;
+    } else if (a.iovr == 3) {   // fac_lcf between layers k-1 and k (RSM:2106-2108), dz in internal order
       double f = 0.0;
       if (k > 0) {
         const int r1 = a.top_at_1 ? nlay - k : k - 1;
@@ -657,7 +661,9 @@ struct ColIn {
   const double* taur;
   const double *aod, *ssa, *asy;   // caller arrays, (i, r, b)
   const double *tcw, *scw, *gcw;   // [k][14]
-  const uint32_t* bits;            // this g-point's nw words
+  const uint32_t* bits;            // this g-point's nw words (McICA)
+  const double* cfr;               // normalised cloud fraction, layer k at cfr[k * cfs] (grid-mean)
+  size_t cfs;
   size_t i;
   int ld, nlay, top_at_1, nw;
   double cosz, sntz;
@@ -665,6 +671,22 @@ struct ColIn {
 };
 
 __device__ __forceinline__ bool cloud_bit(const ColIn& c, int k) { return (c.bits[k >> 5] >> (k & 31)) & 1u; }
+// the all-sky sweep treats layer k as cloudy: its McICA flag, or cldfrc > ftiny (RSM:2919)
+template <bool GRID>
+__device__ __forceinline__ bool cloudy_layer(const ColIn& c, int k) {
+  return GRID ? (c.cfr[(size_t)k * c.cfs] > kFtiny) : cloud_bit(c, k);
+}
+// spcvrtc's mixing of a cloudy layer's optics with its clear optics o
+// (RSM:3039-3042, 3057, 3072): zc0 * clear + zc1 * cloudy
+__device__ __forceinline__ void mix_grid(const ColIn& c, int k, const LayOpt& o, LayOpt& w) {
+  const double zc1 = c.cfr[(size_t)k * c.cfs], zc0 = 1.0 - zc1;
+  w.rb = zc0 * o.rb + zc1 * w.rb;
+  w.rd = zc0 * o.rd + zc1 * w.rd;
+  w.tb = zc0 * o.tb + zc1 * w.tb;
+  w.td = zc0 * o.td + zc1 * w.td;
+  w.e3 = zc0 * o.e3 + zc1 * w.e3;
+  w.e4 = zc0 * o.e4 + zc1 * w.e4;
+}
 
 // the inputs of layer k of g-point g (band b): gas, Rayleigh and aerosol
 // optics, plus the cloud optics when the cloudy pass flags the layer
@@ -672,6 +694,7 @@ struct LayIn {
   double tr, tg, tae, sae, gae, tcw, scw, gcw;
   bool cld;
 };
+template <bool GRID>
 __device__ __forceinline__ void layer_in(const ColIn& c, int g, int b, int k, bool cloudy_pass, LayIn& v) {
   const int r = c.top_at_1 ? c.nlay - 1 - k : k;
   const size_t xa = c.i + (size_t)c.ld * ((size_t)r + (size_t)c.nlay * b);
@@ -680,7 +703,7 @@ __device__ __forceinline__ void layer_in(const ColIn& c, int g, int b, int k, bo
   v.tae = __ldg(c.aod + xa);
   v.sae = __ldg(c.ssa + xa);
   v.gae = __ldg(c.asy + xa);
-  v.cld = cloudy_pass && cloud_bit(c, k);
+  v.cld = cloudy_pass && cloudy_layer<GRID>(c, k);
   if (v.cld) {
     v.tcw = c.tcw[(size_t)k * 14 + b];
     v.scw = c.scw[(size_t)k * 14 + b];
@@ -706,9 +729,10 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-constexpr int kRtWarps = 4;
+constexpr int kRtWarps = 4;   // GRID: isubcsw <= 0, spcvrtc's cloud-fraction mixing; else McICA flags
 constexpr int kLaneVals = 10;   // per-lane stored values per level
 
+template <bool GRID>
 __global__ void __launch_bounds__(32 * kRtWarps, 4)   // 128 registers: sixteen warps per SM
 sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ ET) {
   extern __shared__ double sm[];
@@ -740,7 +764,10 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
   const double ssolar = a.s0fac * a.cosz[i];
   const double albbm[2] = {a.alb_nir_dir[i], a.alb_uvis_dir[i]};
   const double albdf[2] = {a.alb_nir_dif[i], a.alb_uvis_dif[i]};
-  const bool cloudy = s.zcf1[pl] > kEps;
+  const double cf1 = s.zcf1[pl], cf0 = s.zcf0[pl];
+  const bool cloudy = cf1 > kEps;
+  c.cfr = s.aux + pl;
+  c.cfs = (size_t)nc;
   // surface partition and UV-B sums of lane 0: [pass][bm1, bm2, df1, df2, uvb]
   double sfc[2][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
 
@@ -777,10 +804,10 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
       st8(0, 9, udw);
     }
     LayIn vin;
-    layer_in(c, gg, b, 0, cloudy, vin);
+    layer_in<GRID>(c, gg, b, 0, cloudy, vin);
     for (int k = 0; k < nlay; ++k) {
       const LayIn cur = vin;
-      if (k + 1 < nlay) layer_in(c, gg, b, k + 1, cloudy, vin);   // issued ahead of this layer's arithmetic
+      if (k + 1 < nlay) layer_in<GRID>(c, gg, b, k + 1, cloudy, vin);   // issued ahead of this layer's arithmetic
       LayIn clr = cur;
       clr.cld = false;
       LayOpt o;
@@ -797,7 +824,10 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
       }
       if (cloudy) {
         LayOpt w = o;
-        if (cur.cld) layer_opt(c, cur, ET, w);
+        if (cur.cld) {
+          layer_opt(c, cur, ET, w);
+          if (GRID) mix_grid(c, k, o, w);
+        }
         const double zden1 = 1.0 / (1.0 - udw * w.rd);
         const double nb = w.rb + (w.td * ((w.tb - w.e3) * udw + w.e3 * ubw)) * zden1;
         const double nd = w.rd + w.td * w.td * udw * zden1;
@@ -811,10 +841,11 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
     auto fetch = [&](int m, LayOpt& o, LayOpt& w) {
       o.rb = ld8(m, 0); o.rd = ld8(m, 1); o.tb = ld8(m, 2); o.td = ld8(m, 3); o.e3 = ld8(m, 4); o.e4 = ld8(m, 5);
       w = o;
-      if (cloudy && cloud_bit(c, m)) {
+      if (cloudy && cloudy_layer<GRID>(c, m)) {
         LayIn v;
-        layer_in(c, gg, b, m, true, v);
+        layer_in<GRID>(c, gg, b, m, true, v);
         layer_opt(c, v, ET, w);
+        if (GRID) mix_grid(c, m, o, w);
       }
     };
     // one downward step of a sweep: layer optics o, state (tdbt, tdn, rdnd, tdbt0)
@@ -868,8 +899,9 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
           dnc[m] += sdw;
         }
       }
-      if (want_b) {   // total-sky band fluxes
-        const double tu = cloudy ? fuw : fu, td = cloudy ? fdw : fd;
+      if (want_b) {   // total-sky band fluxes (spcvrtc: cf1 * all-sky + cf0 * clear, RSM:3160-3161)
+        const double tu = cloudy ? (GRID ? cf1 * fuw + cf0 * fu : fuw) : fu;
+        const double td = cloudy ? (GRID ? cf1 * fdw + cf0 * fd : fdw) : fd;
         for (int bb = blo; bb <= bhi; ++bb) {
           const double mu = warp_sum(b == bb ? wgt * tu : 0.0), md = warp_sum(b == bb ? wgt * td : 0.0);
           if (lane == 0) {
@@ -894,6 +926,15 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
     }
   }
   __syncwarp();
+  if (cloudy && GRID) {   // spcvrtc's total-sky fluxes (RSM:3158-3178)
+    for (int m = lane; m < nlp1; m += 32) {
+      upc[m] = cf1 * upc[m] + cf0 * up0[m];
+      dnc[m] = cf1 * dnc[m] + cf0 * dn0[m];
+    }
+    if (lane == 0)
+      for (int q = 0; q < 5; ++q) sfc[1][q] = cf1 * sfc[1][q] + cf0 * sfc[0][q];
+    __syncwarp();
+  }
 
   // outputs (RSM:1180-1376)
   const int ld = a.ld;
@@ -955,13 +996,17 @@ cudaError_t optics_launch(const SwArgs& a, const SwScratch& s, int p0, int nc, c
 size_t rt_smem_bytes(int nlay, bool hswb) { return (size_t)kRtWarps * rt_warp_doubles(nlay, hswb) * sizeof(double); }
 
 cudaError_t rt_prepare(int max_smem) {
-  return cudaFuncSetAttribute(sw_rt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  cudaError_t e = cudaFuncSetAttribute(sw_rt_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(sw_rt_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
 }
 
 cudaError_t rt_launch(const SwArgs& a, const SwScratch& s, int p0, int nc, const double* ET, cudaStream_t st) {
   if (nc <= 0) return cudaSuccess;
   const int grid = (nc + kRtWarps - 1) / kRtWarps;
-  sw_rt_kernel<<<grid, 32 * kRtWarps, rt_smem_bytes(a.nlay, a.hswb != nullptr), st>>>(a, s, p0, nc, ET);
+  const size_t smem = rt_smem_bytes(a.nlay, a.hswb != nullptr);
+  if (a.isubcsw <= 0) sw_rt_kernel<true><<<grid, 32 * kRtWarps, smem, st>>>(a, s, p0, nc, ET);
+  else sw_rt_kernel<false><<<grid, 32 * kRtWarps, smem, st>>>(a, s, p0, nc, ET);
   return cudaGetLastError();
 }
 

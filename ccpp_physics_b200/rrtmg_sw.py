@@ -168,7 +168,8 @@ def make_run_args(prof: dict, out: dict, *, flags: dict | None = None, keep=None
     for n in INPUT_FIELDS + ("aeraod", "aerssa", "aerasy", "sfcalb_nir_dir", "sfcalb_nir_dif", "sfcalb_uvis_dir",
                              "sfcalb_uvis_dif", "dzlyr", "delpin", "de_lgth", "alpha", "cosz", "cld_cf"):
         setattr(a, n, _p(prof[n], keep, np.float64))
-    a.icseed = _p(prof["icseed"], keep, np.int32)
+    if prof.get("icseed") is not None:      # isubcsw = 0, 1 draw no seeds from it
+        a.icseed = _p(prof["icseed"], keep, np.int32)
     a.idxday = _p(idx, keep, np.int32)
     for n in OPTIONAL_CLOUD_FIELDS:
         if prof.get(n) is not None:

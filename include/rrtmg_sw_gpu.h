@@ -22,12 +22,12 @@
  * The functions return errflg (0 = success, 1 = error) and copy errmsg into
  * the caller's buffer (NUL-terminated, truncated to errmsg_len).
  *
- * Built: McICA sub-columns (isubcsw = 1, 2) with every overlap of
- * mcica_subcol (iovr 0..5), every cloud-optics option (iswcliq 0, 1, 2;
+ * Every cloud treatment of rrtmg_sw_run is built, in FP64: McICA
+ * sub-columns (isubcsw = 1, 2; transfer spcvrtm) with every overlap of
+ * mcica_subcol (iovr 0..5), and grid-mean clouds (isubcsw = 0; transfer
+ * spcvrtc).  Also built: every cloud-optics option (iswcliq 0, 1, 2;
  * iswcice 1, 2, 3), every two-stream option (iswmode 1, 2, 3) and every
- * output of rrtmg_sw_run; FP64.  Calls asking for the grid-mean cloud
- * transfer (isubcsw = 0, spcvrtc) return errflg = 1 with a message saying
- * so.
+ * output.
  */
 #ifndef RRTMG_SW_GPU_H
 #define RRTMG_SW_GPU_H

@@ -20,8 +20,7 @@
 // FMA contraction disabled, Fortran int() = truncation toward zero,
 // mod(x,1.) = fmod; literals are binary64 (promoted-real build).
 //
-// Not restated: the grid-mean cloud transfer spcvrtc (isubcsw = 0,
-// RSM:2432-3183); calls asking for it are refused.
+//     spcvrtc (isubcsw <= 0)   RSM:2432-3183, as spcvrtm's grid-mean mode
 //
 // Parity of this restatement is NOT pinned by the reference: the reference is
 // Fortran, no Fortran compiler exists in this environment, and the reference
@@ -199,7 +198,7 @@ void mcica_subcol(int nlay, const double* cldf, int ipseed, const double* dz, do
 struct Col {
   int nlay;
   std::vector<double> pavel, tavel, delp, dz, alph, h2ovmr, o3vmr, coldry, temcol, colmol, colamt;
-  std::vector<double> cfrac, cliqp, reliq, cicep, reice, cdat1, cdat2, cdat3, cdat4;
+  std::vector<double> cfrac, cliqp, reliq, cicep, reice, cdat1, cdat2, cdat3, cdat4, cldfrc;
   std::vector<double> taucw, ssacw, asycw, tauae, ssaae, asyae, cldfmc;
   std::vector<double> fac00, fac01, fac10, fac11, forfac, forfrac, selffac, selffrac;
   std::vector<int> jp, jt, jt1, indfor, indself;
@@ -207,7 +206,7 @@ struct Col {
   std::vector<double> fxupc, fxdnc, fxup0, fxdn0;
   explicit Col(int n) : nlay(n) {
     for (auto* v : {&pavel, &tavel, &delp, &dz, &alph, &h2ovmr, &o3vmr, &coldry, &temcol, &colmol, &cfrac,
-                    &cliqp, &reliq, &cicep, &reice, &cdat1, &cdat2, &cdat3, &cdat4, &fac00, &fac01, &fac10,
+                    &cliqp, &reliq, &cicep, &reice, &cdat1, &cdat2, &cdat3, &cdat4, &cldfrc, &fac00, &fac01, &fac10,
                     &fac11, &forfac, &forfrac, &selffac, &selffrac})
       v->assign(n + 1, 0.0);
     colamt.assign((size_t)(n + 1) * 8, 0.0);
@@ -236,7 +235,7 @@ struct Col {
 };
 
 // ---- cldprop (RSM:1566-1938) ----------------------------------------------
-void cldprop(Col& c, int ipseed, double delgth, int iswcliq, int iswcice, int isubcsw, int iovr) {
+void cldprop(Col& c, int ipseed, double delgth, int iswcliq, int iswcice, int isubcsw, int iovr, double cf1) {
   const int nlay = c.nlay;
   for (int ib = 1; ib <= NBDSW; ++ib)
     for (int k = 1; k <= nlay; ++k) { c.TAUCW(k, ib) = f_zero; c.SSACW(k, ib) = f_one; c.ASYCW(k, ib) = f_zero; }
@@ -355,6 +354,8 @@ void cldprop(Col& c, int ipseed, double delgth, int iswcliq, int iswcice, int is
     mcica_subcol(nlay, cldf.data(), ipseed, dz.data(), delgth, al.data(), iovr, lc);
     for (int ig = 1; ig <= NGPT; ++ig)
       for (int k = 1; k <= nlay; ++k) c.CLDFMC(k, ig) = lc[(size_t)(ig - 1) * nlay + (k - 1)] ? f_one : f_zero;
+  } else {   // non-McICA: normalised cloud fraction (RSM:1930-1934)
+    for (int k = 1; k <= nlay; ++k) c.cldfrc[k] = c.cfrac[k] / cf1;
   }
 }
 
@@ -799,8 +800,12 @@ struct SwScalars {
 };
 
 // ---- spcvrtm (RSM:3228-3942) ----------------------------------------------
+// spcvrtc (RSM:2432-3183) is the same sweep with the cloudy layers' optics
+// mixed by the normalised cloud fraction instead of McICA flags
+// (RSM:2925-2928, 3039-3042, 3057, 3072) and the column's fluxes mixed by
+// cf1/cf0 (RSM:3158-3178); grid = true selects it.
 void spcvrtm(Col& c, double ssolar, double cosz, double sntz, const double albbm[2], const double albdf[2],
-             double cf1, int iswmode, SwScalars& o) {
+             double cf1, double cf0, int iswmode, bool grid, SwScalars& o) {
   const int nlay = c.nlay, nlp1 = nlay + 1;
   const double od_lo = 0.06;
   for (auto* v : {&c.fxupc, &c.fxdnc, &c.fxup0, &c.fxdn0}) std::fill(v->begin(), v->end(), 0.0);
@@ -866,21 +871,35 @@ void spcvrtm(Col& c, double ssolar, double cosz, double sntz, const double albbm
       zldbt[1] = f_zero;
       for (int k = nlay; k >= 1; --k) {
         const int kp = k + 1;
-        if (c.CLDFMC(k, jg) > ftiny) {
+        const double zc0 = f_one - c.cldfrc[k], zc1 = c.cldfrc[k];
+        if (grid ? (zc1 > ftiny) : (c.CLDFMC(k, jg) > ftiny)) {
+          const double zrefb1 = zrefb[kp], zrefd1 = zrefd[kp], ztrab1 = ztrab[kp], ztrad1 = ztrad[kp];
           const double ztau0 = ztaus[k] + c.TAUCW(k, ib);
           const double zssa0 = zssas[k] + c.SSACW(k, ib);
           const double zasy0 = zasys[k] + c.ASYCW(k, ib);
           double ztau1;
           two_stream(ztau0, zssa0, zasy0, cosz, sntz, iswmode, zrefb[kp], ztrab[kp], zrefd[kp], ztrad[kp], ztau1);
+          if (grid) {
+            zrefb[kp] = zc0 * zrefb1 + zc1 * zrefb[kp];
+            zrefd[kp] = zc0 * zrefd1 + zc1 * zrefd[kp];
+            ztrab[kp] = zc0 * ztrab1 + zc1 * ztrab[kp];
+            ztrad[kp] = zc0 * ztrad1 + zc1 * ztrad[kp];
+          }
           double zr1 = ztau1 * sntz, zexp3, zexp4;
           if (zr1 <= od_lo) zexp3 = f_one - zr1 + 0.5 * zr1 * zr1;
           else zexp3 = exp_lookup_clamp(zr1);
-          zldbt[kp] = zexp3;
-          ztdbt[k] = zexp3 * ztdbt[kp];
+          if (grid) {
+            zldbt[kp] = zc0 * zldbt[kp] + zc1 * zexp3;
+            ztdbt[k] = zldbt[kp] * ztdbt[kp];
+          } else {
+            zldbt[kp] = zexp3;
+            ztdbt[k] = zexp3 * ztdbt[kp];
+          }
           zr1 = ztau0 * sntz;
           if (zr1 <= od_lo) zexp4 = f_one - zr1 + 0.5 * zr1 * zr1;
           else zexp4 = exp_lookup_clamp(zr1);
-          ztdbt0 = zexp4 * ztdbt0;
+          if (grid) ztdbt0 = (zc0 * zldbt0[k] + zc1 * zexp4) * ztdbt0;
+          else ztdbt0 = zexp4 * ztdbt0;
         } else {
           ztdbt[k] = zldbt[kp] * ztdbt[kp];
           ztdbt0 = zldbt0[k] * ztdbt0;
@@ -929,12 +948,23 @@ void spcvrtm(Col& c, double ssolar, double cosz, double sntz, const double albbm
     o.sfdfc[1] = o.sfdf0[1];
     o.suvbfc = o.suvbf0;
   } else {
+    if (grid)
+      for (int ib = 1; ib <= NBDSW; ++ib)
+        for (int k = 1; k <= nlp1; ++k) {
+          c.FXUPC(k, ib) = cf1 * c.FXUPC(k, ib) + cf0 * c.FXUP0(k, ib);
+          c.FXDNC(k, ib) = cf1 * c.FXDNC(k, ib) + cf0 * c.FXDN0(k, ib);
+        }
     for (int ib = 1; ib <= NBDSW; ++ib) {
       o.ftoauc = o.ftoauc + c.FXUPC(nlp1, ib);
       o.fsfcuc = o.fsfcuc + c.FXUPC(1, ib);
       o.fsfcdc = o.fsfcdc + c.FXDNC(1, ib);
     }
     o.suvbfc = c.FXDNC(1, ibd);
+    if (grid)
+      for (int q = 0; q < 2; ++q) {
+        o.sfbmc[q] = cf1 * o.sfbmc[q] + cf0 * o.sfbm0[q];
+        o.sfdfc[q] = cf1 * o.sfdfc[q] + cf0 * o.sfdf0[q];
+      }
   }
 }
 
@@ -1000,7 +1030,7 @@ void run_column(const rrtmg_sw_run_args& a, int ipt, Col& c) {
   const int nlay = a.nlay, nlp1 = a.nlp1;
   const long ld = a.ldim > 0 ? a.ldim : a.npts;
   const int j1 = a.idxday[ipt - 1];
-  const int ipseed = (a.isubcsw == 1) ? 1 + j1 : a.icseed[j1 - 1];   // ipsdsw0 + i (RSM:849-857)
+  const int ipseed = (a.isubcsw == 2) ? a.icseed[j1 - 1] : 1 + j1;   // ipsdsw0 + i (RSM:849-857)
   const double cosz1 = a.cosz[j1 - 1];
   const double sntz1 = f_one / a.cosz[j1 - 1];
   const double ssolar = (a.solcon / s0) * a.cosz[j1 - 1];
@@ -1026,12 +1056,13 @@ void run_column(const rrtmg_sw_run_args& a, int ipt, Col& c) {
   if (zcf0 > oneminus) zcf0 = f_one;
   zcf1 = f_one - zcf0;
   if (zcf1 > f_zero) {
-    cldprop(c, ipseed, delgth, a.iswcliq, a.iswcice, a.isubcsw, a.iovr);
+    cldprop(c, ipseed, delgth, a.iswcliq, a.iswcice, a.isubcsw, a.iovr, zcf1);
     for (int k = 1; k <= nlay; ++k) {
       const int kk = a.top_at_1 ? nlp1 - k : k;
       a.cldtau[(j1 - 1) + ld * (kk - 1)] = c.TAUCW(k, 10);
     }
   } else {
+    std::fill(c.cldfrc.begin(), c.cldfrc.end(), 0.0);
     std::fill(c.cldfmc.begin(), c.cldfmc.end(), 0.0);
     std::fill(c.taucw.begin(), c.taucw.end(), 0.0);
     std::fill(c.ssacw.begin(), c.ssacw.end(), 0.0);
@@ -1040,7 +1071,7 @@ void run_column(const rrtmg_sw_run_args& a, int ipt, Col& c) {
   const int laytrop = setcoef(c);
   taumol(c, laytrop);
   SwScalars o;
-  spcvrtm(c, ssolar, cosz1, sntz1, albbm, albdf, zcf1, a.iswmode, o);
+  spcvrtm(c, ssolar, cosz1, sntz1, albbm, albdf, zcf1, zcf0, a.iswmode, a.isubcsw <= 0, o);
 
   std::vector<double> flxuc(nlp1 + 1), flxdc(nlp1 + 1), flxu0(nlp1 + 1), flxd0(nlp1 + 1), fnet(nlp1 + 1),
       rfdelp(nlay + 1);
@@ -1115,8 +1146,12 @@ int check_args(const rrtmg_sw_run_args* a, char* errmsg, int errmsg_len) {
             "Logic error: iswcliq<=0 requires the following optional arguments to be present: cld_od, cld_ssa, cld_asy");
     return 1;
   }
-  if (a->isubcsw < 1 || a->isubcsw > 2) {
-    set_err(errmsg, errmsg_len, "oracle: isubcsw must be 1 or 2 (McICA, spcvrtm); spcvrtc is not restated");
+  if (a->isubcsw > 2) {
+    set_err(errmsg, errmsg_len, "oracle: isubcsw must be 0 (spcvrtc), 1 or 2 (McICA, spcvrtm)");
+    return 1;
+  }
+  if (a->isubcsw == 2 && !a->icseed) {
+    set_err(errmsg, errmsg_len, "oracle: isubcsw=2 needs icseed");
     return 1;
   }
   return 0;

@@ -83,16 +83,30 @@ def test_sw_allsky_127(gpu, osw):
     assert (ref["topflx"][:, 0] != ref["topflx"][:, 2]).any()   # cloudy columns present
 
 
-@pytest.mark.parametrize("iovr", [1, 3, 5])
-def test_sw_top_at_1(gpu, osw, iovr):
+@pytest.mark.parametrize("iovr,isubcsw", [(1, 2), (3, 2), (5, 2), (1, 0)])
+def test_sw_top_at_1(gpu, osw, iovr, isubcsw):
     prof = _profile(40, 64, 22, precip=True)
-    out, ref = _both(gpu, osw, _flip(prof), flags=dict(top_at_1=1, iovr=iovr), hswb=True, flxprf=True)
+    out, ref = _both(gpu, osw, _flip(prof), flags=dict(top_at_1=1, iovr=iovr, isubcsw=isubcsw), hswb=True,
+                     flxprf=True)
+    _check(out, ref)
+
+
+def test_sw_grid_mean_without_seeds(gpu, osw):
+    """isubcsw=0 draws no sub-columns: icseed may be absent."""
+    prof = _profile(24, 50, 30, precip=True)
+    prof["icseed"] = None
+    ref = sw.alloc_outputs(24, 50, flxprf=True)
+    rc, msg = osw.run(prof, ref, flags=dict(isubcsw=0))
+    assert rc == 0, msg
+    out = sw.alloc_outputs(24, 50, flxprf=True)
+    gpu.rrtmg_sw_run(prof, out, flags=dict(isubcsw=0))
     _check(out, ref)
 
 
 @pytest.mark.parametrize("flags", [
     dict(iovr=0), dict(iovr=2), dict(iovr=3), dict(iovr=4), dict(iovr=5), dict(iswmode=1), dict(iswmode=3), dict(iswcice=1), dict(iswcice=2),
-    dict(iswcliq=2), dict(isubcsw=1), dict(inc_minor_gas=0),
+    dict(iswcliq=2), dict(isubcsw=1), dict(inc_minor_gas=0), dict(isubcsw=0), dict(isubcsw=0, iovr=0),
+    dict(isubcsw=0, iswmode=3),
 ])
 def test_sw_options(gpu, osw, flags):
     prof = _profile(48, 72, 23, night_fraction=0.1, precip=True)
@@ -159,7 +173,7 @@ def test_sw_gas_optics_stage(gpu, osw):
 
 def test_sw_refusals_and_noops(gpu):
     prof = _profile(4, 20, 29)
-    for flags, word in ((dict(isubcsw=0), "spcvrtc"), (dict(iovr=6), "iovr=6")):
+    for flags, word in ((dict(isubcsw=3), "isubcsw=3"), (dict(iovr=6), "iovr=6")):
         with pytest.raises(sw.RrtmgSwError, match=word):
             gpu.rrtmg_sw_run(prof, sw.alloc_outputs(4, 20), flags=flags)
     out = sw.alloc_outputs(4, 20)

@@ -162,10 +162,23 @@ def test_oracle_mcica_against_numpy_twister(osw, iovr):
     assert np.array_equal(got, want)
 
 
-def test_oracle_refuses_spcvrtc(osw):
-    prof = _profile(4, 10)
-    rc, msg = osw.run(prof, sw.alloc_outputs(4, 10), flags=dict(isubcsw=0))
-    assert rc == 1 and "spcvrtc" in msg
+def test_oracle_spcvrtc_overcast_and_clear_limits(osw):
+    """spcvrtc (isubcsw=0) mixes clear and cloudy optics by cldfrc = cfrac/cf1:
+    with every cloudy layer at cf = 1 it equals the McICA path (every
+    sub-column cloudy there), and a clear column gives clear-sky fluxes."""
+    prof = _profile(16, 30, precip=True)
+    cf = prof["cld_cf"]
+    prof["cld_cf"] = np.where(cf > 0, 1.0, 0.0)
+    a = sw.alloc_outputs(16, 30, flxprf=True)
+    b = sw.alloc_outputs(16, 30, flxprf=True)
+    assert osw.run(prof, a, flags=dict(isubcsw=0))[0] == 0
+    assert osw.run(prof, b, flags=dict(isubcsw=2))[0] == 0
+    for k in ("topflx", "sfcflx", "fdncmp", "flxprf"):
+        assert np.allclose(a[k], b[k], rtol=1e-13, atol=0), k
+    clear = _profile(8, 30, cloudy=False)
+    c = sw.alloc_outputs(8, 30)
+    assert osw.run(clear, c, flags=dict(isubcsw=0))[0] == 0
+    assert np.array_equal(c["topflx"][:, 0], c["topflx"][:, 2])
 
 
 def test_sw_struct_layout_matches_header(tmp_path):
