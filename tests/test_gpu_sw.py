@@ -183,3 +183,20 @@ def test_sw_refusals_and_noops(gpu):
     p2 = dict(prof, idxday=np.array([1, 9], np.int32))
     with pytest.raises(sw.RrtmgSwError, match="idxday"):
         gpu.rrtmg_sw_run(p2, sw.alloc_outputs(4, 20))
+
+
+@pytest.mark.parametrize("name", ["sw_allsky_127lay", "sw_dcorr_127lay", "sw_gridmean_64lay"])
+def test_sw_golden_fixture(gpu, name):
+    """The CUDA path against the committed outputs of the restatement."""
+    import importlib.util
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "make_sw_golden.py")
+    spec = importlib.util.spec_from_file_location("make_sw_golden", path)
+    g = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(g)
+    case = g.CASES[name]
+    prof = g.profile(case)
+    out = sw.alloc_outputs(case["npts"], case["nlay"], hswb=True, flxprf=True)
+    gpu.rrtmg_sw_run(prof, out, flags=case["flags"])
+    ref = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", f"oracle_{name}.npz")))
+    _check(out, ref)
