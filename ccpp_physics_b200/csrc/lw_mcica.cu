@@ -17,6 +17,7 @@
 // Integer arithmetic is exact; the u32 -> real conversion (u/(2^32-1)) and
 // the FP64 comparisons/products of the walk are IEEE operations, so the
 // sub-column flags equal the Fortran's bit for bit.
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 #include <cstdio>
@@ -625,13 +626,13 @@ cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int 
 // cdfunc(k) >= 1 - cldf(k).  stage.alpha holds fac_lcf (iovr 3, entry k is
 // the factor between layers k-1 and k) or alpha (iovr 4, 5), per layer in
 // internal order.
-constexpr int kSwTwoSetWarps = 4;
+constexpr int kSwTwoSetMaxWarps = 8;   // warps per CTA: as many as the shared memory holds, up to 8
 
 __host__ __device__ inline size_t sw_two_set_warp_bytes(int nlay, int cap) {
   return 2 * (((size_t)nlay * 8 + 15) & ~(size_t)15) + 2 * (size_t)cap * 4;
 }
 
-__global__ void __launch_bounds__(32 * kSwTwoSetWarps)
+__global__ void __launch_bounds__(32 * kSwTwoSetMaxWarps)
 sw_mcica_two_set_kernel(int ncols, McicaArgs a, uint32_t* __restrict__ bits) {
   extern __shared__ __align__(16) char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -642,9 +643,10 @@ sw_mcica_two_set_kernel(int ncols, McicaArgs a, uint32_t* __restrict__ bits) {
   double* aux = reinterpret_cast<double*>(my + lb);    // fac_lcf or alpha
   uint32_t* ra = reinterpret_cast<uint32_t*>(my + 2 * lb);
   uint32_t* rb = ra + cap;
-  const int warps_total = gridDim.x * kSwTwoSetWarps;
+  const int wpb = blockDim.x >> 5;
+  const int warps_total = gridDim.x * wpb;
   const long long P0 = (long long)kSwNgpt * nlay;   // set 2 starts here
-  for (int c = blockIdx.x * kSwTwoSetWarps + wib; c < ncols; c += warps_total) {
+  for (int c = blockIdx.x * wpb + wib; c < ncols; c += warps_total) {
     __syncwarp();
     for (int k = lane; k < nlay; k += 32) {
       clr[k] = 1.0 - a.st.cldf[c + (size_t)a.st.ld * k];
@@ -725,13 +727,22 @@ cudaError_t mcica_sw_two_set_launch(int ncols, int nlay, int iovr, const McicaSt
   const long round = (long)kMcicaRound * nlay + 623;
   a.cap = (int)((round + 623) / 624 * 624);
   a.st = stage;
-  const size_t smem = sw_two_set_warp_bytes(nlay, a.cap) * kSwTwoSetWarps;
+  static int max_smem = 0;
+  if (max_smem == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  }
+  const size_t per_warp = sw_two_set_warp_bytes(nlay, a.cap);
+  const int wpb = (int)std::min<size_t>(kSwTwoSetMaxWarps, (size_t)max_smem / per_warp);
+  if (wpb < 1) return cudaErrorInvalidValue;
+  const size_t smem = per_warp * wpb;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sw_mcica_two_set_kernel, 32 * kSwTwoSetWarps, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sw_mcica_two_set_kernel, 32 * wpb, smem);
   if (per_sm < 1) per_sm = 1;
-  const int grid = min((ncols + kSwTwoSetWarps - 1) / kSwTwoSetWarps, num_sms * per_sm);
+  const int grid = min((ncols + wpb - 1) / wpb, num_sms * per_sm);
   if (grid < 1) return cudaSuccess;
-  sw_mcica_two_set_kernel<<<grid, 32 * kSwTwoSetWarps, smem, st>>>(ncols, a, bits);
+  sw_mcica_two_set_kernel<<<grid, 32 * wpb, smem, st>>>(ncols, a, bits);
   return cudaGetLastError();
 }
 
