@@ -397,12 +397,18 @@ extern "C" int rrtmg_sw_gpu_run_ex(const rrtmg_sw_run_args* a, const rrtmg_sw_ex
       {&da.cld_lwp, z.n2}, {&da.cld_ref_liq, z.n2}, {&da.cld_iwp, z.n2}, {&da.cld_ref_ice, z.n2},
       {&da.cld_rwp, z.n2}, {&da.cld_ref_rain, z.n2}, {&da.cld_swp, z.n2}, {&da.cld_ref_snow, z.n2},
       {&da.cld_od, z.n2}, {&da.cld_ssa, z.n2}, {&da.cld_asy, z.n2}};
-  std::vector<std::pair<double**, size_t>> outs = {
-      {&da.hswc, z.n2}, {&da.topflx, z.np * 3}, {&da.sfcflx, z.np * 4}, {&da.cldtau, z.n2},
-      {&da.hsw0, z.n2}, {&da.hswb, z.n3}, {&da.flxprf, z.nlev * 4}, {&da.fdncmp, z.np * 6}};
+  // outputs: (elements, record width, rows); only the first npts of every
+  // row of ldim are the caller's to overwrite
+  struct Out { double** p; size_t n, w, rows; };
+  const size_t ldz = a->ldim > 0 ? (size_t)a->ldim : (size_t)a->npts;
+  std::vector<Out> outs = {
+      {&da.hswc, z.n2, 1, (size_t)a->nlay}, {&da.topflx, z.np * 3, 0, 0}, {&da.sfcflx, z.np * 4, 0, 0},
+      {&da.cldtau, z.n2, 1, (size_t)a->nlay}, {&da.hsw0, z.n2, 1, (size_t)a->nlay},
+      {&da.hswb, z.n3, 1, (size_t)a->nlay * RRTMG_SW_NBANDS}, {&da.flxprf, z.nlev * 4, 4, (size_t)a->nlp1},
+      {&da.fdncmp, z.np * 6, 0, 0}};
   size_t total = align256(z.np * 4) + align256(z.nd * 4);
   for (auto& p : ins) if (*p.first) total += align256(p.second * 8);
-  for (auto& p : outs) if (*p.first) total += align256(p.second * 8);
+  for (auto& p : outs) if (*p.p) total += align256(p.n * 8);
   CK(grow(&w->stage, &w->stage_bytes, total), "staging allocation");
   size_t off = 0;
   auto place = [&](size_t bytes) { char* p = w->stage + off; off += align256(bytes); return p; };
@@ -422,19 +428,26 @@ extern "C" int rrtmg_sw_gpu_run_ex(const rrtmg_sw_run_args* a, const rrtmg_sw_ex
     CK(cudaMemcpyAsync(d, *p.first, p.second * 8, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
     *p.first = d;
   }
-  struct Back { double* host; double* dev; size_t n; };
+  struct Back { double* host; double* dev; Out o; };
   std::vector<Back> back;
   for (auto& p : outs) {
-    if (!*p.first) continue;
-    double* d = (double*)place(p.second * 8);
-    back.push_back({*p.first, d, p.second});
-    *p.first = d;
+    if (!*p.p) continue;
+    double* d = (double*)place(p.n * 8);
+    back.push_back({*p.p, d, p});
+    *p.p = d;
   }
   sw::SwArgs d = device_args(&da);
   int r = run_device(w, d, a->nday, st, x->kernel_ms, errmsg, errmsg_len, z);
   if (r) return r;
-  for (const Back& b : back)
-    CK(cudaMemcpyAsync(b.host, b.dev, b.n * 8, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  for (const Back& b : back) {
+    if (b.o.w == 0) {   // per-column records: exactly npts of them
+      CK(cudaMemcpyAsync(b.host, b.dev, b.o.n * 8, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    } else {            // (ldim, rows) arrays of w-double records: the npts-wide part of each row
+      const size_t pitch = ldz * b.o.w * 8;
+      CK(cudaMemcpy2DAsync(b.host, pitch, b.dev, pitch, (size_t)a->npts * b.o.w * 8, b.o.rows,
+                           cudaMemcpyDeviceToHost, st), "cudaMemcpy2DAsync");
+    }
+  }
   return check_bad(w, st, errmsg, errmsg_len);
 }
 

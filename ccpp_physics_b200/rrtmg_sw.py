@@ -151,17 +151,18 @@ def alloc_outputs(npts, nlay, *, hsw0=True, hswb=False, flxprf=False, fdncmp=Tru
     return out
 
 
-def make_run_args(prof: dict, out: dict, *, flags: dict | None = None, keep=None) -> SwRunArgs:
+def make_run_args(prof: dict, out: dict, *, flags: dict | None = None, keep=None, ldim: int = 0) -> SwRunArgs:
     """Fill SwRunArgs from a profile with SW inputs (``add_sw_inputs``) and
     output arrays.  ``keep`` collects converted arrays so they outlive the
-    call."""
+    call; ``ldim`` > npts describes arrays that are slices of (ldim, ...)
+    arrays."""
     keep = [] if keep is None else keep
     fl = dict(prof.get("sw_flags", DEFAULT_FLAGS))
     if flags:
         fl.update(flags)
     npts, nlay = prof["npts"], prof["nlay"]
     idx = prof["idxday"]
-    a = SwRunArgs(npts=npts, nlay=nlay, nlp1=nlay + 1, ldim=0, nday=int(len(idx)), solcon=prof["solcon"],
+    a = SwRunArgs(npts=npts, nlay=nlay, nlp1=nlay + 1, ldim=ldim, nday=int(len(idx)), solcon=prof["solcon"],
                   **abi.OVERLAP_FLAGS)
     for k in ("lprnt", "lsswr", "top_at_1", "inc_minor_gas", "iovr", "iswcliq", "iswcice", "isubcsw", "iswmode"):
         setattr(a, k, int(fl[k]))
@@ -229,12 +230,12 @@ def rswinit(me=1, rad_hr_units=1, inc_minor_gas=True, iswcliq=1, isubcsw=2, iovr
 
 
 def rrtmg_sw_run(prof: dict, out: dict, *, flags: dict | None = None, device_memory: bool = False,
-                 stream=None, kernel_ms=None):
+                 stream=None, kernel_ms=None, ldim: int = 0):
     """rrtmg_sw_run (radsw_main.F90:493) on the GPU; fills ``out`` in place.
     With ``device_memory`` every array (profile and outputs) must be a CUDA
     tensor (idxday and icseed included).  Raises on errflg."""
     keep = []
-    a = make_run_args(prof, out, flags=flags, keep=keep)
+    a = make_run_args(prof, out, flags=flags, keep=keep, ldim=ldim)
     x = SwExec(precision=0, memory=1 if device_memory else 0, sync=1,
                stream=C.c_void_p(stream.cuda_stream if stream is not None else 0))
     km = None

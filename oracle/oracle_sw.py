@@ -45,11 +45,11 @@ def rswinit(rad_hr_units=1, iovr=1, iswmode=2, iswcliq=1, isubcsw=2):
     return rc, msg.value.decode()
 
 
-def run(prof, out, flags=None, nthreads=0):
+def run(prof, out, flags=None, nthreads=0, ldim=0):
     """rrtmg_sw_run on the CPU; fills ``out`` (numpy) in place.  Returns
     (errflg, errmsg)."""
     keep = []
-    a = sw.make_run_args(prof, out, flags=flags, keep=keep)
+    a = sw.make_run_args(prof, out, flags=flags, keep=keep, ldim=ldim)
     msg = C.create_string_buffer(512)
     rc = lib().oracle_rrtmg_sw_run(C.byref(a), nthreads, msg, 512)
     return rc, msg.value.decode()

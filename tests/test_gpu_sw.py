@@ -200,3 +200,41 @@ def test_sw_golden_fixture(gpu, name):
     gpu.rrtmg_sw_run(prof, out, flags=case["flags"])
     ref = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", f"oracle_{name}.npz")))
     _check(out, ref)
+
+
+def test_sw_edges(gpu, osw):
+    """200 layers (the most this path takes), 2 layers, idxday in arbitrary
+    order, and no daytime point at all (radsw_main.F90:786: outputs untouched)."""
+    for npts, nlay in ((12, 200), (16, 2)):
+        prof = _profile(npts, nlay, 31, night_fraction=0.3, precip=True)
+        out, ref = _both(gpu, osw, prof, hswb=True, flxprf=True)
+        _check(out, ref)
+    prof = _profile(30, 60, 32, night_fraction=0.2)
+    prof["idxday"] = np.random.default_rng(5).permutation(prof["idxday"]).astype(np.int32)
+    out, ref = _both(gpu, osw, prof, flxprf=True)
+    _check(out, ref)
+    prof["idxday"] = np.zeros(0, np.int32)
+    out = sw.alloc_outputs(30, 60)
+    out["hswc"][:] = 5.0
+    gpu.rrtmg_sw_run(prof, out)
+    assert (out["hswc"] == 5.0).all()
+
+
+def test_sw_leading_dimension(gpu, osw):
+    """Arrays that are (ldim, ...) slices with ldim > npts, host and device memory."""
+    import torch
+    npts, ld, nlay = 20, 27, 48
+    big = _profile(ld, nlay, 33, night_fraction=0.25, precip=True)
+    prof = dict(big, npts=npts)
+    prof["idxday"] = big["idxday"][big["idxday"] <= npts].astype(np.int32)
+    ref = sw.alloc_outputs(ld, nlay, flxprf=True)
+    rc, msg = osw.run(prof, ref, flags=None, ldim=ld)
+    assert rc == 0, msg
+    out = sw.alloc_outputs(ld, nlay, flxprf=True)
+    gpu.rrtmg_sw_run(prof, out, ldim=ld)
+    _check({k: v for k, v in out.items()}, ref)
+    dev = {k: (torch.as_tensor(np.ascontiguousarray(v)).cuda() if isinstance(v, np.ndarray) else v)
+           for k, v in prof.items()}
+    outd = sw.alloc_outputs(ld, nlay, flxprf=True, like=dev["plyr"])
+    gpu.rrtmg_sw_run(dev, outd, device_memory=True, ldim=ld)
+    _check({k: v.cpu().numpy() for k, v in outd.items()}, ref)
