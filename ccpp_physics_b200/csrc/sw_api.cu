@@ -50,6 +50,11 @@ struct SwWorkspace {
   char* stage = nullptr;     // device copies of host arguments
   size_t stage_bytes = 0;
   int* bad = nullptr;
+  // pipelined host path: copy streams, double-buffered staging and its events
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_in[2] = {}, ev_done[2] = {}, ev_out[2] = {};
+  char* pbuf = nullptr;
+  size_t pbuf_bytes = 0;
 };
 std::vector<SwWorkspace*> g_ws;
 thread_local SwWorkspace* tl_ws = nullptr;
@@ -254,7 +259,6 @@ int run_device(SwWorkspace* w, const sw::SwArgs& d, int nday, cudaStream_t st, f
   const size_t per = scratch_per_col(d.nlay);
   int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)nday, kScratchBudget / per));
   CK(grow(&w->scratch, &w->scratch_bytes, carve_bytes(chunk, d.nlay)), "scratch allocation");
-  CK(cudaMemsetAsync(w->bad, 0, sizeof(int), st), "cudaMemsetAsync");
   cudaEvent_t ev[4] = {};
   if (kernel_ms) {
     for (auto& e : ev) CK(cudaEventCreate(&e), "cudaEventCreate");
@@ -303,6 +307,129 @@ int check_bad(SwWorkspace* w, cudaStream_t st, char* errmsg, int32_t errmsg_len)
     return 1;
   }
   return 0;
+}
+
+// Host arrays of many columns: chunks of kSwHostChunk columns, double-
+// buffered, each chunk's inputs copied (strided, 2-D) on one copy stream,
+// its kernels on the compute stream and its outputs copied back on a second
+// copy stream, so copies of chunk j+1 and j-1 overlap the kernels of chunk j.
+// The daytime points are split by chunk on the host (chunk-relative indices);
+// seed0 keeps the isubcsw = 1 seeds global.
+constexpr int kSwHostChunk = 4096;
+
+struct HostField {
+  const void* h;   // caller's array
+  void** slot;     // the pointer in the chunk's argument record
+  size_t rows;     // rows of ldim (0: a per-column vector of `width` values)
+  size_t width;    // values per column in a row
+  size_t elem;
+  bool out;
+};
+
+int run_host_pipelined(SwWorkspace* w, const rrtmg_sw_run_args* a, cudaStream_t st, float* kernel_ms, char* errmsg,
+                       int32_t errmsg_len) {
+  const int npts = a->npts, nlay = a->nlay, nlp1 = nlay + 1;
+  const size_t ld = a->ldim > 0 ? (size_t)a->ldim : (size_t)npts;
+  const int nch = (npts + kSwHostChunk - 1) / kSwHostChunk;
+  std::vector<std::vector<int32_t>> days(nch);
+  for (int p = 0; p < a->nday; ++p) {
+    const int j1 = a->idxday[p], ch = (j1 - 1) / kSwHostChunk;
+    days[ch].push_back(j1 - ch * kSwHostChunk);
+  }
+  rrtmg_sw_run_args d = *a;
+  std::vector<HostField> fl;
+  auto in = [&](const double* const* p, size_t rows) {
+    if (*p) fl.push_back({*p, (void**)const_cast<const double**>(p), rows, 1, 8, false});
+  };
+  const size_t L = nlay, LB = (size_t)nlay * RRTMG_SW_NBANDS;
+  in(&d.plyr, L); in(&d.tlyr, L); in(&d.qlyr, L); in(&d.olyr, L); in(&d.gasvmr_co2, L); in(&d.gasvmr_n2o, L);
+  in(&d.gasvmr_ch4, L); in(&d.gasvmr_o2, L); in(&d.aeraod, LB); in(&d.aerssa, LB); in(&d.aerasy, LB);
+  in(&d.sfcalb_nir_dir, 0); in(&d.sfcalb_nir_dif, 0); in(&d.sfcalb_uvis_dir, 0); in(&d.sfcalb_uvis_dif, 0);
+  in(&d.dzlyr, L); in(&d.delpin, L); in(&d.de_lgth, 0); in(&d.alpha, L); in(&d.cosz, 0); in(&d.cld_cf, L);
+  in(&d.cld_lwp, L); in(&d.cld_ref_liq, L); in(&d.cld_iwp, L); in(&d.cld_ref_ice, L); in(&d.cld_rwp, L);
+  in(&d.cld_ref_rain, L); in(&d.cld_swp, L); in(&d.cld_ref_snow, L); in(&d.cld_od, L); in(&d.cld_ssa, L);
+  in(&d.cld_asy, L);
+  if (d.icseed) fl.push_back({d.icseed, (void**)const_cast<const int32_t**>(&d.icseed), 0, 1, 4, false});
+  d.plvl = d.tlvl = nullptr;   // not read by the shortwave scheme
+  d.gasvmr_co = d.gasvmr_cfc11 = d.gasvmr_cfc12 = d.gasvmr_cfc22 = d.gasvmr_ccl4 = nullptr;
+  auto out = [&](double** p, size_t rows, size_t width) {
+    if (*p) fl.push_back({*p, (void**)p, rows, width, 8, true});
+  };
+  out(&d.hswc, L, 1); out(&d.topflx, 0, 3); out(&d.sfcflx, 0, 4); out(&d.cldtau, L, 1); out(&d.hsw0, L, 1);
+  out(&d.hswb, LB, 1); out(&d.flxprf, nlp1, 4); out(&d.fdncmp, 0, 6);
+  std::vector<size_t> off(fl.size() + 1);
+  size_t per = 0;
+  for (size_t k = 0; k < fl.size(); ++k) {
+    off[k] = per;
+    per += align256(std::max<size_t>(fl[k].rows, 1) * fl[k].width * kSwHostChunk * fl[k].elem);
+  }
+  off[fl.size()] = per;   // the chunk's daytime list
+  per += align256((size_t)kSwHostChunk * 4);
+  CK(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  if (!w->h2d) {
+    CK(cudaStreamCreateWithFlags(&w->h2d, cudaStreamNonBlocking), "cudaStreamCreate");
+    CK(cudaStreamCreateWithFlags(&w->d2h, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (int k = 0; k < 2; ++k) {
+      CK(cudaEventCreateWithFlags(&w->ev_in[k], cudaEventDisableTiming), "cudaEventCreate");
+      CK(cudaEventCreateWithFlags(&w->ev_done[k], cudaEventDisableTiming), "cudaEventCreate");
+      CK(cudaEventCreateWithFlags(&w->ev_out[k], cudaEventDisableTiming), "cudaEventCreate");
+    }
+  }
+  CK(grow(&w->pbuf, &w->pbuf_bytes, 2 * per), "staging allocation");
+  // the kernels' scratch for a whole chunk, allocated before any launch
+  const size_t chunk_cols = std::min<size_t>(kSwHostChunk, kScratchBudget / scratch_per_col(nlay));
+  CK(grow(&w->scratch, &w->scratch_bytes, carve_bytes((int)chunk_cols, nlay)), "scratch allocation");
+  CK(cudaMemsetAsync(w->bad, 0, sizeof(int), st), "cudaMemsetAsync");
+  for (int j = 0; j < nch; ++j) {
+    const int b = j & 1, c0 = j * kSwHostChunk, n = std::min(kSwHostChunk, npts - c0);
+    char* base = w->pbuf + (size_t)b * per;
+    if (j >= 2) CK(cudaStreamWaitEvent(w->h2d, w->ev_done[b], 0), "cudaStreamWaitEvent");
+    for (size_t k = 0; k < fl.size(); ++k) {
+      char* dp = base + off[k];
+      *fl[k].slot = dp;
+      if (fl[k].out) continue;
+      const size_t es = fl[k].elem, wd = fl[k].width;
+      const char* hp = static_cast<const char*>(fl[k].h) + (size_t)c0 * wd * es;
+      if (fl[k].rows == 0)
+        CK(cudaMemcpyAsync(dp, hp, (size_t)n * wd * es, cudaMemcpyHostToDevice, w->h2d), "cudaMemcpyAsync(H2D)");
+      else
+        CK(cudaMemcpy2DAsync(dp, (size_t)n * wd * es, hp, ld * wd * es, (size_t)n * wd * es, fl[k].rows,
+                             cudaMemcpyHostToDevice, w->h2d), "cudaMemcpy2DAsync(H2D)");
+    }
+    int32_t* didx = (int32_t*)(base + off[fl.size()]);
+    if (!days[j].empty())
+      CK(cudaMemcpyAsync(didx, days[j].data(), days[j].size() * 4, cudaMemcpyHostToDevice, w->h2d),
+         "cudaMemcpyAsync(H2D)");
+    CK(cudaEventRecord(w->ev_in[b], w->h2d), "cudaEventRecord");
+    CK(cudaStreamWaitEvent(st, w->ev_in[b], 0), "cudaStreamWaitEvent");
+    if (j >= 2) CK(cudaStreamWaitEvent(st, w->ev_out[b], 0), "cudaStreamWaitEvent");
+    rrtmg_sw_run_args dc = d;
+    dc.npts = n;
+    dc.ldim = n;
+    dc.idxday = didx;
+    dc.nday = (int)days[j].size();
+    sw::SwArgs da = device_args(&dc);
+    da.seed0 = c0;
+    const Sizes z = sizes_of(&dc);
+    int r = run_device(w, da, dc.nday, st, (j == 0) ? kernel_ms : nullptr, errmsg, errmsg_len, z);
+    if (r) return r;
+    CK(cudaEventRecord(w->ev_done[b], st), "cudaEventRecord");
+    CK(cudaStreamWaitEvent(w->d2h, w->ev_done[b], 0), "cudaStreamWaitEvent");
+    for (size_t k = 0; k < fl.size(); ++k) {
+      if (!fl[k].out) continue;
+      const size_t es = fl[k].elem, wd = fl[k].width;
+      char* hp = static_cast<char*>(const_cast<void*>(fl[k].h)) + (size_t)c0 * wd * es;
+      const char* dp = base + off[k];
+      if (fl[k].rows == 0)
+        CK(cudaMemcpyAsync(hp, dp, (size_t)n * wd * es, cudaMemcpyDeviceToHost, w->d2h), "cudaMemcpyAsync(D2H)");
+      else
+        CK(cudaMemcpy2DAsync(hp, ld * wd * es, dp, (size_t)n * wd * es, (size_t)n * wd * es, fl[k].rows,
+                             cudaMemcpyDeviceToHost, w->d2h), "cudaMemcpy2DAsync(D2H)");
+    }
+    CK(cudaEventRecord(w->ev_out[b], w->d2h), "cudaEventRecord");
+  }
+  CK(cudaStreamSynchronize(w->d2h), "kernel execution");
+  return check_bad(w, st, errmsg, errmsg_len);
 }
 
 }  // namespace
@@ -378,6 +505,7 @@ extern "C" int rrtmg_sw_gpu_run_ex(const rrtmg_sw_run_args* a, const rrtmg_sw_ex
   if (!w) return rc;
   cudaStream_t st = x->stream ? (cudaStream_t)x->stream : w->stream;
   const Sizes z = sizes_of(a);
+  CK(cudaMemsetAsync(w->bad, 0, sizeof(int), st), "cudaMemsetAsync");
   if (x->memory == 1) {
     sw::SwArgs d = device_args(a);
     int r = run_device(w, d, a->nday, st, x->kernel_ms, errmsg, errmsg_len, z);
@@ -385,7 +513,8 @@ extern "C" int rrtmg_sw_gpu_run_ex(const rrtmg_sw_run_args* a, const rrtmg_sw_ex
     if (x->sync || x->kernel_ms) return check_bad(w, st, errmsg, errmsg_len);
     return 0;
   }
-  // host arrays: stage every argument in one device buffer
+  if (a->npts >= 2 * kSwHostChunk) return run_host_pipelined(w, a, st, x->kernel_ms, errmsg, errmsg_len);
+  // host arrays of few columns: stage every argument in one device buffer
   rrtmg_sw_run_args da = *a;
   std::vector<std::pair<const double**, size_t>> ins = {
       {&da.plyr, z.n2}, {&da.tlyr, z.n2}, {&da.qlyr, z.n2}, {&da.olyr, z.n2},
@@ -491,6 +620,14 @@ extern "C" void rrtmg_sw_gpu_finalize(void) {
     cudaFree(w->scratch);
     cudaFree(w->stage);
     cudaFree(w->bad);
+    cudaFree(w->pbuf);
+    for (int k = 0; k < 2; ++k) {
+      if (w->ev_in[k]) cudaEventDestroy(w->ev_in[k]);
+      if (w->ev_done[k]) cudaEventDestroy(w->ev_done[k]);
+      if (w->ev_out[k]) cudaEventDestroy(w->ev_out[k]);
+    }
+    if (w->h2d) cudaStreamDestroy(w->h2d);
+    if (w->d2h) cudaStreamDestroy(w->d2h);
     if (w->stream) cudaStreamDestroy(w->stream);
     delete w;
   }

@@ -531,7 +531,7 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
     s.zcf1[pl] = zcf1;
     s.zcf0[pl] = zcf0;
     // McICA seed: ipsdsw0 + i or icseed(i) (RSM:849-857); grid-mean clouds draw none
-    s.seed[pl] = (a.isubcsw == 2) ? a.icseed[i] : 1 + j1;
+    s.seed[pl] = (a.isubcsw == 2) ? a.icseed[i] : 1 + a.seed0 + j1;
   }
   zcf1 = __shfl_sync(0xffffffffu, zcf1, 0);
   for (int k = lane; k < nlay; k += 32) {

@@ -21,6 +21,7 @@ struct SwArgs {
   double *hswc, *topflx, *sfcflx, *cldtau, *hsw0, *hswb, *flxprf, *fdncmp;
   int npts, nlay, ld, top_at_1, inc_minor, iovr, iovr_rand, iovr_maxrand, iswcliq, iswcice, isubcsw, iswmode;
   int gas_only;   // 1: taug/taur/sfluxzen only (stage entry point)
+  int seed0;      // global index of column 1 of these arrays (isubcsw = 1 seeds ipsdsw0 + i)
   double s0fac, heatfac;
 };
 

@@ -238,3 +238,31 @@ def test_sw_leading_dimension(gpu, osw):
     outd = sw.alloc_outputs(ld, nlay, flxprf=True, like=dev["plyr"])
     gpu.rrtmg_sw_run(dev, outd, device_memory=True, ldim=ld)
     _check({k: v.cpu().numpy() for k, v in outd.items()}, ref)
+
+
+def test_sw_host_pipeline(gpu, osw):
+    """Host arrays of >= 8,192 columns take the chunked, double-buffered copy
+    path: same results as the device-resident call, isubcsw = 1 seeds global,
+    daytime points in arbitrary order, and a leading dimension above npts."""
+    import torch
+    npts, ld, nlay = 9000, 9011, 40
+    big = _profile(ld, nlay, 34, night_fraction=0.4, precip=True)
+    prof = dict(big, npts=npts)
+    prof["idxday"] = np.random.default_rng(7).permutation(big["idxday"][big["idxday"] <= npts]).astype(np.int32)
+    for flags in (None, dict(isubcsw=1)):
+        out = sw.alloc_outputs(ld, nlay, hswb=True, flxprf=True)
+        gpu.rrtmg_sw_run(prof, out, flags=flags, ldim=ld)
+        dev = {k: (torch.as_tensor(np.ascontiguousarray(v)).cuda() if isinstance(v, np.ndarray) else v)
+               for k, v in prof.items()}
+        outd = sw.alloc_outputs(ld, nlay, hswb=True, flxprf=True, like=dev["plyr"])
+        gpu.rrtmg_sw_run(dev, outd, flags=flags, device_memory=True, ldim=ld)
+        for k, v in outd.items():
+            assert np.array_equal(out[k], v.cpu().numpy()), k
+    # and the oracle on a sample of those columns
+    sel = prof["idxday"][:64]
+    sub = dict(prof, idxday=sel.astype(np.int32))
+    ref = sw.alloc_outputs(ld, nlay, flxprf=True)
+    assert osw.run(sub, ref, flags=dict(isubcsw=1), ldim=ld)[0] == 0
+    cols = sel - 1
+    for k in ("topflx", "sfcflx"):
+        assert _rel(out[k][cols], ref[k][cols], 1e-300) <= FLUX_RTOL, k
