@@ -412,7 +412,31 @@ def sw_leg(args, torch, timed, sh):
     rc, msg = oracle_sw.run(prof, ref3, flags=dict(iovr=3))
     assert rc == 0, msg
     rel = lambda u, v, f: float(np.max(np.abs(u - v) / np.maximum(np.abs(v), f)))
-    return {"workload": f"sw_c2_allsky_mcica_{n}x127", "steps": k, "value": n * k / (ms / 1e3),
+    # roofline of the dominant (transfer) kernel: counted flops and DRAM bytes per
+    # column from the ncu capture, against the FMA peak measured now and the
+    # measured copy bandwidth
+    roof = None
+    try:
+        tf = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "sw_kernels_traffic.txt")
+        with open(tf) as fh:
+            tr = {kk.strip(): float(v) for kk, v in (l.split(":", 1) for l in fh if ":" in l and not l.startswith("#"))}
+        p64, p32 = C.c_double(0.0), C.c_double(0.0)
+        from ccpp_physics_b200 import rrtmg_lw as lwm
+        lwm.lib().rrtmg_lw_gpu_fma_peak.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        rc_peak = lwm.lib().rrtmg_lw_gpu_fma_peak(C.byref(p64), C.byref(p32))
+        t_rt = km[2] / 1e3
+        ach_tf = tr["sw_fp64_flop_per_column_rt"] * n / t_rt / 1e12
+        ach_gbs = tr["sw_dram_bytes_per_column_rt"] * n / t_rt / 1e9
+        hbm = _peaks()[0]
+        roof = {"kernel": "sw_rt_kernel<false>", "fp64_tflops": ach_tf,
+                "fp64_peak_tflops": p64.value if rc_peak == 0 else None,
+                "fp64_frac": ach_tf / p64.value if rc_peak == 0 and p64.value > 0 else None,
+                "dram_gbs": ach_gbs, "hbm_peak_gbs": hbm, "hbm_frac": ach_gbs / hbm if hbm else None,
+                "source": "per-column flops and DRAM bytes: profiles/sw_kernels_traffic.txt (ncu); kernel time: "
+                          "CUDA events of this run; FP64 peak: FMA-chain kernel in this run"}
+    except Exception as exc:   # report, never fake
+        roof = {"unavailable": str(exc)}
+    return {"workload": f"sw_c2_allsky_mcica_{n}x127", "steps": k, "roofline": roof, "value": n * k / (ms / 1e3),
             "unit": "columns/s", "ms_per_step": ms / k,
             "kernel_ms": {"optics": km[1], "mcica": km[0], "transfer": km[2]},
             "e2e_columns_per_s": n / e2e_s, "e2e_h2d_bytes": h2d, "e2e_d2h_bytes": d2h,
