@@ -1,12 +1,15 @@
 """Column sharding across GPUs (one process per GPU).
 
 RRTMG-LW columns are independent (radlw_main.F90:782 loops over columns with
-no exchange), so a multi-GPU run gives each rank whole physics blocks of
-consecutive columns and needs no collective on the data path.  The only
+no exchange), and so are RRTMG-SW's daytime points (radsw_main.F90:892), so
+a multi-GPU run gives each rank whole physics blocks of consecutive columns
+and needs no collective on the data path.  The only
 collective a run makes is the reduction of per-rank timings (max over ranks)
 outside the timed region.
 """
 from __future__ import annotations
+
+import numpy as np
 
 
 def column_range(total: int, rank: int, world: int) -> tuple[int, int]:
@@ -36,3 +39,11 @@ def block_range(block_sizes, rank: int, world: int) -> tuple[int, int]:
         cuts.append(len(block_sizes))
     cuts[world] = len(block_sizes)
     return cuts[rank], cuts[rank + 1]
+
+
+def daytime_points(idxday, start: int, stop: int) -> np.ndarray:
+    """The daytime points of rrtmg_sw_run (idxday: 1-based column indices,
+    any order) that fall in the shard of columns [start, stop), renumbered
+    within the shard and kept in their order."""
+    idx = np.asarray(idxday, dtype=np.int64)
+    return (idx[(idx > start) & (idx <= stop)] - start).astype(np.int32)

@@ -94,3 +94,66 @@ def test_two_rank_shards_equal_single_run(oracle_lib):
     rc, msg, ref = oracle_lib.rrtmg_lw_run(prof, nthreads=1)
     assert rc == 0, msg
     assert np.array_equal(full, ref["topflx"])
+
+
+def _sw_rank(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from ccpp_physics_b200 import rrtmg_sw as sw
+        from oracle import oracle_sw
+        oracle_sw.rswinit()
+        a, b = shard.column_range(NCOLS, rank, world)
+        prof = sw.add_sw_inputs(synthetic.make_profiles(b - a, NLAY, seed=21, col_offset=a), seed=21, col_offset=a,
+                                night_fraction=0.3)
+        out = sw.alloc_outputs(b - a, NLAY)
+        rc, msg = oracle_sw.run(prof, out, nthreads=1)
+        assert rc == 0, msg
+        mx = -(-NCOLS // world)
+        top = torch.zeros(mx, 3, dtype=torch.float64)
+        top[: b - a] = torch.from_numpy(np.ascontiguousarray(out["topflx"]))
+        parts = [torch.zeros_like(top) for _ in range(world)]
+        dist.all_gather(parts, top)
+        days = torch.zeros(mx, dtype=torch.int64)
+        days[: len(prof["idxday"])] = torch.from_numpy(prof["idxday"].astype(np.int64))
+        dparts = [torch.zeros_like(days) for _ in range(world)]
+        dist.all_gather(dparts, days)
+        if rank == 0:
+            sizes = [shard.column_range(NCOLS, r, world) for r in range(world)]
+            full = np.concatenate([parts[r][: e - s].numpy() for r, (s, e) in enumerate(sizes)])
+            q.put((full, [dparts[r].numpy() for r in range(world)]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(240)
+def test_two_rank_sw_shards_equal_single_run():
+    """rrtmg_sw_run sharded by columns over two gloo ranks (isubcsw=2 seeds are
+    per column, so they follow the columns) equals one run over all columns,
+    and each rank's daytime points are the global ones split by
+    shard.daytime_points."""
+    from ccpp_physics_b200 import rrtmg_sw as sw
+    from oracle import oracle_sw
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_sw_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    full, dparts = q.get(timeout=200)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    oracle_sw.rswinit()
+    prof = sw.add_sw_inputs(synthetic.make_profiles(NCOLS, NLAY, seed=21), seed=21, night_fraction=0.3)
+    ref = sw.alloc_outputs(NCOLS, NLAY)
+    rc, msg = oracle_sw.run(prof, ref, nthreads=1)
+    assert rc == 0, msg
+    assert np.array_equal(full, ref["topflx"])
+    for r in range(world):
+        a, b = shard.column_range(NCOLS, r, world)
+        want = shard.daytime_points(prof["idxday"], a, b)
+        assert np.array_equal(dparts[r][: len(want)], want)
