@@ -280,7 +280,7 @@ constexpr int kMcicaWarps = 6;   // 6 warps x 18.5 KB (127 layers): two CTAs, tw
 // NG g-points per column: 140 for the longwave path (every overlap, block or
 // stage inputs), 112 for the shortwave path (stage inputs, iovr 0..2: the
 // shortwave decorrelation-length and exponential overlaps draw in another
-// order, radsw_main.F90:2104-2190, and are not built here).
+// order, radsw_main.F90:2101-2198, and are not built here).
 template <int NG>
 __global__ void __launch_bounds__(32 * kMcicaWarps)
 lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int ncols, McicaArgs a,
@@ -615,7 +615,7 @@ cudaError_t mcica_launch(const Block* blocks, int nblocks, const Block& b0, int 
 }
 
 // Shortwave sub-columns with decorrelation-length (iovr 3) or exponential /
-// exponential-random (iovr 4, 5) overlap (radsw_main.F90:2104-2190).  Both
+// exponential-random (iovr 4, 5) overlap (radsw_main.F90:2101-2198).  Both
 // random sets are g-major, set 1 = draws [0, 112 nlay) and set 2 = draws
 // [112 nlay, 224 nlay) of one stream, cdfunc(k, n) = draw (n-1) nlay + k.
 // Set 2 is read from a second sequence ring that runs 112 nlay draws ahead
@@ -750,7 +750,7 @@ cudaError_t mcica_sw_two_set_launch(int ncols, int nlay, int iovr, const McicaSt
 // (random), 1 (maximum-random) and 2 (maximum): the draws are g-major,
 // rand2d((n-1)*nlay + k) as in the longwave generator, over 112 g-points.
 // stage.cldf is the layer cloud fraction floored at ftiny = 1e-12
-// (radsw_main.F90:1900-1903), internal (surface-first) order.
+// (radsw_main.F90:1904-1908), internal (surface-first) order.
 cudaError_t mcica_sw_launch(int ncols, int nlay, int iovr, const McicaStage& stage, uint32_t* bits, int num_sms,
                             cudaStream_t st) {
   if (iovr < 0 || iovr > 2) return cudaErrorInvalidValue;

@@ -29,7 +29,7 @@ extern "C" const unsigned char rrtmg_sw_tables_blob_end[];
 namespace {
 
 constexpr int kNtbmx = 10000;
-constexpr double kS0 = 1368.22;                  // RSM:332
+constexpr double kS0 = 1368.22;                  // RSM:343
 constexpr size_t kScratchBudget = (size_t)12 << 30;   // 16,384 columns of 127 layers in one chunk
 
 struct SwState {
@@ -159,8 +159,8 @@ Sizes sizes_of(const rrtmg_sw_run_args* a) {
 // 0 = run, -1 = nothing to do, 1 = error
 int validate(const rrtmg_sw_run_args* a, const rrtmg_sw_exec* x, char* errmsg, int32_t errmsg_len) {
   if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_run: null argument struct"); return 1; }
-  if (!a->lsswr || a->nday <= 0) return -1;                 // RSM:785-787
-  if (a->iswcliq > 0) {                                      // RSM:815-828
+  if (!a->lsswr || a->nday <= 0) return -1;                 // RSM:808-809
+  if (a->iswcliq > 0) {                                      // RSM:847-870
     if (!a->cld_lwp || !a->cld_ref_liq || !a->cld_iwp || !a->cld_ref_ice || !a->cld_rwp || !a->cld_ref_rain ||
         !a->cld_swp || !a->cld_ref_snow) {
       set_msg(errmsg, errmsg_len,
@@ -168,7 +168,7 @@ int validate(const rrtmg_sw_run_args* a, const rrtmg_sw_exec* x, char* errmsg, i
               "cld_lwp, cld_ref_liq, cld_iwp, cld_ref_ice, cld_rwp, cld_ref_rain, cld_swp, cld_ref_snow");
       return 1;
     }
-  } else if (!a->cld_od || !a->cld_ssa || !a->cld_asy) {     // RSM:829-838
+  } else if (!a->cld_od || !a->cld_ssa || !a->cld_asy) {     // RSM:847-870
     set_msg(errmsg, errmsg_len,
             "Logic error: iswcliq<=0 requires the following optional arguments to be present: cld_od, cld_ssa, cld_asy");
     return 1;
@@ -233,12 +233,12 @@ sw::SwArgs device_args(const rrtmg_sw_run_args* a) {
   d.top_at_1 = a->top_at_1; d.inc_minor = a->inc_minor_gas; d.iovr = a->iovr;
   d.iovr_rand = a->iovr_rand; d.iovr_maxrand = a->iovr_maxrand;
   d.iswcliq = a->iswcliq; d.iswcice = a->iswcice; d.isubcsw = a->isubcsw; d.iswmode = a->iswmode;
-  d.s0fac = a->solcon / kS0;   // RSM:793
+  d.s0fac = a->solcon / kS0;   // RSM:820
   d.heatfac = g.heatfac;
   return d;
 }
 
-// zero every output of every column (RSM:795-813); device pointers
+// zero every output of every column (RSM:824-845); device pointers
 cudaError_t zero_outputs(const sw::SwArgs& d, const Sizes& z, int nlay, cudaStream_t st) {
   const size_t pitch = (size_t)d.ld * 8, width = (size_t)d.npts * 8;
   cudaError_t e = cudaMemset2DAsync(d.hswc, pitch, 0, width, nlay, st);
@@ -439,11 +439,11 @@ extern "C" int rrtmg_sw_gpu_init(const rrtmg_sw_init_args* a, char* errmsg, int3
   if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_init: null argument struct"); return 1; }
   int errflg = 0;
   if (a->iovr != a->iovr_rand && a->iovr != a->iovr_maxrand && a->iovr != a->iovr_max &&
-      a->iovr != a->iovr_dcorr && a->iovr != a->iovr_exp && a->iovr != a->iovr_exprand) {   // RSM:1450-1455
+      a->iovr != a->iovr_dcorr && a->iovr != a->iovr_exp && a->iovr != a->iovr_exprand) {   // RSM:1466-1471
     errflg = 1;
     set_msg(errmsg, errmsg_len, "ERROR(rswinit): Error in specification of cloud overlap flag");
   }
-  if (a->me == 0) {   // RSM:1457-1487
+  if (a->me == 0) {   // RSM:1473-1503
     std::printf(" - Using AER Shortwave Radiation, Version: NCEP SW v5.1  Nov 2012 -RRTMG-SW v3.8   \n");
     if (a->iswmode == 1) std::printf("   --- Delta-eddington 2-stream transfer scheme\n");
     else if (a->iswmode == 2) std::printf("   --- PIFM 2-stream transfer scheme\n");
@@ -455,8 +455,8 @@ extern "C" int rrtmg_sw_gpu_init(const rrtmg_sw_init_args* a, char* errmsg, int3
     else if (a->isubcsw == 2) std::printf("   --- Using MCICA sub-colum clouds approximation with provided input array of permutation seeds\n");
   }
   std::lock_guard<std::mutex> lk(g_mu);
-  g.heatfac = (a->rad_hr_units == 1) ? 9.80665 * 864.0 / 1.0046e+3 : 9.80665 * 1.0e-2 / 1.0046e+3;   // RSM:1491-1495
-  // exp_tbl (RSM:1516-1531), on the host with the C library's exp
+  g.heatfac = (a->rad_hr_units == 1) ? 9.80665 * 864.0 / 1.0046e+3 : 9.80665 * 1.0e-2 / 1.0046e+3;   // RSM:1507-1511
+  // exp_tbl (RSM:1521-1531), on the host with the C library's exp
   std::vector<double> et(kNtbmx + 1);
   const double bpade = 1.0 / 0.278;
   et[0] = 1.0;

@@ -4,15 +4,15 @@
 // for the McICA configurations runs as three launches over a chunk of
 // daytime columns:
 //   sw_optics_kernel  one warp per column, lanes over layers: the driver's
-//                     layer prologue (RSM:1016-1099), setcoef (RSM:2242-2389),
+//                     layer prologue (RSM:910-1094), setcoef (RSM:2242-2389),
 //                     taumol16..29 (RSM:4094-5573; every lane runs the same
 //                     band's code, so the band branches never diverge),
 //                     the solar source sfluxzen, the clear/cloudy column test
-//                     (RSM:1100-1124) and cldprop (RSM:1566-1938);
+//                     (RSM:1101-1125) and cldprop (RSM:1566-1938);
 //   lw_mcica_kernel<112>  the sub-column generator (lw_mcica.cu);
 //   sw_rt_kernel      one warp per column, lanes over g-points: spcvrtm
 //                     (RSM:3228-3942) with vrtqdr (RSM:3959-4051) and the
-//                     flux / heating-rate outputs (RSM:1180-1376).
+//                     flux / heating-rate outputs (RSM:1225-1373).
 // Per lane (g-point) the clear-sky and all-sky sweeps run side by side: the
 // upward sweep evaluates each layer's clear two-stream optics once (the
 // all-sky sweep re-evaluates only the layers whose McICA flag is set) and
@@ -34,10 +34,10 @@ namespace sw {
 
 __constant__ int c_ng[14] = {6, 12, 8, 8, 10, 10, 2, 10, 8, 6, 6, 8, 6, 12};   // radsw_param.f NG16..29
 __constant__ int c_ns[14] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94, 100};
-__constant__ int c_nspa[14] = {9, 9, 9, 9, 1, 9, 9, 1, 9, 1, 0, 1, 9, 1};      // RSM:370
-__constant__ int c_nspb[14] = {1, 5, 1, 1, 1, 5, 1, 0, 1, 0, 0, 1, 5, 1};      // RSM:371
-__constant__ int c_idxsfc[14] = {1, 1, 1, 1, 1, 1, 1, 1, 0, 2, 2, 2, 2, 1};    // RSM:374
-__constant__ int c_idxebc[14] = {5, 5, 4, 4, 3, 3, 2, 2, 1, 1, 1, 1, 1, 5};    // RSM:375
+__constant__ int c_nspa[14] = {9, 9, 9, 9, 1, 9, 9, 1, 9, 1, 0, 1, 9, 1};      // RSM:359
+__constant__ int c_nspb[14] = {1, 5, 1, 1, 1, 5, 1, 0, 1, 0, 0, 1, 5, 1};      // RSM:360
+__constant__ int c_idxsfc[14] = {1, 1, 1, 1, 1, 1, 1, 1, 0, 2, 2, 2, 2, 1};    // RSM:362
+__constant__ int c_idxebc[14] = {5, 5, 4, 4, 3, 3, 2, 2, 1, 1, 1, 1, 1, 5};    // RSM:363
 
 constexpr double kEps = 1.0e-6, kOneMinus = 1.0 - kEps, kBpade = 1.0 / 0.278, kStpfac = 296.0 / 1013.0;
 constexpr double kFtiny = 1.0e-12, kFlimit = 1.0e-20;
@@ -61,7 +61,7 @@ struct Lay {
   bool lower_plog;   // plog > 4.56
 };
 
-// rrtmg_sw_run's layer prologue (RSM:1016-1050 / 1057-1090) for internal
+// rrtmg_sw_run's layer prologue (RSM:910-946 / 1001-1040) for internal
 // layer k (0-based, surface first) of caller column i, then setcoef.
 __device__ void layer_record(const SwArgs& a, int i, int k, const double* __restrict__ T, Lay& L) {
   const int r = a.top_at_1 ? a.nlay - 1 - k : k;
@@ -138,7 +138,7 @@ __device__ __forceinline__ double k8(const Tab& t, const double (&f)[8], int i01
 __device__ __forceinline__ double k4(const Tab& t, const Lay& L, int i01, int i11, int j) {
   return L.fac00 * t(i01, j) + L.fac10 * t(i01 + 1, j) + L.fac01 * t(i11, j) + L.fac11 * t(i11 + 1, j);
 }
-// speccomb/specmult/js/fs and the eight weights (RSM:4368-4383)
+// speccomb/specmult/js/fs and the eight weights (RSM:4386-4399)
 __device__ __forceinline__ double spec8(const Lay& L, int g1, int g2, double strrat, double mult, int& js, double& fs,
                                         double (&f)[8]) {
   const double speccomb = L.colamt[g1] + strrat * L.colamt[g2];
@@ -320,7 +320,7 @@ __device__ void taumol_layer(const Lay& L, bool lower, const int id0[14], const 
   }
 }
 
-// ---- cldprop for one layer (RSM:1595-1903) --------------------------------
+// ---- cldprop for one layer (RSM:1687-1903) --------------------------------
 __device__ void cloud_layer(const SwArgs& a, size_t x, const double* __restrict__ T, double* __restrict__ tw,
                             double* __restrict__ sw, double* __restrict__ gw) {
   double tauliq[14], ssaliq[14], asyliq[14], tauice[14], ssaice[14], asyice[14];
@@ -431,7 +431,7 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
     return;
   }
   const int i = j1 - 1, nlay = a.nlay;
-  // laytrop: the last layer with ln p > 4.56, nlay if none (RSM:2262, 2297)
+  // laytrop: the last layer with ln p > 4.56, nlay if none (RSM:2305, 2353)
   int laytrop = 0;
   for (int k0 = 0; k0 < nlay; k0 += 32) {
     const int k = k0 + lane;
@@ -469,7 +469,7 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
     taumol_layer(L, lower, id0, id1, T, tg, tr);
   }
 
-  // solar source per band (RSM:4119-4188), one band per lane
+  // solar source per band (RSM:4225-4310), one band per lane
   if (lane < 14) {
     const int b = lane, jb = 16 + b, ng = c_ng[b], ns = c_ns[b];
     const int ibd = (int)T[swtab::ibx + b];
@@ -508,7 +508,7 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
   }
 
   if (a.gas_only) return;
-  // clear / cloudy column (RSM:1100-1124), in layer order on lane 0
+  // clear / cloudy column (RSM:1101-1125), in layer order on lane 0
   double zcf1 = 0.0;
   if (lane == 0) {
     double zcf0 = 1.0, z1 = 1.0;
@@ -530,7 +530,7 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
     zcf1 = 1.0 - zcf0;
     s.zcf1[pl] = zcf1;
     s.zcf0[pl] = zcf0;
-    // McICA seed: ipsdsw0 + i or icseed(i) (RSM:849-857); grid-mean clouds draw none
+    // McICA seed: ipsdsw0 + i or icseed(i) (RSM:875-883); grid-mean clouds draw none
     s.seed[pl] = (a.isubcsw == 2) ? a.icseed[i] : 1 + a.seed0 + j1;
   }
   zcf1 = __shfl_sync(0xffffffffu, zcf1, 0);
@@ -538,7 +538,7 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
     const int r = a.top_at_1 ? nlay - 1 - k : k;
     const size_t x = (size_t)i + (size_t)a.ld * r;
     const double cf = a.cf[x];
-    s.cldf[(size_t)pl + (size_t)nc * k] = (cf < kFtiny) ? 0.0 : cf;   // mcica_subcol input (RSM:1900-1903)
+    s.cldf[(size_t)pl + (size_t)nc * k] = (cf < kFtiny) ? 0.0 : cf;   // mcica_subcol input (RSM:1904-1908)
     if (a.isubcsw <= 0) {   // grid-mean clouds: cldfrc = cfrac / cf1 (RSM:1930-1934)
       s.aux[(size_t)pl + (size_t)nc * k] = (zcf1 > 0.0) ? cf / zcf1 : 0.0;
     } else if (a.iovr == 3) {   // fac_lcf between layers k-1 and k (RSM:2106-2108), dz in internal order
@@ -548,7 +548,7 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
         f = exp(-0.5 * (a.dz[x] + a.dz[(size_t)i + (size_t)a.ld * r1]) / a.delg[i]);
       }
       s.aux[(size_t)pl + (size_t)nc * k] = f;
-    } else if (a.iovr == 4 || a.iovr == 5) {   // alpha, in the caller's row order (RSM:889, 990)
+    } else if (a.iovr == 4 || a.iovr == 5) {   // alpha, in the caller's row order (RSM:921, 1012)
       s.aux[(size_t)pl + (size_t)nc * k] = a.alpha[(size_t)i + (size_t)a.ld * k];
     }
     if (zcf1 > 0.0) {
@@ -556,7 +556,7 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
       double* sw = s.ssacw + ((size_t)pl * nlay + k) * 14;
       double* gw = s.asycw + ((size_t)pl * nlay + k) * 14;
       cloud_layer(a, x, T, tw, sw, gw);
-      a.cldtau[x] = tw[9];   // band 25 (RSM:1128-1137)
+      a.cldtau[x] = tw[9];   // band 25 (RSM:1144-1152)
     }
   }
 }
@@ -568,13 +568,13 @@ struct LayOpt {
 
 __device__ __forceinline__ double exp_tab(const double* __restrict__ ET, double z) {
   // itind = ftind*NTBMX + 0.5 with truncation; ftind in [0, 1) so the
-  // clamped form of RSM:3588-3590 selects the same entry
+  // clamped form of RSM:3601-3602 selects the same entry
   const double ftind = z / (kBpade + z);
   return __ldg(ET + (int)(ftind * kNtbmx + 0.5));
 }
 __device__ __forceinline__ double exp_small(double z) { return 1.0 - z + 0.5 * z * z; }
 
-// the two-stream layer reflectance / transmittance of spcvrtm (RSM:3340-3440)
+// the two-stream layer reflectance / transmittance of spcvrtm (RSM:3447-3600)
 __device__ __forceinline__ void two_stream(double ztau0, double zssa0, double zasy0, double cosz, double sntz,
                                            int iswmode, const double* __restrict__ ET, LayOpt& o) {
   const double zcrit = 0.9999995, od_lo = 0.06, eps1 = 1.0e-8;
@@ -671,7 +671,7 @@ struct ColIn {
 };
 
 __device__ __forceinline__ bool cloud_bit(const ColIn& c, int k) { return (c.bits[k >> 5] >> (k & 31)) & 1u; }
-// the all-sky sweep treats layer k as cloudy: its McICA flag, or cldfrc > ftiny (RSM:2919)
+// the all-sky sweep treats layer k as cloudy: its McICA flag, or cldfrc > ftiny (RSM:2885)
 template <bool GRID>
 __device__ __forceinline__ bool cloudy_layer(const ColIn& c, int k) {
   return GRID ? (c.cfr[(size_t)k * c.cfs] > kFtiny) : cloud_bit(c, k);
@@ -710,7 +710,7 @@ __device__ __forceinline__ void layer_in(const ColIn& c, int g, int b, int k, bo
     v.gcw = c.gcw[(size_t)k * 14 + b];
   }
 }
-// the layer's two-stream optics (RSM:3330-3336 clear, 3495-3501 cloudy)
+// the layer's two-stream optics (RSM:3447-3449 clear, 3678-3680 cloudy)
 __device__ __forceinline__ void layer_opt(const ColIn& c, const LayIn& v, const double* __restrict__ ET, LayOpt& o) {
   double ztau0 = fmax(kFtiny, v.tr + v.tg + v.tae);
   double zssa0 = v.tr + v.tae * v.sae;
@@ -791,11 +791,11 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
     const double refb1 = ibd ? albbm[ibd - 1] : 0.5 * (albbm[0] + albbm[1]);
     const double refd1 = ibd ? albdf[ibd - 1] : 0.5 * (albdf[0] + albdf[1]);
     // The clear-sky sweep and, in a cloudy column, the all-sky sweep of
-    // spcvrtm (RSM:3318-3668, 3680-3920) run side by side: a layer's clear
+    // spcvrtm (RSM:3444-3667, 3668-3893) run side by side: a layer's clear
     // optics are evaluated once and serve both, and the all-sky sweep
     // re-evaluates only the layers its sub-column flags cloudy, as spcvrtm
-    // keeps the clear-pass arrays for clear layers (RSM:3755-3760).
-    // upward adding (vrtqdr, RSM:3990-3999)
+    // keeps the clear-pass arrays for clear layers (RSM:3849-3850).
+    // upward adding (vrtqdr, RSM:4011-4020)
     double ub = refb1, ud = refd1, ubw = refb1, udw = refd1;
     st8(0, 6, ub);
     st8(0, 7, ud);
@@ -837,7 +837,7 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
         st8(k + 1, 9, udw);
       }
     }
-    // downward sweep (RSM:4001-4017) with the fluxes of each level (RSM:4019-4026)
+    // downward sweep (RSM:4026-4040) with the fluxes of each level (RSM:4041-4046)
     auto fetch = [&](int m, LayOpt& o, LayOpt& w) {
       o.rb = ld8(m, 0); o.rd = ld8(m, 1); o.tb = ld8(m, 2); o.td = ld8(m, 3); o.e3 = ld8(m, 4); o.e4 = ld8(m, 5);
       w = o;
@@ -911,7 +911,7 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
         }
       }
     }
-    // surface direct / diffuse partition (RSM:3625-3640) and UV-B (RSM:3925)
+    // surface direct / diffuse partition (RSM:3641-3655) and UV-B (RSM:3907)
     for (int pass = 0; pass < (cloudy ? 2 : 1); ++pass) {
       const double t0 = pass ? tdbt0w : tdbt0, f0 = pass ? fd0w : fd0;
       const double zb1 = wgt * t0, zb2 = wgt * (f0 - t0);
@@ -936,7 +936,7 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
     __syncwarp();
   }
 
-  // outputs (RSM:1180-1376)
+  // outputs (RSM:1225-1373)
   const int ld = a.ld;
   const double* fu_t = cloudy ? upc : up0;
   const double* fd_t = cloudy ? dnc : dn0;

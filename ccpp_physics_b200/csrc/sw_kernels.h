@@ -33,7 +33,7 @@ struct SwScratch {
   double* cldf;                      // [pl + nc*k], floored cloud fraction (McICA input)
   double* aux;                       // [pl + nc*k], fac_lcf (iovr 3) or alpha (iovr 4, 5); cldfrc (isubcsw 0)
   int32_t* seed;                     // [pl]
-  double *zcf1, *zcf0;               // [pl] cloudy / clear column fractions (RSM:1100-1124)
+  double *zcf1, *zcf0;               // [pl] cloudy / clear column fractions (RSM:1101-1125)
   uint32_t* bits;                    // [pl][112][nw] McICA cloudy flags
   double* lane_store;                // [pl][k][10][32] the transfer's per-lane layer optics and recurrences
   int nw;

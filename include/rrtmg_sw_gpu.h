@@ -7,7 +7,7 @@
  *
  *   rswinit       physics/Radiation/RRTMG/radsw_main.F90:1388-1390
  *   rrtmg_sw_run  physics/Radiation/RRTMG/radsw_main.F90:493-510
- *                 (argument declarations radsw_main.F90:515-600)
+ *                 (argument declarations radsw_main.F90:688-782)
  *
  * Array conventions are those of rrtmg_lw_gpu.h: the caller's Fortran arrays,
  * column-major, real(8); element (i, k) of an (npts, nlay) array is at
@@ -106,7 +106,7 @@ typedef struct rrtmg_sw_exec {
 } rrtmg_sw_exec;
 
 /* rswinit (radsw_main.F90:1388): validates iovr, sets heatfac, builds the
- * exp_tbl transmittance table (radsw_main.F90:1516-1531) and uploads every
+ * exp_tbl transmittance table (radsw_main.F90:1521-1531) and uploads every
  * coefficient table to the device.  Returns errflg. */
 int rrtmg_sw_gpu_init(const rrtmg_sw_init_args *args, char *errmsg,
                       int32_t errmsg_len);

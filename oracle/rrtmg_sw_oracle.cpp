@@ -45,7 +45,7 @@
 
 namespace {
 
-// ---- constants (RSM:326-340; physcons.F90) --------------------------------
+// ---- constants (RSM:335-350; physcons.F90) --------------------------------
 const double con_g = 9.80665, con_cp = 1.0046e+3, con_avgd = 6.0221415e23;
 const double con_amd = 28.9644, con_amw = 18.0154, con_amo3 = 47.9982;
 const double eps = 1.0e-6, oneminus = 1.0 - eps, bpade = 1.0 / 0.278;
@@ -55,10 +55,10 @@ const double amdw = con_amd / con_amw, amdo3 = con_amd / con_amo3;
 
 const int NBLOW = 16, NBHGH = 29, NBDSW = 14, NGPT = 112, NTBMX = 10000;
 const int NG[14] = {6, 12, 8, 8, 10, 10, 2, 10, 8, 6, 6, 8, 6, 12};     // radsw_param.f NG16..NG29
-const int NSPA[14] = {9, 9, 9, 9, 1, 9, 9, 1, 9, 1, 0, 1, 9, 1};       // RSM:370
-const int NSPB[14] = {1, 5, 1, 1, 1, 5, 1, 0, 1, 0, 0, 1, 5, 1};       // RSM:371
-const int IDXSFC[14] = {1, 1, 1, 1, 1, 1, 1, 1, 0, 2, 2, 2, 2, 1};     // RSM:374
-const int IDXEBC[14] = {5, 5, 4, 4, 3, 3, 2, 2, 1, 1, 1, 1, 1, 5};     // RSM:375
+const int NSPA[14] = {9, 9, 9, 9, 1, 9, 9, 1, 9, 1, 0, 1, 9, 1};       // RSM:359
+const int NSPB[14] = {1, 5, 1, 1, 1, 5, 1, 0, 1, 0, 0, 1, 5, 1};       // RSM:360
+const int IDXSFC[14] = {1, 1, 1, 1, 1, 1, 1, 1, 0, 2, 2, 2, 2, 1};     // RSM:362
+const int IDXEBC[14] = {5, 5, 4, 4, 3, 3, 2, 2, 1, 1, 1, 1, 1, 5};     // RSM:363
 const int MFR[14] = {3, 4, 3, 3, 4, 4, 3, 3, 3, 0, 0, 0, 0, 4};        // forref rows per band
 const int NUVB = 27;
 
@@ -708,7 +708,7 @@ inline double exp_lookup_clamp(double zr) {     // itind = max(0, min(NTBMX, int
 }
 
 // One layer's two-stream reflectance/transmittance (the body shared by the
-// clear and cloudy sweeps of spcvrtm, RSM:3340-3440 and 3494-3620).
+// clear and cloudy sweeps of spcvrtm, RSM:3444-3624 and 3674-3853).
 void two_stream(double ztau0, double zssa0, double zasy0, double cosz, double sntz, int iswmode, double& zrefb,
                 double& ztrab, double& zrefd, double& ztrad, double& ztau1_out) {
   const double zcrit = 0.9999995, zsr3 = std::sqrt(3.0), od_lo = 0.06, eps1 = 1.0e-8;
@@ -968,7 +968,7 @@ void spcvrtm(Col& c, double ssolar, double cosz, double sntz, const double albbm
   }
 }
 
-// Column prologue of rrtmg_sw_run (RSM:866-1099): internal surface-first arrays.
+// Column prologue of rrtmg_sw_run (RSM:892-1094): internal surface-first arrays.
 void load_column(const rrtmg_sw_run_args& a, int j1, Col& c) {
   const int nlay = a.nlay, nlp1 = a.nlp1;
   const long ld = a.ldim > 0 ? a.ldim : a.npts;
@@ -981,7 +981,7 @@ void load_column(const rrtmg_sw_run_args& a, int j1, Col& c) {
     c.tavel[k] = A2(a.tlyr, kk);
     c.delp[k] = A2(a.delpin, kk);
     c.dz[k] = A2(a.dzlyr, kk);
-    if (a.iovr == a.iovr_exp || a.iovr == a.iovr_exprand) c.alph[k] = A2(a.alpha, k);   // unflipped (RSM:889, 990)
+    if (a.iovr == a.iovr_exp || a.iovr == a.iovr_exprand) c.alph[k] = A2(a.alpha, k);   // unflipped (RSM:921, 1012)
     c.h2ovmr[k] = std::max(f_zero, A2(a.qlyr, kk) * amdw / (f_one - A2(a.qlyr, kk)));
     c.o3vmr[k] = std::max(f_zero, A2(a.olyr, kk) * amdo3);
     const double tem0 = (f_one - c.h2ovmr[k]) * con_amd + c.h2ovmr[k] * con_amw;
@@ -1030,7 +1030,7 @@ void run_column(const rrtmg_sw_run_args& a, int ipt, Col& c) {
   const int nlay = a.nlay, nlp1 = a.nlp1;
   const long ld = a.ldim > 0 ? a.ldim : a.npts;
   const int j1 = a.idxday[ipt - 1];
-  const int ipseed = (a.isubcsw == 2) ? a.icseed[j1 - 1] : 1 + j1;   // ipsdsw0 + i (RSM:849-857)
+  const int ipseed = (a.isubcsw == 2) ? a.icseed[j1 - 1] : 1 + j1;   // ipsdsw0 + i (RSM:875-883)
   const double cosz1 = a.cosz[j1 - 1];
   const double sntz1 = f_one / a.cosz[j1 - 1];
   const double ssolar = (a.solcon / s0) * a.cosz[j1 - 1];
@@ -1039,7 +1039,7 @@ void run_column(const rrtmg_sw_run_args& a, int ipt, Col& c) {
   const double albdf[2] = {a.sfcalb_nir_dif[j1 - 1], a.sfcalb_uvis_dif[j1 - 1]};
   load_column(a, j1, c);
 
-  // clear/cloudy column indicator (RSM:1100-1124)
+  // clear/cloudy column indicator (RSM:1101-1125)
   double zcf0 = f_one, zcf1 = f_one;
   if (a.iovr == a.iovr_rand) {
     for (int k = 1; k <= nlay; ++k) zcf0 = zcf0 * (f_one - c.cfrac[k]);
