@@ -613,6 +613,39 @@ extern "C" int rrtmg_sw_gpu_gas_optics(const rrtmg_sw_run_args* a, double* taug,
   return check_bad(w, st, errmsg, errmsg_len);
 }
 
+extern "C" int rrtmg_sw_gpu_mcica(int32_t npts, int32_t nlay, int32_t ldim, int32_t iovr, const int32_t* seed,
+                                  const double* cldf, const double* dz, const double* de_lgth, const double* alpha,
+                                  uint32_t* bits, void* stream, char* errmsg, int32_t errmsg_len) {
+  set_msg(errmsg, errmsg_len, "");
+  if (!g.ready) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: rrtmg_sw_gpu_init has not been called"); return 1; }
+  const int ld = ldim > 0 ? ldim : npts;
+  if (npts < 1 || nlay < 1 || nlay > sw::kSwMaxLay || ld < npts || iovr < 0 || iovr > 5 || !seed || !cldf || !bits ||
+      (iovr == 3 && (!dz || !de_lgth)) || ((iovr == 4 || iovr == 5) && !alpha)) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_mcica: bad arguments");
+    return 1;
+  }
+  CK(cudaSetDevice(g.device), "cudaSetDevice");
+  int rc = 0;
+  SwWorkspace* w = workspace(errmsg, errmsg_len, &rc);
+  if (!w) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : w->stream;
+  lw::McicaStage ms;
+  ms.cldf = cldf;
+  ms.seed = seed;
+  ms.ld = ld;
+  if (iovr >= 3) {
+    CK(grow(&w->scratch, &w->scratch_bytes, (size_t)ld * nlay * 8), "scratch allocation");
+    double* aux = (double*)w->scratch;
+    CK(sw::overlap_aux_launch(npts, nlay, ld, iovr, dz, de_lgth, alpha, aux, ld, st), "overlap kernel launch");
+    ms.alpha = aux;
+    CK(lw::mcica_sw_two_set_launch(npts, nlay, iovr, ms, bits, g.num_sms, st), "McICA kernel launch");
+  } else {
+    CK(lw::mcica_sw_launch(npts, nlay, iovr, ms, bits, g.num_sms, st), "McICA kernel launch");
+  }
+  CK(cudaStreamSynchronize(st), "McICA kernel execution");
+  return 0;
+}
+
 extern "C" void rrtmg_sw_gpu_finalize(void) {
   std::lock_guard<std::mutex> lk(g_mu);
   for (SwWorkspace* w : g_ws) {

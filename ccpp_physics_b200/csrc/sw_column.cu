@@ -986,6 +986,31 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
   }
 }
 
+// The per-layer overlap parameter of the sub-column generator for the stage
+// entry point: fac_lcf between layers k-1 and k (iovr 3, RSM:2106-2108) or
+// alpha (iovr 4, 5), [c + ldo*k]; inputs [c + ld*k], internal layer order.
+__global__ void sw_overlap_aux_kernel(int ncols, int nlay, int ld, int iovr, const double* __restrict__ dz,
+                                      const double* __restrict__ delg, const double* __restrict__ alpha,
+                                      double* __restrict__ aux, int ldo) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)ncols * nlay) return;
+  const int c = (int)(t % ncols), k = (int)(t / ncols);
+  double v;
+  if (iovr == 3)
+    v = (k > 0) ? exp(-0.5 * (dz[c + (size_t)ld * k] + dz[c + (size_t)ld * (k - 1)]) / delg[c]) : 0.0;
+  else
+    v = alpha[c + (size_t)ld * k];
+  aux[c + (size_t)ldo * k] = v;
+}
+
+cudaError_t overlap_aux_launch(int ncols, int nlay, int ld, int iovr, const double* dz, const double* delg,
+                               const double* alpha, double* aux, int ldo, cudaStream_t st) {
+  const long long n = (long long)ncols * nlay;
+  if (n <= 0) return cudaSuccess;
+  sw_overlap_aux_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ncols, nlay, ld, iovr, dz, delg, alpha, aux, ldo);
+  return cudaGetLastError();
+}
+
 cudaError_t optics_launch(const SwArgs& a, const SwScratch& s, int p0, int nc, const double* T, cudaStream_t st) {
   if (nc <= 0) return cudaSuccess;
   const int grid = (nc + kOptWarps - 1) / kOptWarps;

@@ -42,6 +42,8 @@ struct SwScratch {
 
 __host__ __device__ inline size_t rt_warp_doubles(int nlay, bool hswb) { return (size_t)(hswb ? 32 : 4) * (nlay + 1); }
 
+cudaError_t overlap_aux_launch(int ncols, int nlay, int ld, int iovr, const double* dz, const double* delg,
+                               const double* alpha, double* aux, int ldo, cudaStream_t st);
 cudaError_t optics_launch(const SwArgs& a, const SwScratch& s, int p0, int nc, const double* T, cudaStream_t st);
 cudaError_t rt_prepare(int max_smem);
 size_t rt_smem_bytes(int nlay, bool hswb);

@@ -211,6 +211,7 @@ def lib():
         L.rrtmg_sw_gpu_run.argtypes = [C.POINTER(SwRunArgs), C.c_char_p, C.c_int32]
         L.rrtmg_sw_gpu_run_ex.argtypes = [C.POINTER(SwRunArgs), C.POINTER(SwExec), C.c_char_p, C.c_int32]
         L.rrtmg_sw_gpu_gas_optics.argtypes = [C.POINTER(SwRunArgs)] + [C.c_void_p] * 4 + [C.c_char_p, C.c_int32]
+        L.rrtmg_sw_gpu_mcica.argtypes = ([C.c_int32] * 4 + [C.c_void_p] * 6 + [C.c_void_p, C.c_char_p, C.c_int32])
         L.rrtmg_sw_gpu_finalize.argtypes = []
         L.rrtmg_sw_gpu_finalize.restype = None
         _lib = L

@@ -130,6 +130,21 @@ int rrtmg_sw_gpu_gas_optics(const rrtmg_sw_run_args *args, double *taug,
                             double *taur, double *sfluxzen, void *stream,
                             char *errmsg, int32_t errmsg_len);
 
+/* Sub-column generator alone (mcica_subcol, radsw_main.F90:1952-2212, with
+ * the GFS Mersenne twister), on the GPU, for every overlap iovr 0..5.  For
+ * each column i: seed[i]; cldf (ldim, nlay) the layer cloud fraction already
+ * floored at 1e-12 as cldprop does (radsw_main.F90:1904-1908), internal
+ * (surface-first) layer order; dz (ldim, nlay) [km] and de_lgth (npts) [km]
+ * for iovr 3, alpha (ldim, nlay) for iovr 4, 5 (NULL otherwise).  Writes
+ * lcloudy as bits: bits[(i*RRTMG_SW_NGPT + ig) * nwords + (k >> 5)] bit
+ * (k & 31), nwords = (nlay + 31) / 32.  Device pointers only.  Stage entry
+ * point for bit-exact tests.  Returns errflg. */
+int rrtmg_sw_gpu_mcica(int32_t npts, int32_t nlay, int32_t ldim, int32_t iovr,
+                       const int32_t *seed, const double *cldf,
+                       const double *dz, const double *de_lgth,
+                       const double *alpha, uint32_t *bits, void *stream,
+                       char *errmsg, int32_t errmsg_len);
+
 /* Releases the device tables of rrtmg_sw_gpu_init. */
 void rrtmg_sw_gpu_finalize(void);
 

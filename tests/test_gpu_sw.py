@@ -266,3 +266,38 @@ def test_sw_host_pipeline(gpu, osw):
     cols = sel - 1
     for k in ("topflx", "sfcflx"):
         assert _rel(out[k][cols], ref[k][cols], 1e-300) <= FLUX_RTOL, k
+
+
+@pytest.mark.parametrize("nlay", [33, 127, 200])
+@pytest.mark.parametrize("iovr", [0, 1, 2, 3, 4, 5])
+def test_sw_mcica_bits_exact(gpu, osw, nlay, iovr):
+    """rrtmg_sw_gpu_mcica against the restatement's mcica_subcol, bit for bit:
+    seeds 0 (-> 4357), negative and 2^31-1, cloud fractions of exactly 0, 1
+    and 0.5 beside random ones, and fractions under 1e-12 floored to 0."""
+    import ctypes as C
+    import torch
+    n = 24
+    rng = np.random.default_rng(nlay * 10 + iovr)
+    cf = rng.uniform(0, 1, (nlay, n)) * (rng.uniform(0, 1, (nlay, n)) > 0.4)
+    cf[::7] = 1.0
+    cf[3::11] = 0.5
+    cf[5::13] = 3e-13
+    cldf = np.where(cf < 1e-12, 0.0, cf)
+    seed = rng.integers(-2**31, 2**31 - 1, n).astype(np.int32)
+    seed[:3] = (0, -1, 2**31 - 1)
+    dz = rng.uniform(0.05, 1.5, (nlay, n))
+    dl = rng.uniform(0.5, 4.0, n)
+    alpha = rng.uniform(0, 1, (nlay, n))
+    nw = (nlay + 31) // 32
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a)).cuda()
+    d_seed, d_cf, d_dz, d_dl, d_al = t(seed), t(cldf), t(dz), t(dl), t(alpha)
+    bits = torch.zeros(n * 112 * nw, dtype=torch.int32, device="cuda")
+    msg = C.create_string_buffer(256)
+    rc = sw.lib().rrtmg_sw_gpu_mcica(n, nlay, 0, iovr, d_seed.data_ptr(), d_cf.data_ptr(), d_dz.data_ptr(),
+                                     d_dl.data_ptr(), d_al.data_ptr(), bits.data_ptr(), None, msg, 256)
+    assert rc == 0, msg.value
+    got = bits.cpu().numpy().view(np.uint32).reshape(n, 112, nw)
+    for c in range(n):
+        want = osw.mcica_bits(nlay, int(seed[c]), iovr, cldf[:, c], dz=dz[:, c], de_lgth=float(dl[c]),
+                              alpha=alpha[:, c])
+        assert np.array_equal(got[c], want), (c, iovr)
