@@ -412,6 +412,42 @@ def sw_leg(args, torch, timed, sh):
     rc, msg = oracle_sw.run(prof, ref3, flags=dict(iovr=3))
     assert rc == 0, msg
     rel = lambda u, v, f: float(np.max(np.abs(u - v) / np.maximum(np.abs(v), f)))
+    # the same columns as uneven physics blocks (8..256 columns, the host's
+    # blocking): one rrtmg_sw_gpu_run_blocks call against one call per block
+    sizes = synthetic.physics_blocks(n, seed=7)
+    bprofs, bouts = [], []
+    c0 = 0
+    for nb_cols in sizes:
+        bp = dict(npts=int(nb_cols), nlay=nlay, solcon=prof["solcon"], sw_flags=prof["sw_flags"])
+        for kk, v in prof.items():
+            if isinstance(v, np.ndarray) and v.shape[-1] == n:
+                bp[kk] = torch.as_tensor(np.ascontiguousarray(v[..., c0:c0 + nb_cols])).cuda()
+        idx = prof["idxday"]
+        bp["idxday"] = torch.as_tensor((idx[(idx > c0) & (idx <= c0 + nb_cols)] - c0).astype(np.int32)).cuda()
+        bprofs.append(bp)
+        bouts.append(swm.alloc_outputs(int(nb_cols), nlay, like=like))
+        c0 += nb_cols
+    arr = (swm.SwRunArgs * len(sizes))()
+    for b in range(len(sizes)):
+        arr[b] = swm.make_run_args(bprofs[b], bouts[b], keep=keep)
+
+    def step_blocks():
+        if swm.lib().rrtmg_sw_gpu_run_blocks(arr, len(sizes), C.byref(x), buf, 256):
+            raise RuntimeError(buf.value.decode())
+
+    def step_per_block():
+        for b in range(len(sizes)):
+            if swm.lib().rrtmg_sw_gpu_run_ex(C.byref(arr[b]), C.byref(x), buf, 256):
+                raise RuntimeError(buf.value.decode())
+    for _ in range(args.warmup):
+        step_blocks()
+    ms_bl = timed(step_blocks, k)
+    step_per_block()
+    kp = max(2, k // 2)
+    ms_pb = timed(step_per_block, kp)
+    blocks_ok = all(np.array_equal(bouts[b]["topflx"].cpu().numpy(), got["topflx"][int(sum(sizes[:b])):int(sum(sizes[:b + 1]))])
+                    for b in range(len(sizes)))
+    del bprofs, bouts
     # roofline of the dominant (transfer) kernel: counted flops and DRAM bytes per
     # column from the ncu capture, against the FMA peak measured now and the
     # measured copy bandwidth
@@ -439,6 +475,10 @@ def sw_leg(args, torch, timed, sh):
     return {"workload": f"sw_c2_allsky_mcica_{n}x127", "steps": k, "roofline": roof, "value": n * k / (ms / 1e3),
             "unit": "columns/s", "ms_per_step": ms / k,
             "kernel_ms": {"optics": km[1], "mcica": km[0], "transfer": km[2]},
+            "blocks": {"nblocks": len(sizes), "block_sizes": "8..256 (physics_blocks seed 7)",
+                       "run_blocks_columns_per_s": n * k / (ms_bl / 1e3),
+                       "per_block_calls_columns_per_s": n * kp / (ms_pb / 1e3),
+                       "matches_single_call": bool(blocks_ok)},
             "e2e_columns_per_s": n / e2e_s, "e2e_h2d_bytes": h2d, "e2e_d2h_bytes": d2h,
             "e2e_matches_device_run": e2e_ok,
             "flux_max_rel_vs_oracle": max(rel(got[kk], ref[kk], 1e-300) for kk in ("topflx", "sfcflx", "fdncmp")),

@@ -55,6 +55,12 @@ struct SwWorkspace {
   cudaEvent_t ev_in[2] = {}, ev_done[2] = {}, ev_out[2] = {};
   char* pbuf = nullptr;
   size_t pbuf_bytes = 0;
+  // physics blocks: the block table, its prefixes and the point table on the
+  // device, and the host copies they are uploaded from
+  char* btab = nullptr;
+  size_t btab_bytes = 0;
+  std::vector<sw::SwArgs> h_tab;
+  std::vector<int> h_pre;
 };
 std::vector<SwWorkspace*> g_ws;
 thread_local SwWorkspace* tl_ws = nullptr;
@@ -613,6 +619,108 @@ extern "C" int rrtmg_sw_gpu_gas_optics(const rrtmg_sw_run_args* a, double* taug,
   return check_bad(w, st, errmsg, errmsg_len);
 }
 
+extern "C" int rrtmg_sw_gpu_run_blocks(const rrtmg_sw_run_args* blocks, int32_t nblocks, const rrtmg_sw_exec* x,
+                                       char* errmsg, int32_t errmsg_len) {
+  set_msg(errmsg, errmsg_len, "");
+  if (!g.ready) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu: rrtmg_sw_gpu_init has not been called"); return 1; }
+  if (!blocks || nblocks < 0 || !x || x->memory != 1) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_run_blocks: blocks, nblocks >= 0 and device memory (exec->memory = 1) needed");
+    return 1;
+  }
+  CK(cudaSetDevice(g.device), "cudaSetDevice");
+  int rc = 0;
+  SwWorkspace* w = workspace(errmsg, errmsg_len, &rc);
+  if (!w) return rc;
+  cudaStream_t st = x->stream ? (cudaStream_t)x->stream : w->stream;
+  // validate; blocks with nothing to do (lsswr off, nday <= 0) drop out
+  w->h_tab.clear();
+  std::vector<int> colpre, dayp(1, 0);
+  const rrtmg_sw_run_args* first = nullptr;
+  int total_cols = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    const rrtmg_sw_run_args* a = &blocks[b];
+    const int v = validate(a, x, errmsg, errmsg_len);
+    if (v == -1) continue;
+    if (v) {
+      char tmp[256];
+      std::snprintf(tmp, sizeof tmp, "%s", errmsg ? errmsg : "");
+      set_msg(errmsg, errmsg_len, "block %d: %s", b, tmp);
+      return 1;
+    }
+    if (!first) {
+      first = a;
+    } else if (a->nlay != first->nlay || a->top_at_1 != first->top_at_1 || a->inc_minor_gas != first->inc_minor_gas ||
+               a->iovr != first->iovr || a->iovr_rand != first->iovr_rand || a->iovr_maxrand != first->iovr_maxrand ||
+               a->iswcliq != first->iswcliq || a->iswcice != first->iswcice || a->isubcsw != first->isubcsw ||
+               a->iswmode != first->iswmode || (a->hswb != nullptr) != (first->hswb != nullptr)) {
+      set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_run_blocks: block %d differs from the first in nlay, flags or hswb", b);
+      return 1;
+    }
+    w->h_tab.push_back(device_args(a));
+    colpre.push_back(total_cols);
+    total_cols += a->npts;
+    dayp.push_back(dayp.back() + a->nday);
+  }
+  const int nb = (int)w->h_tab.size(), ndays = dayp.back();
+  if (nb == 0) return 0;
+  const int nlay = first->nlay;
+  // device copies: table, column prefixes, day prefixes, point table
+  w->h_pre.assign(colpre.begin(), colpre.end());
+  w->h_pre.insert(w->h_pre.end(), dayp.begin(), dayp.end());
+  const size_t tab_b = align256((size_t)nb * sizeof(sw::SwArgs)), pre_b = align256(w->h_pre.size() * 4);
+  const size_t pts_b = align256((size_t)std::max(ndays, 1) * sizeof(int2));
+  CK(cudaStreamSynchronize(st), "cudaStreamSynchronize");   // an earlier call may still read the tables
+  CK(grow(&w->btab, &w->btab_bytes, tab_b + pre_b + pts_b), "block table allocation");
+  sw::SwArgs* d_tab = (sw::SwArgs*)w->btab;
+  int* d_pre = (int*)(w->btab + tab_b);
+  int2* d_pts = (int2*)(w->btab + tab_b + pre_b);
+  CK(cudaMemcpyAsync(d_tab, w->h_tab.data(), (size_t)nb * sizeof(sw::SwArgs), cudaMemcpyHostToDevice, st),
+     "cudaMemcpyAsync");
+  CK(cudaMemcpyAsync(d_pre, w->h_pre.data(), w->h_pre.size() * 4, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+  CK(cudaMemsetAsync(w->bad, 0, sizeof(int), st), "cudaMemsetAsync");
+  CK(sw::blocks_prepare(d_tab, d_pre, d_pre + nb, nb, total_cols, d_pts, w->bad, st), "block table kernels");
+  // the kernels over all daytime points, in scratch-sized chunks
+  const sw::SwArgs& f = w->h_tab[0];
+  const size_t per = scratch_per_col(nlay);
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)std::max(ndays, 1), kScratchBudget / per));
+  CK(grow(&w->scratch, &w->scratch_bytes, carve_bytes(chunk, nlay)), "scratch allocation");
+  cudaEvent_t ev[4] = {};
+  float* kms = x->kernel_ms;
+  if (kms)
+    for (auto& e : ev) CK(cudaEventCreate(&e), "cudaEventCreate");
+  for (int p0 = 0; p0 < ndays; p0 += chunk) {
+    const int nc = std::min(chunk, ndays - p0);
+    sw::SwScratch sc = carve(w->scratch, nc, nlay);
+    sc.bad = w->bad;
+    const bool first_chunk = kms && p0 == 0;
+    if (first_chunk) CK(cudaEventRecord(ev[0], st), "cudaEventRecord");
+    CK(sw::optics_blocks_launch(d_tab, d_pts, sc, p0, nc, g.tab, st), "optics kernel launch");
+    if (first_chunk) CK(cudaEventRecord(ev[1], st), "cudaEventRecord");
+    lw::McicaStage ms;
+    ms.cldf = sc.cldf;
+    ms.seed = sc.seed;
+    ms.alpha = sc.aux;
+    ms.ld = nc;
+    if (f.isubcsw > 0 && f.iovr <= 2)
+      CK(lw::mcica_sw_launch(nc, nlay, f.iovr, ms, sc.bits, g.num_sms, st), "McICA kernel launch");
+    else if (f.isubcsw > 0)
+      CK(lw::mcica_sw_two_set_launch(nc, nlay, f.iovr, ms, sc.bits, g.num_sms, st), "McICA kernel launch");
+    if (first_chunk) CK(cudaEventRecord(ev[2], st), "cudaEventRecord");
+    CK(sw::rt_blocks_launch(d_tab, d_pts, f.isubcsw <= 0, f.hswb != nullptr, sc, p0, nc, nlay, g.etab, st),
+       "transfer kernel launch");
+    if (first_chunk) CK(cudaEventRecord(ev[3], st), "cudaEventRecord");
+  }
+  if (kms) {
+    CK(cudaEventSynchronize(ev[3]), "kernel execution");
+    cudaEventElapsedTime(&kms[0], ev[1], ev[2]);
+    cudaEventElapsedTime(&kms[1], ev[0], ev[1]);
+    cudaEventElapsedTime(&kms[2], ev[2], ev[3]);
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  if (x->sync || kms) return check_bad(w, st, errmsg, errmsg_len);
+  return 0;
+}
+
 extern "C" int rrtmg_sw_gpu_mcica(int32_t npts, int32_t nlay, int32_t ldim, int32_t iovr, const int32_t* seed,
                                   const double* cldf, const double* dz, const double* de_lgth, const double* alpha,
                                   uint32_t* bits, void* stream, char* errmsg, int32_t errmsg_len) {
@@ -654,6 +762,7 @@ extern "C" void rrtmg_sw_gpu_finalize(void) {
     cudaFree(w->stage);
     cudaFree(w->bad);
     cudaFree(w->pbuf);
+    cudaFree(w->btab);
     for (int k = 0; k < 2; ++k) {
       if (w->ev_in[k]) cudaEventDestroy(w->ev_in[k]);
       if (w->ev_done[k]) cudaEventDestroy(w->ev_done[k]);

@@ -419,17 +419,10 @@ __device__ void cloud_layer(const SwArgs& a, size_t x, const double* __restrict_
 // ---- kernel 1: optics ------------------------------------------------------
 constexpr int kOptWarps = 4;
 
-__global__ void __launch_bounds__(32 * kOptWarps, 3)   // 168 registers: twelve warps per SM hide the table gathers better than eight
-sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ T) {
-  __shared__ int s_jp[kOptWarps][kSwMaxLay];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int pl = blockIdx.x * kOptWarps + w;
-  if (pl >= nc) return;   // whole warps only: no block barrier below
-  const int j1 = a.idxday[p0 + pl];
-  if (j1 < 1 || j1 > a.npts) {   // idxday outside 1..npts: skip the column, report
-    if (lane == 0) atomicOr(s.bad, 1);
-    return;
-  }
+// One column's optics: a = the argument record of the call (or of the
+// physics block) the column belongs to, j1 its 1-based column there.
+__device__ __forceinline__ void optics_body(const SwArgs& a, const SwScratch& s, int pl, int nc, int j1, int lane,
+                                            int* s_jp_w, const double* __restrict__ T) {
   const int i = j1 - 1, nlay = a.nlay;
   // laytrop: the last layer with ln p > 4.56, nlay if none (RSM:2305, 2353)
   int laytrop = 0;
@@ -439,7 +432,7 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
     if (k < nlay) {
       const int r = a.top_at_1 ? nlay - 1 - k : k;
       const double plog = log(a.plyr[(size_t)i + (size_t)a.ld * r]);
-      s_jp[w][k] = max(1, min(58, (int)(36.0 - 5.0 * (plog + 0.04))));
+      s_jp_w[k] = max(1, min(58, (int)(36.0 - 5.0 * (plog + 0.04))));
       hi = plog > 4.56;
     }
     const unsigned m = __ballot_sync(0xffffffffu, hi);
@@ -484,11 +477,11 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
       if (jb == 17 || jb == 28) {
         ks = nlay;
         for (int k = laytrop; k <= nlay - 1; ++k)
-          if (s_jp[w][k - 1] < lref && s_jp[w][k] >= lref) { ks = k + 1; break; }
+          if (s_jp_w[k - 1] < lref && s_jp_w[k] >= lref) { ks = k + 1; break; }
       } else {
         ks = laytrop;
         for (int k = 1; k <= laytrop - 1; ++k)
-          if (s_jp[w][k - 1] < lref && s_jp[w][k] >= lref) { ks = k + 1; break; }
+          if (s_jp_w[k - 1] < lref && s_jp_w[k] >= lref) { ks = k + 1; break; }
       }
       Lay L;
       layer_record(a, i, ks - 1, T, L);
@@ -559,6 +552,32 @@ sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict
       a.cldtau[x] = tw[9];   // band 25 (RSM:1144-1152)
     }
   }
+}
+
+__global__ void __launch_bounds__(32 * kOptWarps, 3)   // 168 registers: twelve warps per SM hide the table gathers better than eight
+sw_optics_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ T) {
+  __shared__ int s_jp[kOptWarps][kSwMaxLay];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int pl = blockIdx.x * kOptWarps + w;
+  if (pl >= nc) return;   // whole warps only: no block barrier below
+  const int j1 = a.idxday[p0 + pl];
+  if (j1 < 1 || j1 > a.npts) {   // idxday outside 1..npts: skip the column, report
+    if (lane == 0) atomicOr(s.bad, 1);
+    return;
+  }
+  optics_body(a, s, pl, nc, j1, lane, s_jp[w], T);
+}
+
+// many physics blocks in one launch: daytime point p is column pts[p].y of block pts[p].x
+__global__ void __launch_bounds__(32 * kOptWarps, 3)
+sw_optics_blocks_kernel(const SwArgs* __restrict__ tab, const int2* __restrict__ pts, SwScratch s, int p0, int nc,
+                        const double* __restrict__ T) {
+  __shared__ int s_jp[kOptWarps][kSwMaxLay];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int pl = blockIdx.x * kOptWarps + w;
+  if (pl >= nc) return;
+  const int2 q = pts[p0 + pl];
+  optics_body(tab[q.x], s, pl, nc, q.y, lane, s_jp[w], T);
 }
 
 // ---- kernel 3: transfer ------------------------------------------------------
@@ -732,18 +751,15 @@ __device__ __forceinline__ double warp_sum(double v) {
 constexpr int kRtWarps = 4;   // GRID: isubcsw <= 0, spcvrtc's cloud-fraction mixing; else McICA flags
 constexpr int kLaneVals = 10;   // per-lane stored values per level
 
+// One column's transfer and outputs: a = the argument record of the call
+// (or of the physics block) the column belongs to, j1 its 1-based column
+// there, acc0 this warp's shared-memory slice.
 template <bool GRID>
-__global__ void __launch_bounds__(32 * kRtWarps, 4)   // 128 registers: sixteen warps per SM
-sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ ET) {
-  extern __shared__ double sm[];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int pl = blockIdx.x * kRtWarps + w;
-  if (pl >= nc) return;
-  const int j1 = a.idxday[p0 + pl];
-  if (j1 < 1 || j1 > a.npts) return;   // reported by the optics kernel
+__device__ __forceinline__ void rt_body(const SwArgs& a, const SwScratch& s, int pl, int nc, int j1, int lane,
+                                        double* acc0, const double* __restrict__ ET) {
   const int nlay = a.nlay, nlp1 = nlay + 1;
   const bool want_b = a.hswb != nullptr;
-  double* acc = sm + (size_t)w * rt_warp_doubles(nlay, want_b);
+  double* acc = acc0;
   double *up0 = acc, *dn0 = acc + nlp1, *upc = acc + 2 * nlp1, *dnc = acc + 3 * nlp1;
   double* accb = acc + 4 * nlp1;   // [14][2][nlp1] total-sky band fluxes (hswb)
   for (int q = lane; q < (want_b ? 32 : 4) * nlp1; q += 32) acc[q] = 0.0;
@@ -986,6 +1002,77 @@ sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ E
   }
 }
 
+template <bool GRID>
+__global__ void __launch_bounds__(32 * kRtWarps, 4)   // 128 registers: sixteen warps per SM
+sw_rt_kernel(SwArgs a, SwScratch s, int p0, int nc, const double* __restrict__ ET) {
+  extern __shared__ double sm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int pl = blockIdx.x * kRtWarps + w;
+  if (pl >= nc) return;
+  const int j1 = a.idxday[p0 + pl];
+  if (j1 < 1 || j1 > a.npts) return;   // reported by the optics kernel
+  rt_body<GRID>(a, s, pl, nc, j1, lane, sm + (size_t)w * rt_warp_doubles(a.nlay, a.hswb != nullptr), ET);
+}
+
+template <bool GRID>
+__global__ void __launch_bounds__(32 * kRtWarps, 4)
+sw_rt_blocks_kernel(const SwArgs* __restrict__ tab, const int2* __restrict__ pts, bool want_b, SwScratch s, int p0,
+                    int nc, int nlay, const double* __restrict__ ET) {
+  extern __shared__ double sm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int pl = blockIdx.x * kRtWarps + w;
+  if (pl >= nc) return;
+  const int2 q = pts[p0 + pl];
+  rt_body<GRID>(tab[q.x], s, pl, nc, q.y, lane, sm + (size_t)w * rt_warp_doubles(nlay, want_b), ET);
+}
+
+// Zeroes every output of every column of the physics blocks (RSM:824-845):
+// column c of the concatenation is column c - colpre[b] of block b.
+__global__ void sw_zero_blocks_kernel(const SwArgs* __restrict__ tab, const int* __restrict__ colpre, int nb,
+                                      int total) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
+    int lo = 0, hi = nb - 1;   // last block with colpre[b] <= c
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (colpre[mid] <= c) lo = mid;
+      else hi = mid - 1;
+    }
+    const SwArgs& a = tab[lo];
+    const size_t i = (size_t)(c - colpre[lo]), ld = (size_t)a.ld, nlay = (size_t)a.nlay;
+    for (size_t k = 0; k < nlay; ++k) {
+      a.hswc[i + ld * k] = 0.0;
+      a.cldtau[i + ld * k] = 0.0;
+      if (a.hsw0) a.hsw0[i + ld * k] = 0.0;
+      if (a.hswb)
+        for (size_t b = 0; b < 14; ++b) a.hswb[i + ld * (k + nlay * b)] = 0.0;
+    }
+    if (a.flxprf)
+      for (size_t k = 0; k <= nlay; ++k)
+        for (int q = 0; q < 4; ++q) a.flxprf[4 * (i + ld * k) + q] = 0.0;
+    for (int q = 0; q < 3; ++q) a.topflx[3 * i + q] = 0.0;
+    for (int q = 0; q < 4; ++q) a.sfcflx[4 * i + q] = 0.0;
+    if (a.fdncmp)
+      for (int q = 0; q < 6; ++q) a.fdncmp[6 * i + q] = 0.0;
+  }
+}
+
+// The daytime-point table of the physics blocks: point dayp[b] + p is column
+// idxday_b[p] of block b; an index outside 1..npts_b sets *bad.
+__global__ void sw_points_kernel(const SwArgs* __restrict__ tab, const int* __restrict__ dayp, int nb,
+                                 int2* __restrict__ pts, int* bad) {
+  const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (b >= nb) return;
+  const SwArgs& a = tab[b];
+  for (int p = lane; p < dayp[b + 1] - dayp[b]; p += 32) {
+    int j1 = a.idxday[p];
+    if (j1 < 1 || j1 > a.npts) {
+      atomicOr(bad, 1);
+      j1 = 1;   // a valid column; the call reports the error
+    }
+    pts[dayp[b] + p] = make_int2(b, j1);
+  }
+}
+
 // The per-layer overlap parameter of the sub-column generator for the stage
 // entry point: fac_lcf between layers k-1 and k (iovr 3, RSM:2106-2108) or
 // alpha (iovr 4, 5), [c + ldo*k]; inputs [c + ld*k], internal layer order.
@@ -1022,8 +1109,38 @@ size_t rt_smem_bytes(int nlay, bool hswb) { return (size_t)kRtWarps * rt_warp_do
 
 cudaError_t rt_prepare(int max_smem) {
   cudaError_t e = cudaFuncSetAttribute(sw_rt_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(sw_rt_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(sw_rt_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(sw_rt_blocks_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(sw_rt_blocks_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
+  return e;
+}
+
+cudaError_t blocks_prepare(const SwArgs* tab, const int* colpre, const int* dayp, int nb, int total_cols,
+                           int2* pts, int* bad, cudaStream_t st) {
+  sw_points_kernel<<<(nb + 7) / 8, 256, 0, st>>>(tab, dayp, nb, pts, bad);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || total_cols <= 0) return e;
+  sw_zero_blocks_kernel<<<min((total_cols + 127) / 128, 4096), 128, 0, st>>>(tab, colpre, nb, total_cols);
+  return cudaGetLastError();
+}
+
+cudaError_t optics_blocks_launch(const SwArgs* tab, const int2* pts, const SwScratch& s, int p0, int nc,
+                                 const double* T, cudaStream_t st) {
+  if (nc <= 0) return cudaSuccess;
+  sw_optics_blocks_kernel<<<(nc + kOptWarps - 1) / kOptWarps, 32 * kOptWarps, 0, st>>>(tab, pts, s, p0, nc, T);
+  return cudaGetLastError();
+}
+
+cudaError_t rt_blocks_launch(const SwArgs* tab, const int2* pts, bool grid, bool want_b, const SwScratch& s, int p0,
+                             int nc, int nlay, const double* ET, cudaStream_t st) {
+  if (nc <= 0) return cudaSuccess;
+  const int g = (nc + kRtWarps - 1) / kRtWarps;
+  const size_t smem = rt_smem_bytes(nlay, want_b);
+  if (grid) sw_rt_blocks_kernel<true><<<g, 32 * kRtWarps, smem, st>>>(tab, pts, want_b, s, p0, nc, nlay, ET);
+  else sw_rt_blocks_kernel<false><<<g, 32 * kRtWarps, smem, st>>>(tab, pts, want_b, s, p0, nc, nlay, ET);
+  return cudaGetLastError();
 }
 
 cudaError_t rt_launch(const SwArgs& a, const SwScratch& s, int p0, int nc, const double* ET, cudaStream_t st) {

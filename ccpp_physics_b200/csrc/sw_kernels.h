@@ -48,5 +48,13 @@ cudaError_t optics_launch(const SwArgs& a, const SwScratch& s, int p0, int nc, c
 cudaError_t rt_prepare(int max_smem);
 size_t rt_smem_bytes(int nlay, bool hswb);
 cudaError_t rt_launch(const SwArgs& a, const SwScratch& s, int p0, int nc, const double* ET, cudaStream_t st);
+// physics blocks in one call: tab[b] = block b's record (device), colpre[b] / dayp[b]
+// = columns / daytime points before block b (dayp has nb + 1 entries)
+cudaError_t blocks_prepare(const SwArgs* tab, const int* colpre, const int* dayp, int nb, int total_cols,
+                           int2* pts, int* bad, cudaStream_t st);
+cudaError_t optics_blocks_launch(const SwArgs* tab, const int2* pts, const SwScratch& s, int p0, int nc,
+                                 const double* T, cudaStream_t st);
+cudaError_t rt_blocks_launch(const SwArgs* tab, const int2* pts, bool grid, bool want_b, const SwScratch& s, int p0,
+                             int nc, int nlay, const double* ET, cudaStream_t st);
 
 }  // namespace sw

@@ -211,6 +211,8 @@ def lib():
         L.rrtmg_sw_gpu_run.argtypes = [C.POINTER(SwRunArgs), C.c_char_p, C.c_int32]
         L.rrtmg_sw_gpu_run_ex.argtypes = [C.POINTER(SwRunArgs), C.POINTER(SwExec), C.c_char_p, C.c_int32]
         L.rrtmg_sw_gpu_gas_optics.argtypes = [C.POINTER(SwRunArgs)] + [C.c_void_p] * 4 + [C.c_char_p, C.c_int32]
+        L.rrtmg_sw_gpu_run_blocks.argtypes = [C.POINTER(SwRunArgs), C.c_int32, C.POINTER(SwExec), C.c_char_p,
+                                              C.c_int32]
         L.rrtmg_sw_gpu_mcica.argtypes = ([C.c_int32] * 4 + [C.c_void_p] * 6 + [C.c_void_p, C.c_char_p, C.c_int32])
         L.rrtmg_sw_gpu_finalize.argtypes = []
         L.rrtmg_sw_gpu_finalize.restype = None
@@ -246,6 +248,28 @@ def rrtmg_sw_run(prof: dict, out: dict, *, flags: dict | None = None, device_mem
     msg = C.create_string_buffer(512)
     rc = lib().rrtmg_sw_gpu_run_ex(C.byref(a), C.byref(x), msg, 512)
     if rc:
+        raise RrtmgSwError(msg.value.decode())
+    if km is not None:
+        kernel_ms[:] = list(km)
+
+
+def rrtmg_sw_run_blocks(profs, outs, *, flags: dict | None = None, ldims=None, stream=None, kernel_ms=None):
+    """Many physics blocks in one rrtmg_sw_gpu_run_blocks call (device
+    memory): profs[b] / outs[b] are block b's inputs and outputs (CUDA
+    tensors), ldims[b] its leading dimension (0 = npts).  Same results as one
+    rrtmg_sw_run per block.  Raises on errflg."""
+    keep = []
+    n = len(profs)
+    arr = (SwRunArgs * max(n, 1))()
+    for b in range(n):
+        arr[b] = make_run_args(profs[b], outs[b], flags=flags, keep=keep, ldim=(ldims[b] if ldims else 0))
+    x = SwExec(precision=0, memory=1, sync=1, stream=C.c_void_p(stream.cuda_stream if stream is not None else 0))
+    km = None
+    if kernel_ms is not None:
+        km = (C.c_float * 3)()
+        x.kernel_ms = C.cast(km, C.POINTER(C.c_float))
+    msg = C.create_string_buffer(512)
+    if lib().rrtmg_sw_gpu_run_blocks(arr, n, C.byref(x), msg, 512):
         raise RrtmgSwError(msg.value.decode())
     if km is not None:
         kernel_ms[:] = list(km)

@@ -130,6 +130,20 @@ int rrtmg_sw_gpu_gas_optics(const rrtmg_sw_run_args *args, double *taug,
                             double *taur, double *sfluxzen, void *stream,
                             char *errmsg, int32_t errmsg_len);
 
+/* UFS-style physics blocks in one call.  The reference host calls
+ * rrtmg_sw_run once per block of columns; here blocks[b] is the
+ * rrtmg_sw_run argument set of block b, every pointer device memory, all
+ * blocks with the same nlay and flags and all or none with hswb.  The daytime
+ * points of all blocks form one index space and run in one launch of each
+ * kernel (repeated only when the scratch budget splits them), with no
+ * per-block launches; the results equal per-block rrtmg_sw_gpu_run_ex calls
+ * (isubcsw = 1 seeds stay block-relative, as the reference's are).  Blocks
+ * with lsswr = 0 or nday <= 0 are left untouched.  exec: memory must be 1;
+ * stream, sync and kernel_ms as in rrtmg_sw_gpu_run_ex.  Returns errflg. */
+int rrtmg_sw_gpu_run_blocks(const rrtmg_sw_run_args *blocks, int32_t nblocks,
+                            const rrtmg_sw_exec *exec, char *errmsg,
+                            int32_t errmsg_len);
+
 /* Sub-column generator alone (mcica_subcol, radsw_main.F90:1952-2212, with
  * the GFS Mersenne twister), on the GPU, for every overlap iovr 0..5.  For
  * each column i: seed[i]; cldf (ldim, nlay) the layer cloud fraction already

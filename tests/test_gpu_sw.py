@@ -301,3 +301,38 @@ def test_sw_mcica_bits_exact(gpu, osw, nlay, iovr):
         want = osw.mcica_bits(nlay, int(seed[c]), iovr, cldf[:, c], dz=dz[:, c], de_lgth=float(dl[c]),
                               alpha=alpha[:, c])
         assert np.array_equal(got[c], want), (c, iovr)
+
+
+@pytest.mark.parametrize("flags", [None, dict(iovr=3), dict(isubcsw=0), dict(isubcsw=1)])
+def test_sw_run_blocks_equals_per_block_calls(gpu, flags):
+    """rrtmg_sw_gpu_run_blocks over uneven physics blocks (one with ldim >
+    npts, one without a daytime point) gives, bit for bit, what one call per
+    block gives."""
+    import torch
+    sizes = [5, 37, 1, 64, 12, 9, 130]
+    nlay = 50
+    profs, ldims = [], []
+    off = 0
+    for b, n in enumerate(sizes):
+        ld = n + (3 if b == 3 else 0)
+        p = sw.add_sw_inputs(synthetic.make_profiles(ld, nlay, seed=50, col_offset=off), seed=50, col_offset=off,
+                             night_fraction=1.0 if b == 4 else 0.3, precip=True)
+        p["npts"] = n
+        p["idxday"] = p["idxday"][p["idxday"] <= n].astype(np.int32)
+        profs.append({k: (torch.as_tensor(np.ascontiguousarray(v)).cuda() if isinstance(v, np.ndarray) else v)
+                      for k, v in p.items()})
+        ldims.append(ld if ld != n else 0)
+        off += ld
+    assert len(profs[4]["idxday"]) == 0
+    like = profs[0]["plyr"]
+    outs_b = [sw.alloc_outputs(ldims[b] or n, nlay, hswb=True, flxprf=True, like=like) for b, n in enumerate(sizes)]
+    outs_1 = [sw.alloc_outputs(ldims[b] or n, nlay, hswb=True, flxprf=True, like=like) for b, n in enumerate(sizes)]
+    for o in outs_b + outs_1:
+        o["hswc"].fill_(7.0)   # the block without a daytime point keeps this
+    sw.rrtmg_sw_run_blocks(profs, outs_b, flags=flags, ldims=ldims)
+    for b in range(len(sizes)):
+        gpu.rrtmg_sw_run(profs[b], outs_1[b], flags=flags, device_memory=True, ldim=ldims[b])
+    for b in range(len(sizes)):
+        for k in outs_b[b]:
+            assert torch.equal(outs_b[b][k], outs_1[b][k]), (b, k)
+    assert (outs_b[4]["hswc"] == 7.0).all()
