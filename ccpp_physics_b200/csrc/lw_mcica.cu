@@ -727,12 +727,12 @@ cudaError_t mcica_sw_two_set_launch(int ncols, int nlay, int iovr, const McicaSt
   const long round = (long)kMcicaRound * nlay + 623;
   a.cap = (int)((round + 623) / 624 * 624);
   a.st = stage;
-  static int max_smem = 0;
-  if (max_smem == 0) {
-    int dev = 0;
+  static const int max_smem = [] {   // initialised once, thread-safe
+    int dev = 0, v = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  }
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v;
+  }();
   const size_t per_warp = sw_two_set_warp_bytes(nlay, a.cap);
   const int wpb = (int)std::min<size_t>(kSwTwoSetMaxWarps, (size_t)max_smem / per_warp);
   if (wpb < 1) return cudaErrorInvalidValue;
