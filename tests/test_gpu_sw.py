@@ -205,7 +205,7 @@ def test_sw_golden_fixture(gpu, name):
 def test_sw_edges(gpu, osw):
     """200 layers (the most this path takes), 2 layers, idxday in arbitrary
     order, and no daytime point at all (radsw_main.F90:786: outputs untouched)."""
-    for npts, nlay in ((12, 200), (16, 2)):
+    for npts, nlay in ((12, 200), (16, 2), (10, 1)):
         prof = _profile(npts, nlay, 31, night_fraction=0.3, precip=True)
         out, ref = _both(gpu, osw, prof, hswb=True, flxprf=True)
         _check(out, ref)
@@ -268,7 +268,7 @@ def test_sw_host_pipeline(gpu, osw):
         assert _rel(out[k][cols], ref[k][cols], 1e-300) <= FLUX_RTOL, k
 
 
-@pytest.mark.parametrize("nlay", [33, 127, 200])
+@pytest.mark.parametrize("nlay", [1, 33, 127, 200])
 @pytest.mark.parametrize("iovr", [0, 1, 2, 3, 4, 5])
 def test_sw_mcica_bits_exact(gpu, osw, nlay, iovr):
     """rrtmg_sw_gpu_mcica against the restatement's mcica_subcol, bit for bit:
