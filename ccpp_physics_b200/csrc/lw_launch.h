@@ -68,6 +68,8 @@ unsigned int* surrogate_fallback_counter();
 
 // device chosen by rrtmg_lw_gpu_init, -1 before init (lw_api.cu)
 int selected_device();
+// device chosen by rrtmg_sw_gpu_init, -1 before init (sw_api.cu)
+int sw_selected_device();
 // frees the device scratch of the steps either side of the run (lw_prep.cu)
 void prep_release();
 

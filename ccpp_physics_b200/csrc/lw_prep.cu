@@ -10,11 +10,13 @@
 //                                radiation_cloud_overlap.F90:28-145)
 // rrtmg_lw_gpu_post           <- rrtmg_lw_post_run (physics/Radiation/RRTMG/
 //                                rrtmg_lw_post.F90:13-77)
+// rrtmg_sw_gpu_post           <- rrtmg_sw_post_run (physics/Radiation/RRTMG/
+//                                rrtmg_sw_post.F90:13-129)
 //
 // The seed stream is one Mersenne-twister stream walked by one CTA
 // (lw_mcica.cu) into a device buffer of raw words; one thread per column then
 // tempers and converts the two words it uses.  The overlap parameters run one thread per
-// column over its layers (coalesced across columns); the post step one
+// column over its layers (coalesced across columns); the post steps one
 // thread per (column, level) element.  This file is compiled without FMA
 // contraction, so every product and sum rounds as the Fortran's does.
 #include <algorithm>
@@ -30,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/rrtmg_lw_gpu.h"
+#include "../../include/rrtmg_sw_gpu.h"
 #include "lw_launch.h"
 
 namespace {
@@ -134,15 +137,16 @@ struct PostK {
   double *tsflw, *sfcdlw, *htrlw, *lwhc;
 };
 
-// rrtmg_lw_post_run (rrtmg_lw_post.F90:46-73).  Levels 1..lm of htrlw/lwhc
-// are one contiguous block of the source (levels kd+1..kd+lm), copied with
-// four loads in flight per thread; levels lm+1..levs repeat level lm; the
-// per-column fields last.
-__global__ void post_kernel(PostK a) {
-  const size_t stride = (size_t)gridDim.x * blockDim.x, t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const size_t im = (size_t)a.im, nb = im * a.lm;
-  const double* s1 = a.htlwc + im * a.kd;
-  const double* s2 = a.htlw0 + im * a.kd;
+// Level mapping of the post steps (rrtmg_lw_post.F90:48-70,
+// rrtmg_sw_post.F90:54-77): dst(:,k) = src(:,k+kd) for k = 1..lm, and
+// dst(:,lm) for k = lm+1..levs; dst0 from src0 likewise when `both`.  Levels
+// 1..lm are one contiguous block of the source, copied with four loads in
+// flight per thread.
+__device__ void map_levels(const double* src, const double* src0, double* dst, double* dst0, bool both,
+                           size_t im, int lm, int levs, int kd, size_t t0, size_t stride) {
+  const size_t nb = im * lm;
+  const double* s1 = src + im * kd;
+  const double* s2 = src0 + im * kd;
   for (size_t e = t0; e < nb; e += 4 * stride) {
     double v[4], w[4];
 #pragma unroll
@@ -150,29 +154,92 @@ __global__ void post_kernel(PostK a) {
       const size_t q = e + u * stride;
       if (q < nb) {
         v[u] = __ldcs(s1 + q);
-        if (a.lwhtr) w[u] = __ldcs(s2 + q);
+        if (both) w[u] = __ldcs(s2 + q);
       }
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const size_t q = e + u * stride;
       if (q < nb) {
-        __stcs(a.htrlw + q, v[u]);
-        if (a.lwhtr) __stcs(a.lwhc + q, w[u]);
+        __stcs(dst + q, v[u]);
+        if (both) __stcs(dst0 + q, w[u]);
       }
     }
   }
-  if (a.lm >= 1) {
-    for (int k = a.lm; k < a.levs; ++k) {
+  if (lm >= 1) {
+    for (int k = lm; k < levs; ++k) {
       for (size_t i = t0; i < im; i += stride) {
-        a.htrlw[im * k + i] = s1[im * (a.lm - 1) + i];
-        if (a.lwhtr) a.lwhc[im * k + i] = s2[im * (a.lm - 1) + i];
+        dst[im * k + i] = s1[im * (lm - 1) + i];
+        if (both) dst0[im * k + i] = s2[im * (lm - 1) + i];
       }
     }
   }
+}
+
+// rrtmg_lw_post_run (rrtmg_lw_post.F90:42-75): the heating-rate levels, then
+// the per-column fields.
+__global__ void post_kernel(PostK a) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x, t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t im = (size_t)a.im;
+  map_levels(a.htlwc, a.htlw0, a.htrlw, a.lwhc, a.lwhtr != 0, im, a.lm, a.levs, a.kd, t0, stride);
   for (size_t i = t0; i < im; i += stride) {
     a.tsflw[i] = a.tsfa[i];
     a.sfcdlw[i] = a.sfcflw[4 * i + 2];
+  }
+}
+
+struct SwPostK {
+  int im, levs, lm, kd, swhtr, day;
+  const double* alb[4];              // sfcalb1..4
+  const double *htswc, *htsw0;
+  double* dn[4];                     // nirbmdi, nirdfdi, visbmdi, visdfdi
+  double* up[4];                     // nirbmui, nirdfui, visbmui, visdfui
+  double *sfcdsw, *sfcnsw, *htrsw, *swhc, *scmpsw, *sfcfsw, *topfsw;
+};
+
+// rrtmg_sw_post_run (rrtmg_sw_post.F90:52-127).  Daytime (nday > 0): the
+// heating-rate levels as in the longwave step, then per column the four
+// surface components of the cmpfsw record {uvbfc, uvbf0, nirbm, nirdf, visbm,
+// visdf} and their products with the albedos.  No daytime point: the level
+// arrays, the component fields and the three flux records set to zero.  Last,
+// per column, the net and downward surface fluxes from the sfcfsw record
+// {upfxc, dnfxc, upfx0, dnfx0}.
+__global__ void sw_post_kernel(SwPostK a) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x, t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t im = (size_t)a.im;
+  if (a.day) {
+    map_levels(a.htswc, a.htsw0, a.htrsw, a.swhc, a.swhtr != 0, im, a.lm, a.levs, a.kd, t0, stride);
+  } else {
+    const size_t n = im * a.levs;
+    for (size_t e = t0; e < n; e += stride) {
+      __stcs(a.htrsw + e, 0.0);
+      if (a.swhtr) __stcs(a.swhc + e, 0.0);
+    }
+  }
+  for (size_t i = t0; i < im; i += stride) {
+    double* c = a.scmpsw + 6 * i;
+    double* f = a.sfcfsw + 4 * i;
+    if (a.day) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double v = c[2 + j];
+        a.dn[j][i] = v;
+        a.up[j][i] = v * a.alb[j][i];
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 6; ++j) c[j] = 0.0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        f[j] = 0.0;
+        a.dn[j][i] = 0.0;
+        a.up[j][i] = 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < 3; ++j) a.topfsw[3 * i + j] = 0.0;
+    }
+    a.sfcnsw[i] = f[1] - f[0];
+    a.sfcdsw[i] = f[1];
   }
 }
 
@@ -286,18 +353,22 @@ class Stager {
   std::vector<Item> items_;
 };
 
-// Common prologue: exec struct, device and stream.
-int begin(const rrtmg_lw_exec* x, bool* host, cudaStream_t* st, char* errmsg, int32_t errmsg_len) {
-  if (!x) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: null exec struct"); return 1; }
-  if (x->memory != RRTMG_LW_HOST && x->memory != RRTMG_LW_DEVICE) {
+// Common prologue: memory space, device and stream.
+int begin_on(int32_t memory, void* stream, int dev, bool* host, cudaStream_t* st, char* errmsg,
+             int32_t errmsg_len) {
+  if (memory != RRTMG_LW_HOST && memory != RRTMG_LW_DEVICE) {
     set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: memory must be RRTMG_LW_HOST or RRTMG_LW_DEVICE");
     return 1;
   }
-  *host = x->memory == RRTMG_LW_HOST;
-  const int dev = lw::selected_device();
+  *host = memory == RRTMG_LW_HOST;
   if (dev >= 0) CK(cudaSetDevice(dev), "cudaSetDevice");
-  *st = x->stream ? (cudaStream_t)x->stream : cudaStreamPerThread;
+  *st = stream ? (cudaStream_t)stream : cudaStreamPerThread;
   return 0;
+}
+
+int begin(const rrtmg_lw_exec* x, bool* host, cudaStream_t* st, char* errmsg, int32_t errmsg_len) {
+  if (!x) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: null exec struct"); return 1; }
+  return begin_on(x->memory, x->stream, lw::selected_device(), host, st, errmsg, errmsg_len);
 }
 
 int finish(Stager& S, bool host, bool sync, cudaStream_t st, char* errmsg, int32_t errmsg_len) {
@@ -444,7 +515,7 @@ extern "C" int rrtmg_lw_gpu_post(const rrtmg_lw_post_args* a, const rrtmg_lw_exe
                                  int32_t errmsg_len) {
   set_msg(errmsg, errmsg_len, "");
   if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_post: null argument struct"); return 1; }
-  if (!a->lslwr) return 0;   // rrtmg_lw_post.F90:41
+  if (!a->lslwr) return 0;   // rrtmg_lw_post.F90:42
   const int im = a->im, levs = a->levs, lm = a->lm, ltp = a->ltp, kd = a->kd;
   if (im < 0 || levs < 0 || lm < 0 || ltp < 0 || kd < 0 || kd > ltp || lm > levs || (levs > lm && lm < 1)) {
     set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_post: need im, levs, lm, ltp, kd >= 0, kd <= ltp, lm <= levs "
@@ -483,6 +554,96 @@ extern "C" int rrtmg_lw_gpu_post(const rrtmg_lw_post_args* a, const rrtmg_lw_exe
   const long long work = std::max<long long>((long long)im * lm / 4, im);
   const int grid = (int)std::min<long long>(blocks_for(work, 256), 8LL * sms);
   post_kernel<<<grid, 256, 0, st>>>(k);
+  return finish(S, host, x->sync != 0, st, errmsg, errmsg_len);
+}
+
+extern "C" int rrtmg_sw_gpu_post(const rrtmg_sw_post_args* a, const rrtmg_sw_exec* x, char* errmsg,
+                                 int32_t errmsg_len) {
+  set_msg(errmsg, errmsg_len, "");
+  if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_post: null argument struct"); return 1; }
+  if (!a->lsswr) return 0;   // rrtmg_sw_post.F90:52
+  const int im = a->im, levs = a->levs, lm = a->lm, ltp = a->ltp, kd = a->kd;
+  const bool day = a->nday > 0, hc = a->swhtr != 0;
+  if (im < 0 || levs < 0) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_post: need im, levs >= 0");
+    return 1;
+  }
+  if (day && (lm < 0 || ltp < 0 || kd < 0 || kd > ltp || lm > levs || (levs > lm && lm < 1))) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_post: with nday > 0 need lm, ltp, kd >= 0, kd <= ltp, "
+            "lm <= levs and lm >= 1 when levs > lm");
+    return 1;
+  }
+  double* const dn[4] = {a->nirbmdi, a->nirdfdi, a->visbmdi, a->visdfdi};
+  double* const up[4] = {a->nirbmui, a->nirdfui, a->visbmui, a->visdfui};
+  const double* const alb[4] = {a->sfcalb1, a->sfcalb2, a->sfcalb3, a->sfcalb4};
+  bool comps = true, albs = true;
+  for (int j = 0; j < 4; ++j) {
+    comps = comps && dn[j] && up[j];
+    albs = albs && alb[j];
+  }
+  const char* missing = nullptr;
+  if (!a->sfcfsw || !a->sfcdsw || !a->sfcnsw) missing = "sfcfsw, sfcdsw and sfcnsw";
+  else if (!a->scmpsw || !comps) missing = "scmpsw and the eight surface component fields";
+  else if (levs > 0 && !a->htrsw) missing = "htrsw";
+  else if (levs > 0 && hc && !a->swhc) missing = "swhc (swhtr)";
+  else if (day && !albs) missing = "sfcalb1..sfcalb4 (nday > 0)";
+  else if (day && lm > 0 && !a->htswc) missing = "htswc (nday > 0)";
+  else if (day && lm > 0 && hc && !a->htsw0) missing = "htsw0 (nday > 0, swhtr)";
+  else if (!day && !a->topfsw) missing = "topfsw (nday <= 0)";
+  if (missing) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_post: %s are required", missing); return 1; }
+  if (im == 0) return 0;
+  const rrtmg_sw_exec dflt{0, RRTMG_LW_HOST, nullptr, 1, 0, nullptr};
+  if (!x) x = &dflt;
+  bool host;
+  cudaStream_t st;
+  if (begin_on(x->memory, x->stream, lw::sw_selected_device(), &host, &st, errmsg, errmsg_len)) return 1;
+  SwPostK k{};
+  k.im = im;
+  k.levs = levs;
+  k.lm = day ? lm : 0;
+  k.kd = day ? kd : 0;
+  k.swhtr = hc ? 1 : 0;
+  k.day = day ? 1 : 0;
+  for (int j = 0; j < 4; ++j) {
+    k.alb[j] = day ? alb[j] : nullptr;
+    k.dn[j] = dn[j];
+    k.up[j] = up[j];
+  }
+  k.htswc = day ? a->htswc : nullptr;
+  k.htsw0 = day && hc ? a->htsw0 : nullptr;
+  k.sfcdsw = a->sfcdsw;
+  k.sfcnsw = a->sfcnsw;
+  k.htrsw = levs > 0 ? a->htrsw : nullptr;
+  k.swhc = levs > 0 && hc ? a->swhc : nullptr;
+  k.scmpsw = a->scmpsw;
+  k.sfcfsw = a->sfcfsw;
+  k.topfsw = day ? nullptr : a->topfsw;
+  // host memory: inputs copied in; outputs copied in and back (records the
+  // daytime branch only reads go one way)
+  const size_t nin = (size_t)im * (lm + ltp), nout = (size_t)im * levs;
+  Stager S(host, st);
+  for (int j = 0; j < 4; ++j) {
+    S.add(k.alb[j], im, false);
+    S.add(k.dn[j], im, true);
+    S.add(k.up[j], im, true);
+  }
+  S.add(k.sfcdsw, im, true);
+  S.add(k.sfcnsw, im, true);
+  S.add(k.scmpsw, 6 * (size_t)im, !day);
+  S.add(k.sfcfsw, 4 * (size_t)im, !day);
+  S.add(k.topfsw, 3 * (size_t)im, true);
+  S.add(k.htrsw, nout, true);
+  S.add(k.swhc, nout, true);
+  if (day && lm > 0) {
+    S.add(k.htswc, nin, false);
+    S.add(k.htsw0, nin, false);
+  }
+  CK(S.upload(), "staging");
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long work = std::max<long long>((long long)im * std::max(k.lm, 1) / 4, (long long)im * (day ? 1 : levs));
+  const int grid = (int)std::min<long long>(blocks_for(std::max<long long>(work, 1), 256), 8LL * sms);
+  sw_post_kernel<<<grid, 256, 0, st>>>(k);
   return finish(S, host, x->sync != 0, st, errmsg, errmsg_len);
 }
 

@@ -754,6 +754,13 @@ extern "C" int rrtmg_sw_gpu_mcica(int32_t npts, int32_t nlay, int32_t ldim, int3
   return 0;
 }
 
+// Device of the shortwave post step (lw_prep.cu): the init device, or -1
+// before init.
+int lw::sw_selected_device() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return g.ready ? g.device : -1;
+}
+
 extern "C" void rrtmg_sw_gpu_finalize(void) {
   std::lock_guard<std::mutex> lk(g_mu);
   for (SwWorkspace* w : g_ws) {

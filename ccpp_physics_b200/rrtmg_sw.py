@@ -65,6 +65,17 @@ class SwExec(C.Structure):
                 ("sync", C.c_int32), ("reserved", C.c_int32), ("kernel_ms", C.POINTER(C.c_float))]
 
 
+POST_INPUT_FIELDS = ("sfcalb1", "sfcalb2", "sfcalb3", "sfcalb4", "htswc", "htsw0")
+POST_OUTPUT_FIELDS = ("nirbmdi", "nirdfdi", "visbmdi", "visdfdi", "nirbmui", "nirdfui", "visbmui", "visdfui",
+                      "sfcdsw", "sfcnsw", "htrsw", "swhc", "scmpsw", "sfcfsw", "topfsw")
+
+
+class SwPostArgs(C.Structure):
+    """rrtmg_sw_post_args: rrtmg_sw_post_run (rrtmg_sw_post.F90:13-129)."""
+    _fields_ = ([(n, C.c_int32) for n in ("im", "levr", "levs", "ltp", "nday", "lm", "kd", "lsswr", "swhtr")]
+                + [(n, _dp) for n in POST_INPUT_FIELDS + POST_OUTPUT_FIELDS])
+
+
 def make_init_args(rad_hr_units=1, inc_minor_gas=True, iswcliq=1, isubcsw=2, iovr=1, iswmode=2, me=1,
                    device=0) -> SwInitArgs:
     return SwInitArgs(me=me, rad_hr_units=rad_hr_units, inc_minor_gas=int(inc_minor_gas), iswcliq=iswcliq,
@@ -214,6 +225,7 @@ def lib():
         L.rrtmg_sw_gpu_run_blocks.argtypes = [C.POINTER(SwRunArgs), C.c_int32, C.POINTER(SwExec), C.c_char_p,
                                               C.c_int32]
         L.rrtmg_sw_gpu_mcica.argtypes = ([C.c_int32] * 4 + [C.c_void_p] * 6 + [C.c_void_p, C.c_char_p, C.c_int32])
+        L.rrtmg_sw_gpu_post.argtypes = [C.POINTER(SwPostArgs), C.POINTER(SwExec), C.c_char_p, C.c_int32]
         L.rrtmg_sw_gpu_finalize.argtypes = []
         L.rrtmg_sw_gpu_finalize.restype = None
         _lib = L

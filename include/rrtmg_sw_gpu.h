@@ -159,6 +159,37 @@ int rrtmg_sw_gpu_mcica(int32_t npts, int32_t nlay, int32_t ldim, int32_t iovr,
                        const double *alpha, uint32_t *bits, void *stream,
                        char *errmsg, int32_t errmsg_len);
 
+/* rrtmg_sw_post_run (physics/Radiation/RRTMG/rrtmg_sw_post.F90:13-129), same
+ * argument names; every array (im[, levels]) with leading dimension im.
+ * When lsswr:
+ *   nday > 0:  htrsw(:,k) = htswc(:,k+kd) for k = 1..lm and htrsw(:,lm) for
+ *              k = lm+1..levs; the same from htsw0 into swhc when swhtr;
+ *              nirbmdi, nirdfdi, visbmdi, visdfdi = scmpsw%nirbm, %nirdf,
+ *              %visbm, %visdf and the ...ui fields those times sfcalb1..4;
+ *   nday <= 0: htrsw (im, levs), swhc (when swhtr), the eight component
+ *              fields and the sfcfsw, topfsw and scmpsw records set to 0;
+ * then sfcnsw = sfcfsw%dnfxc - sfcfsw%upfxc and sfcdsw = sfcfsw%dnfxc.
+ * levr is accepted and unused, as in the reference.  With nday > 0 it
+ * requires kd <= ltp, lm <= levs and lm >= 1 when levs > lm.  exec: memory,
+ * stream and sync as in rrtmg_sw_gpu_run_ex; precision is not read.  On the
+ * device-resident outputs of a run this keeps them on the device. */
+typedef struct rrtmg_sw_post_args {
+  int32_t im, levr, levs, ltp, nday, lm, kd;
+  int32_t lsswr, swhtr;
+  const double *sfcalb1, *sfcalb2, *sfcalb3, *sfcalb4;   /* (im) */
+  const double *htswc, *htsw0;                          /* (im, lm+ltp) */
+  double *nirbmdi, *nirdfdi, *visbmdi, *visdfdi;         /* (im) */
+  double *nirbmui, *nirdfui, *visbmui, *visdfui;         /* (im) */
+  double *sfcdsw, *sfcnsw;                              /* (im) */
+  double *htrsw, *swhc;          /* (im, levs); swhc only when swhtr */
+  double *scmpsw;                /* (im) cmpfsw_type records, inout */
+  double *sfcfsw;                /* (im) sfcfsw_type records, inout */
+  double *topfsw;                /* (im) topfsw_type records, inout */
+} rrtmg_sw_post_args;
+int rrtmg_sw_gpu_post(const rrtmg_sw_post_args *args,
+                      const rrtmg_sw_exec *exec, char *errmsg,
+                      int32_t errmsg_len);
+
 /* Releases the device tables of rrtmg_sw_gpu_init. */
 void rrtmg_sw_gpu_finalize(void);
 

@@ -33,6 +33,8 @@ def lib():
         L.oracle_sw_gas_optics.argtypes = [C.POINTER(sw.SwRunArgs), C.c_int] + [C.c_void_p] * 3
         L.oracle_sw_mcica.argtypes = [C.c_int, C.c_int32, C.c_int, C.c_void_p, C.c_void_p, C.c_double,
                                       C.c_void_p, C.c_void_p]
+        L.oracle_sw_post.argtypes = [C.POINTER(sw.SwPostArgs)]
+        L.oracle_sw_post.restype = None
         _lib = L
     return _lib
 
@@ -76,3 +78,19 @@ def mcica_bits(nlay, seed, iovr, cldf, dz=None, de_lgth=0.0, alpha=None):
     lib().oracle_sw_mcica(nlay, seed, iovr, cl.ctypes.data_as(C.c_void_p), vp(dz), de_lgth, vp(alpha),
                           bits.ctypes.data_as(C.c_void_p))
     return bits
+
+
+def post(im, levr, levs, ltp, nday, lm, kd, lsswr, swhtr, sfcalb1, sfcalb2, sfcalb3, sfcalb4, htswc, htsw0,
+         nirbmdi, nirdfdi, visbmdi, visdfdi, nirbmui, nirdfui, visbmui, visdfui, sfcdsw, sfcnsw, htrsw, swhc,
+         scmpsw, sfcfsw, topfsw):
+    """rrtmg_sw_post_run on numpy arrays (outputs and records in place), the
+    argument order of ``ccpp_physics_b200.rrtmg_sw_post.rrtmg_sw_post_run``."""
+    vals = locals()
+    a = sw.SwPostArgs(im=im, levr=levr, levs=levs, ltp=ltp, nday=nday, lm=lm, kd=kd, lsswr=int(bool(lsswr)),
+                      swhtr=int(bool(swhtr)))
+    for n in sw.POST_INPUT_FIELDS + sw.POST_OUTPUT_FIELDS:
+        v = vals[n]
+        if v is not None:
+            assert v.dtype == np.float64 and v.flags["C_CONTIGUOUS"], n
+            setattr(a, n, v.ctypes.data_as(C.POINTER(C.c_double)))
+    lib().oracle_sw_post(C.byref(a))

@@ -1263,4 +1263,54 @@ void oracle_sw_mcica(int nlay, int32_t seed, int iovr, const double* cldf, const
       if (lc[(size_t)n * nlay + k]) bits[n * nw + (k >> 5)] |= 1u << (k & 31);
 }
 
+// rrtmg_sw_post_run (physics/Radiation/RRTMG/rrtmg_sw_post.F90:13-129), a
+// scalar loop per statement in the reference's order; (im, ...) arrays
+// column-major with leading dimension im, records as in the run's outputs.
+void oracle_sw_post(const rrtmg_sw_post_args* a) {
+  if (!a->lsswr) return;
+  const int im = a->im, levs = a->levs, lm = a->lm, kd = a->kd;
+  auto at = [im](int i, int k) { return (size_t)i + (size_t)im * (k - 1); };   // (i, k), k 1-based
+  if (a->nday > 0) {
+    for (int k = 1; k <= lm; ++k)
+      for (int i = 0; i < im; ++i) a->htrsw[at(i, k)] = a->htswc[at(i, k + kd)];
+    if (lm < levs)
+      for (int k = lm + 1; k <= levs; ++k)
+        for (int i = 0; i < im; ++i) a->htrsw[at(i, k)] = a->htrsw[at(i, lm)];
+    if (a->swhtr) {
+      for (int k = 1; k <= lm; ++k)
+        for (int i = 0; i < im; ++i) a->swhc[at(i, k)] = a->htsw0[at(i, k + kd)];
+      if (lm < levs)
+        for (int k = lm + 1; k <= levs; ++k)
+          for (int i = 0; i < im; ++i) a->swhc[at(i, k)] = a->swhc[at(i, lm)];
+    }
+    for (int i = 0; i < im; ++i) {
+      const double* c = a->scmpsw + 6 * (size_t)i;   // {uvbfc, uvbf0, nirbm, nirdf, visbm, visdf}
+      a->nirbmdi[i] = c[2];
+      a->nirdfdi[i] = c[3];
+      a->visbmdi[i] = c[4];
+      a->visdfdi[i] = c[5];
+      a->nirbmui[i] = c[2] * a->sfcalb1[i];
+      a->nirdfui[i] = c[3] * a->sfcalb2[i];
+      a->visbmui[i] = c[4] * a->sfcalb3[i];
+      a->visdfui[i] = c[5] * a->sfcalb4[i];
+    }
+  } else {
+    for (size_t e = 0; e < (size_t)im * levs; ++e) a->htrsw[e] = 0.0;
+    for (int i = 0; i < im; ++i) {
+      for (int j = 0; j < 4; ++j) a->sfcfsw[4 * (size_t)i + j] = 0.0;
+      for (int j = 0; j < 3; ++j) a->topfsw[3 * (size_t)i + j] = 0.0;
+      for (int j = 0; j < 6; ++j) a->scmpsw[6 * (size_t)i + j] = 0.0;
+      a->nirbmdi[i] = a->nirdfdi[i] = a->visbmdi[i] = a->visdfdi[i] = 0.0;
+      a->nirbmui[i] = a->nirdfui[i] = a->visbmui[i] = a->visdfui[i] = 0.0;
+    }
+    if (a->swhtr)
+      for (size_t e = 0; e < (size_t)im * levs; ++e) a->swhc[e] = 0.0;
+  }
+  for (int i = 0; i < im; ++i) {
+    const double* f = a->sfcfsw + 4 * (size_t)i;   // {upfxc, dnfxc, upfx0, dnfx0}
+    a->sfcnsw[i] = f[1] - f[0];
+    a->sfcdsw[i] = f[1];
+  }
+}
+
 }  // extern "C"

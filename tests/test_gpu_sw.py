@@ -336,3 +336,89 @@ def test_sw_run_blocks_equals_per_block_calls(gpu, flags):
         for k in outs_b[b]:
             assert torch.equal(outs_b[b][k], outs_1[b][k]), (b, k)
     assert (outs_b[4]["hswc"] == 7.0).all()
+
+
+# ---- rrtmg_sw_post_run (rrtmg_sw_post.F90:13-129): bit-exact
+
+_POST_OUT = ("nirbmdi", "nirdfdi", "visbmdi", "visdfdi", "nirbmui", "nirdfui", "visbmui", "visdfui", "sfcdsw",
+             "sfcnsw", "htrsw", "swhc", "scmpsw", "sfcfsw", "topfsw")
+
+
+def _post_arrays(rng, im, levs, ltp, lm):
+    ins = dict(sfcalb1=rng.uniform(0, 1, im), sfcalb2=rng.uniform(0, 1, im), sfcalb3=rng.uniform(0, 1, im),
+               sfcalb4=rng.uniform(0, 1, im), htswc=rng.normal(size=(lm + ltp, im)),
+               htsw0=rng.normal(size=(lm + ltp, im)))
+    outs = {n: np.full(im, 7.0) for n in _POST_OUT[:10]}
+    outs.update(htrsw=np.full((levs, im), 7.0), swhc=np.full((levs, im), 7.0),
+                scmpsw=rng.uniform(0, 500, (im, 6)), sfcfsw=rng.uniform(0, 900, (im, 4)),
+                topfsw=rng.uniform(0, 1300, (im, 3)))
+    return ins, outs
+
+
+@pytest.mark.parametrize("device", [True, False])
+@pytest.mark.parametrize("nday,lm,ltp,kd,levs,swhtr", [(3, 127, 0, 0, 127, True), (5, 64, 1, 1, 70, True),
+                                                       (2, 64, 1, 0, 64, False), (0, 127, 0, 0, 127, True),
+                                                       (0, 64, 1, 1, 70, False)])
+def test_sw_post_matches_oracle(gpu, osw, device, nday, lm, ltp, kd, levs, swhtr):
+    import torch
+    from ccpp_physics_b200.rrtmg_sw_post import rrtmg_sw_post_run
+    rng = np.random.default_rng(lm + levs + nday)
+    im = 1500
+    ins, outs = _post_arrays(rng, im, levs, ltp, lm)
+    ref = {k: v.copy() for k, v in outs.items()}
+    osw.post(im, lm, levs, ltp, nday, lm, kd, True, swhtr, *ins.values(), *ref.values())
+    if device:
+        ins = {k: torch.from_numpy(v).cuda() for k, v in ins.items()}
+        outs = {k: torch.from_numpy(v).cuda() for k, v in outs.items()}
+    msg, err = rrtmg_sw_post_run(im, lm, levs, ltp, nday, lm, kd, True, swhtr, *ins.values(), *outs.values())
+    assert err == 0, msg
+    for k in _POST_OUT:
+        g = outs[k].cpu().numpy() if device else outs[k]
+        assert np.array_equal(g, ref[k]), k
+
+
+def test_sw_chain_run_post_on_device(gpu, osw):
+    """rrtmg_sw_run -> rrtmg_sw_post_run with every array on the device: the
+    post step moves the run's values bit for bit, and the chain meets the run's
+    bars against the same chain in the oracle."""
+    import torch
+    from ccpp_physics_b200.rrtmg_sw_post import rrtmg_sw_post_run
+    npts, nlay = 96, 127
+    prof = _profile(npts, nlay, 33, night_fraction=0.25, precip=True)
+    nday = len(prof["idxday"])
+    ref = sw.alloc_outputs(npts, nlay)
+    assert osw.run(prof, ref)[0] == 0
+    dev = {k: (torch.as_tensor(np.ascontiguousarray(v)).cuda() if isinstance(v, np.ndarray) else v)
+           for k, v in prof.items()}
+    out = sw.alloc_outputs(npts, nlay, like=torch.zeros(1, device="cuda"))
+    gpu.rrtmg_sw_run(dev, out, device_memory=True)
+    alb = [prof[n] for n in ("sfcalb_nir_dir", "sfcalb_nir_dif", "sfcalb_uvis_dir", "sfcalb_uvis_dif")]
+
+    def post_outs(z):
+        o = {n: z(npts) for n in _POST_OUT[:10]}
+        o.update(htrsw=z(nlay, npts), swhc=z(nlay, npts))
+        return o
+
+    po = post_outs(lambda *s: torch.full(s, 7.0, dtype=torch.float64, device="cuda"))
+    msg, err = rrtmg_sw_post_run(npts, nlay, nlay, 0, nday, nlay, 0, True, True, *[dev[n] for n in (
+        "sfcalb_nir_dir", "sfcalb_nir_dif", "sfcalb_uvis_dir", "sfcalb_uvis_dif")], out["hswc"], out["hsw0"],
+        *po.values(), out["fdncmp"], out["sfcflx"], out["topflx"])
+    assert err == 0, msg
+    got = {k: v.cpu().numpy() for k, v in po.items()}
+    run = {k: v.cpu().numpy() for k, v in out.items()}
+    moved = post_outs(lambda *s: np.full(s, 7.0))
+    osw.post(npts, nlay, nlay, 0, nday, nlay, 0, True, True, *alb, run["hswc"], run["hsw0"], *moved.values(),
+             run["fdncmp"], run["sfcflx"], run["topflx"])
+    for k in got:
+        assert np.array_equal(got[k], moved[k]), k
+    chain = post_outs(lambda *s: np.full(s, 7.0))
+    osw.post(npts, nlay, nlay, 0, nday, nlay, 0, True, True, *alb, ref["hswc"], ref["hsw0"], *chain.values(),
+             ref["fdncmp"], ref["sfcflx"], ref["topflx"])
+    for k in got:
+        floor = 1.0 if k in ("htrsw", "swhc") else 1e-300
+        tol = HR_TOL if k in ("htrsw", "swhc") else FLUX_RTOL
+        if k == "sfcnsw":
+            # a difference of two fluxes: the bar is relative to the downward flux
+            assert np.max(np.abs(got[k] - chain[k]) / np.maximum(chain["sfcdsw"], 1e-300)) <= 2 * FLUX_RTOL
+        else:
+            assert _rel(got[k], chain[k], floor) <= tol, (k, _rel(got[k], chain[k], floor))

@@ -184,7 +184,8 @@ def test_oracle_spcvrtc_overcast_and_clear_limits(osw):
 def test_sw_struct_layout_matches_header(tmp_path):
     if not shutil.which("gcc"):
         pytest.skip("gcc not available")
-    structs = {"rrtmg_sw_run_args": sw.SwRunArgs, "rrtmg_sw_init_args": sw.SwInitArgs, "rrtmg_sw_exec": sw.SwExec}
+    structs = {"rrtmg_sw_run_args": sw.SwRunArgs, "rrtmg_sw_init_args": sw.SwInitArgs, "rrtmg_sw_exec": sw.SwExec,
+               "rrtmg_sw_post_args": sw.SwPostArgs}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rrtmg_sw_gpu.h"', 'int main(void){']
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
@@ -232,3 +233,68 @@ def test_oracle_reproduces_golden_fixture(osw, name):
     ref = np.load(os.path.join(ROOT, "tests", "golden", f"oracle_{name}.npz"))
     for k in ref.files:
         assert np.array_equal(out[k], ref[k]), k
+
+
+def _post_case(rng, im, levs, ltp, lm, fill=7.0):
+    """Inputs and filled outputs of rrtmg_sw_post_run, Fortran-ordered."""
+    ins = dict(sfcalb1=rng.uniform(0, 1, im), sfcalb2=rng.uniform(0, 1, im), sfcalb3=rng.uniform(0, 1, im),
+               sfcalb4=rng.uniform(0, 1, im), htswc=rng.normal(size=(lm + ltp, im)),
+               htsw0=rng.normal(size=(lm + ltp, im)))
+    outs = {n: np.full(im, fill) for n in ("nirbmdi", "nirdfdi", "visbmdi", "visdfdi", "nirbmui", "nirdfui",
+                                           "visbmui", "visdfui", "sfcdsw", "sfcnsw")}
+    outs.update(htrsw=np.full((levs, im), fill), swhc=np.full((levs, im), fill),
+                scmpsw=rng.uniform(0, 500, (im, 6)), sfcfsw=rng.uniform(0, 900, (im, 4)),
+                topfsw=rng.uniform(0, 1300, (im, 3)))
+    return ins, outs
+
+
+@pytest.mark.parametrize("nday", [3, 0])
+def test_oracle_sw_post_restatement(osw, nday):
+    """rrtmg_sw_post_run (rrtmg_sw_post.F90:52-127) against numpy statements."""
+    rng = np.random.default_rng(11 + nday)
+    im, levs, ltp, lm, kd = 13, 9, 1, 6, 1
+    ins, outs = _post_case(rng, im, levs, ltp, lm)
+    before = {k: v.copy() for k, v in outs.items()}
+    osw.post(im, lm, levs, ltp, nday, lm, kd, True, True, *ins.values(), *outs.values())
+    if nday:
+        src = np.minimum(np.arange(levs), lm - 1) + kd
+        assert np.array_equal(outs["htrsw"], ins["htswc"][src]) and np.array_equal(outs["swhc"], ins["htsw0"][src])
+        c = before["scmpsw"]
+        for j, (d, u, alb) in enumerate((("nirbmdi", "nirbmui", "sfcalb1"), ("nirdfdi", "nirdfui", "sfcalb2"),
+                                         ("visbmdi", "visbmui", "sfcalb3"), ("visdfdi", "visdfui", "sfcalb4"))):
+            assert np.array_equal(outs[d], c[:, 2 + j]) and np.array_equal(outs[u], c[:, 2 + j] * ins[alb])
+        for k in ("scmpsw", "sfcfsw", "topfsw"):
+            assert np.array_equal(outs[k], before[k]), k
+    else:
+        for k, v in outs.items():
+            if k not in ("sfcdsw", "sfcnsw"):
+                assert not v.any(), k
+    f = outs["sfcfsw"]
+    assert np.array_equal(outs["sfcnsw"], f[:, 1] - f[:, 0]) and np.array_equal(outs["sfcdsw"], f[:, 1])
+    untouched = {k: v.copy() for k, v in outs.items()}
+    osw.post(im, lm, levs, ltp, nday, lm, kd, False, True, *ins.values(), *outs.values())   # lsswr false
+    assert all(np.array_equal(outs[k], untouched[k]) for k in outs)
+
+
+def test_sw_post_entry_point_validation():
+    """Host-side checks of rrtmg_sw_gpu_post (return before any CUDA call)."""
+    L = sw.lib()
+    x = sw.SwExec(memory=0, sync=1)
+    m = C.create_string_buffer(256)
+    assert L.rrtmg_sw_gpu_post(None, C.byref(x), m, 256) == 1 and b"null" in m.value
+    p = sw.SwPostArgs(im=2, levs=3, ltp=0, nday=1, lm=2, kd=1, lsswr=1)
+    assert L.rrtmg_sw_gpu_post(C.byref(p), C.byref(x), m, 256) == 1 and b"kd <= ltp" in m.value
+    p.lsswr = 0                                   # rrtmg_sw_post.F90:52: nothing to do
+    assert L.rrtmg_sw_gpu_post(C.byref(p), C.byref(x), m, 256) == 0
+    buf = (C.c_double * 64)()
+    dp = C.cast(buf, C.POINTER(C.c_double))
+    p = sw.SwPostArgs(im=2, levs=3, ltp=0, nday=0, lm=9, kd=5, lsswr=1)   # lm, kd unread at night
+    for n in sw.POST_OUTPUT_FIELDS:
+        if n != "topfsw":
+            setattr(p, n, dp)
+    assert L.rrtmg_sw_gpu_post(C.byref(p), C.byref(x), m, 256) == 1 and b"topfsw" in m.value
+    p.nday, p.lm, p.kd = 2, 3, 0
+    assert L.rrtmg_sw_gpu_post(C.byref(p), C.byref(x), m, 256) == 1 and b"sfcalb" in m.value
+    p.im = 0
+    p.sfcalb1 = p.sfcalb2 = p.sfcalb3 = p.sfcalb4 = p.htswc = p.htsw0 = dp
+    assert L.rrtmg_sw_gpu_post(C.byref(p), C.byref(x), m, 256) == 0   # no columns: nothing to do
