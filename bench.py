@@ -225,7 +225,9 @@ def caller_steps_leg(args, torch, timed, sh, peak_gbs):
       * McICA seeds (GFS_rad_time_vary): one twister stream of 2 x 147,456
         draws per face, then each column's pair; six calls, one per face;
       * decorrelation length (Hogan) + alpha for exponential-random overlap;
-      * rrtmg_lw_post_run: heating rates (total and clear sky) onto 127 levels.
+      * rrtmg_lw_post_run: heating rates (total and clear sky) onto 127 levels;
+      * rrtmg_sw_post_run: the same for the shortwave rates, plus the surface
+        component fields, every column daylit.
     Device-resident, timed with CUDA events; the oracle times the same work on
     a sample on one host core, and the GPU results are checked against it."""
     import math
@@ -321,8 +323,39 @@ def caller_steps_leg(args, torch, timed, sh, peak_gbs):
                    "cpu_oracle_columns_per_s": ns / cpu_s, "cpu_cores": 1, "cpu_sample": f"first {ns} columns",
                    "matches_oracle": bool(np.array_equal(outs[2][:, :ns].cpu().numpy(), ref[2])
                                           and np.array_equal(outs[3][:, :ns].cpu().numpy(), ref[3]))}
-    res["peak_gbs"] = peak_gbs
     del htlwc, htlw0, sfc, tsfa, outs
+
+    # rrtmg_sw_post_run, every column daylit (the branch that moves data)
+    from oracle import oracle_sw
+    from ccpp_physics_b200 import rrtmg_sw_post
+    f64 = dict(dtype=torch.float64, device="cuda")
+    sins = [torch.rand(n, generator=g, **f64) for _ in range(4)] + \
+           [torch.randn((nlay, n), generator=g, **f64) for _ in range(2)]
+    souts = [torch.zeros(n, **f64) for _ in range(10)] + [torch.zeros((nlay, n), **f64) for _ in range(2)] + \
+            [500 * torch.rand((n, 6), generator=g, **f64), 900 * torch.rand((n, 4), generator=g, **f64),
+             torch.zeros((n, 3), **f64)]
+
+    def swpost():
+        m, e = rrtmg_sw_post.rrtmg_sw_post_run(n, nlay, nlay, 0, n, nlay, 0, True, True, *sins, *souts,
+                                               stream=sh, sync=False)
+        if e:
+            raise RuntimeError(m)
+    swpost()
+    ms = timed(swpost, k)
+    cut = lambda a: np.ascontiguousarray((a[:, :ns] if a.dim() == 2 and a.shape[0] == nlay else a[:ns]).cpu().numpy())
+    sref_in = [cut(a) for a in sins]
+    sref_out = [np.zeros_like(cut(a)) for a in souts[:12]] + [cut(a) for a in souts[12:]]
+    t0 = time.perf_counter()
+    oracle_sw.post(ns, nlay, nlay, 0, ns, nlay, 0, True, True, *sref_in, *sref_out)
+    cpu_s = time.perf_counter() - t0
+    sbytes = (4 * nlay + 20) * 8 * n    # in: htswc, htsw0, 4 albedos, 4 of scmpsw, 2 of sfcfsw; out: the rest
+    res["sw_post"] = {"ms_per_step": ms / k, "columns_per_s": n * k / (ms / 1e3),
+                      "achieved_gbs": sbytes * k / (ms / 1e3) / 1e9, "bytes_per_step": sbytes,
+                      "hbm_frac": sbytes * k / (ms / 1e3) / 1e9 / peak_gbs,
+                      "cpu_oracle_columns_per_s": ns / cpu_s, "cpu_cores": 1, "cpu_sample": f"first {ns} columns",
+                      "matches_oracle": bool(all(np.array_equal(cut(a), r) for a, r in zip(souts, sref_out)))}
+    res["peak_gbs"] = peak_gbs
+    del sins, souts
     torch.cuda.empty_cache()
     return res
 
