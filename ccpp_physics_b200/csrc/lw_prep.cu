@@ -10,6 +10,8 @@
 //                                radiation_cloud_overlap.F90:28-145)
 // rrtmg_lw_gpu_post           <- rrtmg_lw_post_run (physics/Radiation/RRTMG/
 //                                rrtmg_lw_post.F90:13-77)
+// rrtmg_sw_gpu_pre            <- rad_sw_pre_run (physics/Radiation/RRTMG/
+//                                rad_sw_pre.F90:14-51)
 // rrtmg_sw_gpu_post           <- rrtmg_sw_post_run (physics/Radiation/RRTMG/
 //                                rrtmg_sw_post.F90:13-129)
 //
@@ -186,6 +188,77 @@ __global__ void post_kernel(PostK a) {
     a.tsflw[i] = a.tsfa[i];
     a.sfcdlw[i] = a.sfcflw[4 * i + 2];
   }
+}
+
+// rad_sw_pre_run (rad_sw_pre.F90:36-49): the daytime columns in increasing
+// order, as an ordered compaction in two passes over tiles of kPreTile
+// columns.  Pass 1 counts each tile's daytime columns; pass 2 gives each tile
+// its offset (the sum of the counts before it: a block-wide sum over at most
+// a few thousand tiles) and writes its columns at their ballot ranks.
+constexpr int kPreTile = 1024;
+constexpr double kCoszenMin = 0.0001;   // rad_sw_pre.F90:41
+
+__global__ void __launch_bounds__(kPreTile) sw_pre_count_kernel(const double* __restrict__ coszen, int im,
+                                                                int* __restrict__ counts) {
+  const long long i = (long long)blockIdx.x * kPreTile + threadIdx.x;
+  const int c = __syncthreads_count(i < im && coszen[i] >= kCoszenMin);
+  if (threadIdx.x == 0) counts[blockIdx.x] = c;
+}
+
+// idxday(1:nday) = daytime columns; idxday(nday+1:im) = 0 (rad_sw_pre.F90:39);
+// nday into *nday_out by tile 0.
+__global__ void __launch_bounds__(kPreTile) sw_pre_scatter_kernel(const double* __restrict__ coszen, int im,
+                                                                  const int* __restrict__ counts, int ntiles,
+                                                                  int32_t* __restrict__ idxday,
+                                                                  int32_t* __restrict__ nday_out) {
+  __shared__ int red[2][32];
+  __shared__ int wbase[32];
+  __shared__ int s_nday;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  int before = 0, all = 0;
+  for (int j = t; j < ntiles; j += kPreTile) {
+    const int c = counts[j];
+    all += c;
+    if (j < (int)blockIdx.x) before += c;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    before += __shfl_xor_sync(0xffffffffu, before, o);
+    all += __shfl_xor_sync(0xffffffffu, all, o);
+  }
+  if (lane == 0) {
+    red[0][w] = before;
+    red[1][w] = all;
+  }
+  const long long i = (long long)blockIdx.x * kPreTile + t;
+  const bool day = i < im && coszen[i] >= kCoszenMin;
+  const unsigned m = __ballot_sync(0xffffffffu, day);
+  if (lane == 0) wbase[w] = __popc(m);
+  __syncthreads();
+  if (w == 0) {
+    int b = red[0][lane], a = red[1][lane];
+    const int n = wbase[lane];
+    int incl = n;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    wbase[lane] = b + incl - n;   // tile offset + daytime columns of the warps before
+    if (lane == 0) s_nday = a;
+  }
+  __syncthreads();
+  const int nday = s_nday;
+  // a daytime column's rank is below nday and at most its own index, so the
+  // two stores never meet
+  if (day) idxday[wbase[w] + __popc(m & ((1u << lane) - 1u))] = (int32_t)(i + 1);
+  if (i < im && i >= nday) idxday[i] = 0;
+  if (blockIdx.x == 0 && t == 0) *nday_out = nday;
 }
 
 struct SwPostK {
@@ -555,6 +628,47 @@ extern "C" int rrtmg_lw_gpu_post(const rrtmg_lw_post_args* a, const rrtmg_lw_exe
   const int grid = (int)std::min<long long>(blocks_for(work, 256), 8LL * sms);
   post_kernel<<<grid, 256, 0, st>>>(k);
   return finish(S, host, x->sync != 0, st, errmsg, errmsg_len);
+}
+
+extern "C" int rrtmg_sw_gpu_pre(const rrtmg_sw_pre_args* a, const rrtmg_sw_exec* x, char* errmsg,
+                                int32_t errmsg_len) {
+  set_msg(errmsg, errmsg_len, "");
+  if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_pre: null argument struct"); return 1; }
+  const int im = a->im;
+  if (im < 0) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_pre: need im >= 0"); return 1; }
+  if (!a->nday || (im > 0 && !a->idxday) || (im > 0 && a->lsswr && !a->coszen)) {
+    set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_pre: nday, idxday and (lsswr) coszen are required");
+    return 1;
+  }
+  *a->nday = 0;   // rad_sw_pre.F90:38, 47
+  if (im == 0) return 0;
+  const rrtmg_sw_exec dflt{0, RRTMG_LW_HOST, nullptr, 1, 0, nullptr};
+  if (!x) x = &dflt;
+  bool host;
+  cudaStream_t st;
+  if (begin_on(x->memory, x->stream, lw::sw_selected_device(), &host, &st, errmsg, errmsg_len)) return 1;
+  const double* coszen = a->coszen;
+  int32_t* idxday = a->idxday;
+  const int ntiles = (int)(((long long)im + kPreTile - 1) / kPreTile);
+  Stager S(host, st);
+  if (a->lsswr) S.add(coszen, im, false);
+  S.add(idxday, im, true);
+  char* extra = nullptr;
+  CK(S.upload(sizeof(int32_t) * ((size_t)ntiles + 1), &extra), "staging");
+  int32_t nday = 0;
+  if (!a->lsswr) {
+    CK(cudaMemsetAsync(idxday, 0, sizeof(int32_t) * (size_t)im, st), "cudaMemsetAsync");   // rad_sw_pre.F90:48
+  } else {
+    int* counts = (int*)extra;
+    int32_t* nday_dev = (int32_t*)(extra + sizeof(int32_t) * (size_t)ntiles);
+    sw_pre_count_kernel<<<ntiles, kPreTile, 0, st>>>(coszen, im, counts);
+    sw_pre_scatter_kernel<<<ntiles, kPreTile, 0, st>>>(coszen, im, counts, ntiles, idxday, nday_dev);
+    CK(cudaGetLastError(), "kernel launch");
+    CK(cudaMemcpyAsync(&nday, nday_dev, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  }
+  if (finish(S, host, true, st, errmsg, errmsg_len)) return 1;
+  *a->nday = nday;
+  return 0;
 }
 
 extern "C" int rrtmg_sw_gpu_post(const rrtmg_sw_post_args* a, const rrtmg_sw_exec* x, char* errmsg,

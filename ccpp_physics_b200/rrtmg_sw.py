@@ -65,6 +65,11 @@ class SwExec(C.Structure):
                 ("sync", C.c_int32), ("reserved", C.c_int32), ("kernel_ms", C.POINTER(C.c_float))]
 
 
+class SwPreArgs(C.Structure):
+    """rrtmg_sw_pre_args: rad_sw_pre_run (rad_sw_pre.F90:14-51)."""
+    _fields_ = [("im", C.c_int32), ("lsswr", C.c_int32), ("coszen", _dp), ("nday", _ip), ("idxday", _ip)]
+
+
 POST_INPUT_FIELDS = ("sfcalb1", "sfcalb2", "sfcalb3", "sfcalb4", "htswc", "htsw0")
 POST_OUTPUT_FIELDS = ("nirbmdi", "nirdfdi", "visbmdi", "visdfdi", "nirbmui", "nirdfui", "visbmui", "visdfui",
                       "sfcdsw", "sfcnsw", "htrsw", "swhc", "scmpsw", "sfcfsw", "topfsw")
@@ -225,6 +230,7 @@ def lib():
         L.rrtmg_sw_gpu_run_blocks.argtypes = [C.POINTER(SwRunArgs), C.c_int32, C.POINTER(SwExec), C.c_char_p,
                                               C.c_int32]
         L.rrtmg_sw_gpu_mcica.argtypes = ([C.c_int32] * 4 + [C.c_void_p] * 6 + [C.c_void_p, C.c_char_p, C.c_int32])
+        L.rrtmg_sw_gpu_pre.argtypes = [C.POINTER(SwPreArgs), C.POINTER(SwExec), C.c_char_p, C.c_int32]
         L.rrtmg_sw_gpu_post.argtypes = [C.POINTER(SwPostArgs), C.POINTER(SwExec), C.c_char_p, C.c_int32]
         L.rrtmg_sw_gpu_finalize.argtypes = []
         L.rrtmg_sw_gpu_finalize.restype = None

@@ -159,6 +159,23 @@ int rrtmg_sw_gpu_mcica(int32_t npts, int32_t nlay, int32_t ldim, int32_t iovr,
                        const double *alpha, uint32_t *bits, void *stream,
                        char *errmsg, int32_t errmsg_len);
 
+/* rad_sw_pre_run (physics/Radiation/RRTMG/rad_sw_pre.F90:14-51), same
+ * argument names: the daytime points of the call.  When lsswr, idxday(1:nday)
+ * lists, in increasing order, the 1-based columns i with coszen(i) >= 0.0001,
+ * and idxday(nday+1:im) = 0; otherwise nday = 0 and idxday = 0.  coszen and
+ * idxday are (im) arrays in the exec's memory space; nday is always a host
+ * int32, so the call waits for its stream to read it back (exec.sync is not
+ * read).  With memory = 1 the idxday it writes feeds rrtmg_sw_gpu_run_ex
+ * directly.  Returns errflg. */
+typedef struct rrtmg_sw_pre_args {
+  int32_t im, lsswr;
+  const double *coszen;  /* (im) */
+  int32_t *nday;         /* host */
+  int32_t *idxday;       /* (im) */
+} rrtmg_sw_pre_args;
+int rrtmg_sw_gpu_pre(const rrtmg_sw_pre_args *args, const rrtmg_sw_exec *exec,
+                     char *errmsg, int32_t errmsg_len);
+
 /* rrtmg_sw_post_run (physics/Radiation/RRTMG/rrtmg_sw_post.F90:13-129), same
  * argument names; every array (im[, levels]) with leading dimension im.
  * When lsswr:

@@ -33,6 +33,8 @@ def lib():
         L.oracle_sw_gas_optics.argtypes = [C.POINTER(sw.SwRunArgs), C.c_int] + [C.c_void_p] * 3
         L.oracle_sw_mcica.argtypes = [C.c_int, C.c_int32, C.c_int, C.c_void_p, C.c_void_p, C.c_double,
                                       C.c_void_p, C.c_void_p]
+        L.oracle_sw_pre.argtypes = [C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int32), C.c_void_p]
+        L.oracle_sw_pre.restype = None
         L.oracle_sw_post.argtypes = [C.POINTER(sw.SwPostArgs)]
         L.oracle_sw_post.restype = None
         _lib = L
@@ -94,3 +96,13 @@ def post(im, levr, levs, ltp, nday, lm, kd, lsswr, swhtr, sfcalb1, sfcalb2, sfca
             assert v.dtype == np.float64 and v.flags["C_CONTIGUOUS"], n
             setattr(a, n, v.ctypes.data_as(C.POINTER(C.c_double)))
     lib().oracle_sw_post(C.byref(a))
+
+
+def pre(im, lsswr, coszen):
+    """rad_sw_pre_run: returns (nday, idxday (im,) int32)."""
+    idx = np.zeros(im, np.int32)
+    nday = C.c_int32(0)
+    cz = np.ascontiguousarray(coszen, np.float64)
+    lib().oracle_sw_pre(im, int(bool(lsswr)), cz.ctypes.data_as(C.c_void_p), C.byref(nday),
+                        idx.ctypes.data_as(C.c_void_p))
+    return nday.value, idx

@@ -1263,6 +1263,19 @@ void oracle_sw_mcica(int nlay, int32_t seed, int iovr, const double* cldf, const
       if (lc[(size_t)n * nlay + k]) bits[n * nw + (k >> 5)] |= 1u << (k & 31);
 }
 
+// rad_sw_pre_run (physics/Radiation/RRTMG/rad_sw_pre.F90:14-51): the daytime
+// columns, in the reference's loop.
+void oracle_sw_pre(int im, int lsswr, const double* coszen, int32_t* nday, int32_t* idxday) {
+  *nday = 0;
+  for (int i = 0; i < im; ++i) idxday[i] = 0;
+  if (!lsswr) return;
+  for (int i = 1; i <= im; ++i)
+    if (coszen[i - 1] >= 0.0001) {
+      *nday += 1;
+      idxday[*nday - 1] = i;
+    }
+}
+
 // rrtmg_sw_post_run (physics/Radiation/RRTMG/rrtmg_sw_post.F90:13-129), a
 // scalar loop per statement in the reference's order; (im, ...) arrays
 // column-major with leading dimension im, records as in the run's outputs.

@@ -422,3 +422,75 @@ def test_sw_chain_run_post_on_device(gpu, osw):
             assert np.max(np.abs(got[k] - chain[k]) / np.maximum(chain["sfcdsw"], 1e-300)) <= 2 * FLUX_RTOL
         else:
             assert _rel(got[k], chain[k], floor) <= tol, (k, _rel(got[k], chain[k], floor))
+
+
+# ---- rad_sw_pre_run (rad_sw_pre.F90:14-51): bit-exact
+
+@pytest.mark.parametrize("device", [True, False])
+@pytest.mark.parametrize("im", [1, 31, 1024, 1025, 5000, 884_736])
+def test_sw_pre_matches_oracle(gpu, osw, device, im):
+    import torch
+    from ccpp_physics_b200.rad_sw_pre import rad_sw_pre_run
+    rng = np.random.default_rng(im)
+    cz = rng.uniform(-1, 1, im)
+    cz[::7] = 1e-4
+    cz[1::11] = np.nextafter(1e-4, 0)
+    cz[2::13] = np.nextafter(1e-4, 1)
+    for lsswr in (True, False):
+        nref, iref = osw.pre(im, lsswr, cz)
+        idx = np.full(im, 9, np.int32)
+        czg = cz
+        if device:
+            idx, czg = torch.from_numpy(idx).cuda(), torch.from_numpy(cz).cuda()
+        nday, msg, err = rad_sw_pre_run(im, lsswr, czg, idx)
+        assert err == 0, msg
+        got = idx.cpu().numpy() if device else idx
+        assert nday == nref and np.array_equal(got, iref), (lsswr, nday, nref)
+
+
+def test_sw_chain_pre_run_post_on_device(gpu, osw):
+    """rad_sw_pre_run -> rrtmg_sw_run -> rrtmg_sw_post_run, every array on the
+    device, against the same chain in the oracle."""
+    import torch
+    from ccpp_physics_b200.rad_sw_pre import rad_sw_pre_run
+    from ccpp_physics_b200.rrtmg_sw_post import rrtmg_sw_post_run
+    npts, nlay = 200, 127
+    prof = _profile(npts, nlay, 41, night_fraction=0.4, precip=True)
+    night = np.ones(npts, bool)
+    night[prof["idxday"] - 1] = False
+    coszen = np.where(night, -0.3, prof["cosz"])
+    nref, iref = osw.pre(npts, True, coszen)
+    assert nref == len(prof["idxday"]) and np.array_equal(iref[:nref], prof["idxday"])
+    ref = sw.alloc_outputs(npts, nlay)
+    assert osw.run(dict(prof, idxday=iref[:nref].copy()), ref)[0] == 0
+
+    dev = {k: (torch.as_tensor(np.ascontiguousarray(v)).cuda() if isinstance(v, np.ndarray) else v)
+           for k, v in prof.items()}
+    idx = torch.zeros(npts, dtype=torch.int32, device="cuda")
+    nday, msg, err = rad_sw_pre_run(npts, True, torch.from_numpy(coszen).cuda(), idx)
+    assert err == 0 and nday == nref, msg
+    dev["idxday"] = idx[:nday]
+    out = sw.alloc_outputs(npts, nlay, like=torch.zeros(1, device="cuda"))
+    gpu.rrtmg_sw_run(dev, out, device_memory=True)
+    _check({k: v.cpu().numpy() for k, v in out.items()}, ref)
+
+    names = ("sfcalb_nir_dir", "sfcalb_nir_dif", "sfcalb_uvis_dir", "sfcalb_uvis_dif")
+    po = {n: torch.zeros(npts, dtype=torch.float64, device="cuda") for n in _POST_OUT[:10]}
+    po.update(htrsw=torch.zeros((nlay, npts), dtype=torch.float64, device="cuda"),
+              swhc=torch.zeros((nlay, npts), dtype=torch.float64, device="cuda"))
+    msg, err = rrtmg_sw_post_run(npts, nlay, nlay, 0, nday, nlay, 0, True, True, *[dev[n] for n in names],
+                                 out["hswc"], out["hsw0"], *po.values(), out["fdncmp"], out["sfcflx"],
+                                 out["topflx"])
+    assert err == 0, msg
+    pr = {n: np.zeros(npts) for n in _POST_OUT[:10]}
+    pr.update(htrsw=np.zeros((nlay, npts)), swhc=np.zeros((nlay, npts)))
+    osw.post(npts, nlay, nlay, 0, nref, nlay, 0, True, True, *[prof[n] for n in names], ref["hswc"], ref["hsw0"],
+             *pr.values(), ref["fdncmp"], ref["sfcflx"], ref["topflx"])
+    for k, v in po.items():
+        g = v.cpu().numpy()
+        if k in ("htrsw", "swhc"):
+            assert _rel(g, pr[k], 1.0) <= HR_TOL, k
+        elif k == "sfcnsw":
+            assert np.max(np.abs(g - pr[k]) / np.maximum(pr["sfcdsw"], 1e-300)) <= 2 * FLUX_RTOL
+        else:
+            assert _rel(g, pr[k], 1e-300) <= FLUX_RTOL, k

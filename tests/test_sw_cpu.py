@@ -185,7 +185,7 @@ def test_sw_struct_layout_matches_header(tmp_path):
     if not shutil.which("gcc"):
         pytest.skip("gcc not available")
     structs = {"rrtmg_sw_run_args": sw.SwRunArgs, "rrtmg_sw_init_args": sw.SwInitArgs, "rrtmg_sw_exec": sw.SwExec,
-               "rrtmg_sw_post_args": sw.SwPostArgs}
+               "rrtmg_sw_post_args": sw.SwPostArgs, "rrtmg_sw_pre_args": sw.SwPreArgs}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "rrtmg_sw_gpu.h"', 'int main(void){']
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
@@ -298,3 +298,33 @@ def test_sw_post_entry_point_validation():
     p.im = 0
     p.sfcalb1 = p.sfcalb2 = p.sfcalb3 = p.sfcalb4 = p.htswc = p.htsw0 = dp
     assert L.rrtmg_sw_gpu_post(C.byref(p), C.byref(x), m, 256) == 0   # no columns: nothing to do
+
+
+def test_oracle_sw_pre_restatement(osw):
+    """rad_sw_pre_run (rad_sw_pre.F90:36-49) against numpy, with values on the
+    0.0001 threshold and either side of it."""
+    rng = np.random.default_rng(5)
+    im = 3000
+    cz = rng.uniform(-1, 1, im)
+    cz[::7] = 1e-4
+    cz[1::11] = np.nextafter(1e-4, 0)
+    cz[2::13] = np.nextafter(1e-4, 1)
+    nday, idx = osw.pre(im, True, cz)
+    want = np.nonzero(cz >= 1e-4)[0] + 1
+    assert nday == len(want) and np.array_equal(idx[:nday], want) and not idx[nday:].any()
+    nday, idx = osw.pre(im, False, cz)
+    assert nday == 0 and not idx.any()
+
+
+def test_sw_pre_entry_point_validation():
+    L = sw.lib()
+    x = sw.SwExec(memory=0, sync=1)
+    m = C.create_string_buffer(256)
+    nd = C.c_int32(5)
+    assert L.rrtmg_sw_gpu_pre(None, C.byref(x), m, 256) == 1 and b"null" in m.value
+    p = sw.SwPreArgs(im=-1, lsswr=1, nday=C.pointer(nd))
+    assert L.rrtmg_sw_gpu_pre(C.byref(p), C.byref(x), m, 256) == 1 and b"im >= 0" in m.value
+    p.im = 4
+    assert L.rrtmg_sw_gpu_pre(C.byref(p), C.byref(x), m, 256) == 1 and b"required" in m.value
+    p.im = 0                                      # no columns: nday = 0, nothing else to do
+    assert L.rrtmg_sw_gpu_pre(C.byref(p), C.byref(x), m, 256) == 0 and nd.value == 0
