@@ -9,6 +9,11 @@
  *   rrtmg_sw_run  physics/Radiation/RRTMG/radsw_main.F90:493-510
  *                 (argument declarations radsw_main.F90:688-782)
  *
+ * and the CCPP schemes either side of the run:
+ *
+ *   rad_sw_pre_run     physics/Radiation/RRTMG/rad_sw_pre.F90:14-51
+ *   rrtmg_sw_post_run  physics/Radiation/RRTMG/rrtmg_sw_post.F90:13-129
+ *
  * Array conventions are those of rrtmg_lw_gpu.h: the caller's Fortran arrays,
  * column-major, real(8); element (i, k) of an (npts, nlay) array is at
  * ptr[(i-1) + (k-1)*ldim], element (i, k, b) of an (npts, nlay, nbands)
