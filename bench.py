@@ -227,7 +227,8 @@ def caller_steps_leg(args, torch, timed, sh, peak_gbs):
       * decorrelation length (Hogan) + alpha for exponential-random overlap;
       * rrtmg_lw_post_run: heating rates (total and clear sky) onto 127 levels;
       * rrtmg_sw_post_run: the same for the shortwave rates, plus the surface
-        component fields, every column daylit.
+        component fields, every column daylit;
+      * rad_sw_pre_run: the daytime points of all 884,736 columns.
     Device-resident, timed with CUDA events; the oracle times the same work on
     a sample on one host core, and the GPU results are checked against it."""
     import math
@@ -354,8 +355,33 @@ def caller_steps_leg(args, torch, timed, sh, peak_gbs):
                       "hbm_frac": sbytes * k / (ms / 1e3) / 1e9 / peak_gbs,
                       "cpu_oracle_columns_per_s": ns / cpu_s, "cpu_cores": 1, "cpu_sample": f"first {ns} columns",
                       "matches_oracle": bool(all(np.array_equal(cut(a), r) for a, r in zip(souts, sref_out)))}
-    res["peak_gbs"] = peak_gbs
     del sins, souts
+
+    # rad_sw_pre_run: the daytime points of the whole call (nday read back each call)
+    from ccpp_physics_b200 import rad_sw_pre
+    cz = 2 * torch.rand(n, generator=g, **f64) - 1
+    idx = torch.zeros(n, dtype=torch.int32, device="cuda")
+    got = {}
+
+    def swpre():
+        nd, m, e = rad_sw_pre.rad_sw_pre_run(n, True, cz, idx, stream=sh)
+        if e:
+            raise RuntimeError(m)
+        got["nday"] = nd
+    swpre()
+    ms = timed(swpre, k)
+    czh = cz.cpu().numpy()
+    t0 = time.perf_counter()
+    nref, iref = oracle_sw.pre(n, True, czh)
+    cpu_s = time.perf_counter() - t0
+    pre_bytes = 12 * n                  # coszen in, idxday out
+    res["sw_pre"] = {"ms_per_step": ms / k, "columns_per_s": n * k / (ms / 1e3),
+                     "achieved_gbs": pre_bytes * k / (ms / 1e3) / 1e9, "bytes_per_step": pre_bytes,
+                     "note": "two launches and a 4-byte read-back of nday per call: latency-bound",
+                     "cpu_oracle_columns_per_s": n / cpu_s, "cpu_cores": 1, "cpu_sample": f"all {n} columns",
+                     "matches_oracle": bool(got["nday"] == nref and np.array_equal(idx.cpu().numpy(), iref))}
+    res["peak_gbs"] = peak_gbs
+    del cz, idx
     torch.cuda.empty_cache()
     return res
 
