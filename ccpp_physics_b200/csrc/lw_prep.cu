@@ -318,6 +318,9 @@ __global__ void sw_post_kernel(SwPostK a) {
 
 // ------------------------------------------------------------------- host --
 
+// Entry point of the calling thread's current call, named in error messages.
+thread_local const char* tl_who = "rrtmg_lw_gpu";
+
 void set_msg(char* errmsg, int32_t len, const char* fmt, ...) {
   if (!errmsg || len <= 0) return;
   va_list ap;
@@ -327,7 +330,7 @@ void set_msg(char* errmsg, int32_t len, const char* fmt, ...) {
 }
 
 int fail(char* errmsg, int32_t len, const char* what, cudaError_t e) {
-  set_msg(errmsg, len, "rrtmg_lw_gpu: %s failed: %s", what, cudaGetErrorString(e));
+  set_msg(errmsg, len, "%s: %s failed: %s", tl_who, what, cudaGetErrorString(e));
   return 1;
 }
 
@@ -430,7 +433,7 @@ class Stager {
 int begin_on(int32_t memory, void* stream, int dev, bool* host, cudaStream_t* st, char* errmsg,
              int32_t errmsg_len) {
   if (memory != RRTMG_LW_HOST && memory != RRTMG_LW_DEVICE) {
-    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: memory must be RRTMG_LW_HOST or RRTMG_LW_DEVICE");
+    set_msg(errmsg, errmsg_len, "%s: memory must be 0 (host) or 1 (device)", tl_who);
     return 1;
   }
   *host = memory == RRTMG_LW_HOST;
@@ -440,7 +443,7 @@ int begin_on(int32_t memory, void* stream, int dev, bool* host, cudaStream_t* st
 }
 
 int begin(const rrtmg_lw_exec* x, bool* host, cudaStream_t* st, char* errmsg, int32_t errmsg_len) {
-  if (!x) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu: null exec struct"); return 1; }
+  if (!x) { set_msg(errmsg, errmsg_len, "%s: null exec struct", tl_who); return 1; }
   return begin_on(x->memory, x->stream, lw::selected_device(), host, st, errmsg, errmsg_len);
 }
 
@@ -457,6 +460,7 @@ int blocks_for(long long n, int threads) { return (int)((n + threads - 1) / thre
 
 extern "C" int rrtmg_lw_gpu_seeds(const rrtmg_lw_seed_args* a, const rrtmg_lw_exec* x, char* errmsg,
                                   int32_t errmsg_len) {
+  tl_who = "rrtmg_lw_gpu_seeds";
   set_msg(errmsg, errmsg_len, "");
   if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_seeds: null argument struct"); return 1; }
   // GFS_rad_time_vary.fv3.F90:59, :64
@@ -526,6 +530,7 @@ extern "C" int rrtmg_lw_gpu_seeds(const rrtmg_lw_seed_args* a, const rrtmg_lw_ex
 
 extern "C" int rrtmg_lw_gpu_overlap_params(const rrtmg_lw_overlap_args* a, const rrtmg_lw_exec* x, char* errmsg,
                                            int32_t errmsg_len) {
+  tl_who = "rrtmg_lw_gpu_overlap_params";
   set_msg(errmsg, errmsg_len, "");
   if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_overlap_params: null argument struct"); return 1; }
   if (a->mode < RRTMG_LW_OVERLAP_CLOUDS || a->mode > RRTMG_LW_OVERLAP_ALPHA) {
@@ -586,6 +591,7 @@ extern "C" int rrtmg_lw_gpu_overlap_params(const rrtmg_lw_overlap_args* a, const
 
 extern "C" int rrtmg_lw_gpu_post(const rrtmg_lw_post_args* a, const rrtmg_lw_exec* x, char* errmsg,
                                  int32_t errmsg_len) {
+  tl_who = "rrtmg_lw_gpu_post";
   set_msg(errmsg, errmsg_len, "");
   if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_post: null argument struct"); return 1; }
   if (!a->lslwr) return 0;   // rrtmg_lw_post.F90:42
@@ -632,6 +638,7 @@ extern "C" int rrtmg_lw_gpu_post(const rrtmg_lw_post_args* a, const rrtmg_lw_exe
 
 extern "C" int rrtmg_sw_gpu_pre(const rrtmg_sw_pre_args* a, const rrtmg_sw_exec* x, char* errmsg,
                                 int32_t errmsg_len) {
+  tl_who = "rrtmg_sw_gpu_pre";
   set_msg(errmsg, errmsg_len, "");
   if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_pre: null argument struct"); return 1; }
   const int im = a->im;
@@ -673,6 +680,7 @@ extern "C" int rrtmg_sw_gpu_pre(const rrtmg_sw_pre_args* a, const rrtmg_sw_exec*
 
 extern "C" int rrtmg_sw_gpu_post(const rrtmg_sw_post_args* a, const rrtmg_sw_exec* x, char* errmsg,
                                  int32_t errmsg_len) {
+  tl_who = "rrtmg_sw_gpu_post";
   set_msg(errmsg, errmsg_len, "");
   if (!a) { set_msg(errmsg, errmsg_len, "rrtmg_sw_gpu_post: null argument struct"); return 1; }
   if (!a->lsswr) return 0;   // rrtmg_sw_post.F90:52
