@@ -129,3 +129,37 @@ def test_packed_blocks_layout():
         assert addr(arr[2], name) - addr(arr[0], name) == 35 * per_col, name
     with pytest.raises(ValueError):
         lw.block_args(pp, o, sizes)          # profile packed, outputs not
+
+
+def test_fortran_shims_match_the_c_abi():
+    """No Fortran compiler here, so the shims are checked as text: every
+    bind(c) name is a function declared in include/*.h and exported, and every
+    bind(c) record has the C struct's fields in order with matching kinds
+    (the ctypes mirrors are pinned to the header by the gcc layout tests)."""
+    from ccpp_physics_b200 import rrtmg_lw as lw, rrtmg_sw as sw
+    L = lw.lib()
+    declared = _declared()
+    mirrors = {"c_init_args": abi.InitArgs, "c_run_args": abi.RunArgs, "c_sw_init_args": sw.SwInitArgs,
+               "c_sw_run_args": sw.SwRunArgs, "c_sw_exec": sw.SwExec, "c_sw_pre_args": sw.SwPreArgs,
+               "c_sw_post_args": sw.SwPostArgs}
+    kinds = {"integer(c_int32_t)": C.c_int32, "real(c_double)": C.c_double}
+    seen = set()
+    for path in sorted(glob.glob(os.path.join(ROOT, "ccpp_physics_b200", "fortran", "*.F90"))):
+        txt = open(path).read()
+        for name in re.findall(r'bind\(c,\s*name="(\w+)"\)', txt):
+            assert name in declared and hasattr(L, name), (path, name)
+        for tname, body in re.findall(r"type, bind\(c\) :: (\w+)\n(.*?)\n\s*end type", txt, re.S):
+            fields = []
+            for line in body.splitlines():
+                kind, names = (p.strip() for p in line.split("::"))
+                for n in names.split(","):
+                    fields.append((n.split("=")[0].strip(), kind))
+            py = mirrors[tname]._fields_
+            assert [f for f, _ in fields] == [f for f, _ in py], (path, tname)
+            for (f, kind), (_, ct) in zip(fields, py):
+                if kind == "type(c_ptr)":
+                    assert issubclass(ct, (C._Pointer, C.c_void_p)), (tname, f)
+                else:
+                    assert kinds[kind] is ct, (tname, f)
+            seen.add(tname)
+    assert seen == set(mirrors)
