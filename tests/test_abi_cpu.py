@@ -141,7 +141,7 @@ def test_fortran_shims_match_the_c_abi():
     declared = _declared()
     mirrors = {"c_init_args": abi.InitArgs, "c_run_args": abi.RunArgs, "c_sw_init_args": sw.SwInitArgs,
                "c_sw_run_args": sw.SwRunArgs, "c_sw_exec": sw.SwExec, "c_sw_pre_args": sw.SwPreArgs,
-               "c_sw_post_args": sw.SwPostArgs}
+               "c_sw_post_args": sw.SwPostArgs, "c_lw_exec": abi.ExecArgs, "c_lw_post_args": abi.PostArgs}
     kinds = {"integer(c_int32_t)": C.c_int32, "real(c_double)": C.c_double}
     seen = set()
     for path in sorted(glob.glob(os.path.join(ROOT, "ccpp_physics_b200", "fortran", "*.F90"))):
