@@ -22,6 +22,10 @@
 //
 //     spcvrtc (isubcsw <= 0)   RSM:2432-3183, as spcvrtm's grid-mean mode
 //
+// and the CCPP schemes either side of the run:
+//     rad_sw_pre_run           physics/Radiation/RRTMG/rad_sw_pre.F90:14-51
+//     rrtmg_sw_post_run        physics/Radiation/RRTMG/rrtmg_sw_post.F90:13-129
+//
 // Parity of this restatement is NOT pinned by the reference: the reference is
 // Fortran, no Fortran compiler exists in this environment, and the reference
 // tree holds no tests or golden vectors for this path.  The coefficient
