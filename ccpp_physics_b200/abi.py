@@ -101,6 +101,17 @@ OVERLAP_FLAGS = dict(iovr_rand=0, iovr_maxrand=1, iovr_max=2, iovr_dcorr=3,
                      iovr_exp=4, iovr_exprand=5)
 
 
+def _check_dtype(name, x, kind):
+    """Raise TypeError unless numpy array / torch tensor ``x`` holds ``kind``
+    ("f8" for real(8), "i4" for int32); None passes."""
+    if x is None:
+        return
+    want = {"f8": ("float64",), "i4": ("int32",)}[kind]
+    got = str(x.dtype).replace("torch.", "")
+    if got not in want:
+        raise TypeError(f"{name} must be {want[0]}, got {got}")
+
+
 def _ptr(x, ctype):
     """Pointer to the data of a numpy array or torch tensor (None -> NULL)."""
     if x is None:

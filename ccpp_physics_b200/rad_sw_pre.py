@@ -19,6 +19,8 @@ from .rrtmg_sw import SwExec, SwPreArgs, lib
 
 
 def rad_sw_pre_run(im, lsswr, coszen, idxday, *, stream=None):
+    abi._check_dtype("coszen", coszen, "f8")
+    abi._check_dtype("idxday", idxday, "i4")
     nday = C.c_int32(0)
     a = SwPreArgs(im=int(im), lsswr=int(bool(lsswr)), coszen=abi._ptr(coszen, C.c_double),
                   nday=C.pointer(nday), idxday=abi._ptr(idxday, C.c_int32))

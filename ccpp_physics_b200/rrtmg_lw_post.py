@@ -25,6 +25,7 @@ def rrtmg_lw_post_run(im, levs, ltp, lm, kd, lslwr, lwhtr, tsfa, htlwc, htlw0, s
                      lwhtr=int(bool(lwhtr)))
     for n, v in (("tsfa", tsfa), ("htlwc", htlwc), ("htlw0", htlw0), ("sfcflw", sfcflw), ("tsflw", tsflw),
                  ("sfcdlw", sfcdlw), ("htrlw", htrlw), ("lwhc", lwhc)):
+        abi._check_dtype(n, v, "f8")
         setattr(a, n, abi._ptr(v, C.c_double))
     st = torch_stream(stream, htrlw)
     x = abi.ExecArgs(memory=abi.DEVICE if _is_device(htrlw) else abi.HOST,

@@ -30,6 +30,7 @@ def rrtmg_sw_post_run(im, levr, levs, ltp, nday, lm, kd, lsswr, swhtr, sfcalb1, 
     a = SwPostArgs(im=int(im), levr=int(levr), levs=int(levs), ltp=int(ltp), nday=int(nday), lm=int(lm),
                    kd=int(kd), lsswr=int(bool(lsswr)), swhtr=int(bool(swhtr)))
     for n in POST_INPUT_FIELDS + POST_OUTPUT_FIELDS:
+        abi._check_dtype(n, vals[n], "f8")
         setattr(a, n, abi._ptr(vals[n], C.c_double))
     st = torch_stream(stream, sfcfsw)
     x = SwExec(precision=0, memory=abi.DEVICE if _is_device(sfcfsw) else abi.HOST,

@@ -328,3 +328,17 @@ def test_sw_pre_entry_point_validation():
     assert L.rrtmg_sw_gpu_pre(C.byref(p), C.byref(x), m, 256) == 1 and b"required" in m.value
     p.im = 0                                      # no columns: nday = 0, nothing else to do
     assert L.rrtmg_sw_gpu_pre(C.byref(p), C.byref(x), m, 256) == 0 and nd.value == 0
+
+
+def test_pre_post_wrappers_refuse_wrong_dtypes():
+    """A wrong element type would be read through the wrong pointer type: the
+    Python mirrors refuse it before any call."""
+    from ccpp_physics_b200.rad_sw_pre import rad_sw_pre_run
+    from ccpp_physics_b200.rrtmg_sw_post import rrtmg_sw_post_run
+    with pytest.raises(TypeError, match="idxday must be int32"):
+        rad_sw_pre_run(4, True, np.ones(4), np.zeros(4, np.int64))
+    with pytest.raises(TypeError, match="coszen must be float64"):
+        rad_sw_pre_run(4, True, np.ones(4, np.float32), np.zeros(4, np.int32))
+    z = np.zeros(2)
+    with pytest.raises(TypeError, match="sfcalb1 must be float64"):
+        rrtmg_sw_post_run(2, 1, 1, 0, 1, 1, 0, True, False, z.astype(np.float32), *[z] * 20)
