@@ -1,25 +1,44 @@
 """Benchmark of the B200 RRTMG-LW column path (rrtmg_lw_run replacement).
 
-Workload (default): 16,384 columns x 127 layers, all-sky McICA with maximum-
-random overlap (ilwcliq=1, ilwcice=3, isubclw=2, seeds = column index),
-seeded synthetic profiles (ccpp_physics_b200.synthetic).  One step = one
-rrtmg_lw_run over all columns of the rank.  `value` is the FP64 GPU path
-with inputs resident in HBM (columns/s, whole job); `e2e` is the same call
-through the C ABI with pinned host buffers, copies inside the timed region.
-Other precision paths are reported under `paths` with their flux and
-heating-rate RMSE against the FP64 GPU path.
+Workload: 884,736 columns x 127 layers (six 384 x 384 cubed-sphere faces),
+all-sky McICA with maximum-random overlap (ilwcliq=1, ilwcice=3, isubclw=2,
+seeds = column index), seeded synthetic profiles
+(ccpp_physics_b200.synthetic), split into uneven physics blocks of 8..256
+columns (sizes U{8..256}, seed 7), each block its own (n_b, nlay) array as a
+UFS host allocates them.  One step = one rrtmg_lw_gpu_run_blocks call over
+every block of the rank (autotuned launch shape, replayed as a CUDA graph).
+
+The last line printed is the headline JSON record:
+  value      plain FP64 path, inputs resident in HBM, columns/s of the job;
+  paths      the FP32 and learned-gas-optics paths on the same blocks, with
+             their flux / heating-rate RMSE against FP64 and speed-up;
+  parity     FP64 GPU outputs against the CPU restatement (oracle/) on the
+             first 65,536 columns of the workload and on the 16,384-column
+             all-sky case (with flux profiles);
+  e2e        the same FP64 work through rrtmg_lw_gpu_run with pinned host
+             arrays, host<->device copies inside the timed region;
+  roofline   the column kernels against the measured HBM copy bandwidth, and
+             fp_pipe their FP64 flops against the measured FMA peak;
+  cpu_baseline  the oracle on all host cores, timed on the parity sample.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--config c2|c3|c1]
-Multi-GPU: one process per GPU (torchrun), each rank a shard of columns
-(weak scaling, no data-path collective).
+                    [--legs sw,callers,train]
+--gpus N > 1 starts N ranks itself (torch.distributed.run) unless it already
+runs under a launcher (WORLD_SIZE set).  Each rank takes whole physics blocks
+of the workload (ccpp_physics_b200.shard.block_range): the total work is
+fixed ("scaling": "strong"), no collective touches the data path, and only
+the per-rank times are reduced (max over ranks).  --legs prints the
+auxiliary legs (shortwave scheme, the steps either side of the run, the
+surrogate's training throughput) as JSON lines before the headline.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import datetime
 import json
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -30,21 +49,29 @@ sys.path.insert(0, ROOT)
 
 METRIC = "LW columns/s @127 lev: plain FP64 vs FP32 vs surrogate, flux RMSE vs FP64"
 BYTES_PER_COL = 61052     # compulsory HBM bytes per column at 127 layers (FP64 interface)
-CONFIGS = {
-    "c2": dict(ncols=16384, nlay=127, cloudy=True, name="c2_allsky_mcica_16384x127"),
-    "c3": dict(ncols=884736, nlay=127, cloudy=True, name="c3_block_884736x127"),
-    "c1": dict(ncols=1024, nlay=64, cloudy=False, name="c1_clear_1024x64"),
-}
+NCOLS, NLAY = 884_736, 127
+WORKLOAD = "c3_physics_blocks_884736x127"
+PARITY_SAMPLE = 65_536    # columns of the workload checked against the oracle
+C2_COLS = 16_384          # the all-sky McICA case (first columns of the same generator)
 
 
-def n_chunks(ncols, nlay, real_bytes=8, budget=6 << 30):
-    """Chunks the library splits a call into (its scratch budget, 6 GiB by
-    default): tau/frac (140 g-points) + 3x16 band fields per padded layer,
-    plus a 48-double column record."""
-    v = 2 if nlay <= 63 else 4 if nlay <= 127 else 8
-    per = (2 * 140 + 3 * 16) * 32 * v * real_bytes + 48 * 8
-    budget = int(os.environ.get("RRTMG_LW_GPU_SCRATCH_MB", budget >> 20)) << 20
-    return -(-ncols // max(1, budget // per))
+def workload_config(world):
+    """The `config` object of both arms (identical for the same N)."""
+    return {"workload": WORKLOAD, "ncols": NCOLS, "nlay": NLAY,
+            "blocks": "U{8..256} (seed 7), 6,686 blocks, each its own (n_b, nlay) array",
+            "clouds": "all-sky McICA, max-random overlap (iovr=1, isubclw=2)",
+            "parallelism": f"block shards x{world}",
+            "l2": "inputs 54 GB per step > 126 MB L2, no flush needed"}
+
+
+def rank_blocks(rank, world):
+    """Physics-block sizes of the workload and this rank's shard of them:
+    (all sizes, this rank's sizes, first global column of the shard)."""
+    import numpy as np
+    from ccpp_physics_b200 import shard, synthetic
+    sizes = synthetic.physics_blocks(NCOLS, seed=7)
+    b0, b1 = shard.block_range(sizes, rank, world)
+    return sizes, sizes[b0:b1], int(np.sum(sizes[:b0]))
 
 
 def _peaks():
@@ -54,6 +81,21 @@ def _peaks():
         return p.get("hbm_gbs", 6650.0), "measured"
     except OSError:
         return 6650.0, "fallback"
+
+
+def fma_peak():
+    """(FP64, FP32) FMA throughput of the current GPU in TFLOP/s from the
+    separate microbenchmark library (libfma_peak.so), or (None, None)."""
+    path = os.path.join(ROOT, "ccpp_physics_b200", "libfma_peak.so")
+    try:
+        L = ctypes.CDLL(path)
+        L.fma_peak_tflops.argtypes = [ctypes.POINTER(ctypes.c_double)] * 2
+        p64, p32 = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        if L.fma_peak_tflops(ctypes.byref(p64), ctypes.byref(p32)) == 0:
+            return p64.value, p32.value
+    except OSError:
+        pass
+    return None, None
 
 
 class ClockSampler:
@@ -107,116 +149,86 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_rate(prof_np, seconds=10.0, nthreads=0):
-    """Oracle (CPU restatement) columns/s on a bounded sample of the workload."""
-    from oracle import oracle
-    from ccpp_physics_b200 import synthetic
-    oracle.rlwinit()
-    n = min(256, prof_np["npts"])
-    sub = synthetic.slice_columns(prof_np, 0, n)
-    t0 = time.perf_counter()
-    rc, msg, _ = oracle.rrtmg_lw_run(sub, nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    assert rc == 0, msg
-    target = int(min(prof_np["npts"], max(n, n * seconds / max(dt, 1e-6))))
-    sub = synthetic.slice_columns(prof_np, 0, target)
-    t0 = time.perf_counter()
-    rc, msg, _ = oracle.rrtmg_lw_run(sub, nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    assert rc == 0, msg
-    return target / dt, target, dt
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
 
 
-def run_reference(args, cfg, rank, world):
-    """Reference arm: the CPU restatement of rrtmg_lw_run (no Fortran
-    compiler exists on these machines) on all host threads."""
+def relaunch(args):
+    """--gpus N > 1 outside a launcher: start N ranks with torch.distributed.run
+    (same arguments) and return its exit code."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={_free_port()}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def dry_run(args, rank, world, local):
+    """The multi-rank plumbing alone (no GPU work): process group (NCCL with a
+    GPU, gloo without), the max-over-ranks reduction of a per-rank time, and
+    rank 0's line with n_gpus."""
+    import torch
+    import torch.distributed as dist
+    use_cuda = torch.cuda.is_available()
+    if world > 1:
+        if use_cuda:
+            torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if use_cuda else "gloo", timeout=datetime.timedelta(seconds=60))
+    dev = torch.device("cuda", local) if use_cuda else torch.device("cpu")
+    t = torch.tensor([1.0 + rank], dtype=torch.float64, device=dev)
+    seen = torch.tensor([1 << rank], dtype=torch.int64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(seen, op=dist.ReduceOp.SUM)
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        _, mine, c0 = rank_blocks(rank, world)
+        print(json.dumps({"dry_run": True, "n_gpus": world, "ranks_seen": int(seen.item()),
+                          "max_over_ranks": float(t.item()), "rank0_columns": int(sum(mine)),
+                          "config": workload_config(world)}), flush=True)
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the CPU restatement of rrtmg_lw_run (no Fortran compiler
+    exists on these machines to build the reference itself) on all host
+    threads; each step is one bounded sample of the workload's columns, a
+    different one per step."""
     if rank != 0:
         return
     from ccpp_physics_b200 import synthetic
     from oracle import oracle
     ncores = os.cpu_count() or 1
-    oracle.rlwinit()
-    sample = min(cfg["ncols"], 4096)
-    prof = synthetic.make_profiles(sample, cfg["nlay"], seed=1, cloudy=cfg["cloudy"])
-    for _ in range(args.warmup):
-        oracle.rrtmg_lw_run(synthetic.slice_columns(prof, 0, min(512, sample)), nthreads=ncores)
+    rc, msg = oracle.rlwinit()
+    assert rc == 0, msg
+    sample = 16_384
+    profs = {}
+
+    def prof(i):
+        c0 = (i * sample) % (NCOLS - sample)
+        if c0 not in profs:
+            profs[c0] = synthetic.make_profiles(sample, NLAY, seed=1, col_offset=c0)
+        return profs[c0]
+    for i in range(args.warmup):
+        oracle.rrtmg_lw_run(synthetic.slice_columns(prof(0), 0, 1024), nthreads=ncores)
     times = []
-    for _ in range(args.steps):
+    for i in range(args.steps):
+        p = prof(i)
         t0 = time.perf_counter()
-        rc, msg, _ = oracle.rrtmg_lw_run(prof, nthreads=ncores)
+        rc, msg, _ = oracle.rrtmg_lw_run(p, nthreads=ncores)
         times.append(time.perf_counter() - t0)
         assert rc == 0, msg
     rate = sample * len(times) / sum(times)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": rate, "unit": "columns/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": {"workload": cfg["name"], "ncols_sampled_per_step": sample, "nlay": cfg["nlay"]},
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(world),
         "cpu_baseline": {"value": rate, "unit": "columns/s", "cores": ncores, "kind": "port",
-                         "sample": f"{sample} columns of {cfg['name']} per step, OpenMP over columns"},
+                         "sample": f"{sample} consecutive columns of {WORKLOAD} per step (a different range "
+                                   f"each step), OpenMP over columns"},
         "e2e": {"value": rate, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
-
-
-def batched_leg(args, lw, abi, synthetic, torch, rank, world, sh, timed, rmse):
-    """FP32 (and FP64) rrtmg_lw over 884,736 columns x 127 layers split into
-    uneven physics blocks of 8..256 columns (sizes U{8..256}, fixed seed), all
-    blocks in one rrtmg_lw_gpu_run_blocks call: one persistent launch per
-    kernel and chunk, launch shape from the autotuner, replayed as a CUDA
-    graph.  Inputs (56 GB) are far larger than L2."""
-    import ctypes as C
-    cfg = CONFIGS["c3"]
-    n3, nlay = cfg["ncols"], cfg["nlay"]
-    sizes = synthetic.physics_blocks(n3, seed=7)
-    prof = synthetic.make_profiles(n3, nlay, seed=1, cloudy=True, col_offset=rank * n3, device="cuda")
-    # each physics block is its own (n_b, nlay) array, as the GFS host allocates its blocks
-    lw.pack_blocks(prof, sizes, inplace=True)
-    torch.cuda.empty_cache()
-    res = {"workload": cfg["name"], "nblocks": int(len(sizes)), "block_sizes": "U{8..256}, seed 7",
-           "block_layout": "one contiguous (n_b, nlay) array per block (ldim = n_b)"}
-    outs = {}
-    k = max(2, min(args.steps, 5))
-    precs = ("fp32", "fp64", "surrogate") if args.surrogate_ready else ("fp32", "fp64")
-    for prec in precs:
-        out = lw.pack_blocks(abi.alloc_outputs(n3, nlay, hlw0=True, like="cuda"), sizes, inplace=True)
-        if prec == "surrogate":
-            from ccpp_physics_b200 import surrogate as sg
-        t0 = time.time()
-        best, tune_ms = lw.autotune(prof, out, sizes, precision=prec, sample_cols=65536, stream=sh)
-        tune_s = time.time() - t0
-        arr, keep = lw.block_args(prof, out, sizes)
-        x = abi.ExecArgs(precision=lw.PRECISIONS[prec], memory=abi.DEVICE, stream=sh, sync=0)
-        tun = abi.Tuning(**dict(best, use_graph=1))
-        buf = C.create_string_buffer(256)
-
-        def call():
-            if lw.lib().rrtmg_lw_gpu_run_blocks(arr, len(arr), C.byref(x), C.byref(tun), buf, 256):
-                raise RuntimeError(buf.value.decode())
-        for _ in range(2):
-            call()
-        if prec == "surrogate":
-            sg.stats(reset=True)
-        ms = timed(call, k)
-        res[prec] = {"value": world * n3 * k / (ms / 1e3), "ms_per_step": ms / k, "steps": k,
-                     "tuning": best, "autotune_s": round(tune_s, 2), "graph": True}
-        if prec == "surrogate":
-            fb, mma_err = sg.stats()
-            res[prec]["fallback_layer_fraction"] = fb / float(k * n3 * nlay)
-            res[prec]["mma_error"] = mma_err
-        outs[prec] = out
-    b = outs["fp64"]
-    for prec in precs:
-        if prec == "fp64":
-            continue
-        a = outs[prec]
-        res[prec].update({
-            "flux_rmse_wm2": rmse(torch.cat([a["topflx"], a["sfcflx"]], 1), torch.cat([b["topflx"], b["sfcflx"]], 1)),
-            "hr_rmse_kday": rmse(a["hlwc"], b["hlwc"]), "hr0_rmse_kday": rmse(a["hlw0"], b["hlw0"]),
-            "speedup_vs_fp64": res[prec]["value"] / res["fp64"]["value"]})
-    del prof, outs, a, b
-    torch.cuda.empty_cache()
-    return res
 
 
 def caller_steps_leg(args, torch, timed, sh, peak_gbs):
@@ -515,10 +527,9 @@ def sw_leg(args, torch, timed, sh):
         tf = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "sw_kernels_traffic.txt")
         with open(tf) as fh:
             tr = {kk.strip(): float(v) for kk, v in (l.split(":", 1) for l in fh if ":" in l and not l.startswith("#"))}
-        p64, p32 = C.c_double(0.0), C.c_double(0.0)
-        from ccpp_physics_b200 import rrtmg_lw as lwm
-        lwm.lib().rrtmg_lw_gpu_fma_peak.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
-        rc_peak = lwm.lib().rrtmg_lw_gpu_fma_peak(C.byref(p64), C.byref(p32))
+        p64v, _ = fma_peak()
+        rc_peak = 0 if p64v else 1
+        p64 = C.c_double(p64v or 0.0)
         t_rt = km[2] / 1e3
         ach_tf = tr["sw_fp64_flop_per_column_rt"] * n / t_rt / 1e12
         ach_gbs = tr["sw_dram_bytes_per_column_rt"] * n / t_rt / 1e9
@@ -582,78 +593,52 @@ def training_leg(args, torch, sg):
                                 "final_loss": float(meta["losses"][-1])}}
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ncols", type=int, default=0, help="override the column count (profiling runs)")
-    ap.add_argument("--quick", action="store_true", help="FP64 device-resident loop only (profiling runs)")
-    ap.add_argument("--no-batch", action="store_true", help="skip the 884,736-column batched-block leg")
-    ap.add_argument("--no-callers", action="store_true",
-                    help="skip the leg of the steps either side of rrtmg_lw_run (seeds, overlap, post)")
-    ap.add_argument("--no-train", action="store_true", help="skip the surrogate training-throughput leg")
-    ap.add_argument("--no-sw", action="store_true", help="skip the shortwave (rrtmg_sw_run) leg")
-    ap.add_argument("--sw-only", action="store_true", help="run the shortwave leg alone (profiling runs)")
-    ap.add_argument("--sw-ncols", type=int, default=16384, help="columns of the shortwave leg")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "surrogate"],
-                    help="with --quick: the path to loop over (profiling runs)")
-    args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
-    cfg = dict(CONFIGS[args.config])
-    if args.ncols:
-        cfg["ncols"] = args.ncols
-        cfg["name"] = f"{cfg['name']}_first{args.ncols}"
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        run_reference(args, cfg, rank, world)
-        return
-
+def _rel(a, b, floor):
     import numpy as np
-    import torch
-    from ccpp_physics_b200 import abi, synthetic
-    from ccpp_physics_b200 import rrtmg_lw as lw
+    return np.abs(a - b) / np.maximum(np.abs(b), floor)
 
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    rc, msg = lw.rlwinit(device=local, me=1)   # me != 0: no banner, stdout carries only the JSON line
-    assert rc == 0, msg
-    ncols, nlay = cfg["ncols"], cfg["nlay"]
-    # each rank owns its own shard of columns (weak scaling)
-    prof = synthetic.make_profiles(ncols, nlay, seed=1, cloudy=cfg["cloudy"], col_offset=rank * ncols,
-                                   device="cuda")
-    out = abi.alloc_outputs(ncols, nlay, hlw0=True, like="cuda")
-    # a dedicated stream: the library and the CUDA events must share it (the
-    # legacy default stream does not order work of non-blocking streams)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    sh = stream.cuda_stream
 
-    def step(precision="fp64", o=out, kernel_ms=None, flags=None):
-        keep = []
-        a = abi.make_run_args(prof, o, flags=flags, keep=keep)
-        x = abi.ExecArgs(precision=lw.PRECISIONS[precision], memory=abi.DEVICE, stream=sh, sync=0,
-                         kernel_ms=kernel_ms)
-        buf = __import__("ctypes").create_string_buffer(256)
-        r = lw.lib().rrtmg_lw_gpu_run_ex(__import__("ctypes").byref(a), __import__("ctypes").byref(x), buf, 256)
-        if r:
-            raise RuntimeError(buf.value.decode())
+def parity_check(gpu, ref, ncheck, c_start, flux_keys=("topflx", "sfcflx"), tol=1e-10):
+    """Max relative difference of the GPU FP64 outputs (numpy, first ncheck
+    columns) from the oracle's; the columns over `tol` are counted and the
+    first few named by global index."""
+    import numpy as np
+    bad = np.zeros(ncheck, dtype=bool)
+    fmax = 0.0
+    for k in flux_keys:
+        r = _rel(gpu[k], ref[k], 1e-300)
+        fmax = max(fmax, float(r.max()))
+        col_axis = 1 if k == "flxprf" else 0
+        rr = r.reshape(r.shape[0], -1) if col_axis == 0 else np.moveaxis(r, 1, 0).reshape(ncheck, -1)
+        bad |= rr.max(axis=1) > tol
+    hmax = 0.0
+    for k in ("hlwc", "hlw0"):
+        r = _rel(gpu[k], ref[k], 1.0)   # K/day, floored at 1 K/day as in the parity tests
+        hmax = max(hmax, float(r.max()))
+    idx = np.nonzero(bad)[0]
+    return {"flux_max_rel": fmax, "hr_max_rel": hmax, "cols": ncheck, "cols_over_1e-10": int(idx.size),
+            "cols_over_named": [int(c_start + i) for i in idx[:8]]}
+
+
+def headline(args, rank, world, local, dist, torch, sh, stream, lw, abi, synthetic):
+    """The default workload on this rank's blocks: FP64 (the headline value),
+    FP32 and the learned gas optics, parity against the oracle, end to end
+    from pinned host memory, roofline and CPU baseline."""
+    import ctypes as C
+    import numpy as np
 
     def barrier():
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
+
+    def maxr(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
 
     def timed(fn, k):
         barrier()
@@ -663,6 +648,198 @@ def main():
             fn()
         e1.record(stream)
         barrier()
+        return maxr(e0.elapsed_time(e1))
+
+    def rmse(a, b):
+        return float(torch.sqrt(torch.mean((a - b) ** 2)).item())
+
+    _, sizes, c_start = rank_blocks(rank, world)
+    ncols = int(np.sum(sizes))
+    prof = synthetic.make_profiles(ncols, NLAY, seed=1, cloudy=True, col_offset=c_start, device="cuda")
+    # pinned host copy (the caller's Fortran arrays) for the end-to-end leg
+    hprof, h2d = None, 0
+    if not args.no_e2e:
+        hprof = dict(npts=ncols, nlay=NLAY, flags=dict(prof["flags"]))
+        for k, v in prof.items():
+            if isinstance(v, torch.Tensor):
+                hv = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+                hv.copy_(v)
+                hprof[k] = hv
+                h2d += hv.numel() * hv.element_size()
+    lw.pack_blocks(prof, sizes, inplace=True)
+    torch.cuda.empty_cache()
+
+    k_main = args.steps
+    k_other = max(3, min(args.steps, 10))
+    res, outs = {}, {}
+    from ccpp_physics_b200 import surrogate as sg
+    try:
+        sg.load()
+        precs = ("fp64", "fp32", "surrogate")
+    except Exception as exc:   # weights missing: report, do not fake
+        res["surrogate"] = {"value": None, "note": f"no trained network: {exc}"}
+        precs = ("fp64", "fp32")
+    clk = None
+    buf = C.create_string_buffer(512)
+    for prec in precs:
+        out = lw.pack_blocks(abi.alloc_outputs(ncols, NLAY, hlw0=True, like="cuda"), sizes, inplace=True)
+        best, _ = lw.autotune(prof, out, sizes, precision=prec, sample_cols=65536, stream=sh)
+        arr, keep = lw.block_args(prof, out, sizes)
+        x = abi.ExecArgs(precision=lw.PRECISIONS[prec], memory=abi.DEVICE, stream=sh, sync=0)
+        tun = abi.Tuning(**dict(best, use_graph=1))
+
+        def call():
+            if lw.lib().rrtmg_lw_gpu_run_blocks(arr, len(arr), C.byref(x), C.byref(tun), buf, 512):
+                raise RuntimeError(buf.value.decode())
+        for _ in range(args.warmup):
+            call()
+        if prec == "surrogate":
+            sg.stats(reset=True)
+        if prec == "fp64":
+            with ClockSampler(local) as clk:
+                ms = timed(call, k_main)
+            k = k_main
+        else:
+            ms = timed(call, k_other)
+            k = k_other
+        launches = int(lw.lib().rrtmg_lw_gpu_last_launch_count())
+        # per-kernel device times of one call without the graph
+        kms = (C.c_float * 3)()
+        xk = abi.ExecArgs(precision=lw.PRECISIONS[prec], memory=abi.DEVICE, stream=sh, sync=1,
+                          kernel_ms=C.cast(kms, C.POINTER(C.c_float)))
+        tk = abi.Tuning(**dict(best, use_graph=0))
+        if lw.lib().rrtmg_lw_gpu_run_blocks(arr, len(arr), C.byref(xk), C.byref(tk), buf, 512):
+            raise RuntimeError(buf.value.decode())
+        r = {"value": NCOLS * k / (ms / 1e3), "ms_per_step": ms / k, "steps": k, "launches_per_step": launches,
+             "mcica_ms": kms[0], "tuning": {kk: int(v) for kk, v in best.items()}}
+        if prec == "surrogate":
+            fb, mma_err = sg.stats()
+            r["fallback_layer_frac"] = fb / float(k * ncols * NLAY)
+            r["mma_error"] = mma_err
+        res[prec] = r
+        outs[prec] = out
+    b = outs["fp64"]
+    for prec in precs[1:]:
+        a = outs[prec]
+        res[prec].update({
+            "speedup_vs_fp64": res[prec]["value"] / res["fp64"]["value"],
+            "flux_rmse_wm2": rmse(torch.cat([a["topflx"], a["sfcflx"]], 1), torch.cat([b["topflx"], b["sfcflx"]], 1)),
+            "hr_rmse_kday": rmse(a["hlwc"], b["hlwc"]), "hr0_rmse_kday": rmse(a["hlw0"], b["hlw0"])})
+        del a
+        outs[prec] = None
+    # FP64 outputs in the caller's (unpacked) layout, on the host
+    gpu64 = {kk: v.cpu().numpy() for kk, v in lw.unpack_blocks(outs["fp64"]).items()}
+    del outs, b, prof
+    torch.cuda.empty_cache()
+
+    # ---- end to end: rrtmg_lw_gpu_run on pinned host arrays ----
+    e2e = None
+    if hprof is not None:
+        hout = {kk: torch.empty(v.shape, dtype=torch.float64, pin_memory=True) for kk, v in gpu64.items()}
+        d2h = sum(v.numel() * v.element_size() for v in hout.values())
+        m, e = lw.run_profile(hprof, hout, precision="fp64")
+        assert e == 0, m
+        ke = max(1, min(args.steps, 3))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            m, e = lw.run_profile(hprof, hout, precision="fp64")
+            assert e == 0, m
+        t_e2e = maxr(time.perf_counter() - t0)
+        e2e = {"value": NCOLS * ke / t_e2e, "unit": "columns/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": ke,
+               "matches_device_run": bool(all(np.array_equal(hout[kk].numpy(), gpu64[kk]) for kk in hout))}
+        del hprof, hout
+
+    # ---- parity against the oracle + CPU baseline (rank 0) ----
+    parity, cpu = None, None
+    if rank == 0 and not args.no_parity:
+        from oracle import oracle
+        rc, msg = oracle.rlwinit()
+        assert rc == 0, msg
+        ncores = os.cpu_count() or 1
+        ns = min(ncols, PARITY_SAMPLE)
+        pnp = synthetic.make_profiles(ns, NLAY, seed=1, col_offset=c_start)
+        t0 = time.perf_counter()
+        rc, msg, ref = oracle.rrtmg_lw_run(pnp, hlw0=True, flxprf=True, nthreads=ncores)
+        dt = time.perf_counter() - t0
+        assert rc == 0, msg
+        cpu = {"value": ns / dt, "unit": "columns/s", "cores": ncores, "kind": "port",
+               "sample": f"first {ns} columns of {WORKLOAD} ({dt:.1f} s), OpenMP over columns"}
+        sub = {kk: (v[:ns] if kk in ("topflx", "sfcflx") else v[:, :ns]) for kk, v in gpu64.items()}
+        parity = {"c3_first_%d" % ns: parity_check(sub, ref, ns, c_start)}
+        # the 16,384-column all-sky case as one call, flux profiles included
+        n2 = min(ns, C2_COLS)
+        p2 = synthetic.make_profiles(n2, NLAY, seed=1, col_offset=c_start, device="cuda")
+        o2 = abi.alloc_outputs(n2, NLAY, hlw0=True, flxprf=True, like="cuda")
+        m, e = lw.run_profile(p2, o2, precision="fp64")
+        assert e == 0, m
+        g2 = {kk: v.cpu().numpy() for kk, v in o2.items()}
+        r2 = {kk: (v[:n2] if kk in ("topflx", "sfcflx") else v[:, :n2] if kk != "flxprf" else v[:, :n2, :])
+              for kk, v in ref.items()}
+        parity["c2_%d" % n2] = parity_check(g2, r2, n2, c_start, flux_keys=("topflx", "sfcflx", "flxprf"))
+        del p2, o2
+    return res, e2e, parity, cpu, clk, ncols
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--legs", default="", help="comma list of auxiliary legs printed before the headline: "
+                                                "sw, callers, train")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-memory leg")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle parity check and CPU baseline")
+    ap.add_argument("--dry-run", action="store_true", help="launcher and process-group plumbing only")
+    ap.add_argument("--ncols", type=int, default=0, help="profiling runs: one device-resident call of the "
+                                                         "first NCOLS columns, --precision, no other legs")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "surrogate"])
+    ap.add_argument("--sw-ncols", type=int, default=16384, help="columns of the shortwave leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch(args))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.dry_run:
+        dry_run(args, rank, world, local)
+        return
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    from ccpp_physics_b200 import abi, synthetic
+    from ccpp_physics_b200 import rrtmg_lw as lw
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    rc, msg = lw.rlwinit(device=local, me=1)   # me != 0: no banner, stdout carries only JSON lines
+    assert rc == 0, msg
+    # a dedicated stream: the library and the CUDA events must share it (the
+    # legacy default stream does not order work of non-blocking streams)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sh = stream.cuda_stream
+
+    def timed(fn, k):
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         if dist is not None:
             t = torch.tensor([ms], device="cuda", dtype=torch.float64)
@@ -670,206 +847,104 @@ def main():
             ms = float(t.item())
         return ms
 
-    if args.sw_only:
-        if rank == 0:
-            print(json.dumps({"rrtmg_sw": sw_leg(args, torch, timed, sh)}), flush=True)
-        return
-
-    if args.quick and args.precision != "fp64":
-        # profiling runs of another path: the same loop, no other legs
+    if args.ncols:
+        # profiling runs: one path over the first NCOLS columns, device resident
+        import ctypes as C
+        prof = synthetic.make_profiles(args.ncols, NLAY, seed=1, device="cuda")
+        out = abi.alloc_outputs(args.ncols, NLAY, hlw0=True, like="cuda")
         if args.precision == "surrogate":
             from ccpp_physics_b200 import surrogate as sg
             sg.load()
+        keep = []
+        a = abi.make_run_args(prof, out, keep=keep)
+        x = abi.ExecArgs(precision=lw.PRECISIONS[args.precision], memory=abi.DEVICE, stream=sh, sync=0)
+        buf = C.create_string_buffer(512)
+
+        def step():
+            if lw.lib().rrtmg_lw_gpu_run_ex(C.byref(a), C.byref(x), buf, 512):
+                raise RuntimeError(buf.value.decode())
         for _ in range(args.warmup):
-            step(args.precision)
-        msq = timed(lambda: step(args.precision), args.steps)
+            step()
+        ms = timed(step, args.steps)
         if rank == 0:
-            print(json.dumps({"quick": True, "precision": args.precision, "value": world * ncols * args.steps / (msq / 1e3),
-                              "ms_per_step": msq / args.steps, "config": cfg["name"]}), flush=True)
+            print(json.dumps({"profiling_run": True, "precision": args.precision, "ncols": args.ncols,
+                              "value": world * args.ncols * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                              "launches_per_step": int(lw.lib().rrtmg_lw_gpu_last_launch_count())}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
         return
 
-    # ---- FP64 path, inputs resident in HBM (the headline value) ----
-    for _ in range(args.warmup):
-        step("fp64")
-    with ClockSampler(local) as clk:
-        ms64 = timed(lambda: step("fp64"), args.steps)
-    value = world * ncols * args.steps / (ms64 / 1e3)
-    ref64 = {k: v.clone() for k, v in out.items()}
-    if args.quick:
-        if rank == 0:
-            print(json.dumps({"quick": True, "value": value, "ms_per_step": ms64 / args.steps,
-                              "config": cfg["name"]}), flush=True)
-        return
+    legs = [l for l in args.legs.split(",") if l]
+    if legs and world == 1 and rank == 0:
+        peak_gbs = _peaks()[0]
+        if "sw" in legs:
+            print(json.dumps({"leg": "rrtmg_sw", **sw_leg(args, torch, timed, sh)}), flush=True)
+        if "callers" in legs:
+            print(json.dumps({"leg": "caller_steps", **caller_steps_leg(args, torch, timed, sh, peak_gbs)}),
+                  flush=True)
+        if "train" in legs:
+            from ccpp_physics_b200 import surrogate as sg
+            print(json.dumps({"leg": "c4_training", **training_leg(args, torch, sg)}), flush=True)
+        torch.cuda.empty_cache()
 
-    # per-kernel device time (dominant kernel for the roofline)
-    import ctypes as C
-    kms = (C.c_float * 3)()
-    kt = []
-    for _ in range(3):
-        step("fp64", kernel_ms=kms)
-        kt.append((kms[0], kms[1], kms[2]))
-    mcica_ms = sum(k[0] for k in kt) / len(kt)
-    gas_ms = sum(k[1] for k in kt) / len(kt)
-    rt_ms = sum(k[2] for k in kt) / len(kt)
-    col_ms = gas_ms + rt_ms
-
-    # ---- FP32 path ----
-    out32 = abi.alloc_outputs(ncols, nlay, hlw0=True, like="cuda")
-    for _ in range(args.warmup):
-        step("fp32", out32)
-    ms32 = timed(lambda: step("fp32", out32), args.steps)
-
-    def rmse(a, b):
-        return float(torch.sqrt(torch.mean((a - b) ** 2)).item())
-
-    # ---- FP64 path with decorrelation-length overlap (iovr=3, the GFS v16 setting) ----
-    dcorr = dict(iovr=3)
-    outdc = abi.alloc_outputs(ncols, nlay, hlw0=True, like="cuda")
-    for _ in range(args.warmup):
-        step("fp64", outdc, flags=dcorr)
-    msdc = timed(lambda: step("fp64", outdc, flags=dcorr), args.steps)
-    kdc = (C.c_float * 3)()
-    step("fp64", outdc, kernel_ms=kdc, flags=dcorr)
-    del outdc
-
-    paths = {
-        "fp64": {"value": value, "ms_per_step": ms64 / args.steps, "gas_kernel_ms": gas_ms,
-                 "rt_kernel_ms": rt_ms, "mcica_kernel_ms": mcica_ms},
-        "fp32": {"value": world * ncols * args.steps / (ms32 / 1e3), "ms_per_step": ms32 / args.steps,
-                 "flux_rmse_wm2": rmse(torch.cat([out32["topflx"], out32["sfcflx"]], 1),
-                                       torch.cat([ref64["topflx"], ref64["sfcflx"]], 1)),
-                 "hr_rmse_kday": rmse(out32["hlwc"], ref64["hlwc"]),
-                 "hr0_rmse_kday": rmse(out32["hlw0"], ref64["hlw0"])},
-        "fp64_iovr3": {"value": world * ncols * args.steps / (msdc / 1e3), "ms_per_step": msdc / args.steps,
-                       "overlap": "decorrelation length (iovr=3), de_lgth 2 km", "mcica_kernel_ms": kdc[0],
-                       "gas_kernel_ms": kdc[1], "rt_kernel_ms": kdc[2]},
-    }
-
-    # ---- learned gas optics: committed network (trained on this GPU by the library's kernels) ----
-    from ccpp_physics_b200 import surrogate as sg
-    args.surrogate_ready = False
-    try:
-        sg.load()
-        args.surrogate_ready = True
-    except Exception as exc:   # weights missing: report, do not fake
-        paths["surrogate"] = {"value": None, "note": f"no trained network: {exc}"}
-    if args.surrogate_ready:
-        outsg = abi.alloc_outputs(ncols, nlay, hlw0=True, like="cuda")
-        for _ in range(args.warmup):
-            step("surrogate", outsg)
-        sg.stats(reset=True)
-        mssg = timed(lambda: step("surrogate", outsg), args.steps)
-        fb, mma_err = sg.stats()
-        kms_sg = (C.c_float * 3)()
-        step("surrogate", outsg, kernel_ms=kms_sg)
-        paths["surrogate"] = {
-            "value": world * ncols * args.steps / (mssg / 1e3), "ms_per_step": mssg / args.steps,
-            "speedup_vs_fp64": (ms64 / mssg), "mcica_kernel_ms": kms_sg[0], "mlp_plus_gas_kernel_ms": kms_sg[1],
-            "rt_kernel_ms": kms_sg[2],
-            "flux_rmse_wm2": rmse(torch.cat([outsg["topflx"], outsg["sfcflx"]], 1),
-                                  torch.cat([ref64["topflx"], ref64["sfcflx"]], 1)),
-            "hr_rmse_kday": rmse(outsg["hlwc"], ref64["hlwc"]), "hr0_rmse_kday": rmse(outsg["hlw0"], ref64["hlw0"]),
-            "fallback_layer_fraction": fb / float(args.steps * ncols * nlay), "mma_error": mma_err}
-        if not args.no_train:
-            paths["c4_training"] = training_leg(args, torch, sg)
-
-    # ---- batched production blocks (884,736 columns in uneven blocks of 8..256) ----
-    if not args.no_batch:
-        paths["c3_batched"] = batched_leg(args, lw, abi, synthetic, torch, rank, world, sh, timed, rmse)
-
-    # ---- the steps either side of rrtmg_lw_run (seeds, overlap parameters, post) ----
-    if not args.no_callers and world == 1 and not args.quick:
-        paths["caller_steps"] = caller_steps_leg(args, torch, timed, sh, _peaks()[0])
-    # ---- the shortwave scheme (rrtmg_sw_run) at 16,384 x 127 ----
-    if not args.no_sw and world == 1 and not args.quick:
-        paths["rrtmg_sw"] = sw_leg(args, torch, timed, sh)
-
-    # ---- end to end through the C ABI with pinned host buffers ----
-    hprof = dict(npts=ncols, nlay=nlay, flags=dict(prof["flags"]))
-    h2d = 0
-    for k, v in prof.items():
-        if isinstance(v, torch.Tensor):
-            hv = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
-            hv.copy_(v)
-            hprof[k] = hv
-            h2d += hv.numel() * hv.element_size()
-    hout = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for k, v in out.items()}
-    d2h = sum(v.numel() * v.element_size() for v in hout.values())
-    for _ in range(2):
-        m, e = lw.run_profile(hprof, hout, precision="fp64")
-        assert e == 0, m
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        m, e = lw.run_profile(hprof, hout, precision="fp64")
-    t_e2e = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
-    e2e = world * ncols * args.steps / t_e2e
-    ok_e2e = all(torch.equal(hout[k], ref64[k].cpu()) for k in hout)
-
-    peak, peak_kind = _peaks()
-    achieved = BYTES_PER_COL * ncols / (col_ms / 1e3) / 1e9
-    traffic = None
-    tr = {}
-    tfile = os.path.join(ROOT, "profiles", "column_kernels_traffic.txt")
-    if os.path.exists(tfile):
-        # "dram_bytes_per_column_fp64: N" lines from the ncu summary
-        with open(tfile) as fh:
-            tr = dict(l.split(":", 1) for l in fh if ":" in l and not l.startswith("#"))
-        if "dram_bytes_per_column_fp64" in tr:
-            traffic = float(tr["dram_bytes_per_column_fp64"]) * ncols
-    # FP-pipe side of the roofline: counted FP64 flops of the step's kernels (ncu instruction
-    # counts) against the FMA throughput measured on this GPU now
-    fp_pipe = None
-    try:
-        flop_col = sum(float(tr[k]) for k in ("fp64_flop_per_column_mcica", "fp64_flop_per_column_gas",
-                                              "fp64_flop_per_column_rt"))
-        p64, p32 = C.c_double(0.0), C.c_double(0.0)
-        lw.lib().rrtmg_lw_gpu_fma_peak.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
-        if lw.lib().rrtmg_lw_gpu_fma_peak(C.byref(p64), C.byref(p32)) == 0 and p64.value > 0:
-            ach = flop_col * value / world / 1e12
-            fp_pipe = {"flop_per_column": flop_col, "achieved_tflops": ach, "peak_tflops": p64.value,
-                       "peak_fp32_tflops": p32.value, "frac": ach / p64.value,
-                       "source": "flops: ncu FP64 dadd+dmul+2*dfma counts (profiles/column_kernels_traffic.txt); "
-                                 "peak: FMA-chain kernel (rrtmg_lw_gpu_fma_peak) in this run"}
-    except Exception as exc:   # report, never fake
-        fp_pipe = {"unavailable": str(exc)}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        prof_np = {k: (v.cpu().numpy() if isinstance(v, torch.Tensor) else v) for k, v in prof.items()}
-        ncores = os.cpu_count() or 1
-        rate, nsamp, dt = cpu_rate(prof_np, seconds=10.0, nthreads=ncores)
-        cpu = {"value": rate, "unit": "columns/s", "cores": ncores, "kind": "port",
-               "sample": f"first {nsamp} columns of {cfg['name']} ({dt:.1f} s), OpenMP over columns"}
-
+    res, e2e, parity, cpu, clk, ncols = headline(args, rank, world, local, dist, torch, sh, stream, lw, abi,
+                                                 synthetic)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return
+    peak, peak_kind = _peaks()
+    r64 = res["fp64"]
+    # the column kernels (gas optics + transfer, every chunk) take the step
+    # minus the McICA kernel; their algorithmic bytes are the interface bytes
+    col_s = max(1e-9, (r64["ms_per_step"] - r64["mcica_ms"]) / 1e3)
+    achieved = BYTES_PER_COL * ncols / col_s / 1e9
+    traffic, fp_pipe, tr = None, None, {}
+    tfile = os.path.join(ROOT, "profiles", "column_kernels_traffic.txt")
+    if os.path.exists(tfile):
+        with open(tfile) as fh:
+            tr = dict(l.split(":", 1) for l in fh if ":" in l and not l.startswith("#"))
+        if "dram_bytes_per_column_fp64" in tr:
+            nch = max(1, (r64["launches_per_step"] - 1) // 2)
+            traffic = float(tr["dram_bytes_per_column_fp64"]) * ncols / nch   # per launch pair
+    try:
+        flop_col = sum(float(tr[k]) for k in ("fp64_flop_per_column_mcica", "fp64_flop_per_column_gas",
+                                              "fp64_flop_per_column_rt"))
+        p64, p32 = fma_peak()
+        if p64:
+            ach = flop_col * ncols / (r64["ms_per_step"] / 1e3) / 1e12
+            fp_pipe = {"achieved_tflops": ach, "peak_tflops": p64, "frac": ach / p64,
+                       "flop_per_column": flop_col}
+    except Exception as exc:   # report, never fake
+        fp_pipe = {"unavailable": str(exc)[:80]}
+    paths = {"fp64": {"value": r64["value"], "ms_per_step": r64["ms_per_step"], "launches": r64["launches_per_step"],
+                      "mcica_ms": r64["mcica_ms"]}}
+    for prec in ("fp32", "surrogate"):
+        if prec in res and res[prec].get("value"):
+            p = res[prec]
+            paths[prec] = {kk: p[kk] for kk in ("value", "ms_per_step", "speedup_vs_fp64", "flux_rmse_wm2",
+                                                "hr_rmse_kday", "hr0_rmse_kday", "launches_per_step")}
+            if prec == "surrogate":
+                paths[prec]["fallback_layer_frac"] = p["fallback_layer_frac"]
+                paths[prec]["mma_error"] = p["mma_error"]
+        elif prec in res:
+            paths[prec] = res[prec]
     rec = {
-        "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms64 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": cfg["name"], "ncols_per_gpu": ncols, "nlay": nlay,
-                   "overlap": "max-random McICA (iovr=1, isubclw=2)", "parallelism": f"column shards x{world}",
-                   "l2": "inputs %.2f GB per GPU > 126 MB L2, no flush needed" % (h2d / 1e9)},
-        "clocks": clk.summary(),
-        "e2e": {"value": e2e, "unit": "columns/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "matches_device_run": ok_e2e},
-        "gpu_launches": args.steps * (1 + 2 * n_chunks(ncols, nlay)),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": "lw_gas_kernel<double,4> + lw_rt_kernel<double,4,0>",
-                     "note": "compulsory bytes 61,052 B/column / (gas + transfer kernel time); the "
-                             "kernels are FP64-issue and gather-latency bound, not HBM bound"},
+        "metric": METRIC, "value": r64["value"], "unit": "columns/s", "n_gpus": world, "steps": r64["steps"],
+        "warmup": args.warmup, "ms_per_step": r64["ms_per_step"], "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(world),
+        "gpu_launches": r64["steps"] * r64["launches_per_step"],
+        "clocks": clk.summary() if clk else None,
+        "e2e": e2e,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "kernel": "lw_gas_kernel<double,4> + lw_rt_kernel<double,4> (per chunk)"},
         "fp_pipe": fp_pipe,
         "cpu_baseline": cpu,
         "paths": paths,
+        "parity_fp64_vs_oracle": parity,
     }
     print(json.dumps(rec), flush=True)
 

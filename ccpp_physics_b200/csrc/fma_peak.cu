@@ -1,5 +1,7 @@
-// lw_peak.cu -- measured FMA throughput of the current GPU, the denominator of
-// the FP-pipe roofline the benchmark reports beside the HBM one.
+// fma_peak.cu -- measured FMA throughput of the current GPU, the denominator of
+// the FP-pipe roofline the benchmark reports beside the HBM one.  Built as a
+// library of its own (libfma_peak.so) that only bench.py loads; it is not
+// part of the RRTMG library.
 //
 // Each thread runs 8 independent FMA chains (so issue, not latency, limits
 // it) over `iters` steps; the grid covers every SM several times.  The result
@@ -10,7 +12,6 @@
 
 #include <cuda_runtime.h>
 
-#include "../../include/rrtmg_lw_gpu.h"
 
 namespace {
 
@@ -58,7 +59,8 @@ int time_chains(int iters, double* tflops) {
 
 }  // namespace
 
-extern "C" int rrtmg_lw_gpu_fma_peak(double* fp64_tflops, double* fp32_tflops) {
+// FP64 and FP32 FMA throughput in TFLOP/s (either pointer may be NULL); 0 on success.
+extern "C" int fma_peak_tflops(double* fp64_tflops, double* fp32_tflops) {
   if (fp64_tflops && time_chains<double>(4096, fp64_tflops)) return 1;
   if (fp32_tflops && time_chains<float>(8192, fp32_tflops)) return 1;
   return 0;

@@ -28,18 +28,6 @@
 extern "C" const unsigned char rrtmg_lw_tables_blob[];
 extern "C" const unsigned char rrtmg_lw_tables_blob_end[];
 
-namespace lw {
-struct NoAllocView {
-  int ready, device, num_sms;
-  const double* kt64;
-  const float* kt32;
-  const double* tbl64;
-  const float* tbl32;
-  Consts cs;
-};
-NoAllocView noalloc_view();
-}  // namespace lw
-
 using namespace lw;
 
 namespace {
@@ -75,6 +63,7 @@ struct Workspace {
   Block* hblocks = nullptr;   // pinned host copy of the descriptors
   size_t hblocks_n = 0;
   uint64_t gen = 0;           // bumped whenever bits/scratch move (graphs hold their addresses)
+  int last_launches = 0;      // kernels enqueued by the thread's last run call
   // pipelined host-memory calls: copy streams, double-buffered staging, events
   cudaStream_t h2d = nullptr, d2h = nullptr;
   cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
@@ -93,6 +82,7 @@ struct GraphEntry {
   int ncols = 0;
   uint64_t gen = 0;
   uint64_t last_use = 0;
+  int launches = 0;           // kernels the graph holds
   Block* dblocks = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -249,10 +239,12 @@ extern "C" int rrtmg_lw_gpu_init(const rrtmg_lw_init_args* a, char* errmsg, int3
   CK(mcica_prepare(optin), "kernel attributes (mcica)");
   CK(prepare_column_fp64(), "kernel attributes (column, fp64)");
   CK(prepare_column_fp32(), "kernel attributes (column, fp32)");
-  // per-thread stack for the spilled kernels (a context setting, gone with the process)
-  size_t stack = 0;
-  CK(cudaDeviceGetLimit(&stack, cudaLimitStackSize), "cudaDeviceGetLimit");
-  if (stack < 4096) CK(cudaDeviceSetLimit(cudaLimitStackSize, 4096), "cudaDeviceSetLimit(stack)");
+  // No context limit is changed: every kernel's stack frame (at most 864
+  // bytes per thread, -Xptxas -v) fits the default per-thread stack.
+  // make the allocation-free entry point's fixed scratch resident now, before
+  // a host hands the rest of the GPU's memory to its own pool; a failure here
+  // is reported by that entry point's first call instead
+  if (noalloc_prepare(g.device) != cudaSuccess) (void)cudaGetLastError();
   g.ready = true;
   return errflg;
 }
@@ -448,6 +440,14 @@ int upload_blocks(Workspace* w, cudaStream_t st, const Block* hblocks, int nbloc
 cudaError_t enqueue(Workspace* w, cudaStream_t st, const Block* dblk, const Block& b0, int nblocks, int ncols,
                     const Flags& f, int precision, const Shape& sh, cudaEvent_t* ev) {
   cudaError_t e;
+  {
+    // kernels of this call: McICA, then per scratch chunk the network stage
+    // (learned gas optics), gas optics and transfer
+    const int V = pick_v(f.nlay);
+    const int col = precision == RRTMG_LW_FP64 ? launches_column_fp64(V, ncols, w->scratch_bytes, sh)
+                                                : launches_column_fp32(V, ncols, w->scratch_bytes, sh);
+    w->last_launches = (f.isubclw > 0 && !f.gas_only ? 1 : 0) + col + (f.surrogate ? col / 2 : 0);
+  }
   if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return e;
   if (f.isubclw > 0 && !f.gas_only) {
     e = mcica_launch(dblk, nblocks, b0, ncols, f.nlay, f.iovr, f.isubclw, f.top_at_1, McicaStage(), w->bits,
@@ -555,6 +555,7 @@ int launch_graph(Workspace* w, cudaStream_t st, const std::vector<Block>& hb, in
       ce = cudaStreamEndCapture(w->stream, &graph);
       if (ke != cudaSuccess) ce = ke;
     }
+    e->launches = w->last_launches;
     if (ce == cudaSuccess) ce = cudaGraphInstantiate(&e->exec, graph, 0);
     if (graph) cudaGraphDestroy(graph);
     if (ce != cudaSuccess) {
@@ -565,6 +566,7 @@ int launch_graph(Workspace* w, cudaStream_t st, const std::vector<Block>& hb, in
     hit = e;
   }
   hit->last_use = ++tick;
+  w->last_launches = hit->launches;
   CK(cudaGraphLaunch(hit->exec, st), "cudaGraphLaunch");
   return 0;
 }
@@ -1034,6 +1036,8 @@ extern "C" int rrtmg_lw_gpu_autotune(const rrtmg_lw_run_args* blocks, int32_t nb
   return 0;
 }
 
+extern "C" int32_t rrtmg_lw_gpu_last_launch_count(void) { return tl_ws ? tl_ws->last_launches : 0; }
+
 extern "C" void rrtmg_lw_gpu_finalize(void) {
   lw::prep_release();
   std::lock_guard<std::mutex> lk(g_mu);
@@ -1070,6 +1074,17 @@ extern "C" void rrtmg_lw_gpu_finalize(void) {
 lw::NoAllocView lw::noalloc_view() {
   std::lock_guard<std::mutex> lk(g_mu);
   return NoAllocView{g.ready ? 1 : 0, g.device, g.num_sms, g.kt64, g.kt32, g.tbl64, g.tbl32, g.cs};
+}
+
+int lw::run_args_check(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg, int32_t errmsg_len,
+                       bool need_outputs) {
+  return validate(a, x, errmsg, errmsg_len, need_outputs);
+}
+void lw::flags_from_args(const rrtmg_lw_run_args* a, Flags* f) { fill_flags(a, f); }
+void lw::block_from_run_args(const rrtmg_lw_run_args* a, Block* B) { block_from_args(a, B); }
+Shape lw::launch_shape(int precision, int V) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return default_shape(precision, V);
 }
 
 // Device of the steps either side of the run (lw_prep.cu): the init device,

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/rrtmg_lw_gpu.h"
 #include "lw_common.cuh"
 
 namespace lw {
@@ -75,5 +76,32 @@ void prep_release();
 
 // layers per lane of the column kernels (NLP = 32 V padded layers)
 inline int pick_v(int nlay) { return nlay <= 63 ? 2 : nlay <= 127 ? 4 : 8; }
+
+// Argument handling shared by the entry points of lw_api.cu and lw_noalloc.cu.
+// run_args_check: the error checks of rrtmg_lw_run (RLM:713-760); returns 0,
+// 1 (error), 2 (a required optional cloud input is missing: the caller zeroes
+// cldtau first, RLM:736) or -1 (nothing to do: lslwr false or npts == 0).
+int run_args_check(const rrtmg_lw_run_args* a, const rrtmg_lw_exec* x, char* errmsg, int32_t errmsg_len,
+                   bool need_outputs);
+void flags_from_args(const rrtmg_lw_run_args* a, Flags* f);
+void block_from_run_args(const rrtmg_lw_run_args* a, Block* B);
+// launch shape of the column kernels: the autotuned one for (precision, V) if
+// rrtmg_lw_gpu_autotune ran, else the defaults
+Shape launch_shape(int precision, int V);
+// device tables and constants written by rrtmg_lw_gpu_init (lw_api.cu)
+struct NoAllocView {
+  int ready, device, num_sms;
+  const double* kt64;
+  const float* kt32;
+  const double* tbl64;
+  const float* tbl32;
+  Consts cs;
+};
+NoAllocView noalloc_view();
+// looks up the device address of the allocation-free entry point's fixed
+// scratch array on `device` (current), which loads the module that holds it
+// (lw_noalloc.cu); rrtmg_lw_gpu_init calls it so the array is resident from
+// init on
+cudaError_t noalloc_prepare(int device);
 
 }  // namespace lw

@@ -209,6 +209,12 @@ __device__ __forceinline__ void lw_out_quarter(uint32_t tb, int wl, bool live, f
   }
 }
 
+// Polls of a tensor-core wait in the forward kernel before it gives up and
+// records the error (default 1 << 22, seconds of waiting); lowered only by
+// the failure-detection hook rrtmg_lw_gpu_surrogate_wait_limit.
+constexpr uint32_t kFwdWaitPollsDefault = 1u << 22;
+__constant__ uint32_t c_fwd_wait_polls = kFwdWaitPollsDefault;
+
 template <int MODE>
 __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
@@ -256,7 +262,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
 
   bool failed = false;   // uniform across the CTA
   auto wait_mma = [&]() -> bool {
-    const bool ok = umma::mbar_wait(mbar, phase);
+    const bool ok = umma::mbar_wait(mbar, phase, c_fwd_wait_polls);
     phase ^= 1u;
     umma::fence_after_sync();
     if (__syncthreads_or(!ok)) {
@@ -1122,6 +1128,12 @@ extern "C" int rrtmg_lw_gpu_surrogate_train(const float* feats, const float* tar
 // Layers of surrogate runs that fell outside the training envelope and were
 // recomputed with taumol, since the last reset; and the tensor-core error
 // flag of the last surrogate launches.
+extern "C" int rrtmg_lw_gpu_surrogate_wait_limit(int64_t polls) {
+  std::lock_guard<std::mutex> lk(net_mu);
+  const uint32_t v = polls < 0 ? kFwdWaitPollsDefault : (uint32_t)std::min<int64_t>(polls, 0xffffffffll);
+  return cudaMemcpyToSymbol(c_fwd_wait_polls, &v, sizeof(v)) == cudaSuccess ? 0 : 1;
+}
+
 extern "C" int rrtmg_lw_gpu_surrogate_stats(uint64_t* fallback_layers, int32_t* mma_error, int32_t reset) {
   std::lock_guard<std::mutex> lk(net_mu);
   if (!net.err) return 1;

@@ -6,16 +6,20 @@
 // fragments their arena, and time-step loops that must not call cudaMalloc
 // or cudaFree because those calls synchronize the whole device.  For them,
 // rrtmg_lw_gpu_run_noalloc runs the same McICA, gas-optics and transfer
-// kernels as rrtmg_lw_gpu_run_ex, but the kernels' scratch (the McICA
-// sub-column flags and the gas-optics -> transfer hand-off) lives in one
-// fixed array compiled into the library instead of in memory allocated at
-// run time.  The caller still owns and passes every input and output array.
+// kernels as rrtmg_lw_gpu_run_ex, with the same argument checks, flags and
+// launch shape, but the kernels' scratch (the McICA sub-column flags and the
+// gas-optics -> transfer hand-off) lives in one fixed array compiled into the
+// library instead of in memory allocated at run time.  The caller still owns
+// and passes every input and output array.
 //
 // Limits and rules of use:
 //   * the scratch array is kNoAllocScratchBytes (64 MiB) per GPU, held by
 //     every GPU that loads the library until the process exits; a call whose
 //     columns do not fit is rejected with an error that states the maximum
 //     (about 190 columns of 127 layers in FP64, about 380 in FP32);
+//   * McICA sub-columns (isubclw 1 or 2) with the overlaps iovr 0, 1 and 2
+//     only: the decorrelation-length and exponential overlaps (iovr 3..5)
+//     and grid-mean clouds (isubclw 0) are refused with an error;
 //   * all calls share the one array, so two calls that overlap on the GPU
 //     (different streams or host threads without ordering) race on it and
 //     corrupt each other's results: order them on one stream or serialize;
@@ -24,9 +28,12 @@
 //     kernel reads only the layers, g-points and columns that the
 //     gas-optics kernel wrote, and the sub-column flags only of the columns
 //     the McICA kernel flagged cloudy), so no clearing is done;
-//   * the first call on a device looks up the device address of the array
-//     (cudaGetSymbolAddress, once per device, with that device current);
-//     make that first call before any stream capture.
+//   * rrtmg_lw_gpu_init looks up the device address of the array on its
+//     device (cudaGetSymbolAddress, with that device current), which loads the
+//     array there: call init before the host hands the GPU's free memory to
+//     its own pool.  If that look-up failed at init, the first call on the
+//     device repeats it; make that first call before any stream capture.
+//   * the caller's current device is restored before return.
 // This entry point has no counterpart in the reference.
 #include <cstdarg>
 #include <cstdint>
@@ -41,26 +48,14 @@
 
 #include "lw_launch.h"
 
-namespace lw {
-// device tables and constants written by rrtmg_lw_gpu_init (lw_api.cu)
-struct NoAllocView {
-  int ready, device, num_sms;
-  const double* kt64;
-  const float* kt32;
-  const double* tbl64;
-  const float* tbl32;
-  Consts cs;
-};
-NoAllocView noalloc_view();
-}  // namespace lw
-
 using namespace lw;
 
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = (size_t)64 << 20;   // 64 MiB per GPU
 
-// The scratch itself: device memory reserved when the library is loaded.
+// The scratch itself: a fixed device array, resident on a device once its
+// module is loaded there (rrtmg_lw_gpu_init forces that load).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;
@@ -89,24 +84,45 @@ cudaError_t scratch_address(int device, void** out) {
   return cudaSuccess;
 }
 
+// Restores the caller's current device when the call returns.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() { if (cudaGetDevice(&prev) != cudaSuccess) prev = -1; }
+  ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
 }  // namespace
+
+cudaError_t lw::noalloc_prepare(int device) {
+  void* p = nullptr;
+  return scratch_address(device, &p);
+}
 
 extern "C" int rrtmg_lw_gpu_run_noalloc(const rrtmg_lw_run_args* a, int32_t precision, void* stream,
                                         char* errmsg, int32_t errmsg_len) {
   msg(errmsg, errmsg_len, "");
   const NoAllocView v = noalloc_view();
   if (!v.ready) { msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_noalloc: rrtmg_lw_gpu_init has not been called"); return 1; }
-  if (!a) { msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_noalloc: null argument struct"); return 1; }
-  if (!a->lslwr) return 0;
-  if (a->nlay < 1 || a->nlay > 255 || a->nlp1 != a->nlay + 1 || a->npts < 0 || (a->ldim != 0 && a->ldim < a->npts)) {
-    msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_noalloc: inconsistent dimensions (nlay=%d nlp1=%d npts=%d ldim=%d)",
-        a->nlay, a->nlp1, a->npts, a->ldim);
-    return 1;
-  }
   if (precision != RRTMG_LW_FP64 && precision != RRTMG_LW_FP32) {
-    msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_noalloc: precision %d not available", precision);
+    msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_noalloc: precision %d not available (FP64 and FP32 are)", precision);
     return 1;
   }
+  DeviceGuard guard;
+  // the checks of the regular entry point (rrtmg_lw_gpu_run_ex), device memory
+  const rrtmg_lw_exec x{precision, RRTMG_LW_DEVICE, stream, 1, 0, nullptr};
+  const int chk = run_args_check(a, &x, errmsg, errmsg_len, true);
+  if (chk == -1) return 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (chk == 2) {
+    // the reference zeroes cldtau before the optional-argument check (RLM:736)
+    if (a->cldtau && cudaSetDevice(v.device) == cudaSuccess) {
+      const size_t ld = a->ldim > 0 ? (size_t)a->ldim : (size_t)a->npts;
+      if (cudaMemsetAsync(a->cldtau, 0, ld * a->nlay * sizeof(double), st) == cudaSuccess)
+        cudaStreamSynchronize(st);
+    }
+    return 1;
+  }
+  if (chk) return 1;
   if (a->isubclw != 1 && a->isubclw != 2) {
     msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_noalloc: isubclw=%d not supported (1, 2 are)", a->isubclw);
     return 1;
@@ -115,22 +131,9 @@ extern "C" int rrtmg_lw_gpu_run_noalloc(const rrtmg_lw_run_args* a, int32_t prec
     msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_noalloc: overlap iovr=%d not supported (0, 1, 2 are)", a->iovr);
     return 1;
   }
-  const bool liq = a->ilwcliq > 0;
-  const double* need[] = {a->plyr, a->plvl, a->tlyr, a->tlvl, a->qlyr, a->olyr, a->gasvmr_co2, a->gasvmr_n2o,
-                          a->gasvmr_ch4, a->gasvmr_o2, a->gasvmr_co, a->gasvmr_cfc11, a->gasvmr_cfc12,
-                          a->gasvmr_cfc22, a->gasvmr_ccl4, a->aeraod, a->aerssa, a->sfemis, a->sfgtmp, a->delpin,
-                          a->cld_cf, a->hlwc, a->topflx, a->sfcflx, a->cldtau,
-                          liq ? a->cld_lwp : a->cld_od, liq ? a->cld_ref_liq : a->cld_od,
-                          liq ? a->cld_iwp : a->cld_od, liq ? a->cld_ref_ice : a->cld_od,
-                          liq ? a->cld_rwp : a->cld_od, liq ? a->cld_swp : a->cld_od,
-                          liq ? a->cld_ref_snow : a->cld_od};
-  for (const double* p : need)
-    if (!p) { msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_noalloc: a required array pointer is NULL"); return 1; }
-  if (a->isubclw == 2 && !a->icseed) { msg(errmsg, errmsg_len, "rrtmg_lw_gpu_run_noalloc: icseed is NULL"); return 1; }
-  if (a->npts == 0) return 0;
 
   // scratch needed: McICA flags, then the per-column hand-off of the kernels
-  const int V = a->nlay <= 63 ? 2 : a->nlay <= 127 ? 4 : 8;
+  const int V = pick_v(a->nlay);
   const size_t nw = (size_t)(a->nlay + 31) / 32;
   const size_t bits_bytes = (((size_t)a->npts * NGPT * nw * sizeof(uint32_t)) + 255) & ~(size_t)255;
   const size_t per = (precision == RRTMG_LW_FP64) ? scratch_per_column_fp64(V) : scratch_per_column_fp32(V);
@@ -154,38 +157,12 @@ extern "C" int rrtmg_lw_gpu_run_noalloc(const rrtmg_lw_run_args* a, int32_t prec
   uint32_t* bits = static_cast<uint32_t*>(base);
   void* scratch = static_cast<unsigned char*>(base) + bits_bytes;
   const size_t scratch_bytes = kNoAllocScratchBytes - bits_bytes;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
 
   Block B;
-  const double* in[N_IN] = {a->plyr, a->plvl, a->tlyr, a->tlvl, a->qlyr, a->olyr, a->gasvmr_co2,
-                            a->gasvmr_n2o, a->gasvmr_ch4, a->gasvmr_o2, a->gasvmr_co, a->gasvmr_cfc11,
-                            a->gasvmr_cfc12, a->gasvmr_cfc22, a->gasvmr_ccl4, a->aeraod, a->aerssa,
-                            a->sfemis, a->sfgtmp, a->dzlyr, a->delpin, a->de_lgth, a->alpha, a->cld_cf,
-                            a->cld_lwp, a->cld_ref_liq, a->cld_iwp, a->cld_ref_ice, a->cld_rwp,
-                            a->cld_ref_rain, a->cld_swp, a->cld_ref_snow, a->cld_od};
-  std::memcpy(B.in, in, sizeof(in));
-  B.icseed = a->icseed;
-  double* out[N_OUT] = {a->hlwc, a->topflx, a->sfcflx, a->cldtau, a->hlw0, a->hlwb, a->flxprf};
-  std::memcpy(B.out, out, sizeof(out));
-  B.npts = a->npts;
-  B.ld = a->ldim > 0 ? a->ldim : a->npts;
-  B.col0 = 0;
-  B.seed0 = 0;
+  block_from_run_args(a, &B);
   Flags f;
-  f.nlay = a->nlay;
-  f.top_at_1 = a->top_at_1 != 0;
-  f.inc_minor_gas = a->inc_minor_gas != 0;
-  f.iovr = a->iovr;
-  f.iovr_dcorr = a->iovr_dcorr;
-  f.iovr_exp = a->iovr_exp;
-  f.iovr_exprand = a->iovr_exprand;
-  f.ilwcliq = a->ilwcliq;
-  f.ilwcice = a->ilwcice;
-  f.isubclw = a->isubclw;
-  f.want_hlw0 = a->hlw0 != nullptr;
-  f.want_hlwb = a->hlwb != nullptr;
-  f.want_flxprf = a->flxprf != nullptr;
-  f.gas_only = 0;
+  flags_from_args(a, &f);
+  const Shape sh = launch_shape(precision, V);
 
   e = mcica_launch(nullptr, 1, B, a->npts, a->nlay, a->iovr, a->isubclw, f.top_at_1, McicaStage(), bits,
                    v.num_sms, st);
@@ -193,12 +170,12 @@ extern "C" int rrtmg_lw_gpu_run_noalloc(const rrtmg_lw_run_args* a, int32_t prec
     if (precision == RRTMG_LW_FP64) {
       Tables<double> t{v.kt64, v.tbl64};
       e = launch_column_fp64(V, f.want_hlwb != 0, nullptr, 1, B, a->npts, f, v.cs, t, t, bits, scratch,
-                             scratch_bytes, nullptr, nullptr, v.num_sms, Shape(), st, nullptr);
+                             scratch_bytes, nullptr, nullptr, v.num_sms, sh, st, nullptr);
     } else {
       Tables<float> t{v.kt32, v.tbl32};
       Tables<double> t64{v.kt64, v.tbl64};
       e = launch_column_fp32(V, f.want_hlwb != 0, nullptr, 1, B, a->npts, f, v.cs, t, t64, bits, scratch,
-                             scratch_bytes, nullptr, nullptr, v.num_sms, Shape(), st, nullptr);
+                             scratch_bytes, nullptr, nullptr, v.num_sms, sh, st, nullptr);
     }
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);

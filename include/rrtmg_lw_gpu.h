@@ -273,12 +273,13 @@ int rrtmg_lw_gpu_surrogate_grads(const float *feats, const float *targets,
  * wait-timeout flag of the surrogate kernels.  Returns 0 on success. */
 int rrtmg_lw_gpu_surrogate_stats(uint64_t *fallback_layers, int32_t *mma_error,
                                  int32_t reset);
-
-/* Measured FMA throughput of the current device in TFLOP/s (FP64 and FP32,
- * either pointer may be NULL): independent FMA chains over every SM, timed
- * with CUDA events.  The denominator of the FP-pipe roofline of the
- * benchmark.  No counterpart in the reference.  Returns 0 on success. */
-int rrtmg_lw_gpu_fma_peak(double *fp64_tflops, double *fp32_tflops);
+/* Failure-detection hook: the number of polls a tensor-core wait of the
+ * network's forward kernel makes before it gives up (polls < 0 restores the
+ * default of 2^22; 0 gives up at the first wait).  A kernel that gives up
+ * still waits, bounded, for the MMA it issued, frees its tensor memory, and
+ * the call reports "tensor-core wait timed out" (mma_error of _stats).  For
+ * tests; returns 0 on success. */
+int rrtmg_lw_gpu_surrogate_wait_limit(int64_t polls);
 
 /* ---- Steps either side of rrtmg_lw_run ------------------------------------
  * They need no tables: they run on the device rrtmg_lw_gpu_init selected (the
@@ -367,6 +368,12 @@ typedef struct rrtmg_lw_post_args {
 } rrtmg_lw_post_args;
 int rrtmg_lw_gpu_post(const rrtmg_lw_post_args *args, const rrtmg_lw_exec *exec,
                       char *errmsg, int32_t errmsg_len);
+
+/* Kernels enqueued by the calling thread's most recent rrtmg_lw_gpu_run,
+ * _run_ex or _run_blocks call (a replayed CUDA graph counts the kernels it
+ * holds; a host-memory call counts its last chunk).  Diagnostics for
+ * benchmarks; no counterpart in the reference. */
+int32_t rrtmg_lw_gpu_last_launch_count(void);
 
 /* Release device tables and per-thread workspaces (call once at exit). */
 void rrtmg_lw_gpu_finalize(void);

@@ -69,7 +69,10 @@ def dtb_literals(ref_root):
 
 
 def main(argv):
-    ref_root = argv[1] if len(argv) > 1 else "/root/reference"
+    if len(argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <ccpp-physics source tree>  "
+                 "(the checkout whose radlw_datatb.f the DTB literals are read from)")
+    ref_root = argv[1]
     lits = dtb_literals(ref_root)
     with open(os.path.join(HERE, "dtb_literals.json"), "w") as fh:
         json.dump(lits, fh, indent=1)

@@ -343,3 +343,22 @@ def test_pipelined_host_call_matches_device(gpu, isubclw):
         assert np.all(np.isnan(h[(slice(npts, None),) if k in ("topflx", "sfcflx") else
                                  (Ellipsis, slice(npts, None)) if k != "flxprf" else
                                  (slice(None), slice(npts, None))])), k     # padding columns untouched
+
+
+def test_fp64_benchmark_scale_16384(gpu, orc):
+    """The 16,384-column all-sky McICA case of the benchmark (the first
+    columns of its 884,736-column workload) against the oracle: every column
+    within the FP64 bars, flux profiles included.  At this size the
+    discontinuous table indices (jp from ln p, RLM:2290-2294; itgas, RLM:3602-
+    3614) would show as single columns far outside 1e-10 if a libm difference
+    flipped one; the failing columns are named."""
+    prof = synthetic.make_profiles(16384, 127, seed=1)
+    out, ref = _run_both(gpu, orc, prof, hlw0=True, flxprf=True)
+    rel = np.maximum(np.abs(out["topflx"] - ref["topflx"]) / np.abs(ref["topflx"]),
+                     0).max(axis=1)
+    rel = np.maximum(rel, (np.abs(out["sfcflx"] - ref["sfcflx"]) / np.abs(ref["sfcflx"])).max(axis=1))
+    rp = np.abs(out["flxprf"] - ref["flxprf"]) / np.maximum(np.abs(ref["flxprf"]), 1e-300)
+    rel = np.maximum(rel, rp.max(axis=(0, 2)))
+    bad = np.nonzero(rel > FLUX_RTOL_FP64)[0]
+    assert bad.size == 0, f"columns over 1e-10: {bad[:20].tolist()} (max {rel.max():.3e})"
+    _check_fp64(out, ref)

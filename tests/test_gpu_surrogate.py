@@ -172,3 +172,34 @@ def test_trained_network_gain(sg, trained):
     sg.set_weights(w, norm)
     assert err_trained < 0.02 * err_untrained, (err_trained, err_untrained)
     assert t_sg < 0.9 * t_fp32, (t_sg, t_fp32)
+
+
+def test_forward_wait_timeout_is_reported_and_recovers(sg, small_set):
+    """Failure detection without a GPU fault: with the tensor-core wait limit
+    at zero polls every wait of the forward kernel gives up at once.  The call
+    must return the time-out error (and mma_error), the kernels must still
+    wait for their MMAs and free their tensor memory, and with the default
+    limit restored the next call runs and gives the same outputs as before."""
+    import ctypes as C
+    import torch
+    feats, _, _ = small_set
+    sg.load()                 # the committed network
+    x = feats[:4096].contiguous()
+    y_ref = sg.forward(x)
+    L = sg._lib()
+    L.rrtmg_lw_gpu_surrogate_wait_limit.argtypes = [C.c_int64]
+    assert L.rrtmg_lw_gpu_surrogate_wait_limit(0) == 0
+    try:
+        y = torch.empty((x.shape[0], 288), dtype=torch.float32, device="cuda")
+        msg = C.create_string_buffer(512)
+        rc = L.rrtmg_lw_gpu_surrogate_forward(C.c_void_p(x.data_ptr()), x.shape[0], C.c_void_p(y.data_ptr()),
+                                              None, msg, 512)
+        assert rc == 1 and "timed out" in msg.value.decode(), msg.value
+        _, err = sg.stats(reset=True)
+        assert err == 1
+    finally:
+        assert L.rrtmg_lw_gpu_surrogate_wait_limit(-1) == 0
+    y2 = sg.forward(x)        # every SM allocates its tensor memory again
+    assert torch.equal(y2, y_ref)
+    _, err = sg.stats(reset=True)
+    assert err == 0
