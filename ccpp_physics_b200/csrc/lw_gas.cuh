@@ -133,27 +133,70 @@ __host__ __device__ constexpr size_t gas_smem_bytes(int V) {
   return sizeof(double) * (2 * NLP + 24 + 8 * NLP) + sizeof(R) * N_LF * NLP + sizeof(int) * (NLP + 4);
 }
 
-template <typename R, int V, bool SG>
-__global__ void __launch_bounds__(32 * V, SG ? LW_GAS_MINB_SG : LW_GAS_MINB)
-lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int ncols, Flags f,
-              Tables<R> tab, Tables<double> tab64, Scratch<R> sc, double* __restrict__ gas_taug,
-              double* __restrict__ gas_fracs) {
+// Barrier of the threads that run gas_column together: the whole CTA
+// (lw_gas_kernel), or a named barrier over the first `n` threads of a CTA
+// whose other warps do other work (the fused learned-gas-optics kernel).
+struct CtaSync {
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  __device__ __forceinline__ int count(bool p) const { return __syncthreads_count(p); }
+  __device__ __forceinline__ int any(bool p) const { return __syncthreads_or(p); }
+};
+struct GroupSync {
+  int id, n;   // named barrier id (1..15) and thread count (a multiple of 32)
+  __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+  __device__ __forceinline__ int count(bool p) const {
+    int r;
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.popc.u32 %0, %2, %3, q;\n\t}"
+                 : "=r"(r) : "r"((unsigned)p), "r"(id), "r"(n) : "memory");
+    return r;
+  }
+  __device__ __forceinline__ int any(bool p) const { return count(p) != 0; }
+};
+
+// Per-column working arrays of gas_column (shared memory in lw_gas_kernel,
+// any memory the caller's threads can reach elsewhere); gas_smem_bytes<R>(V).
+template <typename R, int V>
+struct GasWork {
+  double* red;   // [2 NLP]
+  double* col;   // [24]
+  double* cld;   // [8 NLP] cloud inputs of the layer
+  R* lay;        // [N_LF NLP] setcoef record (LayRef)
+  int* li;       // [NLP]
+  int* ci;       // [4]
+  __device__ __forceinline__ static GasWork at(void* base) {
+    constexpr int NLP = 32 * V;
+    GasWork w;
+    w.red = reinterpret_cast<double*>(base);
+    w.col = w.red + 2 * NLP;
+    w.cld = w.col + 24;
+    w.lay = reinterpret_cast<R*>(w.cld + 8 * NLP);
+    w.li = reinterpret_cast<int*>(w.lay + N_LF * NLP);
+    w.ci = w.li + NLP;
+    return w;
+  }
+};
+
+// Kernel A's work for one column cc of the chunk (global column sc.c0 + cc),
+// run by the 32 V threads t = 0 .. 32 V - 1 that S synchronizes.
+template <typename R, int V, bool SG, typename Sync>
+__device__ __forceinline__ void gas_column(int cc, int t, const Sync& S, const GasWork<R, V>& W,
+                                           const Block* __restrict__ blocks, int nblocks, const Block& b0,
+                                           const Flags& f, const Tables<R>& tab, const Tables<double>& tab64,
+                                           const Scratch<R>& sc, double* __restrict__ gas_taug,
+                                           double* __restrict__ gas_fracs) {
   constexpr int NLP = 32 * V;
-  extern __shared__ __align__(16) char smem_raw[];   // gas_smem_bytes<R>(V)
-  double* s_red = reinterpret_cast<double*>(smem_raw);       // [2 * NLP]
-  double* s_col = s_red + 2 * NLP;                            // [24]
-  double* s_cld = s_col + 24;                                 // [8 * NLP] cloud inputs of the layer
-  R* s_lay = reinterpret_cast<R*>(s_cld + 8 * NLP);           // [N_LF * NLP] setcoef record (LayRef)
-  int* s_li = reinterpret_cast<int*>(s_lay + N_LF * NLP);     // [NLP]
-  int* s_ci = s_li + NLP;                                     // [4]
+  double* s_red = W.red;
+  double* s_col = W.col;
+  double* s_cld = W.cld;
+  R* s_lay = W.lay;
+  int* s_li = W.li;
+  int* s_ci = W.ci;
   const int nlay = f.nlay, nlp1 = nlay + 1;
-  const int t = threadIdx.x;
   const KT<R> kt{tab.kt};
   const double* kt64 = tab64.kt;
-
-  for (int cc = blockIdx.x; cc < ncols; cc += gridDim.x) {
+  {
     const int c = sc.c0 + cc;                        // global column
-    __syncthreads();
+    S.sync();
     const Block& B = (nblocks == 1) ? b0 : blocks[find_block(blocks, nblocks, c)];
     const int i = c - B.col0;
     const size_t ld = (size_t)B.ld;
@@ -282,8 +325,8 @@ lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int
       s_red[t] = coldry;
       s_red[NLP + t] = colh2o;
     }
-    const int laytrop = __syncthreads_count(lowerk);
-    const int lcf1 = __syncthreads_or(cldk);
+    const int laytrop = S.count(lowerk);
+    const int lcf1 = S.any(cldk);
     if (t == 0) {
       // precipitable water (RLM:910-919 / 1012-1019): sequential, reference order
       double tem1 = 0.0, tem2 = 0.0;
@@ -303,7 +346,7 @@ lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int
       s_ci[0] = min(180, max(1, (int)(stemp - 159.0)));
       s_ci[1] = min(180, max(1, (int)(tz0 - 159.0)));
     }
-    __syncthreads();
+    S.sync();
     const bool write_scratch = sc.tau != nullptr;
     double* crec = write_scratch ? sc.col + (size_t)cc * kColRec : nullptr;
     if (crec && !LW_OK(cc < sc.cap, 18, cc)) crec = nullptr;
@@ -362,6 +405,17 @@ lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int
       if (t == 0 && bcol) __stcs(bcol + (1 * NBANDS + b) * NLP, R(planck_int(kt64, b, s_ci[1], s_col[19])));
     }
   }
+}
+
+template <typename R, int V, bool SG>
+__global__ void __launch_bounds__(32 * V, SG ? LW_GAS_MINB_SG : LW_GAS_MINB)
+lw_gas_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, int ncols, Flags f,
+              Tables<R> tab, Tables<double> tab64, Scratch<R> sc, double* __restrict__ gas_taug,
+              double* __restrict__ gas_fracs) {
+  extern __shared__ __align__(16) char smem_raw[];   // gas_smem_bytes<R>(V)
+  const GasWork<R, V> W = GasWork<R, V>::at(smem_raw);
+  for (int cc = blockIdx.x; cc < ncols; cc += gridDim.x)
+    gas_column<R, V, SG>(cc, threadIdx.x, CtaSync{}, W, blocks, nblocks, b0, f, tab, tab64, sc, gas_taug, gas_fracs);
 }
 
 }  // namespace lw

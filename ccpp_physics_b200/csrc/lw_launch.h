@@ -65,6 +65,14 @@ cudaError_t seed_gather_launch(const uint32_t* raw, const int32_t* imap, const i
 cudaError_t mlp_lw_launch(const Block* blocks, int nblocks, const Block& b0, int nc, const Flags& f,
                           const Scratch<float>& sc, int num_sms, cudaStream_t st);
 const float* surrogate_norm();
+// the learned gas optics, network and transfer fused in one persistent kernel
+// (lw_fused.cu): used for McICA calls of up to 127 layers without hlwb
+bool sg_fused_applies(const Flags& f);
+size_t sg_fused_work_bytes(int num_sms);
+cudaError_t sg_fused_prepare();
+cudaError_t sg_fused_launch(const Block* blocks, int nblocks, const Block& b0, int ncols, const Flags& f,
+                            const Consts& cs, const Tables<float>& tab, const Tables<double>& tab64,
+                            const uint32_t* bits, void* work, size_t work_bytes, int num_sms, cudaStream_t st);
 unsigned int* surrogate_fallback_counter();
 
 // device chosen by rrtmg_lw_gpu_init, -1 before init (lw_api.cu)

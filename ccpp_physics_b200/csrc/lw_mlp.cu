@@ -42,28 +42,12 @@
 #include "lw_common.cuh"
 #include "lw_features.cuh"
 #include "lw_launch.h"
+#include "lw_net.h"
 #include "lw_umma.cuh"
 
 namespace lw {
 
-typedef __nv_bfloat16 bf16;
-
-// ---------------------------------------------------------------------------
-// parameter / operand / gradient layouts
-constexpr int HID = SG_HID, NOP = SG_NOUTP, NIN = SG_NFEAT, KIN = 16;
-constexpr int P_W1 = 0;                      // [128][8]   (column 7: bias of layer 1)
-constexpr int P_W2 = P_W1 + HID * NIN;       // [128][128]
-constexpr int P_B2 = P_W2 + HID * HID;       // [128]
-constexpr int P_W3 = P_B2 + HID;             // [288][128] (pad rows 140..143, 284..287 stay 0)
-constexpr int P_B3 = P_W3 + NOP * HID;       // [288]
-constexpr int P_N = P_B3 + NOP;              // 54,688 (53,656 trainable)
-
-constexpr int O_W1 = 0;                      // bf16 [128][16]
-constexpr int O_W2 = O_W1 + HID * KIN;       // bf16 [128][128]
-constexpr int O_W2T = O_W2 + HID * HID;      // bf16 [128][128] = W2^T
-constexpr int O_W3 = O_W2T + HID * HID;      // bf16 [288][128]
-constexpr int O_W3T = O_W3 + NOP * HID;      // bf16 [128][288] = W3^T
-constexpr int O_N = O_W3T + HID * NOP;
+// parameter / operand layouts (lw_net.h)
 
 constexpr int GW2_LD = 144, GW3_ROWS = 384;  // gradients of [W | b] (column 128 = bias)
 constexpr int G_W1 = 0;                      // f32 [128][16]
@@ -73,9 +57,7 @@ constexpr int G_N = G_W3 + GW3_ROWS * GW2_LD;
 
 __host__ __device__ inline bool pad_out_row(int j) { return (j >= 140 && j < 144) || j >= 284; }
 
-// SiLU and its derivative with the fast exp and division (the same functions
-// in training and inference)
-__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+// derivative of silu (lw_net.h) with the same fast exp and division
 __device__ __forceinline__ float dsilu(float z) {
   const float s = __fdividef(1.0f, 1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
@@ -896,6 +878,7 @@ cudaError_t mlp_lw_launch(const Block* blocks, int nblocks, const Block& b0, int
 }
 
 const float* surrogate_norm() { return net.ready ? net.norm : nullptr; }
+SgNetView sg_net_view() { return SgNetView{net.ops, net.P, net.norm, net.err, net.fallback, net.ready ? 1 : 0}; }
 unsigned int* surrogate_fallback_counter() { return net.fallback; }
 
 }  // namespace lw

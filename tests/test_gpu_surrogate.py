@@ -117,8 +117,13 @@ def test_surrogate_path_meets_accuracy_bounds(sg, trained):
 
 def test_out_of_envelope_layers_fall_back_to_taumol(sg, trained):
     """Doubled CO2 (the training set holds 400 ppmv) puts every layer outside
-    the envelope: the gas-optics kernel then recomputes all of them with plain
-    taumol and the result is the FP32 path's, bit for bit."""
+    the envelope: every layer's optical depths and Planck fractions then come
+    from plain FP32 taumol, the FP32 path's gas optics, so the result is the
+    FP32 path's up to the fused kernel's FP16 copy of the Planck fractions
+    (relative rounding 2^-11 per fraction) and the summation order of its
+    transfer (the fused kernel sums g-points per warp, the FP32 transfer
+    kernel per lane): fluxes within 3e-4 relative, heating rates within
+    1e-2 K/day, cloud optical depth equal."""
     import torch
     from ccpp_physics_b200 import rrtmg_lw as lw
     n, nlay = 512, 127
@@ -130,8 +135,13 @@ def test_out_of_envelope_layers_fall_back_to_taumol(sg, trained):
     fallback, _ = sg.stats()
     assert fallback == n * nlay
     f = _run(lw, prof, "fp32", n, nlay)
-    for k in s:
-        assert torch.equal(s[k], f[k]), k
+    assert torch.equal(s["cldtau"], f["cldtau"])
+    for k in ("topflx", "sfcflx"):
+        rel = float(((s[k] - f[k]).abs() / f[k].abs()).max())
+        assert rel <= 3e-4, (k, rel)
+    for k in ("hlwc", "hlw0"):
+        d = float((s[k] - f[k]).abs().max())
+        assert d <= 1e-2, (k, d)
     # only the upper half of every column outside: exactly those layers fall back
     p2 = synthetic.make_profiles(n, nlay, seed=21)
     p2["gasvmr_co2"][64:] *= 2.0
