@@ -41,7 +41,7 @@ struct DeviceState {
   double* tbl64 = nullptr;   // records {exp, tfn, tau, 0} (4 x (NTBL+1))
   float* tbl32 = nullptr;
   Consts cs{};
-  bool fused = false;        // the fused learned-gas-optics kernel is usable on this device
+  bool sgpath = false;       // the learned-gas-optics column path (lw_sg_path.cu) is usable on this device
   Shape tuned[2][9];         // autotuned launch shape per [fp32?][V]
   bool has_tuned[2][9] = {};
 };
@@ -240,8 +240,8 @@ extern "C" int rrtmg_lw_gpu_init(const rrtmg_lw_init_args* a, char* errmsg, int3
   CK(mcica_prepare(optin), "kernel attributes (mcica)");
   CK(prepare_column_fp64(), "kernel attributes (column, fp64)");
   CK(prepare_column_fp32(), "kernel attributes (column, fp32)");
-  g.fused = sg_fused_prepare() == cudaSuccess;
-  if (!g.fused) (void)cudaGetLastError();
+  g.sgpath = sg_path_prepare() == cudaSuccess;
+  if (!g.sgpath) (void)cudaGetLastError();
   // No context limit is changed: every kernel's stack frame (at most 864
   // bytes per thread, -Xptxas -v) fits the default per-thread stack.
   // make the allocation-free entry point's fixed scratch resident now, before
@@ -406,9 +406,11 @@ int reserve(Workspace* w, int ncols, const Flags& f, int precision, const Shape&
   const int nw = (f.nlay + 31) / 32;
   if (f.isubclw > 0 && !f.gas_only)
     CK(grow_ws(w, &w->bits, &w->bits_bytes, (size_t)ncols * NGPT * nw * sizeof(uint32_t)), "cudaMalloc(mcica bits)");
-  if (precision != RRTMG_LW_FP64 && g.fused && sg_fused_applies(f)) {
-    // the fused kernel's per-CTA work area (columns outside the network's envelope)
-    CK(grow_ws(w, &w->scratch, &w->scratch_bytes, sg_fused_work_bytes(g.num_sms)), "cudaMalloc(scratch)");
+  if (precision != RRTMG_LW_FP64 && g.sgpath && sg_path_applies(f)) {
+    // the learned-gas-optics path's work area: column map, fallback list,
+    // band-field slots and the FP16 network -> transfer hand-off
+    CK(grow_ws(w, &w->scratch, &w->scratch_bytes, sg_path_bytes(ncols, f.nlay, g.num_sms, scratch_budget())),
+       "cudaMalloc(scratch)");
     return 0;
   }
   const int V = pick_v(f.nlay);
@@ -448,9 +450,10 @@ int upload_blocks(Workspace* w, cudaStream_t st, const Block* hblocks, int nbloc
 cudaError_t enqueue(Workspace* w, cudaStream_t st, const Block* dblk, const Block& b0, int nblocks, int ncols,
                     const Flags& f, int precision, const Shape& sh, cudaEvent_t* ev) {
   cudaError_t e;
-  const bool fused = precision != RRTMG_LW_FP64 && g.fused && sg_fused_applies(f);
-  if (fused) {
-    w->last_launches = 2;   // McICA, then the fused network + transfer kernel
+  const bool sgpath = precision != RRTMG_LW_FP64 && g.sgpath && sg_path_applies(f);
+  if (sgpath) {
+    // McICA, then the column map and per hand-off chunk network, fallback and transfer
+    w->last_launches = 1 + sg_path_launches(ncols, f.nlay, g.num_sms, scratch_budget(), nblocks);
   } else {
     // kernels of this call: McICA, then per scratch chunk the network stage
     // (learned gas optics), gas optics and transfer
@@ -469,10 +472,10 @@ cudaError_t enqueue(Workspace* w, cudaStream_t st, const Block* dblk, const Bloc
   const int V = pick_v(f.nlay);
   const bool hlwb = f.want_hlwb != 0;
   Tables<double> t64{g.kt64, g.tbl64};
-  if (fused) {
+  if (sgpath) {
     Tables<float> t{g.kt32, g.tbl32};
-    e = sg_fused_launch(dblk, nblocks, b0, ncols, f, g.cs, t, t64, w->bits, w->scratch, w->scratch_bytes, g.num_sms,
-                        st);
+    e = sg_path_launch(dblk, nblocks, b0, ncols, f, g.cs, t, t64, w->bits, w->scratch, w->scratch_bytes,
+                       scratch_budget(), g.num_sms, st);
     if (e == cudaSuccess && ev) e = cudaEventRecord(ev[3], st);
   } else if (precision == RRTMG_LW_FP64) {
     e = launch_column_fp64(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t64, t64, w->bits, w->scratch,

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "../../include/rrtmg_lw_gpu.h"
@@ -65,14 +66,24 @@ cudaError_t seed_gather_launch(const uint32_t* raw, const int32_t* imap, const i
 cudaError_t mlp_lw_launch(const Block* blocks, int nblocks, const Block& b0, int nc, const Flags& f,
                           const Scratch<float>& sc, int num_sms, cudaStream_t st);
 const float* surrogate_norm();
-// the learned gas optics, network and transfer fused in one persistent kernel
-// (lw_fused.cu): used for McICA calls of up to 127 layers without hlwb
-bool sg_fused_applies(const Flags& f);
-size_t sg_fused_work_bytes(int num_sms);
-cudaError_t sg_fused_prepare();
-cudaError_t sg_fused_launch(const Block* blocks, int nblocks, const Block& b0, int ncols, const Flags& f,
-                            const Consts& cs, const Tables<float>& tab, const Tables<double>& tab64,
-                            const uint32_t* bits, void* work, size_t work_bytes, int num_sms, cudaStream_t st);
+// network stage of the learned-gas-optics column path: the FP16 hand-off
+// [nc][nlay][{tau, frac} x 140] of chunk columns [c0, c0 + nc) and the list
+// of its columns with a layer outside the training envelope (lw_mlp.cu)
+cudaError_t mlp_h_launch(const Block* blocks, int nblocks, const Block& b0, const int* colmap, int c0, int nc,
+                         const Flags& f, __half* hnd, unsigned int* fb_flag, int* fb_list, int* fb_count, int num_sms,
+                         cudaStream_t st);
+// the learned-gas-optics column path (lw_sg_path.cu): network, fallback for
+// out-of-envelope layers and the g-point-per-lane transfer, per chunk of
+// columns; used for McICA calls of up to 127 layers without hlwb.  Work-area
+// size, launch count and launcher take the same (ncols, nlay, SMs, budget).
+bool sg_path_applies(const Flags& f);
+size_t sg_path_bytes(int ncols, int nlay, int num_sms, size_t budget);
+int sg_path_launches(int ncols, int nlay, int num_sms, size_t budget, int nblocks);
+cudaError_t sg_path_prepare();
+cudaError_t sg_path_launch(const Block* blocks, int nblocks, const Block& b0, int ncols, const Flags& f,
+                           const Consts& cs, const Tables<float>& tab, const Tables<double>& tab64,
+                           const uint32_t* bits, void* work, size_t work_bytes, size_t budget, int num_sms,
+                           cudaStream_t st);
 unsigned int* surrogate_fallback_counter();
 
 // device chosen by rrtmg_lw_gpu_init, -1 before init (lw_api.cu)

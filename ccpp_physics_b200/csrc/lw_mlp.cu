@@ -14,6 +14,11 @@
 //                         tau = exp(y) * coldry + aerosol and the band-
 //                         normalised Planck fractions straight into the
 //                         gas-optics -> transfer scratch of the column path.
+//                         MODE_H: rows as MODE_LW; writes tau and the
+//                         Planck fractions as FP16 into 8-layer blocks of
+//                         the compact hand-off of the learned-gas-optics
+//                         transfer kernel (lw_sg_path.cu) and lists the
+//                         columns that have a layer outside the envelope.
 //   gemm_tn_kernel<EPI>   C = A * B^T for the backward pass: dH = dZ W with
 //                         the activation derivative fused (EPI_DACT), and
 //                         split-K weight gradients dW = dZ^T H with FP32
@@ -36,6 +41,7 @@
 #include <vector>
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "../../include/rrtmg_lw_gpu.h"
@@ -65,7 +71,7 @@ __device__ __forceinline__ float dsilu(float z) {
 
 // ---------------------------------------------------------------------------
 // forward kernel
-enum { MODE_FEATS = 0, MODE_TRAIN = 1, MODE_LW = 2 };
+enum { MODE_FEATS = 0, MODE_TRAIN = 1, MODE_LW = 2, MODE_H = 3 };
 
 struct FwdArgs {
   const bf16* ops;      // operand copies (O_*)
@@ -91,6 +97,13 @@ struct FwdArgs {
   Flags f;
   Scratch<float> sc;
   int nc;               // columns of this chunk
+  // MODE_H (blocks, nblocks, b0, f, nc as MODE_LW)
+  __half* hnd;          // [nc][nlay/8][tau 140 | frac 140][8 layers] (lw_sg_path.cu)
+  const int* colmap;    // block of every global column (nblocks > 1)
+  int c0;               // first global column of the chunk
+  unsigned int* fb_flag;   // per global column: set once the column is listed
+  int* fb_list;         // columns of the chunk with a layer outside the envelope
+  int* fb_count;
 };
 
 // Thread layout: 4 warpgroups.  Thread tid serves tile row (tid & 127) -- the
@@ -191,6 +204,46 @@ __device__ __forceinline__ void lw_out_quarter(uint32_t tb, int wl, bool live, f
   }
 }
 
+// MODE_H output stage of one quarter, g-points [GA, GB) (whole bands): the
+// same values as lw_out_quarter, rounded to FP16 in the hand-off.  A row is
+// one column at one layer; hrow points at its layer's slot of g-point 0 in
+// the column's 8-layer block [tau: 140 g][frac: 140 g][8 layers], so g-point
+// g sits at hrow[8 g].  Optical depths are clamped below the FP16 maximum
+// (any depth above 7.2e4 selects the last transmittance record, ~0).
+constexpr float kHandTauMax = 6.0e4f;
+template <int GA, int GB>
+__device__ __forceinline__ void h_out_quarter(uint32_t tb, int wl, bool live, __half* hrow, const float* osc,
+                                              const float* osh, const float* aer_row, float cd) {
+  constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
+  float v[NCH * 16];
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, 256 + C0 + 16 * c), v + 16 * c);
+  if (live) {
+#pragma unroll
+    for (int g = GA; g < GB; ++g) {
+      const float tau = fmaf(__expf(fmaf(v[g - C0], osc[g], osh[g])), cd, aer_row[band_of_g(g) * 128]);
+      hrow[8 * g] = __float2half_rn(fminf(tau, kHandTauMax));
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, C0 + 16 * c), v + 16 * c);
+  if (live) {
+    float bsum[NBANDS];
+#pragma unroll
+    for (int b = 0; b < NBANDS; ++b) bsum[b] = 0.0f;
+#pragma unroll
+    for (int g = GA; g < GB; ++g) {
+      const float fr = __saturatef(fmaf(v[g - C0], osc[144 + g], osh[144 + g]));
+      v[g - C0] = fr;
+      bsum[band_of_g(g)] += fr;
+    }
+#pragma unroll
+    for (int b = 0; b < NBANDS; ++b) bsum[b] = bsum[b] > 0.0f ? 1.0f / bsum[b] : 1.0f;
+#pragma unroll
+    for (int g = GA; g < GB; ++g) hrow[8 * (NGPT + g)] = __float2half_rn(v[g - C0] * bsum[band_of_g(g)]);
+  }
+}
+
 // Polls of a tensor-core wait in the forward kernel before it gives up and
 // records the error (default 1 << 22, seconds of waiting); lowered only by
 // the failure-detection hook rrtmg_lw_gpu_surrogate_wait_limit.
@@ -263,6 +316,10 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
   int parity = 0;   // double buffer of the per-tile aerosol / coldry rows
   for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, parity ^= 1) {
     const long row = tile * 128 + tr;
+    // MODE_H: this row is layer ht of chunk column hcc (rows are the layers
+    // of consecutive columns, so a warp's hand-off stores are contiguous)
+    const int hcc = MODE == MODE_H ? (int)(row / a.f.nlay) : 0;
+    const int ht = MODE == MODE_H ? (int)(row - (long)hcc * a.f.nlay) : 0;
     const bool live = row < a.nrows;
     float* saer = saer0 + parity * NBANDS * 128;
     float* scd = scd0 + parity * 128;
@@ -288,7 +345,21 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
       for (int j = 0; j < KIN; ++j) x[j] = 0.0f;
       if (live) {
         float raw[NIN];
-        if (MODE == MODE_LW) {
+        if (MODE == MODE_H) {
+          const int c = a.c0 + hcc;
+          const Block* B = (a.nblocks == 1) ? &a.b0 : &a.blocks[__ldg(a.colmap + c)];
+          const size_t o = (size_t)(c - B->col0) + (size_t)B->ld * (a.f.top_at_1 ? a.f.nlay - ht - 1 : ht);
+          const double pavel = B->in[F_PLYR][o], tavel = B->in[F_TLYR][o], qv = B->in[F_QLYR][o];
+          const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
+          const double h2ovmr = fmax(0.0, qv * amdw / (1.0 - qv));
+          const double o3vmr = fmax(0.0, B->in[F_OLYR][o] * amdo3);
+          const double tem0 = (1.0 - h2ovmr) * 28.9644 + h2ovmr * 18.0154;
+          scd[tr] = (float)((1.0e-20 * 1.0e3 * 6.0221415e23) * B->in[F_DELPIN][o] /
+                            (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr)));
+          layer_features(pavel, tavel, h2ovmr, o3vmr, B->in[F_CO2][o], B->in[F_CH4][o], B->in[F_N2O][o], raw);
+          // a layer outside the training envelope: list its column once for the fallback
+          if (!in_envelope(raw, a.norm) && atomicExch(a.fb_flag + c, 1u) == 0u) a.fb_list[atomicAdd(a.fb_count, 1)] = c;
+        } else if (MODE == MODE_LW) {
           const LwRow w = lw_row(a, row, sblk, cfirst);
           const size_t o = (size_t)w.i + (size_t)w.B->ld * w.r;
           const double pavel = w.B->in[F_PLYR][o], tavel = w.B->in[F_TLYR][o], qv = w.B->in[F_QLYR][o];
@@ -322,6 +393,22 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
         const size_t ab = (size_t)w.i + ldl * ((size_t)w.r + (size_t)a.f.nlay * b);
         saer[b * 128 + tr] = (float)(w.B->in[F_AERAOD][ab] * (1.0 - w.B->in[F_AERSSA][ab]));
       }
+    } else if (MODE == MODE_H && live) {
+      const int c = a.c0 + hcc;
+      const Block* B = (a.nblocks == 1) ? &a.b0 : &a.blocks[__ldg(a.colmap + c)];
+      const size_t ldl = (size_t)B->ld;
+      const size_t o = (size_t)(c - B->col0) + ldl * (size_t)(a.f.top_at_1 ? a.f.nlay - ht - 1 : ht);
+      const int b0 = q == 1 ? 0 : q == 2 ? 6 : 11, b1 = q == 1 ? 6 : q == 2 ? 11 : 16;
+      double aod[6], ssa[6];
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {   // every load first, so their latencies overlap
+        const size_t ab = o + ldl * (size_t)a.f.nlay * (size_t)min(b0 + j, b1 - 1);
+        aod[j] = B->in[F_AERAOD][ab];
+        ssa[j] = B->in[F_AERSSA][ab];
+      }
+#pragma unroll
+      for (int j = 0; j < 6; ++j)
+        if (b0 + j < b1) saer[(b0 + j) * 128 + tr] = (float)(aod[j] * (1.0 - ssa[j]));
     }
     sync_for_mma();
     if (tid == 0) {
@@ -441,6 +528,15 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
         for (int o = 16; o > 0; o >>= 1) sse += __shfl_xor_sync(0xffffffffu, sse, o);
         if ((tid & 31) == 0) atomicAdd(a.loss, sse);
       }
+    } else if (MODE == MODE_H) {
+      const int nchk = (a.f.nlay + 7) >> 3;
+      __half* hrow = a.hnd + ((size_t)hcc * nchk + (ht >> 3)) * (2 * NGPT * 8) + (ht & 7);
+      const float cd = scd[tr];
+      const float* ar = saer + tr;
+      if (q == 0) h_out_quarter<0, 38>(tb, wl, live, hrow, osc, osh, ar, cd);
+      else if (q == 1) h_out_quarter<38, 68>(tb, wl, live, hrow, osc, osh, ar, cd);
+      else if (q == 2) h_out_quarter<68, 108>(tb, wl, live, hrow, osc, osh, ar, cd);
+      else h_out_quarter<108, 140>(tb, wl, live, hrow, osc, osh, ar, cd);
     } else {   // MODE_LW
       // quarters own whole bands: g-points [0,38), [38,68), [68,108), [108,140)
       const size_t nlp = (size_t)a.f.nlay <= 63 ? 64 : (size_t)a.f.nlay <= 127 ? 128 : 256;   // 32 V
@@ -714,17 +810,20 @@ cudaError_t set_attrs() {
     return e;
   if ((e = cudaFuncSetAttribute(mlp_fwd_kernel<MODE_LW>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM)))
     return e;
+  if ((e = cudaFuncSetAttribute(mlp_fwd_kernel<MODE_H>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM)))
+    return e;
   if ((e = cudaFuncSetAttribute(gemm_tn_kernel<EPI_ATOMIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM)))
     return e;
   if ((e = cudaFuncSetAttribute(gemm_tn_kernel<EPI_DACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM)))
     return e;
   // one CTA per SM is what makes the 512-column TMEM allocations safe
-  int occ[5] = {0, 0, 0, 0, 0};
+  int occ[6] = {0, 0, 0, 0, 0, 0};
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], mlp_fwd_kernel<MODE_FEATS>, FWD_THREADS, FWD_SMEM);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], mlp_fwd_kernel<MODE_TRAIN>, FWD_THREADS, FWD_SMEM);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], mlp_fwd_kernel<MODE_LW>, FWD_THREADS, FWD_SMEM);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], gemm_tn_kernel<EPI_ATOMIC>, 128, GEMM_SMEM);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[4], gemm_tn_kernel<EPI_DACT>, 128, GEMM_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[5], mlp_fwd_kernel<MODE_H>, FWD_THREADS, FWD_SMEM);
   for (int o : occ)
     if (o != 1) return cudaErrorLaunchOutOfResources;
   net.attrs = true;
@@ -874,6 +973,33 @@ cudaError_t mlp_lw_launch(const Block* blocks, int nblocks, const Block& b0, int
   const int grid = (int)std::min<long>(tiles, num_sms);
   if (grid < 1) return cudaSuccess;
   mlp_fwd_kernel<MODE_LW><<<grid, FWD_THREADS, FWD_SMEM, st>>>(a);
+  return cudaGetLastError();
+}
+
+// MLP stage of the learned-gas-optics path (lw_sg_path.cu): the compact FP16
+// hand-off of chunk columns [c0, c0 + nc) and the list of columns with a
+// layer outside the envelope.  Enqueue only.
+cudaError_t mlp_h_launch(const Block* blocks, int nblocks, const Block& b0, const int* colmap, int c0, int nc,
+                         const Flags& f, __half* hnd, unsigned int* fb_flag, int* fb_list, int* fb_count, int num_sms,
+                         cudaStream_t st) {
+  if (!net.ready || !net.attrs) return cudaErrorNotReady;
+  FwdArgs a = base_args();
+  a.blocks = blocks;
+  a.nblocks = nblocks;
+  a.b0 = b0;
+  a.f = f;
+  a.nc = nc;
+  a.hnd = hnd;
+  a.colmap = colmap;
+  a.c0 = c0;
+  a.fb_flag = fb_flag;
+  a.fb_list = fb_list;
+  a.fb_count = fb_count;
+  a.nrows = (long)nc * f.nlay;
+  const long tiles = (a.nrows + 127) / 128;
+  const int grid = (int)std::min<long>(tiles, num_sms);
+  if (grid < 1) return cudaSuccess;
+  mlp_fwd_kernel<MODE_H><<<grid, FWD_THREADS, FWD_SMEM, st>>>(a);
   return cudaGetLastError();
 }
 

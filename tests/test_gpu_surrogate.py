@@ -119,11 +119,13 @@ def test_out_of_envelope_layers_fall_back_to_taumol(sg, trained):
     """Doubled CO2 (the training set holds 400 ppmv) puts every layer outside
     the envelope: every layer's optical depths and Planck fractions then come
     from plain FP32 taumol, the FP32 path's gas optics, so the result is the
-    FP32 path's up to the fused kernel's FP16 copy of the Planck fractions
-    (relative rounding 2^-11 per fraction) and the summation order of its
-    transfer (the fused kernel sums g-points per warp, the FP32 transfer
-    kernel per lane): fluxes within 3e-4 relative, heating rates within
-    1e-2 K/day, cloud optical depth equal."""
+    FP32 path's up to the learned-gas-optics path's FP16 copies (relative
+    rounding 2^-11) of the optical depths, Planck fractions, transmittance
+    records and up-sweep terms, and the order of its sums over g-points:
+    fluxes within 3e-4 relative, heating rates within 0.01 K/day RMSE and
+    5 % of max(|rate|, 1 K/day) everywhere, cloud optical depth equal.  The
+    network's own error against FP32 taumol is ten times larger (flux RMSE
+    ~0.1 W/m2, heating rates ~0.05 K/day)."""
     import torch
     from ccpp_physics_b200 import rrtmg_lw as lw
     n, nlay = 512, 127
@@ -140,8 +142,9 @@ def test_out_of_envelope_layers_fall_back_to_taumol(sg, trained):
         rel = float(((s[k] - f[k]).abs() / f[k].abs()).max())
         assert rel <= 3e-4, (k, rel)
     for k in ("hlwc", "hlw0"):
-        d = float((s[k] - f[k]).abs().max())
-        assert d <= 1e-2, (k, d)
+        assert _rmse(s[k], f[k]) <= 1e-2, (k, _rmse(s[k], f[k]))
+        d = float(((s[k] - f[k]).abs() / f[k].abs().clamp_min(1.0)).max())
+        assert d <= 5e-2, (k, d)
     # only the upper half of every column outside: exactly those layers fall back
     p2 = synthetic.make_profiles(n, nlay, seed=21)
     p2["gasvmr_co2"][64:] *= 2.0
