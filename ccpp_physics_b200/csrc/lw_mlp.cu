@@ -14,11 +14,11 @@
 //                         tau = exp(y) * coldry + aerosol and the band-
 //                         normalised Planck fractions straight into the
 //                         gas-optics -> transfer scratch of the column path.
-//                         MODE_H: rows as MODE_LW; writes tau and the
-//                         Planck fractions as FP16 into 8-layer blocks of
-//                         the compact hand-off of the learned-gas-optics
-//                         transfer kernel (lw_sg_path.cu) and lists the
-//                         columns that have a layer outside the envelope.
+//   mlp_h_kernel          the same network for the learned-gas-optics column
+//                         path (lw_sg_path.cu): one column per tile, tau and
+//                         the Planck fractions as FP16 8-layer blocks of its
+//                         compact hand-off, and the list of the columns that
+//                         have a layer outside the envelope.
 //   gemm_tn_kernel<EPI>   C = A * B^T for the backward pass: dH = dZ W with
 //                         the activation derivative fused (EPI_DACT), and
 //                         split-K weight gradients dW = dZ^T H with FP32
@@ -71,7 +71,7 @@ __device__ __forceinline__ float dsilu(float z) {
 
 // ---------------------------------------------------------------------------
 // forward kernel
-enum { MODE_FEATS = 0, MODE_TRAIN = 1, MODE_LW = 2, MODE_H = 3 };
+enum { MODE_FEATS = 0, MODE_TRAIN = 1, MODE_LW = 2 };
 
 struct FwdArgs {
   const bf16* ops;      // operand copies (O_*)
@@ -97,7 +97,7 @@ struct FwdArgs {
   Flags f;
   Scratch<float> sc;
   int nc;               // columns of this chunk
-  // MODE_H (blocks, nblocks, b0, f, nc as MODE_LW)
+  // mlp_h_kernel (blocks, nblocks, b0, f, nc as MODE_LW)
   __half* hnd;          // [nc][nlay/8][tau 140 | frac 140][8 layers] (lw_sg_path.cu)
   const int* colmap;    // block of every global column (nblocks > 1)
   int c0;               // first global column of the chunk
@@ -204,46 +204,6 @@ __device__ __forceinline__ void lw_out_quarter(uint32_t tb, int wl, bool live, f
   }
 }
 
-// MODE_H output stage of one quarter, g-points [GA, GB) (whole bands): the
-// same values as lw_out_quarter, rounded to FP16 in the hand-off.  A row is
-// one column at one layer; hrow points at its layer's slot of g-point 0 in
-// the column's 8-layer block [tau: 140 g][frac: 140 g][8 layers], so g-point
-// g sits at hrow[8 g].  Optical depths are clamped below the FP16 maximum
-// (any depth above 7.2e4 selects the last transmittance record, ~0).
-constexpr float kHandTauMax = 6.0e4f;
-template <int GA, int GB>
-__device__ __forceinline__ void h_out_quarter(uint32_t tb, int wl, bool live, __half* hrow, const float* osc,
-                                              const float* osh, const float* aer_row, float cd) {
-  constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
-  float v[NCH * 16];
-#pragma unroll
-  for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, 256 + C0 + 16 * c), v + 16 * c);
-  if (live) {
-#pragma unroll
-    for (int g = GA; g < GB; ++g) {
-      const float tau = fmaf(__expf(fmaf(v[g - C0], osc[g], osh[g])), cd, aer_row[band_of_g(g) * 128]);
-      hrow[8 * g] = __float2half_rn(fminf(tau, kHandTauMax));
-    }
-  }
-#pragma unroll
-  for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, C0 + 16 * c), v + 16 * c);
-  if (live) {
-    float bsum[NBANDS];
-#pragma unroll
-    for (int b = 0; b < NBANDS; ++b) bsum[b] = 0.0f;
-#pragma unroll
-    for (int g = GA; g < GB; ++g) {
-      const float fr = __saturatef(fmaf(v[g - C0], osc[144 + g], osh[144 + g]));
-      v[g - C0] = fr;
-      bsum[band_of_g(g)] += fr;
-    }
-#pragma unroll
-    for (int b = 0; b < NBANDS; ++b) bsum[b] = bsum[b] > 0.0f ? 1.0f / bsum[b] : 1.0f;
-#pragma unroll
-    for (int g = GA; g < GB; ++g) hrow[8 * (NGPT + g)] = __float2half_rn(v[g - C0] * bsum[band_of_g(g)]);
-  }
-}
-
 // Polls of a tensor-core wait in the forward kernel before it gives up and
 // records the error (default 1 << 22, seconds of waiting); lowered only by
 // the failure-detection hook rrtmg_lw_gpu_surrogate_wait_limit.
@@ -316,10 +276,6 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
   int parity = 0;   // double buffer of the per-tile aerosol / coldry rows
   for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, parity ^= 1) {
     const long row = tile * 128 + tr;
-    // MODE_H: this row is layer ht of chunk column hcc (rows are the layers
-    // of consecutive columns, so a warp's hand-off stores are contiguous)
-    const int hcc = MODE == MODE_H ? (int)(row / a.f.nlay) : 0;
-    const int ht = MODE == MODE_H ? (int)(row - (long)hcc * a.f.nlay) : 0;
     const bool live = row < a.nrows;
     float* saer = saer0 + parity * NBANDS * 128;
     float* scd = scd0 + parity * 128;
@@ -345,21 +301,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
       for (int j = 0; j < KIN; ++j) x[j] = 0.0f;
       if (live) {
         float raw[NIN];
-        if (MODE == MODE_H) {
-          const int c = a.c0 + hcc;
-          const Block* B = (a.nblocks == 1) ? &a.b0 : &a.blocks[__ldg(a.colmap + c)];
-          const size_t o = (size_t)(c - B->col0) + (size_t)B->ld * (a.f.top_at_1 ? a.f.nlay - ht - 1 : ht);
-          const double pavel = B->in[F_PLYR][o], tavel = B->in[F_TLYR][o], qv = B->in[F_QLYR][o];
-          const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
-          const double h2ovmr = fmax(0.0, qv * amdw / (1.0 - qv));
-          const double o3vmr = fmax(0.0, B->in[F_OLYR][o] * amdo3);
-          const double tem0 = (1.0 - h2ovmr) * 28.9644 + h2ovmr * 18.0154;
-          scd[tr] = (float)((1.0e-20 * 1.0e3 * 6.0221415e23) * B->in[F_DELPIN][o] /
-                            (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr)));
-          layer_features(pavel, tavel, h2ovmr, o3vmr, B->in[F_CO2][o], B->in[F_CH4][o], B->in[F_N2O][o], raw);
-          // a layer outside the training envelope: list its column once for the fallback
-          if (!in_envelope(raw, a.norm) && atomicExch(a.fb_flag + c, 1u) == 0u) a.fb_list[atomicAdd(a.fb_count, 1)] = c;
-        } else if (MODE == MODE_LW) {
+        if (MODE == MODE_LW) {
           const LwRow w = lw_row(a, row, sblk, cfirst);
           const size_t o = (size_t)w.i + (size_t)w.B->ld * w.r;
           const double pavel = w.B->in[F_PLYR][o], tavel = w.B->in[F_TLYR][o], qv = w.B->in[F_QLYR][o];
@@ -393,22 +335,6 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
         const size_t ab = (size_t)w.i + ldl * ((size_t)w.r + (size_t)a.f.nlay * b);
         saer[b * 128 + tr] = (float)(w.B->in[F_AERAOD][ab] * (1.0 - w.B->in[F_AERSSA][ab]));
       }
-    } else if (MODE == MODE_H && live) {
-      const int c = a.c0 + hcc;
-      const Block* B = (a.nblocks == 1) ? &a.b0 : &a.blocks[__ldg(a.colmap + c)];
-      const size_t ldl = (size_t)B->ld;
-      const size_t o = (size_t)(c - B->col0) + ldl * (size_t)(a.f.top_at_1 ? a.f.nlay - ht - 1 : ht);
-      const int b0 = q == 1 ? 0 : q == 2 ? 6 : 11, b1 = q == 1 ? 6 : q == 2 ? 11 : 16;
-      double aod[6], ssa[6];
-#pragma unroll
-      for (int j = 0; j < 6; ++j) {   // every load first, so their latencies overlap
-        const size_t ab = o + ldl * (size_t)a.f.nlay * (size_t)min(b0 + j, b1 - 1);
-        aod[j] = B->in[F_AERAOD][ab];
-        ssa[j] = B->in[F_AERSSA][ab];
-      }
-#pragma unroll
-      for (int j = 0; j < 6; ++j)
-        if (b0 + j < b1) saer[(b0 + j) * 128 + tr] = (float)(aod[j] * (1.0 - ssa[j]));
     }
     sync_for_mma();
     if (tid == 0) {
@@ -528,15 +454,6 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
         for (int o = 16; o > 0; o >>= 1) sse += __shfl_xor_sync(0xffffffffu, sse, o);
         if ((tid & 31) == 0) atomicAdd(a.loss, sse);
       }
-    } else if (MODE == MODE_H) {
-      const int nchk = (a.f.nlay + 7) >> 3;
-      __half* hrow = a.hnd + ((size_t)hcc * nchk + (ht >> 3)) * (2 * NGPT * 8) + (ht & 7);
-      const float cd = scd[tr];
-      const float* ar = saer + tr;
-      if (q == 0) h_out_quarter<0, 38>(tb, wl, live, hrow, osc, osh, ar, cd);
-      else if (q == 1) h_out_quarter<38, 68>(tb, wl, live, hrow, osc, osh, ar, cd);
-      else if (q == 2) h_out_quarter<68, 108>(tb, wl, live, hrow, osc, osh, ar, cd);
-      else h_out_quarter<108, 140>(tb, wl, live, hrow, osc, osh, ar, cd);
     } else {   // MODE_LW
       // quarters own whole bands: g-points [0,38), [38,68), [68,108), [108,140)
       const size_t nlp = (size_t)a.f.nlay <= 63 ? 64 : (size_t)a.f.nlay <= 127 ? 128 : 256;   // 32 V
@@ -560,6 +477,278 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
   }
   // leave: every MMA this CTA issued has completed (or the wait timed out and
   // the error is recorded); release tensor memory
+  if (failed) umma::mbar_wait(mbar, phase ^ 1u, 1u << 20);   // one more bounded wait for the MMA in flight
+  umma::fence_before_sync();
+  __syncthreads();
+  if (tid == 0 && *sfail && a.err) atomicCAS(a.err, 0, 1);
+  if (warp == 0) umma::tmem_dealloc(tb, 512);
+}
+
+// ---------------------------------------------------------------------------
+// Network stage of the learned-gas-optics column path (lw_sg_path.cu).  One
+// column per 128-row tile: row t is layer t (surface first), rows nlay..127
+// are padding.  Per tile: the layers' features and aerosol depths (their
+// loads issued during the previous tile's output stage), MMA1 -> SiLU ->
+// MMA2 -> SiLU -> MMA3, then the 140 optical depths and the 140 band-
+// normalised Planck fractions (the values of lw_out_quarter), each staged as
+// written straight into the column's hand-off [nlay/8][tau 140 | frac 140]
+// [8 layers] (a warp's 32 rows cover four 8-layer blocks, 16 contiguous
+// bytes each per g-point).  The hidden layers' SiLU is 0.5 z (1 + tanh(0.5 z))
+// with the hardware tanh, one special-function operation per value.
+constexpr float kLog2e = 1.4426950408889634f;
+
+// SiLU of a pair, rounded to a BF16 pair: z sigmoid(z) = 0.5 z (1 + tanh(0.5 z))
+// in FP32 with the hardware tanh (relative error ~2^-11, below the BF16
+// rounding that follows)
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ uint32_t silu_bf16x2(float z0, float z1) {
+  const float h0 = 0.5f * z0, h1 = 0.5f * z1;
+  const __nv_bfloat162 r = __floats2bfloat162_rn(fmaf(h0, tanh_fast(h0), h0), fmaf(h1, tanh_fast(h1), h1));
+  return *reinterpret_cast<const uint32_t*>(&r);
+}
+__device__ __forceinline__ float ex2_fast(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// optical depths of g-points [GA, GB) of this thread's row, FP16 at dst[g stride]:
+// exp(y * std + mean) * coldry + aerosol (the exponent in base 2, scales folded)
+template <int GA, int GB>
+__device__ __forceinline__ void h_out_tau(uint32_t tb, int wl, int stride, bool live, __half* dst, const float* osc2,
+                                            const float* osh2, const float* aer_row, float cd) {
+  constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
+  float v[NCH * 16];
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, 256 + C0 + 16 * c), v + 16 * c);
+#pragma unroll
+  for (int g = GA; g < GB; ++g) {
+    const float tau = live ? fmaf(ex2_fast(fmaf(v[g - C0], osc2[g], osh2[g])), cd, aer_row[band_of_g(g) * 128]) : 0.0f;
+    dst[g * stride] = __float2half_rn(fminf(tau, 6.0e4f));   // below the FP16 maximum
+  }
+}
+
+// band-normalised Planck fractions of g-points [GA, GB) (whole bands), FP16 at dst[g stride]
+template <int GA, int GB>
+__device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool live, __half* dst, const float* osc,
+                                             const float* osh) {
+  constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
+  float v[NCH * 16];
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, C0 + 16 * c), v + 16 * c);
+  float bsum[NBANDS];
+#pragma unroll
+  for (int b = 0; b < NBANDS; ++b) bsum[b] = 0.0f;
+#pragma unroll
+  for (int g = GA; g < GB; ++g) {
+    const float fr = __saturatef(fmaf(v[g - C0], osc[144 + g], osh[144 + g]));
+    v[g - C0] = fr;
+    bsum[band_of_g(g)] += fr;
+  }
+#pragma unroll
+  for (int b = 0; b < NBANDS; ++b) bsum[b] = bsum[b] > 0.0f ? 1.0f / bsum[b] : 1.0f;
+#pragma unroll
+  for (int g = GA; g < GB; ++g) dst[g * stride] = __float2half_rn(live ? v[g - C0] * bsum[band_of_g(g)] : 0.0f);
+}
+
+__global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int tid = threadIdx.x, warp = tid >> 5, wl = warp & 3, q = tid >> 7, t = tid & 127;
+  float* sb2 = reinterpret_cast<float*>(sm + SM_B2);
+  float* snorm = reinterpret_cast<float*>(sm + SM_NORM);
+  float* saer0 = reinterpret_cast<float*>(sm + SM_AER);
+  float* scd0 = reinterpret_cast<float*>(sm + SM_CD);
+  float* osc = reinterpret_cast<float*>(sm + SM_OSC);
+  float* osh = reinterpret_cast<float*>(sm + SM_OSH);
+  float* osc2 = reinterpret_cast<float*>(sm + SM_B3);   // [0, 144): tau scales in base 2 (b3 is folded into osh)
+  float* osh2 = osc2 + 144;                             // SM_B3 holds 288 floats
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + SM_BAR);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SM_BAR + 8);
+  int* sfail = reinterpret_cast<int*>(sm + SM_BAR + 12);
+
+  copy_rows_canon(sm + SM_W1, a.ops + O_W1, HID, KIN, tid);
+  copy_rows_canon(sm + SM_W2, a.ops + O_W2, HID, HID, tid);
+  copy_rows_canon(sm + SM_W3, a.ops + O_W3, NOP, HID, tid);
+  for (int j = tid; j < HID; j += FWD_THREADS) sb2[j] = a.params[P_B2 + j];
+  for (int j = tid; j < SG_NORM_FLOATS; j += FWD_THREADS) snorm[j] = a.norm[j];
+  for (int j = tid; j < NOP; j += FWD_THREADS) {
+    const float sd = a.norm[SG_OUT_STD + j];
+    osc[j] = sd;
+    osh[j] = fmaf(a.params[P_B3 + j], sd, a.norm[SG_OUT_MEAN + j]);
+    if (j < 144) {
+      osc2[j] = sd * kLog2e;
+      osh2[j] = fmaf(a.params[P_B3 + j], sd, a.norm[SG_OUT_MEAN + j]) * kLog2e;
+    }
+  }
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, 512);
+    umma::tmem_relinquish();
+  }
+  if (tid == 0) {
+    umma::mbar_init(mbar, 1);
+    *sfail = 0;
+  }
+  umma::fence_smem_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tb = *tslot;
+  const uint32_t sbase = umma::smem_u32(sm);
+  constexpr uint32_t ID128 = umma::idesc_bf16(128, 128), ID144 = umma::idesc_bf16(128, 144);
+  uint32_t phase = 0;
+  bool failed = false;   // uniform across the CTA
+  auto wait_mma = [&]() -> bool {
+    const bool ok = umma::mbar_wait(mbar, phase, c_fwd_wait_polls);
+    phase ^= 1u;
+    umma::fence_after_sync();
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) *sfail = 1;
+      failed = true;
+      return false;
+    }
+    return true;
+  };
+  auto sync_for_mma = [&]() {
+    umma::fence_smem_async();
+    umma::fence_before_sync();
+    __syncthreads();
+  };
+
+  const int nlay = a.f.nlay, nchk = (nlay + 7) >> 3;
+  const bool live = t < nlay;
+  const int r = a.f.top_at_1 ? nlay - 1 - t : t;   // input row of layer t
+  const int b0 = q == 1 ? 0 : q == 2 ? 6 : 11, b1 = q == 1 ? 6 : q == 2 ? 11 : 16;
+  // inputs of this thread's layer, loaded one column ahead: quarter 0 the
+  // eight state fields, quarters 1-3 aod/ssa of their bands
+  double pf[12];
+#pragma unroll
+  for (int j = 0; j < 12; ++j) pf[j] = 0.0;
+  auto prefetch = [&](int cc) {
+    if (cc >= a.nc || !live) return;
+    const int c = a.c0 + cc;
+    const Block* B = (a.nblocks == 1) ? &a.b0 : &a.blocks[__ldg(a.colmap + c)];
+    const size_t ld = (size_t)B->ld;
+    const size_t o = (size_t)(c - B->col0) + ld * (size_t)r;
+    if (q == 0) {
+      pf[0] = B->in[F_PLYR][o]; pf[1] = B->in[F_TLYR][o]; pf[2] = B->in[F_QLYR][o]; pf[3] = B->in[F_OLYR][o];
+      pf[4] = B->in[F_CO2][o]; pf[5] = B->in[F_CH4][o]; pf[6] = B->in[F_N2O][o]; pf[7] = B->in[F_DELPIN][o];
+    } else {
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const size_t ab = o + ld * (size_t)nlay * (size_t)min(b0 + j, b1 - 1);
+        pf[2 * j] = B->in[F_AERAOD][ab];
+        pf[2 * j + 1] = B->in[F_AERSSA][ab];
+      }
+    }
+  };
+  prefetch(blockIdx.x);
+
+  int parity = 0;   // double buffer of the per-tile aerosol / coldry rows
+  for (int cc = blockIdx.x; cc < a.nc; cc += gridDim.x, parity ^= 1) {
+    const int c = a.c0 + cc;
+    float* saer = saer0 + parity * NBANDS * 128;
+    float* scd = scd0 + parity * 128;
+    // ---------------- layer inputs -> X (features), aerosol depths, coldry ----------------
+    if (q == 0) {
+      float x[KIN];
+#pragma unroll
+      for (int j = 0; j < KIN; ++j) x[j] = 0.0f;
+      if (live) {
+        const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
+        const double h2ovmr = fmax(0.0, pf[2] * amdw / (1.0 - pf[2]));
+        const double o3vmr = fmax(0.0, pf[3] * amdo3);
+        const double tem0 = (1.0 - h2ovmr) * 28.9644 + h2ovmr * 18.0154;
+        scd[t] = (float)((1.0e-20 * 1.0e3 * 6.0221415e23) * pf[7] / (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr)));
+        float raw[NIN];
+        layer_features(pf[0], pf[1], h2ovmr, o3vmr, pf[4], pf[5], pf[6], raw);
+        // a layer outside the training envelope: list its column once for the fallback
+        if (!in_envelope(raw, a.norm) && atomicExch(a.fb_flag + c, 1u) == 0u) a.fb_list[atomicAdd(a.fb_count, 1)] = c;
+#pragma unroll
+        for (int j = 0; j < 7; ++j) x[j] = (raw[j] - snorm[SG_IN_MEAN + j]) / snorm[SG_IN_STD + j];
+        x[7] = 1.0f;
+      }
+      umma::st_canon8(sm + SM_X, t, 0, KIN, x);
+      umma::st_canon8(sm + SM_X, t, 8, KIN, x + 8);
+    } else if (live) {
+#pragma unroll
+      for (int j = 0; j < 6; ++j)
+        if (b0 + j < b1) saer[(b0 + j) * 128 + t] = (float)(pf[2 * j] * (1.0 - pf[2 * j + 1]));
+    }
+    sync_for_mma();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      umma::mma(tb, umma::tile_desc(sbase + SM_X, KIN, 0), umma::tile_desc(sbase + SM_W1, KIN, 0), ID128, 0u);
+      umma::commit(mbar);
+    }
+    if (!wait_mma()) break;
+
+    // ---------------- hidden layers: quarter q owns hidden units [32q, 32q+32) ----------------
+#pragma unroll 1
+    for (int layer = 0; layer < 2; ++layer) {
+      const int dcol = layer == 0 ? 0 : 128;
+      float v32[32];
+      umma::tmem_ld32(umma::tmem_addr(tb, wl, dcol + 32 * q), v32);
+#pragma unroll
+      for (int h8 = 0; h8 < 4; ++h8) {
+        const int c0 = 32 * q + 8 * h8;
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float z0 = v32[8 * h8 + 2 * j] + (layer == 1 ? sb2[c0 + 2 * j] : 0.0f);
+          const float z1 = v32[8 * h8 + 2 * j + 1] + (layer == 1 ? sb2[c0 + 2 * j + 1] : 0.0f);
+          w[j] = silu_bf16x2(z0, z1);
+        }
+        *reinterpret_cast<uint4*>(sm + SM_H + umma::canon_off(t, c0, HID)) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
+      sync_for_mma();
+      if (tid == 0) {
+        umma::fence_after_sync();
+        if (layer == 0) {
+#pragma unroll 1
+          for (int s = 0; s < HID / 16; ++s)
+            umma::mma(tb + 128, umma::tile_desc(sbase + SM_H, HID, s), umma::tile_desc(sbase + SM_W2, HID, s), ID128,
+                      s > 0 ? 1u : 0u);
+        } else {
+#pragma unroll 1
+          for (int s = 0; s < HID / 16; ++s)
+            umma::mma(tb + 256, umma::tile_desc(sbase + SM_H, HID, s), umma::tile_desc(sbase + SM_W3, HID, s), ID144,
+                      s > 0 ? 1u : 0u);
+#pragma unroll 1
+          for (int s = 0; s < HID / 16; ++s)
+            umma::mma(tb, umma::tile_desc(sbase + SM_H, HID, s), umma::tile_desc(sbase + SM_W3 + W3_HALF, HID, s),
+                      ID144, s > 0 ? 1u : 0u);
+        }
+        umma::commit(mbar);
+      }
+      if (!wait_mma()) break;
+    }
+    if (failed) break;
+    // the next column's inputs load while this one's outputs are formed
+    prefetch(cc + (int)gridDim.x);
+
+    // ---------------- outputs: optical depths and fractions into the hand-off ----------------
+    // this row's slot of g-point 0 in its 8-layer block; g-point g at [8 g]
+    __half* hrow = a.hnd + ((size_t)cc * nchk + (t >> 3)) * (2 * NGPT * 8) + (t & 7);
+    const float cd = live ? scd[t] : 0.0f;
+    const float* ar = saer + t;
+    // quarters own whole bands: g-points [0,38), [38,68), [68,108), [108,140)
+    if (q == 0) h_out_tau<0, 38>(tb, wl, 8, live, hrow, osc2, osh2, ar, cd);
+    else if (q == 1) h_out_tau<38, 68>(tb, wl, 8, live, hrow, osc2, osh2, ar, cd);
+    else if (q == 2) h_out_tau<68, 108>(tb, wl, 8, live, hrow, osc2, osh2, ar, cd);
+    else h_out_tau<108, 140>(tb, wl, 8, live, hrow, osc2, osh2, ar, cd);
+    hrow += 8 * NGPT;
+    if (q == 0) h_out_frac<0, 38>(tb, wl, 8, live, hrow, osc, osh);
+    else if (q == 1) h_out_frac<38, 68>(tb, wl, 8, live, hrow, osc, osh);
+    else if (q == 2) h_out_frac<68, 108>(tb, wl, 8, live, hrow, osc, osh);
+    else h_out_frac<108, 140>(tb, wl, 8, live, hrow, osc, osh);
+    // the accumulators are free for the next tile once every thread has read them
+    umma::fence_before_sync();
+    __syncthreads();
+  }
   if (failed) umma::mbar_wait(mbar, phase ^ 1u, 1u << 20);   // one more bounded wait for the MMA in flight
   umma::fence_before_sync();
   __syncthreads();
@@ -810,8 +999,7 @@ cudaError_t set_attrs() {
     return e;
   if ((e = cudaFuncSetAttribute(mlp_fwd_kernel<MODE_LW>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM)))
     return e;
-  if ((e = cudaFuncSetAttribute(mlp_fwd_kernel<MODE_H>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM)))
-    return e;
+  if ((e = cudaFuncSetAttribute(mlp_h_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM))) return e;
   if ((e = cudaFuncSetAttribute(gemm_tn_kernel<EPI_ATOMIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM)))
     return e;
   if ((e = cudaFuncSetAttribute(gemm_tn_kernel<EPI_DACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM)))
@@ -823,7 +1011,7 @@ cudaError_t set_attrs() {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], mlp_fwd_kernel<MODE_LW>, FWD_THREADS, FWD_SMEM);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], gemm_tn_kernel<EPI_ATOMIC>, 128, GEMM_SMEM);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[4], gemm_tn_kernel<EPI_DACT>, 128, GEMM_SMEM);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[5], mlp_fwd_kernel<MODE_H>, FWD_THREADS, FWD_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[5], mlp_h_kernel, FWD_THREADS, FWD_SMEM);
   for (int o : occ)
     if (o != 1) return cudaErrorLaunchOutOfResources;
   net.attrs = true;
@@ -995,11 +1183,10 @@ cudaError_t mlp_h_launch(const Block* blocks, int nblocks, const Block& b0, cons
   a.fb_flag = fb_flag;
   a.fb_list = fb_list;
   a.fb_count = fb_count;
-  a.nrows = (long)nc * f.nlay;
-  const long tiles = (a.nrows + 127) / 128;
-  const int grid = (int)std::min<long>(tiles, num_sms);
+  if (f.nlay > 127) return cudaErrorInvalidValue;   // one column per 128-row tile
+  const int grid = std::min(nc, num_sms);
   if (grid < 1) return cudaSuccess;
-  mlp_fwd_kernel<MODE_H><<<grid, FWD_THREADS, FWD_SMEM, st>>>(a);
+  mlp_h_kernel<<<grid, FWD_THREADS, FWD_SMEM, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -166,6 +166,56 @@ __device__ __forceinline__ void cloud_terms(float od, int it, float odcld, const
   }
 }
 
+// cldprop band optics of one layer (RLM:1589-1799), FP64: the layer's
+// band-independent terms once (set: indices and interpolation fractions,
+// one division), then each band's table interpolation (band); the
+// arithmetic of band_taucld (lw_gas.cuh) with the per-band work hoisted.
+struct CloudLayer {
+  double cf, clwp, ciwp, cda1, tauran, tausnw, fliq, fice, refice;
+  int iliq, iice;
+  __device__ __forceinline__ void set(const Flags& f, double cf_, double clwp_, double relw, double ciwp_,
+                                      double reiw, double cda1_, double cda3, double cda4) {
+    cf = cf_; clwp = clwp_; ciwp = ciwp_; cda1 = cda1_;
+    tauran = kAbsrain * cda1;
+    tausnw = (cda3 > 0.0 && cda4 > 10.0) ? kAbssnow0 * 1.05756 * cda3 / cda4 : 0.0;
+    const double lfac = relw - 1.5;
+    iliq = max(1, min(57, (int)lfac));
+    fliq = lfac - (double)iliq;
+    refice = fmin(130.0, fmax(13.0, reiw));
+    double ifac = 0.0;
+    int ihi = 45;
+    if (f.ilwcice == 2) { ifac = (reiw - 2.0) / 3.0; ihi = 42; }
+    else if (f.ilwcice == 3) { ifac = (fmax(5.0, 1.0315 * reiw) - 2.0) / 3.0; }
+    iice = max(1, min(ihi, (int)ifac));
+    fice = ifac - (double)iice;
+  }
+  __device__ __forceinline__ double band(int b, const Flags& f, const double* kt) const {
+    if (!(cf > 2.2250738585072014e-308)) return 0.0;   // cfrac(k) > cldmin = tiny
+    if (f.ilwcliq <= 0) return cda1;                    // diagnostic cloud optical depth
+    double tauliq = 0.0, tauice = 0.0;
+    if (clwp > 0.0 && f.ilwcliq == 1) {
+      const double a = t64(kt, lwtab::absliq1 + (iliq - 1) + 58 * b);
+      const double c = t64(kt, lwtab::absliq1 + iliq + 58 * b);
+      tauliq = fmax(0.0, clwp * (a + fliq * (c - a)));
+    }
+    if (ciwp > 0.0) {
+      if (f.ilwcice == 1) {
+        const int ia = (int)t64(kt, lwtab::ipat + b);
+        tauice = fmax(0.0, ciwp * (t64(kt, lwtab::absice1 + 2 * (ia - 1)) + t64(kt, lwtab::absice1 + 1 + 2 * (ia - 1)) / refice));
+      } else if (f.ilwcice == 2) {
+        const double a = t64(kt, lwtab::absice2 + (iice - 1) + 43 * b);
+        const double c = t64(kt, lwtab::absice2 + iice + 43 * b);
+        tauice = fmax(0.0, ciwp * (a + fice * (c - a)));
+      } else if (f.ilwcice == 3) {
+        const double a = t64(kt, lwtab::absice3 + (iice - 1) + 46 * b);
+        const double c = t64(kt, lwtab::absice3 + iice + 46 * b);
+        tauice = fmax(0.0, ciwp * (a + fice * (c - a)));
+      }
+    }
+    return tauice + tauliq + tauran + tausnw;
+  }
+};
+
 __device__ __forceinline__ int band_of(int g) {
   return g < 10 ? 0 : g < 22 ? 1 : g < 38 ? 2 : g < 52 ? 3 : g < 68 ? 4 : g < 76 ? 5 : g < 88 ? 6 : g < 96 ? 7
        : g < 108 ? 8 : g < 114 ? 9 : g < 122 ? 10 : g < 130 ? 11 : g < 134 ? 12 : g < 136 ? 13 : g < 138 ? 14 : 15;
@@ -294,9 +344,11 @@ __global__ void __launch_bounds__(SR_THREADS, 1) lw_sg_rt_kernel(SrArgs a) {
       }
       sync.sync();
       if (live) {
+        CloudLayer CL;
+        CL.set(f, cf, clwp, relw, ciwp, reiw, cda1, cda3, cda4);
 #pragma unroll 1
         for (int b = 0; b < NBANDS; ++b) {
-          const double tc = lcf1 ? band_taucld(b, f, kt64, cf, clwp, relw, ciwp, reiw, cda1, cda3, cda4) : 0.0;
+          const double tc = lcf1 ? CL.band(b, f, kt64) : 0.0;
           if (b == 6) B.out[O_CLDTAU][i + ld * r] = tc;   // band 7 cloud optical depth (RLM:1087-1097)
           S.bf[t][b] = make_float4(pkl[b], S.u.p.pkv[t + 1][b] - pkl[b], S.u.p.pkv[t][b] - pkl[b], S.secd[b] * (float)tc);
         }
