@@ -22,7 +22,7 @@ The last line printed is the headline JSON record:
   cpu_baseline  the oracle on all host cores, timed on the parity sample.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--legs sw,callers,train]
+                    [--legs sw,callers,train [--only-legs]]
 --gpus N > 1 starts N ranks itself (torch.distributed.run) unless it already
 runs under a launcher (WORLD_SIZE set).  Each rank takes whole physics blocks
 of the workload (ccpp_physics_b200.shard.block_range): the total work is
@@ -790,6 +790,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--legs", default="", help="comma list of auxiliary legs printed before the headline: "
                                                 "sw, callers, train")
+    ap.add_argument("--only-legs", action="store_true", help="print the --legs lines and stop (no headline); "
+                                                              "profiling runs of the auxiliary legs")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-memory leg")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle parity check and CPU baseline")
     ap.add_argument("--dry-run", action="store_true", help="launcher and process-group plumbing only")
@@ -886,6 +888,10 @@ def main():
             from ccpp_physics_b200 import surrogate as sg
             print(json.dumps({"leg": "c4_training", **training_leg(args, torch, sg)}), flush=True)
         torch.cuda.empty_cache()
+    if args.only_legs:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     res, e2e, parity, cpu, clk, ncols = headline(args, rank, world, local, dist, torch, sh, stream, lw, abi,
                                                  synthetic)
