@@ -133,9 +133,10 @@ __host__ __device__ constexpr size_t gas_smem_bytes(int V) {
   return sizeof(double) * (2 * NLP + 24 + 8 * NLP) + sizeof(R) * N_LF * NLP + sizeof(int) * (NLP + 4);
 }
 
-// Barrier of the threads that run gas_column together: the whole CTA
-// (lw_gas_kernel), or a named barrier over the first `n` threads of a CTA
-// whose other warps do other work (the fused learned-gas-optics kernel).
+// Barrier of a group of threads: the whole CTA (gas_column in lw_gas_kernel
+// and the fallback kernel of the learned-gas-optics path), or a named
+// barrier over `n` threads of a CTA that holds several groups (that path's
+// transfer kernel).
 struct CtaSync {
   __device__ __forceinline__ void sync() const { __syncthreads(); }
   __device__ __forceinline__ int count(bool p) const { return __syncthreads_count(p); }
