@@ -123,9 +123,11 @@ __device__ __forceinline__ float warp_sum_all(float v) {
   return v;
 }
 
-// record index it = int(10000 x / (bpade + x) + 0.5) of an optical depth (RLM:3602-3603)
+// record index it = int(10000 x / (bpade + x) + 0.5) of an optical depth
+// (RLM:3602-3603); x is finite and >= 0 here (the hand-off clamps optical
+// depths below the FP16 maximum), so the index is >= 0
 __device__ __forceinline__ int tbl_index(float x) {
-  return min(NTBL, max(0, (int)(float(kTblint) * __fdividef(x, float(kBpade) + x) + 0.5f)));
+  return min(NTBL, (int)(float(kTblint) * __fdividef(x, float(kBpade) + x) + 0.5f));
 }
 
 // The gas terms of one layer and g-point (RLM:3598-3614) in FP32: optical
@@ -432,7 +434,17 @@ __global__ void __launch_bounds__(SR_THREADS, 1) lw_sg_rt_kernel(SrArgs a) {
           itv[ii] = small ? -1 : it;
         }
         // the recurrences, top layer of the chunk first; the total-sky terms
-        // where the warp has a cloudy sub-column layer
+        // where the warp has a cloudy sub-column layer (a chunk without any
+        // takes the clear-sky recurrence alone)
+        if (!__any_sync(0xffffffffu, cb != 0u)) {
+#pragma unroll
+          for (int ii = SR_CH - 1; ii >= 0; --ii) {
+            radc = radc * trv[ii] + gsdv[ii];
+            radt = radt * trv[ii] + gsdv[ii];
+            aT[ii] = radt;
+            aC[ii] = radc;
+          }
+        } else {
 #pragma unroll
         for (int ii = SR_CH - 1; ii >= 0; --ii) {
           const float tr = trv[ii], gsd = gsdv[ii];
@@ -453,6 +465,7 @@ __global__ void __launch_bounds__(SR_THREADS, 1) lw_sg_rt_kernel(SrArgs a) {
           }
           aT[ii] = radt;
           aC[ii] = radc;
+        }
         }
         umma::tmem_st8(tw + SR_CH * j, stash);
         if (j == 0) fr0 = fr[0];
@@ -494,6 +507,17 @@ __global__ void __launch_bounds__(SR_THREADS, 1) lw_sg_rt_kernel(SrArgs a) {
         umma::tmem_ld8(tw + SR_CH * j, stash);
         const uint32_t cb = chunk_bits(j);
         float aT[SR_CH], aC[SR_CH];
+        if (!__any_sync(0xffffffffu, cb != 0u)) {   // no cloudy sub-column layer in the chunk
+#pragma unroll
+          for (int ii = 0; ii < SR_CH; ++ii) {
+            const float2 ag = __half22float2(*reinterpret_cast<const __half2*>(&stash[ii]));
+            const float tr = 1.0f - ag.x, gsu = ag.y * su_scale;
+            ruclr = ruclr * tr + gsu;
+            rutot = rutot * tr + gsu;
+            aT[ii] = rutot;
+            aC[ii] = ruclr;
+          }
+        } else {
 #pragma unroll
         for (int ii = 0; ii < SR_CH; ++ii) {
           const float2 ag = __half22float2(*reinterpret_cast<const __half2*>(&stash[ii]));
@@ -517,6 +541,7 @@ __global__ void __launch_bounds__(SR_THREADS, 1) lw_sg_rt_kernel(SrArgs a) {
           }
           aT[ii] = rutot;
           aC[ii] = ruclr;
+        }
         }
         const float sT = warp_sum8(aT, lane), sC = warp_sum8(aC, lane);
         const int lvl = SR_CH * j + 1 + ((lane >> 2) & 7);
