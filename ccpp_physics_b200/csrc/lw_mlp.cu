@@ -490,11 +490,33 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
 // are padding.  Per tile: the layers' features and aerosol depths (their
 // loads issued during the previous tile's output stage), MMA1 -> SiLU ->
 // MMA2 -> SiLU -> MMA3, then the 140 optical depths and the 140 band-
-// normalised Planck fractions (the values of lw_out_quarter), each staged as
-// written straight into the column's hand-off [nlay/8][tau 140 | frac 140]
-// [8 layers] (a warp's 32 rows cover four 8-layer blocks, 16 contiguous
-// bytes each per g-point).  The hidden layers' SiLU is 0.5 z (1 + tanh(0.5 z))
-// with the hardware tanh, one special-function operation per value.
+// normalised Planck fractions (the values of lw_out_quarter), written
+// straight into the column's hand-off [nlay/8][tau 140 | frac 140][8 layers]
+// (a warp's 32 rows cover four 8-layer blocks, 16 contiguous bytes each per
+// g-point).  The hidden layers' SiLU is 0.5 z (1 + tanh(0.5 z)) with the
+// hardware tanh, one special-function operation per value.
+//
+// The output layer's normalisation is folded into MMA3: each CTA builds its
+// W3 tile from the FP32 master weights with row j scaled by the output's
+// standard deviation (times log2 e for the optical depths), and three extra
+// K columns that carry the output's shift (b3 std + mean, the same scaling)
+// as a BF16 hi + mid + lo split against constant-one columns of H2 (K = 144).
+// The accumulator then holds log2(tau / coldry) and the fraction itself.
+constexpr int KH3 = HID + 16;                                  // K of MMA3: H2 + {1, 1, 1, 0 ...}
+constexpr uint32_t HSM_W1 = 0;                                 // canon [128][16]
+constexpr uint32_t HSM_W2 = HSM_W1 + HID * KIN * 2;            // canon [128][128]
+constexpr uint32_t HSM_W3 = HSM_W2 + HID * HID * 2;            // canon [288][144]
+constexpr uint32_t HSM_X = HSM_W3 + NOP * KH3 * 2;             // canon [128][16]
+constexpr uint32_t HSM_H = HSM_X + 128 * KIN * 2;              // canon [128][128] (H1) / [128][144] (H2)
+constexpr uint32_t HSM_B2 = HSM_H + 128 * KH3 * 2;             // f32 [128]
+constexpr uint32_t HSM_NORM = HSM_B2 + HID * 4;                // f32 [16] input mean, std
+constexpr uint32_t HSM_AER = HSM_NORM + 16 * 4;                // f32 [2][16][128] aerosol tau of the tile's layers
+constexpr uint32_t HSM_CD = HSM_AER + 2 * NBANDS * 128 * 4;    // f32 [2][128] coldry of the tile's layers
+constexpr uint32_t HSM_BAR = (HSM_CD + 2 * 128 * 4 + 15) & ~15u;
+constexpr uint32_t H_SMEM = HSM_BAR + 32;
+static_assert(H_SMEM > 116 * 1024 && H_SMEM <= 227 * 1024, "one CTA per SM (512 TMEM columns), within shared memory");
+static_assert(HSM_W3 % 128 == 0 && HSM_X % 128 == 0 && HSM_H % 128 == 0, "canonical tiles");
+constexpr uint32_t W3H_HALF = 144 * KH3 * 2;                   // second 144-row B operand of MMA3
 constexpr float kLog2e = 1.4426950408889634f;
 
 // SiLU of a pair, rounded to a BF16 pair: z sigmoid(z) = 0.5 z (1 + tanh(0.5 z))
@@ -517,25 +539,24 @@ __device__ __forceinline__ float ex2_fast(float x) {
 }
 
 // optical depths of g-points [GA, GB) of this thread's row, FP16 at dst[g stride]:
-// exp(y * std + mean) * coldry + aerosol (the exponent in base 2, scales folded)
+// 2^acc * coldry + aerosol
 template <int GA, int GB>
-__device__ __forceinline__ void h_out_tau(uint32_t tb, int wl, int stride, bool live, __half* dst, const float* osc2,
-                                            const float* osh2, const float* aer_row, float cd) {
+__device__ __forceinline__ void h_out_tau(uint32_t tb, int wl, int stride, bool live, __half* dst,
+                                          const float* aer_row, float cd) {
   constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
   float v[NCH * 16];
 #pragma unroll
   for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, 256 + C0 + 16 * c), v + 16 * c);
 #pragma unroll
   for (int g = GA; g < GB; ++g) {
-    const float tau = live ? fmaf(ex2_fast(fmaf(v[g - C0], osc2[g], osh2[g])), cd, aer_row[band_of_g(g) * 128]) : 0.0f;
+    const float tau = live ? fmaf(ex2_fast(v[g - C0]), cd, aer_row[band_of_g(g) * 128]) : 0.0f;
     dst[g * stride] = __float2half_rn(fminf(tau, 6.0e4f));   // below the FP16 maximum
   }
 }
 
 // band-normalised Planck fractions of g-points [GA, GB) (whole bands), FP16 at dst[g stride]
 template <int GA, int GB>
-__device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool live, __half* dst, const float* osc,
-                                             const float* osh) {
+__device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool live, __half* dst) {
   constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
   float v[NCH * 16];
 #pragma unroll
@@ -545,7 +566,7 @@ __device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool
   for (int b = 0; b < NBANDS; ++b) bsum[b] = 0.0f;
 #pragma unroll
   for (int g = GA; g < GB; ++g) {
-    const float fr = __saturatef(fmaf(v[g - C0], osc[144 + g], osh[144 + g]));
+    const float fr = __saturatef(v[g - C0]);
     v[g - C0] = fr;
     bsum[band_of_g(g)] += fr;
   }
@@ -558,32 +579,40 @@ __device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool
 __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const int tid = threadIdx.x, warp = tid >> 5, wl = warp & 3, q = tid >> 7, t = tid & 127;
-  float* sb2 = reinterpret_cast<float*>(sm + SM_B2);
-  float* snorm = reinterpret_cast<float*>(sm + SM_NORM);
-  float* saer0 = reinterpret_cast<float*>(sm + SM_AER);
-  float* scd0 = reinterpret_cast<float*>(sm + SM_CD);
-  float* osc = reinterpret_cast<float*>(sm + SM_OSC);
-  float* osh = reinterpret_cast<float*>(sm + SM_OSH);
-  float* osc2 = reinterpret_cast<float*>(sm + SM_B3);   // [0, 144): tau scales in base 2 (b3 is folded into osh)
-  float* osh2 = osc2 + 144;                             // SM_B3 holds 288 floats
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + SM_BAR);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SM_BAR + 8);
-  int* sfail = reinterpret_cast<int*>(sm + SM_BAR + 12);
+  float* sb2 = reinterpret_cast<float*>(sm + HSM_B2);
+  float* snorm = reinterpret_cast<float*>(sm + HSM_NORM);
+  float* saer0 = reinterpret_cast<float*>(sm + HSM_AER);
+  float* scd0 = reinterpret_cast<float*>(sm + HSM_CD);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + HSM_BAR);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + HSM_BAR + 8);
+  int* sfail = reinterpret_cast<int*>(sm + HSM_BAR + 12);
 
-  copy_rows_canon(sm + SM_W1, a.ops + O_W1, HID, KIN, tid);
-  copy_rows_canon(sm + SM_W2, a.ops + O_W2, HID, HID, tid);
-  copy_rows_canon(sm + SM_W3, a.ops + O_W3, NOP, HID, tid);
-  for (int j = tid; j < HID; j += FWD_THREADS) sb2[j] = a.params[P_B2 + j];
-  for (int j = tid; j < SG_NORM_FLOATS; j += FWD_THREADS) snorm[j] = a.norm[j];
-  for (int j = tid; j < NOP; j += FWD_THREADS) {
+  copy_rows_canon(sm + HSM_W1, a.ops + O_W1, HID, KIN, tid);
+  copy_rows_canon(sm + HSM_W2, a.ops + O_W2, HID, HID, tid);
+  // W3 with the output normalisation folded in (rows scaled, the shift as
+  // three BF16 terms in columns 128..130), from the FP32 master weights
+  for (int ch = tid; ch < NOP * (KH3 / 8); ch += FWD_THREADS) {
+    const int j = ch / (KH3 / 8), k = (ch % (KH3 / 8)) * 8;
+    const bool pad = pad_out_row(j);
     const float sd = a.norm[SG_OUT_STD + j];
-    osc[j] = sd;
-    osh[j] = fmaf(a.params[P_B3 + j], sd, a.norm[SG_OUT_MEAN + j]);
-    if (j < 144) {
-      osc2[j] = sd * kLog2e;
-      osh2[j] = fmaf(a.params[P_B3 + j], sd, a.norm[SG_OUT_MEAN + j]) * kLog2e;
+    const float scale = j < 144 ? sd * kLog2e : sd;
+    float w[8];
+    if (k < HID) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) w[u] = pad ? 0.0f : a.params[P_W3 + j * HID + k + u] * scale;
+    } else {
+      const float sh = fmaf(a.params[P_B3 + j], sd, a.norm[SG_OUT_MEAN + j]) * (j < 144 ? kLog2e : 1.0f);
+      const float hi = pad ? 0.0f : __bfloat162float(__float2bfloat16_rn(sh));
+      const float mid = pad ? 0.0f : __bfloat162float(__float2bfloat16_rn(sh - hi));
+      const float lo = pad ? 0.0f : sh - hi - mid;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) w[u] = 0.0f;
+      if (k == HID) { w[0] = hi; w[1] = mid; w[2] = lo; }
     }
+    umma::st_canon8(sm + HSM_W3, j, k, KH3, w);
   }
+  for (int j = tid; j < HID; j += FWD_THREADS) sb2[j] = a.params[P_B2 + j];
+  if (tid < 16) snorm[tid] = a.norm[tid < 8 ? SG_IN_MEAN + tid : SG_IN_STD + tid - 8];
   if (warp == 0) {
     umma::tmem_alloc(tslot, 512);
     umma::tmem_relinquish();
@@ -668,11 +697,11 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
         // a layer outside the training envelope: list its column once for the fallback
         if (!in_envelope(raw, a.norm) && atomicExch(a.fb_flag + c, 1u) == 0u) a.fb_list[atomicAdd(a.fb_count, 1)] = c;
 #pragma unroll
-        for (int j = 0; j < 7; ++j) x[j] = (raw[j] - snorm[SG_IN_MEAN + j]) / snorm[SG_IN_STD + j];
+        for (int j = 0; j < 7; ++j) x[j] = (raw[j] - snorm[j]) / snorm[8 + j];
         x[7] = 1.0f;
       }
-      umma::st_canon8(sm + SM_X, t, 0, KIN, x);
-      umma::st_canon8(sm + SM_X, t, 8, KIN, x + 8);
+      umma::st_canon8(sm + HSM_X, t, 0, KIN, x);
+      umma::st_canon8(sm + HSM_X, t, 8, KIN, x + 8);
     } else if (live) {
 #pragma unroll
       for (int j = 0; j < 6; ++j)
@@ -681,7 +710,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
     sync_for_mma();
     if (tid == 0) {
       umma::fence_after_sync();
-      umma::mma(tb, umma::tile_desc(sbase + SM_X, KIN, 0), umma::tile_desc(sbase + SM_W1, KIN, 0), ID128, 0u);
+      umma::mma(tb, umma::tile_desc(sbase + HSM_X, KIN, 0), umma::tile_desc(sbase + HSM_W1, KIN, 0), ID128, 0u);
       umma::commit(mbar);
     }
     if (!wait_mma()) break;
@@ -690,6 +719,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
 #pragma unroll 1
     for (int layer = 0; layer < 2; ++layer) {
       const int dcol = layer == 0 ? 0 : 128;
+      const int KH = layer == 0 ? HID : KH3;   // H1 feeds MMA2 (K = 128), H2 feeds MMA3 (K = 144)
       float v32[32];
       umma::tmem_ld32(umma::tmem_addr(tb, wl, dcol + 32 * q), v32);
 #pragma unroll
@@ -702,7 +732,14 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
           const float z1 = v32[8 * h8 + 2 * j + 1] + (layer == 1 ? sb2[c0 + 2 * j + 1] : 0.0f);
           w[j] = silu_bf16x2(z0, z1);
         }
-        *reinterpret_cast<uint4*>(sm + SM_H + umma::canon_off(t, c0, HID)) = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4*>(sm + HSM_H + umma::canon_off(t, c0, KH)) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
+      if (layer == 1 && q == 0) {
+        // the constant-one columns of H2 that carry the output shift
+        const float one[8] = {1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        const float zero[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        umma::st_canon8(sm + HSM_H, t, HID, KH3, one);
+        umma::st_canon8(sm + HSM_H, t, HID + 8, KH3, zero);
       }
       sync_for_mma();
       if (tid == 0) {
@@ -710,16 +747,16 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
         if (layer == 0) {
 #pragma unroll 1
           for (int s = 0; s < HID / 16; ++s)
-            umma::mma(tb + 128, umma::tile_desc(sbase + SM_H, HID, s), umma::tile_desc(sbase + SM_W2, HID, s), ID128,
-                      s > 0 ? 1u : 0u);
+            umma::mma(tb + 128, umma::tile_desc(sbase + HSM_H, HID, s), umma::tile_desc(sbase + HSM_W2, HID, s),
+                      ID128, s > 0 ? 1u : 0u);
         } else {
 #pragma unroll 1
-          for (int s = 0; s < HID / 16; ++s)
-            umma::mma(tb + 256, umma::tile_desc(sbase + SM_H, HID, s), umma::tile_desc(sbase + SM_W3, HID, s), ID144,
-                      s > 0 ? 1u : 0u);
+          for (int s = 0; s < KH3 / 16; ++s)
+            umma::mma(tb + 256, umma::tile_desc(sbase + HSM_H, KH3, s), umma::tile_desc(sbase + HSM_W3, KH3, s),
+                      ID144, s > 0 ? 1u : 0u);
 #pragma unroll 1
-          for (int s = 0; s < HID / 16; ++s)
-            umma::mma(tb, umma::tile_desc(sbase + SM_H, HID, s), umma::tile_desc(sbase + SM_W3 + W3_HALF, HID, s),
+          for (int s = 0; s < KH3 / 16; ++s)
+            umma::mma(tb, umma::tile_desc(sbase + HSM_H, KH3, s), umma::tile_desc(sbase + HSM_W3 + W3H_HALF, KH3, s),
                       ID144, s > 0 ? 1u : 0u);
         }
         umma::commit(mbar);
@@ -736,15 +773,15 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
     const float cd = live ? scd[t] : 0.0f;
     const float* ar = saer + t;
     // quarters own whole bands: g-points [0,38), [38,68), [68,108), [108,140)
-    if (q == 0) h_out_tau<0, 38>(tb, wl, 8, live, hrow, osc2, osh2, ar, cd);
-    else if (q == 1) h_out_tau<38, 68>(tb, wl, 8, live, hrow, osc2, osh2, ar, cd);
-    else if (q == 2) h_out_tau<68, 108>(tb, wl, 8, live, hrow, osc2, osh2, ar, cd);
-    else h_out_tau<108, 140>(tb, wl, 8, live, hrow, osc2, osh2, ar, cd);
+    if (q == 0) h_out_tau<0, 38>(tb, wl, 8, live, hrow, ar, cd);
+    else if (q == 1) h_out_tau<38, 68>(tb, wl, 8, live, hrow, ar, cd);
+    else if (q == 2) h_out_tau<68, 108>(tb, wl, 8, live, hrow, ar, cd);
+    else h_out_tau<108, 140>(tb, wl, 8, live, hrow, ar, cd);
     hrow += 8 * NGPT;
-    if (q == 0) h_out_frac<0, 38>(tb, wl, 8, live, hrow, osc, osh);
-    else if (q == 1) h_out_frac<38, 68>(tb, wl, 8, live, hrow, osc, osh);
-    else if (q == 2) h_out_frac<68, 108>(tb, wl, 8, live, hrow, osc, osh);
-    else h_out_frac<108, 140>(tb, wl, 8, live, hrow, osc, osh);
+    if (q == 0) h_out_frac<0, 38>(tb, wl, 8, live, hrow);
+    else if (q == 1) h_out_frac<38, 68>(tb, wl, 8, live, hrow);
+    else if (q == 2) h_out_frac<68, 108>(tb, wl, 8, live, hrow);
+    else h_out_frac<108, 140>(tb, wl, 8, live, hrow);
     // the accumulators are free for the next tile once every thread has read them
     umma::fence_before_sync();
     __syncthreads();
@@ -999,7 +1036,7 @@ cudaError_t set_attrs() {
     return e;
   if ((e = cudaFuncSetAttribute(mlp_fwd_kernel<MODE_LW>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM)))
     return e;
-  if ((e = cudaFuncSetAttribute(mlp_h_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM))) return e;
+  if ((e = cudaFuncSetAttribute(mlp_h_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, H_SMEM))) return e;
   if ((e = cudaFuncSetAttribute(gemm_tn_kernel<EPI_ATOMIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM)))
     return e;
   if ((e = cudaFuncSetAttribute(gemm_tn_kernel<EPI_DACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM)))
@@ -1011,7 +1048,7 @@ cudaError_t set_attrs() {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], mlp_fwd_kernel<MODE_LW>, FWD_THREADS, FWD_SMEM);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], gemm_tn_kernel<EPI_ATOMIC>, 128, GEMM_SMEM);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[4], gemm_tn_kernel<EPI_DACT>, 128, GEMM_SMEM);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[5], mlp_h_kernel, FWD_THREADS, FWD_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[5], mlp_h_kernel, FWD_THREADS, H_SMEM);
   for (int o : occ)
     if (o != 1) return cudaErrorLaunchOutOfResources;
   net.attrs = true;
@@ -1186,7 +1223,7 @@ cudaError_t mlp_h_launch(const Block* blocks, int nblocks, const Block& b0, cons
   if (f.nlay > 127) return cudaErrorInvalidValue;   // one column per 128-row tile
   const int grid = std::min(nc, num_sms);
   if (grid < 1) return cudaSuccess;
-  mlp_h_kernel<<<grid, FWD_THREADS, FWD_SMEM, st>>>(a);
+  mlp_h_kernel<<<grid, FWD_THREADS, H_SMEM, st>>>(a);
   return cudaGetLastError();
 }
 
