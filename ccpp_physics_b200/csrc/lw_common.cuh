@@ -134,6 +134,28 @@ __device__ __forceinline__ int find_block(const Block* blocks, int nblocks, int 
 template <typename T>
 __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
 
+// Barrier of a group of threads: the whole CTA (gas_column in lw_gas_kernel
+// and the fallback kernel of the learned-gas-optics path), or a named
+// barrier over `n` threads of a CTA that holds several groups (that path's
+// network and transfer kernels).
+struct CtaSync {
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  __device__ __forceinline__ int count(bool p) const { return __syncthreads_count(p); }
+  __device__ __forceinline__ int any(bool p) const { return __syncthreads_or(p); }
+};
+struct GroupSync {
+  int id, n;   // named barrier id (1..15) and thread count (a multiple of 32)
+  __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+  __device__ __forceinline__ int count(bool p) const {
+    int r;
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.popc.u32 %0, %2, %3, q;\n\t}"
+                 : "=r"(r) : "r"((unsigned)p), "r"(id), "r"(n) : "memory");
+    return r;
+  }
+  __device__ __forceinline__ int any(bool p) const { return count(p) != 0; }
+};
+
+
 // Debug builds (-DLW_DEBUG_CHECKS=1) bounds-check every table, scratch,
 // input and output access of the column kernels: the first violation is
 // recorded in lw_dbg_err {site, index, block, thread} and the access is

@@ -133,27 +133,6 @@ __host__ __device__ constexpr size_t gas_smem_bytes(int V) {
   return sizeof(double) * (2 * NLP + 24 + 8 * NLP) + sizeof(R) * N_LF * NLP + sizeof(int) * (NLP + 4);
 }
 
-// Barrier of a group of threads: the whole CTA (gas_column in lw_gas_kernel
-// and the fallback kernel of the learned-gas-optics path), or a named
-// barrier over `n` threads of a CTA that holds several groups (that path's
-// transfer kernel).
-struct CtaSync {
-  __device__ __forceinline__ void sync() const { __syncthreads(); }
-  __device__ __forceinline__ int count(bool p) const { return __syncthreads_count(p); }
-  __device__ __forceinline__ int any(bool p) const { return __syncthreads_or(p); }
-};
-struct GroupSync {
-  int id, n;   // named barrier id (1..15) and thread count (a multiple of 32)
-  __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
-  __device__ __forceinline__ int count(bool p) const {
-    int r;
-    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.popc.u32 %0, %2, %3, q;\n\t}"
-                 : "=r"(r) : "r"((unsigned)p), "r"(id), "r"(n) : "memory");
-    return r;
-  }
-  __device__ __forceinline__ int any(bool p) const { return count(p) != 0; }
-};
-
 // Per-column working arrays of gas_column (shared memory in lw_gas_kernel,
 // any memory the caller's threads can reach elsewhere); gas_smem_bytes<R>(V).
 template <typename R, int V>

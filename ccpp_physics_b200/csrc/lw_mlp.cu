@@ -496,6 +496,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
 // g-point).  The hidden layers' SiLU is 0.5 z (1 + tanh(0.5 z)) with the
 // hardware tanh, one special-function operation per value.
 //
+// Two pipelines per CTA (below) each run that chain on their own columns.
 // The output layer's normalisation is folded into MMA3: each CTA builds its
 // W3 tile from the FP32 master weights with row j scaled by the output's
 // standard deviation (times log2 e for the optical depths), and three extra
@@ -503,19 +504,27 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
 // as a BF16 hi + mid + lo split against constant-one columns of H2 (K = 144).
 // The accumulator then holds log2(tau / coldry) and the fraction itself.
 constexpr int KH3 = HID + 16;                                  // K of MMA3: H2 + {1, 1, 1, 0 ...}
+// Two independent tile pipelines per CTA (warps 0-7 and 8-15): while one
+// waits for its MMAs or its barrier, the other runs its epilogues.  Each
+// pipeline owns 144 TMEM columns, its X and H tiles and its per-tile rows;
+// the weights are shared.
+constexpr int HP = 2;                                          // pipelines per CTA
+constexpr int HP_THREADS = FWD_THREADS / HP;                   // 256: two threads per tile row
 constexpr uint32_t HSM_W1 = 0;                                 // canon [128][16]
 constexpr uint32_t HSM_W2 = HSM_W1 + HID * KIN * 2;            // canon [128][128]
 constexpr uint32_t HSM_W3 = HSM_W2 + HID * HID * 2;            // canon [288][144]
-constexpr uint32_t HSM_X = HSM_W3 + NOP * KH3 * 2;             // canon [128][16]
-constexpr uint32_t HSM_H = HSM_X + 128 * KIN * 2;              // canon [128][128] (H1) / [128][144] (H2)
-constexpr uint32_t HSM_B2 = HSM_H + 128 * KH3 * 2;             // f32 [128]
+constexpr uint32_t HSM_P = HSM_W3 + NOP * KH3 * 2;             // per pipeline, HSM_PB bytes each:
+constexpr uint32_t HPO_X = 0;                                  //   canon [128][16]
+constexpr uint32_t HPO_H = HPO_X + 128 * KIN * 2;              //   canon [128][128] (H1) / [128][144] (H2)
+constexpr uint32_t HPO_AER = HPO_H + 128 * KH3 * 2;            //   f32 [16][128] aerosol tau of the tile's layers
+constexpr uint32_t HPO_CD = HPO_AER + NBANDS * 128 * 4;        //   f32 [128] coldry of the tile's layers
+constexpr uint32_t HSM_PB = HPO_CD + 128 * 4;
+constexpr uint32_t HSM_B2 = HSM_P + HP * HSM_PB;               // f32 [128]
 constexpr uint32_t HSM_NORM = HSM_B2 + HID * 4;                // f32 [16] input mean, std
-constexpr uint32_t HSM_AER = HSM_NORM + 16 * 4;                // f32 [2][16][128] aerosol tau of the tile's layers
-constexpr uint32_t HSM_CD = HSM_AER + 2 * NBANDS * 128 * 4;    // f32 [2][128] coldry of the tile's layers
-constexpr uint32_t HSM_BAR = (HSM_CD + 2 * 128 * 4 + 15) & ~15u;
-constexpr uint32_t H_SMEM = HSM_BAR + 32;
+constexpr uint32_t HSM_BAR = HSM_NORM + 16 * 4;                // per pipeline: mbarrier (8 B); TMEM base; failure flag
+constexpr uint32_t H_SMEM = HSM_BAR + 64;
 static_assert(H_SMEM > 116 * 1024 && H_SMEM <= 227 * 1024, "one CTA per SM (512 TMEM columns), within shared memory");
-static_assert(HSM_W3 % 128 == 0 && HSM_X % 128 == 0 && HSM_H % 128 == 0, "canonical tiles");
+static_assert(HSM_W3 % 128 == 0 && HSM_P % 128 == 0 && HSM_PB % 128 == 0 && HPO_H % 128 == 0, "canonical tiles");
 constexpr uint32_t W3H_HALF = 144 * KH3 * 2;                   // second 144-row B operand of MMA3
 constexpr float kLog2e = 1.4426950408889634f;
 
@@ -538,19 +547,21 @@ __device__ __forceinline__ float ex2_fast(float x) {
   return y;
 }
 
-// optical depths of g-points [GA, GB) of this thread's row, FP16 at dst[g stride]:
-// 2^acc * coldry + aerosol
+// optical depths of g-points [GA, GB) of this thread's row, FP16 at
+// dst[g stride]: 2^acc * coldry + aerosol.  Every lane runs the TMEM loads
+// (tcgen05.ld is a warp-wide instruction); padding rows store zeros.
 template <int GA, int GB>
 __device__ __forceinline__ void h_out_tau(uint32_t tb, int wl, int stride, bool live, __half* dst,
                                           const float* aer_row, float cd) {
   constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
   float v[NCH * 16];
 #pragma unroll
-  for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, 256 + C0 + 16 * c), v + 16 * c);
+  for (int c = 0; c < NCH; ++c) umma::tmem_ld16(umma::tmem_addr(tb, wl, C0 + 16 * c), v + 16 * c);
 #pragma unroll
   for (int g = GA; g < GB; ++g) {
-    const float tau = live ? fmaf(ex2_fast(v[g - C0]), cd, aer_row[band_of_g(g) * 128]) : 0.0f;
-    dst[g * stride] = __float2half_rn(fminf(tau, 6.0e4f));   // below the FP16 maximum
+    const float e = ex2_fast(v[g - C0]);   // unconditional: a select, not a branch, drops padding rows
+    const float tau = live ? fminf(fmaf(e, cd, aer_row[band_of_g(g) * 128]), 6.0e4f) : 0.0f;   // below the FP16 maximum
+    dst[g * stride] = __float2half_rn(tau);
   }
 }
 
@@ -578,14 +589,19 @@ __device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool
 
 __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  const int tid = threadIdx.x, warp = tid >> 5, wl = warp & 3, q = tid >> 7, t = tid & 127;
+  const int tid = threadIdx.x, warp = tid >> 5, wl = warp & 3;
+  const int P = warp / (HP_THREADS / 32);            // this thread's pipeline
+  const int ptid = tid - P * HP_THREADS;              // thread within the pipeline
+  const int h = (warp % (HP_THREADS / 32)) / 4;       // half of the pipeline: two threads per row
+  const int t = 32 * wl + (tid & 31);                 // tile row = layer
   float* sb2 = reinterpret_cast<float*>(sm + HSM_B2);
   float* snorm = reinterpret_cast<float*>(sm + HSM_NORM);
-  float* saer0 = reinterpret_cast<float*>(sm + HSM_AER);
-  float* scd0 = reinterpret_cast<float*>(sm + HSM_CD);
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + HSM_BAR);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + HSM_BAR + 8);
-  int* sfail = reinterpret_cast<int*>(sm + HSM_BAR + 12);
+  unsigned char* pbase = sm + HSM_P + P * HSM_PB;
+  float* saer = reinterpret_cast<float*>(pbase + HPO_AER);
+  float* scd = reinterpret_cast<float*>(pbase + HPO_CD);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + HSM_BAR) + P;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + HSM_BAR + 16);
+  int* sfail = reinterpret_cast<int*>(sm + HSM_BAR + 20);
 
   copy_rows_canon(sm + HSM_W1, a.ops + O_W1, HID, KIN, tid);
   copy_rows_canon(sm + HSM_W2, a.ops + O_W2, HID, HID, tid);
@@ -618,24 +634,28 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
     umma::tmem_relinquish();
   }
   if (tid == 0) {
-    umma::mbar_init(mbar, 1);
+    umma::mbar_init(reinterpret_cast<uint64_t*>(sm + HSM_BAR), 1);
+    umma::mbar_init(reinterpret_cast<uint64_t*>(sm + HSM_BAR) + 1, 1);
     *sfail = 0;
   }
   umma::fence_smem_async();
   umma::fence_before_sync();
   __syncthreads();
   umma::fence_after_sync();
-  const uint32_t tb = *tslot;
+  const uint32_t tb = *tslot + 256u * (uint32_t)P;     // this pipeline's TMEM columns [0, 144)
   const uint32_t sbase = umma::smem_u32(sm);
+  const uint32_t sX = umma::smem_u32(pbase + HPO_X), sH = umma::smem_u32(pbase + HPO_H);
   constexpr uint32_t ID128 = umma::idesc_bf16(128, 128), ID144 = umma::idesc_bf16(128, 144);
+  const GroupSync psync{1 + P, HP_THREADS};           // this pipeline's barrier
+  const bool issuer = ptid == 0;
   uint32_t phase = 0;
-  bool failed = false;   // uniform across the CTA
+  bool failed = false;   // uniform across the pipeline
   auto wait_mma = [&]() -> bool {
     const bool ok = umma::mbar_wait(mbar, phase, c_fwd_wait_polls);
     phase ^= 1u;
     umma::fence_after_sync();
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) *sfail = 1;
+    if (psync.any(!ok)) {
+      if (ptid == 0) atomicExch(sfail, 1);
       failed = true;
       return false;
     }
@@ -644,153 +664,153 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
   auto sync_for_mma = [&]() {
     umma::fence_smem_async();
     umma::fence_before_sync();
-    __syncthreads();
+    psync.sync();
+  };
+  auto mma3 = [&](uint32_t w3) {   // one half of the output layer into the pipeline's columns
+    if (issuer) {
+      umma::fence_after_sync();
+#pragma unroll 1
+      for (int s = 0; s < KH3 / 16; ++s)
+        umma::mma(tb, umma::tile_desc(sH, KH3, s), umma::tile_desc(sbase + HSM_W3 + w3, KH3, s), ID144,
+                  s > 0 ? 1u : 0u);
+      umma::commit(mbar);
+    }
   };
 
   const int nlay = a.f.nlay, nchk = (nlay + 7) >> 3;
   const bool live = t < nlay;
   const int r = a.f.top_at_1 ? nlay - 1 - t : t;   // input row of layer t
-  const int b0 = q == 1 ? 0 : q == 2 ? 6 : 11, b1 = q == 1 ? 6 : q == 2 ? 11 : 16;
-  // inputs of this thread's layer, loaded one column ahead: quarter 0 the
-  // eight state fields, quarters 1-3 aod/ssa of their bands
-  double pf[12];
-#pragma unroll
-  for (int j = 0; j < 12; ++j) pf[j] = 0.0;
-  auto prefetch = [&](int cc) {
-    if (cc >= a.nc || !live) return;
-    const int c = a.c0 + cc;
-    const Block* B = (a.nblocks == 1) ? &a.b0 : &a.blocks[__ldg(a.colmap + c)];
-    const size_t ld = (size_t)B->ld;
-    const size_t o = (size_t)(c - B->col0) + ld * (size_t)r;
-    if (q == 0) {
-      pf[0] = B->in[F_PLYR][o]; pf[1] = B->in[F_TLYR][o]; pf[2] = B->in[F_QLYR][o]; pf[3] = B->in[F_OLYR][o];
-      pf[4] = B->in[F_CO2][o]; pf[5] = B->in[F_CH4][o]; pf[6] = B->in[F_N2O][o]; pf[7] = B->in[F_DELPIN][o];
-    } else {
-#pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        const size_t ab = o + ld * (size_t)nlay * (size_t)min(b0 + j, b1 - 1);
-        pf[2 * j] = B->in[F_AERAOD][ab];
-        pf[2 * j + 1] = B->in[F_AERSSA][ab];
-      }
-    }
-  };
-  prefetch(blockIdx.x);
 
-  int parity = 0;   // double buffer of the per-tile aerosol / coldry rows
-  for (int cc = blockIdx.x; cc < a.nc; cc += gridDim.x, parity ^= 1) {
+  for (int cc = HP * blockIdx.x + P; cc < a.nc; cc += HP * gridDim.x) {
     const int c = a.c0 + cc;
-    float* saer = saer0 + parity * NBANDS * 128;
-    float* scd = scd0 + parity * 128;
-    // ---------------- layer inputs -> X (features), aerosol depths, coldry ----------------
-    if (q == 0) {
-      float x[KIN];
-#pragma unroll
-      for (int j = 0; j < KIN; ++j) x[j] = 0.0f;
-      if (live) {
+    // ---------------- layer inputs -> X (features) and coldry, aerosol depths ----------------
+    if (live) {
+      const Block* B = (a.nblocks == 1) ? &a.b0 : &a.blocks[__ldg(a.colmap + c)];
+      const size_t ld = (size_t)B->ld;
+      const size_t o = (size_t)(c - B->col0) + ld * (size_t)r;
+      if (h == 0) {
+        const double pavel = B->in[F_PLYR][o], tavel = B->in[F_TLYR][o], qv = B->in[F_QLYR][o];
+        const double o3 = B->in[F_OLYR][o], co2 = B->in[F_CO2][o], ch4 = B->in[F_CH4][o], n2o = B->in[F_N2O][o];
+        const double delp = B->in[F_DELPIN][o];
         const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
-        const double h2ovmr = fmax(0.0, pf[2] * amdw / (1.0 - pf[2]));
-        const double o3vmr = fmax(0.0, pf[3] * amdo3);
+        const double h2ovmr = fmax(0.0, qv * amdw / (1.0 - qv));
+        const double o3vmr = fmax(0.0, o3 * amdo3);
         const double tem0 = (1.0 - h2ovmr) * 28.9644 + h2ovmr * 18.0154;
-        scd[t] = (float)((1.0e-20 * 1.0e3 * 6.0221415e23) * pf[7] / (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr)));
+        scd[t] = (float)((1.0e-20 * 1.0e3 * 6.0221415e23) * delp / (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr)));
         float raw[NIN];
-        layer_features(pf[0], pf[1], h2ovmr, o3vmr, pf[4], pf[5], pf[6], raw);
+        layer_features(pavel, tavel, h2ovmr, o3vmr, co2, ch4, n2o, raw);
         // a layer outside the training envelope: list its column once for the fallback
         if (!in_envelope(raw, a.norm) && atomicExch(a.fb_flag + c, 1u) == 0u) a.fb_list[atomicAdd(a.fb_count, 1)] = c;
+        float x[KIN];
 #pragma unroll
         for (int j = 0; j < 7; ++j) x[j] = (raw[j] - snorm[j]) / snorm[8 + j];
         x[7] = 1.0f;
-      }
-      umma::st_canon8(sm + HSM_X, t, 0, KIN, x);
-      umma::st_canon8(sm + HSM_X, t, 8, KIN, x + 8);
-    } else if (live) {
 #pragma unroll
-      for (int j = 0; j < 6; ++j)
-        if (b0 + j < b1) saer[(b0 + j) * 128 + t] = (float)(pf[2 * j] * (1.0 - pf[2 * j + 1]));
+        for (int j = 8; j < KIN; ++j) x[j] = 0.0f;
+        umma::st_canon8(pbase + HPO_X, t, 0, KIN, x);
+        umma::st_canon8(pbase + HPO_X, t, 8, KIN, x + 8);
+      } else {
+        double aod[NBANDS], ssa[NBANDS];
+#pragma unroll
+        for (int b = 0; b < NBANDS; ++b) {   // every load first, so their latencies overlap
+          const size_t ab = o + ld * (size_t)nlay * (size_t)b;
+          aod[b] = B->in[F_AERAOD][ab];
+          ssa[b] = B->in[F_AERSSA][ab];
+        }
+#pragma unroll
+        for (int b = 0; b < NBANDS; ++b) saer[b * 128 + t] = (float)(aod[b] * (1.0 - ssa[b]));
+      }
+    } else if (h == 0) {
+      const float x[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+      umma::st_canon8(pbase + HPO_X, t, 0, KIN, x);
+      umma::st_canon8(pbase + HPO_X, t, 8, KIN, x);
     }
     sync_for_mma();
-    if (tid == 0) {
+    if (issuer) {
       umma::fence_after_sync();
-      umma::mma(tb, umma::tile_desc(sbase + HSM_X, KIN, 0), umma::tile_desc(sbase + HSM_W1, KIN, 0), ID128, 0u);
+      umma::mma(tb, umma::tile_desc(sX, KIN, 0), umma::tile_desc(sbase + HSM_W1, KIN, 0), ID128, 0u);
       umma::commit(mbar);
     }
     if (!wait_mma()) break;
 
-    // ---------------- hidden layers: quarter q owns hidden units [32q, 32q+32) ----------------
+    // ---------------- hidden layers: half h owns hidden units [64h, 64h+64) ----------------
 #pragma unroll 1
     for (int layer = 0; layer < 2; ++layer) {
-      const int dcol = layer == 0 ? 0 : 128;
       const int KH = layer == 0 ? HID : KH3;   // H1 feeds MMA2 (K = 128), H2 feeds MMA3 (K = 144)
-      float v32[32];
-      umma::tmem_ld32(umma::tmem_addr(tb, wl, dcol + 32 * q), v32);
+#pragma unroll 1
+      for (int part = 0; part < 2; ++part) {
+        const int u0 = 64 * h + 32 * part;
+        float v32[32];
+        umma::tmem_ld32(umma::tmem_addr(tb, wl, u0), v32);
 #pragma unroll
-      for (int h8 = 0; h8 < 4; ++h8) {
-        const int c0 = 32 * q + 8 * h8;
-        uint32_t w[4];
+        for (int h8 = 0; h8 < 4; ++h8) {
+          const int c0 = u0 + 8 * h8;
+          uint32_t w[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const float z0 = v32[8 * h8 + 2 * j] + (layer == 1 ? sb2[c0 + 2 * j] : 0.0f);
-          const float z1 = v32[8 * h8 + 2 * j + 1] + (layer == 1 ? sb2[c0 + 2 * j + 1] : 0.0f);
-          w[j] = silu_bf16x2(z0, z1);
+          for (int j = 0; j < 4; ++j) {
+            const float z0 = v32[8 * h8 + 2 * j] + (layer == 1 ? sb2[c0 + 2 * j] : 0.0f);
+            const float z1 = v32[8 * h8 + 2 * j + 1] + (layer == 1 ? sb2[c0 + 2 * j + 1] : 0.0f);
+            w[j] = silu_bf16x2(z0, z1);
+          }
+          *reinterpret_cast<uint4*>(pbase + HPO_H + umma::canon_off(t, c0, KH)) = make_uint4(w[0], w[1], w[2], w[3]);
         }
-        *reinterpret_cast<uint4*>(sm + HSM_H + umma::canon_off(t, c0, KH)) = make_uint4(w[0], w[1], w[2], w[3]);
       }
-      if (layer == 1 && q == 0) {
+      if (layer == 1 && h == 0) {
         // the constant-one columns of H2 that carry the output shift
         const float one[8] = {1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
         const float zero[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-        umma::st_canon8(sm + HSM_H, t, HID, KH3, one);
-        umma::st_canon8(sm + HSM_H, t, HID + 8, KH3, zero);
+        umma::st_canon8(pbase + HPO_H, t, HID, KH3, one);
+        umma::st_canon8(pbase + HPO_H, t, HID + 8, KH3, zero);
       }
       sync_for_mma();
-      if (tid == 0) {
-        umma::fence_after_sync();
-        if (layer == 0) {
+      if (layer == 0) {
+        if (issuer) {
+          umma::fence_after_sync();
 #pragma unroll 1
           for (int s = 0; s < HID / 16; ++s)
-            umma::mma(tb + 128, umma::tile_desc(sbase + HSM_H, HID, s), umma::tile_desc(sbase + HSM_W2, HID, s),
-                      ID128, s > 0 ? 1u : 0u);
-        } else {
-#pragma unroll 1
-          for (int s = 0; s < KH3 / 16; ++s)
-            umma::mma(tb + 256, umma::tile_desc(sbase + HSM_H, KH3, s), umma::tile_desc(sbase + HSM_W3, KH3, s),
-                      ID144, s > 0 ? 1u : 0u);
-#pragma unroll 1
-          for (int s = 0; s < KH3 / 16; ++s)
-            umma::mma(tb, umma::tile_desc(sbase + HSM_H, KH3, s), umma::tile_desc(sbase + HSM_W3 + W3H_HALF, KH3, s),
-                      ID144, s > 0 ? 1u : 0u);
+            umma::mma(tb, umma::tile_desc(sH, HID, s), umma::tile_desc(sbase + HSM_W2, HID, s), ID128, s > 0 ? 1u : 0u);
+          umma::commit(mbar);
         }
-        umma::commit(mbar);
+      } else {
+        mma3(0);   // optical depths: W3 rows [0, 144)
       }
       if (!wait_mma()) break;
     }
     if (failed) break;
-    // the next column's inputs load while this one's outputs are formed
-    prefetch(cc + (int)gridDim.x);
 
-    // ---------------- outputs: optical depths and fractions into the hand-off ----------------
+    // ---------------- outputs into the hand-off ----------------
     // this row's slot of g-point 0 in its 8-layer block; g-point g at [8 g]
     __half* hrow = a.hnd + ((size_t)cc * nchk + (t >> 3)) * (2 * NGPT * 8) + (t & 7);
     const float cd = live ? scd[t] : 0.0f;
     const float* ar = saer + t;
-    // quarters own whole bands: g-points [0,38), [38,68), [68,108), [108,140)
-    if (q == 0) h_out_tau<0, 38>(tb, wl, 8, live, hrow, ar, cd);
-    else if (q == 1) h_out_tau<38, 68>(tb, wl, 8, live, hrow, ar, cd);
-    else if (q == 2) h_out_tau<68, 108>(tb, wl, 8, live, hrow, ar, cd);
-    else h_out_tau<108, 140>(tb, wl, 8, live, hrow, ar, cd);
+    // the two halves of a row own whole bands: g-points [0, 68) and [68, 140), in two passes each
+    if (h == 0) {
+      h_out_tau<0, 38>(tb, wl, 8, live, hrow, ar, cd);
+      h_out_tau<38, 68>(tb, wl, 8, live, hrow, ar, cd);
+    } else {
+      h_out_tau<68, 108>(tb, wl, 8, live, hrow, ar, cd);
+      h_out_tau<108, 140>(tb, wl, 8, live, hrow, ar, cd);
+    }
+    sync_for_mma();   // the optical depths are read out of TMEM
+    mma3(W3H_HALF);   // fractions: W3 rows [144, 288)
+    if (!wait_mma()) break;
     hrow += 8 * NGPT;
-    if (q == 0) h_out_frac<0, 38>(tb, wl, 8, live, hrow);
-    else if (q == 1) h_out_frac<38, 68>(tb, wl, 8, live, hrow);
-    else if (q == 2) h_out_frac<68, 108>(tb, wl, 8, live, hrow);
-    else h_out_frac<108, 140>(tb, wl, 8, live, hrow);
-    // the accumulators are free for the next tile once every thread has read them
+    if (h == 0) {
+      h_out_frac<0, 38>(tb, wl, 8, live, hrow);
+      h_out_frac<38, 68>(tb, wl, 8, live, hrow);
+    } else {
+      h_out_frac<68, 108>(tb, wl, 8, live, hrow);
+      h_out_frac<108, 140>(tb, wl, 8, live, hrow);
+    }
+    // the accumulators and this tile's rows are free for the next tile
     umma::fence_before_sync();
-    __syncthreads();
+    psync.sync();
   }
   if (failed) umma::mbar_wait(mbar, phase ^ 1u, 1u << 20);   // one more bounded wait for the MMA in flight
   umma::fence_before_sync();
   __syncthreads();
   if (tid == 0 && *sfail && a.err) atomicCAS(a.err, 0, 1);
-  if (warp == 0) umma::tmem_dealloc(tb, 512);
+  if (warp == 0) umma::tmem_dealloc(*tslot, 512);
 }
 
 // ---------------------------------------------------------------------------
@@ -1221,7 +1241,7 @@ cudaError_t mlp_h_launch(const Block* blocks, int nblocks, const Block& b0, cons
   a.fb_list = fb_list;
   a.fb_count = fb_count;
   if (f.nlay > 127) return cudaErrorInvalidValue;   // one column per 128-row tile
-  const int grid = std::min(nc, num_sms);
+  const int grid = std::min((nc + HP - 1) / HP, num_sms);
   if (grid < 1) return cudaSuccess;
   mlp_h_kernel<<<grid, FWD_THREADS, H_SMEM, st>>>(a);
   return cudaGetLastError();

@@ -130,25 +130,6 @@ __device__ __forceinline__ int tbl_index(float x) {
   return min(NTBL, (int)(float(kTblint) * __fdividef(x, float(kBpade) + x) + 0.5f));
 }
 
-// The gas terms of one layer and g-point (RLM:3598-3614) in FP32: optical
-// depth od = secdiff * tautot; for od <= 0.06 the Pade-free forms, else the
-// rlwinit record of its index.  Returns the transmittance, 1 - transmittance,
-// the Planck weight and the record index (-1 for the small-depth forms).
-__device__ __forceinline__ void gas_terms(float od, const __half2* tab, float& tr, float& atr, float& fac, int& it) {
-  if (od <= 0.06f) {
-    atr = od - 0.5f * od * od;
-    tr = 1.0f - atr;
-    fac = float(kRec6) * od;
-    it = -1;
-  } else {
-    it = tbl_index(od);
-    const float2 e = __half22float2(tab[it]);
-    atr = e.x;
-    tr = 1.0f - e.x;
-    fac = e.y;
-  }
-}
-
 // Total-sky terms of a cloudy sub-column layer (RLM:3627-3660, clfm = 1):
 // efclrfr and {1 - exp_tbl, tfn_tbl} of odtot = odepth + odcld, where odepth
 // is tau_tbl(it) = bpade it / (10000 - it) when the gas lookup used the table
