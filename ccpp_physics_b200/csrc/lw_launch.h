@@ -67,11 +67,14 @@ cudaError_t mlp_lw_launch(const Block* blocks, int nblocks, const Block& b0, int
                           const Scratch<float>& sc, int num_sms, cudaStream_t st);
 const float* surrogate_norm();
 // network stage of the learned-gas-optics column path: the FP16 hand-off
-// [nc][nlay][{tau, frac} x 140] of chunk columns [c0, c0 + nc) and the list
-// of its columns with a layer outside the training envelope (lw_mlp.cu)
+// [nc][nlay/8][{tau, frac} x 140][8 layers] of chunk columns [c0, c0 + nc)
+// and the list of its columns with a layer outside the training envelope
+// (lw_mlp.cu); `pack` holds kSgPackBytes per chunk column for the packed
+// network inputs (two launches: input packing, network)
+constexpr size_t kSgPackBytes = 6656;
 cudaError_t mlp_h_launch(const Block* blocks, int nblocks, const Block& b0, const int* colmap, int c0, int nc,
-                         const Flags& f, __half* hnd, unsigned int* fb_flag, int* fb_list, int* fb_count, int num_sms,
-                         cudaStream_t st);
+                         const Flags& f, __half* hnd, unsigned int* fb_flag, int* fb_list, int* fb_count,
+                         unsigned char* pack, int num_sms, cudaStream_t st);
 // the learned-gas-optics column path (lw_sg_path.cu): network, fallback for
 // out-of-envelope layers and the g-point-per-lane transfer, per chunk of
 // columns; used for McICA calls of up to 127 layers without hlwb.  Work-area

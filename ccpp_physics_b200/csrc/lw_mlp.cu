@@ -104,6 +104,7 @@ struct FwdArgs {
   unsigned int* fb_flag;   // per global column: set once the column is listed
   int* fb_list;         // columns of the chunk with a layer outside the envelope
   int* fb_count;
+  unsigned char* pk;    // [nc] packed column inputs, kSgPackBytes each (mlp_h_pack_kernel)
 };
 
 // Thread layout: 4 warpgroups.  Thread tid serves tile row (tid & 127) -- the
@@ -494,7 +495,9 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
 // straight into the column's hand-off [nlay/8][tau 140 | frac 140][8 layers]
 // (a warp's 32 rows cover four 8-layer blocks, 16 contiguous bytes each per
 // g-point).  The hidden layers' SiLU is 0.5 z (1 + tanh(0.5 z)) with the
-// hardware tanh, one special-function operation per value.
+// packed FP16 hardware tanh, one special-function operation per two values;
+// H1, H2, W2 and W3 are FP16 operands (W2 the trained BF16 weights, exact in
+// FP16), the features and W1 BF16.
 //
 // Two pipelines per CTA (below) each run that chain on their own columns.
 // The output layer's normalisation is folded into MMA3: each CTA builds its
@@ -503,7 +506,11 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_fwd_kernel(FwdArgs a) {
 // K columns that carry the output's shift (b3 std + mean, the same scaling)
 // as a BF16 hi + mid + lo split against constant-one columns of H2 (K = 144).
 // The accumulator then holds log2(tau / coldry) and the fraction itself.
-constexpr int KH3 = HID + 16;                                  // K of MMA3: H2 + {1, 1, 1, 0 ...}
+// The second layer's bias rides on MMA2 the same way (three extra K columns
+// of W2 against the constant-one columns of H1), so the hidden epilogues
+// read no bias.  The constant columns [128, 144) of the H tile are written
+// once: the SiLU epilogues only write columns [0, 128).
+constexpr int KH3 = HID + 16;                                  // K of MMA2 and MMA3: H + {1, 1, 1, 0 ...}
 // Two independent tile pipelines per CTA (warps 0-7 and 8-15): while one
 // waits for its MMAs or its barrier, the other runs its epilogues.  Each
 // pipeline owns 144 TMEM columns, its X and H tiles and its per-tile rows;
@@ -511,16 +518,15 @@ constexpr int KH3 = HID + 16;                                  // K of MMA3: H2 
 constexpr int HP = 2;                                          // pipelines per CTA
 constexpr int HP_THREADS = FWD_THREADS / HP;                   // 256: two threads per tile row
 constexpr uint32_t HSM_W1 = 0;                                 // canon [128][16]
-constexpr uint32_t HSM_W2 = HSM_W1 + HID * KIN * 2;            // canon [128][128]
-constexpr uint32_t HSM_W3 = HSM_W2 + HID * HID * 2;            // canon [288][144]
+constexpr uint32_t HSM_W2 = HSM_W1 + HID * KIN * 2;            // canon [128][144]
+constexpr uint32_t HSM_W3 = HSM_W2 + HID * KH3 * 2;            // canon [288][144]
 constexpr uint32_t HSM_P = HSM_W3 + NOP * KH3 * 2;             // per pipeline, HSM_PB bytes each:
 constexpr uint32_t HPO_X = 0;                                  //   canon [128][16]
-constexpr uint32_t HPO_H = HPO_X + 128 * KIN * 2;              //   canon [128][128] (H1) / [128][144] (H2)
-constexpr uint32_t HPO_AER = HPO_H + 128 * KH3 * 2;            //   f32 [16][128] aerosol tau of the tile's layers
-constexpr uint32_t HPO_CD = HPO_AER + NBANDS * 128 * 4;        //   f32 [128] coldry of the tile's layers
+constexpr uint32_t HPO_H = HPO_X + 128 * KIN * 2;              //   canon [128][144]: H1 / H2 + {1, 1, 1, 0 ...}
+constexpr uint32_t HPO_AER = HPO_H + 128 * KH3 * 2;            //   f16 [16][128] aerosol tau of the tile's layers
+constexpr uint32_t HPO_CD = HPO_AER + NBANDS * 128 * 2;        //   f32 [128] coldry of the tile's layers
 constexpr uint32_t HSM_PB = HPO_CD + 128 * 4;
-constexpr uint32_t HSM_B2 = HSM_P + HP * HSM_PB;               // f32 [128]
-constexpr uint32_t HSM_NORM = HSM_B2 + HID * 4;                // f32 [16] input mean, std
+constexpr uint32_t HSM_NORM = HSM_P + HP * HSM_PB;             // f32 [16] input mean, 1 / std
 constexpr uint32_t HSM_BAR = HSM_NORM + 16 * 4;                // per pipeline: mbarrier (8 B); TMEM base; failure flag
 constexpr uint32_t H_SMEM = HSM_BAR + 64;
 static_assert(H_SMEM > 116 * 1024 && H_SMEM <= 227 * 1024, "one CTA per SM (512 TMEM columns), within shared memory");
@@ -528,17 +534,18 @@ static_assert(HSM_W3 % 128 == 0 && HSM_P % 128 == 0 && HSM_PB % 128 == 0 && HPO_
 constexpr uint32_t W3H_HALF = 144 * KH3 * 2;                   // second 144-row B operand of MMA3
 constexpr float kLog2e = 1.4426950408889634f;
 
-// SiLU of a pair, rounded to a BF16 pair: z sigmoid(z) = 0.5 z (1 + tanh(0.5 z))
-// in FP32 with the hardware tanh (relative error ~2^-11, below the BF16
-// rounding that follows)
-__device__ __forceinline__ float tanh_fast(float x) {
-  float y;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ uint32_t silu_bf16x2(float z0, float z1) {
-  const float h0 = 0.5f * z0, h1 = 0.5f * z1;
-  const __nv_bfloat162 r = __floats2bfloat162_rn(fmaf(h0, tanh_fast(h0), h0), fmaf(h1, tanh_fast(h1), h1));
+// SiLU of a pair, z sigmoid(z) = 0.5 z (1 + tanh(0.5 z)), in FP16 arithmetic:
+// the pair rounded to FP16 (the operand type of MMA2 and MMA3 here), then
+// h + h tanh(h) with h = z / 2 (exact), the packed hardware tanh (relative
+// error ~2^-11, as the FP32 one) and one packed FMA.  FP16 keeps three more
+// mantissa bits than the BF16 the network was trained with; BF16 pair
+// arithmetic here raised the flux RMSE from 0.097 to 0.40 W/m2.
+__device__ __forceinline__ uint32_t silu_f16x2(float z0, float z1) {
+  const __half2 hz = __hmul2(__floats2half2_rn(z0, z1), __float2half2_rn(0.5f));
+  const uint32_t hb = *reinterpret_cast<const uint32_t*>(&hz);
+  uint32_t tb;
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(tb) : "r"(hb));
+  const __half2 r = __hfma2(hz, *reinterpret_cast<const __half2*>(&tb), hz);
   return *reinterpret_cast<const uint32_t*>(&r);
 }
 __device__ __forceinline__ float ex2_fast(float x) {
@@ -547,12 +554,27 @@ __device__ __forceinline__ float ex2_fast(float x) {
   return y;
 }
 
+// FP16 values of g-points g and g + 1 of this row and of the neighbouring
+// row (lane ^ 1) as one 4-byte store each: the even row stores g-point g of
+// rows (t, t + 1), the odd row g-point g + 1 of rows (t - 1, t).  dst_g is
+// this row's slot of g-point g; a g-point's rows are adjacent in the hand-off.
+// Every lane takes part in the exchange; rows past the column's last 8-layer
+// block (store false, both rows of a pair alike) store nothing.
+__device__ __forceinline__ void st_pair(__half* dst_g, int stride, bool odd, bool store, float v0, float v1) {
+  const __half2 w = __floats2half2_rn(v0, v1);
+  const uint32_t W = *reinterpret_cast<const uint32_t*>(&w);
+  const uint32_t X = __shfl_xor_sync(0xffffffffu, W, 1);
+  if (store) *reinterpret_cast<uint32_t*>(odd ? dst_g + stride - 1 : dst_g) = __byte_perm(W, X, odd ? 0x3276u : 0x5410u);
+}
+
 // optical depths of g-points [GA, GB) of this thread's row, FP16 at
 // dst[g stride]: 2^acc * coldry + aerosol.  Every lane runs the TMEM loads
-// (tcgen05.ld is a warp-wide instruction); padding rows store zeros.
+// (tcgen05.ld is a warp-wide instruction) and the pair exchanges; padding
+// rows inside the column's last 8-layer block store zeros.
 template <int GA, int GB>
-__device__ __forceinline__ void h_out_tau(uint32_t tb, int wl, int stride, bool live, __half* dst,
-                                          const float* aer_row, float cd) {
+__device__ __forceinline__ void h_out_tau(uint32_t tb, int wl, int stride, bool live, bool odd, bool store, __half* dst,
+                                          const __half* aer_row, float cd) {
+  static_assert((GB - GA) % 2 == 0, "g-point pairs");
   constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
   float v[NCH * 16];
 #pragma unroll
@@ -560,14 +582,18 @@ __device__ __forceinline__ void h_out_tau(uint32_t tb, int wl, int stride, bool 
 #pragma unroll
   for (int g = GA; g < GB; ++g) {
     const float e = ex2_fast(v[g - C0]);   // unconditional: a select, not a branch, drops padding rows
-    const float tau = live ? fminf(fmaf(e, cd, aer_row[band_of_g(g) * 128]), 6.0e4f) : 0.0f;   // below the FP16 maximum
-    dst[g * stride] = __float2half_rn(tau);
+    v[g - C0] = live ? fminf(fmaf(e, cd, __half2float(aer_row[band_of_g(g) * 128])), 6.0e4f)
+                     : 0.0f;   // below the FP16 maximum
   }
+#pragma unroll
+  for (int g = GA; g < GB; g += 2) st_pair(dst + g * stride, stride, odd, store, v[g - C0], v[g + 1 - C0]);
 }
 
 // band-normalised Planck fractions of g-points [GA, GB) (whole bands), FP16 at dst[g stride]
 template <int GA, int GB>
-__device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool live, __half* dst) {
+__device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool live, bool odd, bool store,
+                                           __half* dst) {
+  static_assert((GB - GA) % 2 == 0, "g-point pairs");
   constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
   float v[NCH * 16];
 #pragma unroll
@@ -582,9 +608,107 @@ __device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool
     bsum[band_of_g(g)] += fr;
   }
 #pragma unroll
-  for (int b = 0; b < NBANDS; ++b) bsum[b] = bsum[b] > 0.0f ? 1.0f / bsum[b] : 1.0f;
+  for (int b = 0; b < NBANDS; ++b) bsum[b] = bsum[b] > 0.0f ? __fdividef(1.0f, bsum[b]) : 1.0f;   // FP16 results
 #pragma unroll
-  for (int g = GA; g < GB; ++g) dst[g * stride] = __float2half_rn(live ? v[g - C0] * bsum[band_of_g(g)] : 0.0f);
+  for (int g = GA; g < GB; g += 2)
+    st_pair(dst + g * stride, stride, odd, store, live ? v[g - C0] * bsum[band_of_g(g)] : 0.0f,
+            live ? v[g + 1 - C0] * bsum[band_of_g(g + 1)] : 0.0f);
+}
+
+// Per-column network inputs of the column path, packed by mlp_h_pack_kernel
+// into the work area (kSgPackBytes per chunk column):
+//   [128 rows][8] BF16  the normalised features x0..x6 and the constant 1
+//                       (padding rows zero): the first 8 columns of the X tile
+//   [128] FP32          coldry (RLM:823-836)
+//   [16 bands][128] FP16 aerosol optical depth aod (1 - ssa) (RLM:1000-1012)
+// The inputs lie column-fastest ((ldim, nlay) arrays), so the network's
+// one-column tiles read them at a stride of a whole layer row; the pack
+// kernel reads them four columns at a time (one 32-byte sector per layer and
+// field), stages four records in shared memory and writes them contiguously,
+// and the network then reads a column's 6.5 KB record with coalesced
+// 16-byte loads.  The same kernel runs the envelope test and lists the
+// columns that need the fallback.
+constexpr uint32_t PK_X = 0, PK_CD = 128 * 16, PK_AER = PK_CD + 128 * 4;
+static_assert(PK_AER + NBANDS * 128 * 2 == kSgPackBytes, "packed column record");
+constexpr int PK_COLS = 4, PK_THREADS = 256;   // 4 columns x 64 layers per step
+
+__global__ void __launch_bounds__(PK_THREADS, 2) mlp_h_pack_kernel(FwdArgs a) {
+  __shared__ __align__(16) unsigned char st[PK_COLS * kSgPackBytes];
+  __shared__ float snorm[16];   // input mean, 1 / std
+  if (threadIdx.x < 16)
+    snorm[threadIdx.x] = threadIdx.x < 8 ? a.norm[SG_IN_MEAN + threadIdx.x] : 1.0f / a.norm[SG_IN_STD + threadIdx.x - 8];
+  __syncthreads();
+  const int j = threadIdx.x & (PK_COLS - 1), tl = threadIdx.x / PK_COLS;
+  const int nlay = a.f.nlay;
+  const bool top = a.f.top_at_1 != 0;
+  unsigned char* rec = st + j * kSgPackBytes;
+  for (int cb = blockIdx.x * PK_COLS; cb < a.nc; cb += gridDim.x * PK_COLS) {
+    const int cc = cb + j;
+    const int c = a.c0 + cc;
+    const bool colok = cc < a.nc;
+    // the column's block: its field pointers straight from the kernel
+    // arguments (one block) or from the block table
+    const int bi = (a.nblocks == 1 || !colok) ? 0 : __ldg(a.colmap + c);
+    auto fld = [&](int k) -> const double* { return a.nblocks == 1 ? a.b0.in[k] : a.blocks[bi].in[k]; };
+    const size_t ld = (size_t)(a.nblocks == 1 ? a.b0.ld : a.blocks[bi].ld);
+    const int col0 = a.nblocks == 1 ? a.b0.col0 : a.blocks[bi].col0;
+#pragma unroll 1
+    for (int t = tl; t < 128; t += PK_THREADS / PK_COLS) {
+      float x[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+      float cd = 0.0f;
+      __half2 aer[NBANDS / 2];
+#pragma unroll
+      for (int b = 0; b < NBANDS / 2; ++b) aer[b] = __floats2half2_rn(0.0f, 0.0f);
+      if (colok && t < nlay) {
+        const size_t o = (size_t)(c - col0) + ld * (size_t)(top ? nlay - 1 - t : t);
+        const double pavel = fld(F_PLYR)[o], tavel = fld(F_TLYR)[o], qv = fld(F_QLYR)[o];
+        const double o3 = fld(F_OLYR)[o], co2 = fld(F_CO2)[o], ch4 = fld(F_CH4)[o], n2o = fld(F_N2O)[o];
+        const double delp = fld(F_DELPIN)[o];
+        const double* paod = fld(F_AERAOD);
+        const double* pssa = fld(F_AERSSA);
+        double aod[NBANDS], ssa[NBANDS];
+#pragma unroll
+        for (int b = 0; b < NBANDS; ++b) {   // every load first, so their latencies overlap
+          const size_t ab = o + ld * (size_t)nlay * (size_t)b;
+          aod[b] = paod[ab];
+          ssa[b] = pssa[ab];
+        }
+        const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
+        const double h2ovmr = fmax(0.0, qv * amdw / (1.0 - qv));
+        const double o3vmr = fmax(0.0, o3 * amdo3);
+        const double tem0 = (1.0 - h2ovmr) * 28.9644 + h2ovmr * 18.0154;
+        cd = (float)((1.0e-20 * 1.0e3 * 6.0221415e23) * delp / (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr)));
+        float raw[NIN];
+        layer_features(pavel, tavel, h2ovmr, o3vmr, co2, ch4, n2o, raw);
+        // a layer outside the training envelope: list its column once for the fallback
+        if (!in_envelope(raw, a.norm) && atomicExch(a.fb_flag + c, 1u) == 0u) a.fb_list[atomicAdd(a.fb_count, 1)] = c;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) x[k] = (raw[k] - snorm[k]) * snorm[8 + k];
+        x[7] = 1.0f;
+#pragma unroll
+        for (int b = 0; b < NBANDS / 2; ++b)
+          aer[b] = __floats2half2_rn((float)(aod[2 * b] * (1.0 - ssa[2 * b])), (float)(aod[2 * b + 1] * (1.0 - ssa[2 * b + 1])));
+      }
+      __nv_bfloat162 xb[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) xb[k] = __floats2bfloat162_rn(x[2 * k], x[2 * k + 1]);
+      *reinterpret_cast<uint4*>(rec + PK_X + 16 * t) = *reinterpret_cast<const uint4*>(xb);
+      *reinterpret_cast<float*>(rec + PK_CD + 4 * t) = cd;
+      __half* ra = reinterpret_cast<__half*>(rec + PK_AER) + t;
+#pragma unroll
+      for (int b = 0; b < NBANDS / 2; ++b) {
+        ra[(2 * b) * 128] = __low2half(aer[b]);
+        ra[(2 * b + 1) * 128] = __high2half(aer[b]);
+      }
+    }
+    __syncthreads();
+    // the records of chunk columns [cb, cb + n) are contiguous in the work area
+    const int n = min(PK_COLS, a.nc - cb);
+    const uint4* src = reinterpret_cast<const uint4*>(st);
+    uint4* dst = reinterpret_cast<uint4*>(a.pk + (size_t)cb * kSgPackBytes);
+    for (int q = threadIdx.x; q < n * (int)(kSgPackBytes / 16); q += PK_THREADS) dst[q] = src[q];
+    __syncthreads();
+  }
 }
 
 __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
@@ -594,17 +718,40 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
   const int ptid = tid - P * HP_THREADS;              // thread within the pipeline
   const int h = (warp % (HP_THREADS / 32)) / 4;       // half of the pipeline: two threads per row
   const int t = 32 * wl + (tid & 31);                 // tile row = layer
-  float* sb2 = reinterpret_cast<float*>(sm + HSM_B2);
   float* snorm = reinterpret_cast<float*>(sm + HSM_NORM);
   unsigned char* pbase = sm + HSM_P + P * HSM_PB;
-  float* saer = reinterpret_cast<float*>(pbase + HPO_AER);
+  __half* saer = reinterpret_cast<__half*>(pbase + HPO_AER);
   float* scd = reinterpret_cast<float*>(pbase + HPO_CD);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + HSM_BAR) + P;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + HSM_BAR + 16);
   int* sfail = reinterpret_cast<int*>(sm + HSM_BAR + 20);
 
   copy_rows_canon(sm + HSM_W1, a.ops + O_W1, HID, KIN, tid);
-  copy_rows_canon(sm + HSM_W2, a.ops + O_W2, HID, HID, tid);
+  // W2 in FP16: the trained BF16 weights (exact in FP16 down to 2^-14), the
+  // bias as three FP16 terms in columns 128..130
+  for (int ch = tid; ch < HID * (KH3 / 8); ch += FWD_THREADS) {
+    const int j = ch / (KH3 / 8), k = (ch % (KH3 / 8)) * 8;
+    float w[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    if (k < HID) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) w[u] = __bfloat162float(a.ops[O_W2 + (size_t)j * HID + k + u]);
+    } else if (k == HID) {
+      const float b = a.params[P_B2 + j];
+      w[0] = __half2float(__float2half_rn(b));
+      w[1] = __half2float(__float2half_rn(b - w[0]));
+      w[2] = b - w[0] - w[1];
+    }
+    umma::st_canon8_h(sm + HSM_W2, j, k, KH3, w);
+  }
+  // the constant columns of both pipelines' H tiles, and the zero columns 8..15 of their X tiles
+  for (int r = tid; r < HP * 128; r += FWD_THREADS) {
+    const float one[8] = {1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    const float zero[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    unsigned char* pt = sm + HSM_P + (r >> 7) * HSM_PB;
+    umma::st_canon8_h(pt + HPO_H, r & 127, HID, KH3, one);
+    umma::st_canon8_h(pt + HPO_H, r & 127, HID + 8, KH3, zero);
+    umma::st_canon8(pt + HPO_X, r & 127, 8, KIN, zero);
+  }
   // W3 with the output normalisation folded in (rows scaled, the shift as
   // three BF16 terms in columns 128..130), from the FP32 master weights
   for (int ch = tid; ch < NOP * (KH3 / 8); ch += FWD_THREADS) {
@@ -618,17 +765,16 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
       for (int u = 0; u < 8; ++u) w[u] = pad ? 0.0f : a.params[P_W3 + j * HID + k + u] * scale;
     } else {
       const float sh = fmaf(a.params[P_B3 + j], sd, a.norm[SG_OUT_MEAN + j]) * (j < 144 ? kLog2e : 1.0f);
-      const float hi = pad ? 0.0f : __bfloat162float(__float2bfloat16_rn(sh));
-      const float mid = pad ? 0.0f : __bfloat162float(__float2bfloat16_rn(sh - hi));
+      const float hi = pad ? 0.0f : __half2float(__float2half_rn(sh));
+      const float mid = pad ? 0.0f : __half2float(__float2half_rn(sh - hi));
       const float lo = pad ? 0.0f : sh - hi - mid;
 #pragma unroll
       for (int u = 0; u < 8; ++u) w[u] = 0.0f;
       if (k == HID) { w[0] = hi; w[1] = mid; w[2] = lo; }
     }
-    umma::st_canon8(sm + HSM_W3, j, k, KH3, w);
+    umma::st_canon8_h(sm + HSM_W3, j, k, KH3, w);
   }
-  for (int j = tid; j < HID; j += FWD_THREADS) sb2[j] = a.params[P_B2 + j];
-  if (tid < 16) snorm[tid] = a.norm[tid < 8 ? SG_IN_MEAN + tid : SG_IN_STD + tid - 8];
+  if (tid < 16) snorm[tid] = tid < 8 ? a.norm[SG_IN_MEAN + tid] : 1.0f / a.norm[SG_IN_STD + tid - 8];
   if (warp == 0) {
     umma::tmem_alloc(tslot, 512);
     umma::tmem_relinquish();
@@ -645,7 +791,9 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
   const uint32_t tb = *tslot + 256u * (uint32_t)P;     // this pipeline's TMEM columns [0, 144)
   const uint32_t sbase = umma::smem_u32(sm);
   const uint32_t sX = umma::smem_u32(pbase + HPO_X), sH = umma::smem_u32(pbase + HPO_H);
-  constexpr uint32_t ID128 = umma::idesc_bf16(128, 128), ID144 = umma::idesc_bf16(128, 144);
+  // MMA1: BF16 features and W1; MMA2, MMA3: FP16 hidden activations and weights
+  constexpr uint32_t ID1 = umma::idesc_bf16(128, 128), ID128 = umma::idesc_f16(128, 128),
+                     ID144 = umma::idesc_f16(128, 144);
   const GroupSync psync{1 + P, HP_THREADS};           // this pipeline's barrier
   const bool issuer = ptid == 0;
   uint32_t phase = 0;
@@ -678,57 +826,29 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
   };
 
   const int nlay = a.f.nlay, nchk = (nlay + 7) >> 3;
-  const bool live = t < nlay;
-  const int r = a.f.top_at_1 ? nlay - 1 - t : t;   // input row of layer t
+  const bool live = t < nlay, odd = t & 1;
+  const bool inblk = t < 8 * nchk;   // the row lies in one of the column's 8-layer hand-off blocks
 
   for (int cc = HP * blockIdx.x + P; cc < a.nc; cc += HP * gridDim.x) {
-    const int c = a.c0 + cc;
-    // ---------------- layer inputs -> X (features) and coldry, aerosol depths ----------------
-    if (live) {
-      const Block* B = (a.nblocks == 1) ? &a.b0 : &a.blocks[__ldg(a.colmap + c)];
-      const size_t ld = (size_t)B->ld;
-      const size_t o = (size_t)(c - B->col0) + ld * (size_t)r;
-      if (h == 0) {
-        const double pavel = B->in[F_PLYR][o], tavel = B->in[F_TLYR][o], qv = B->in[F_QLYR][o];
-        const double o3 = B->in[F_OLYR][o], co2 = B->in[F_CO2][o], ch4 = B->in[F_CH4][o], n2o = B->in[F_N2O][o];
-        const double delp = B->in[F_DELPIN][o];
-        const double amdw = 28.9644 / 18.0154, amdo3 = 28.9644 / 47.9982;
-        const double h2ovmr = fmax(0.0, qv * amdw / (1.0 - qv));
-        const double o3vmr = fmax(0.0, o3 * amdo3);
-        const double tem0 = (1.0 - h2ovmr) * 28.9644 + h2ovmr * 18.0154;
-        scd[t] = (float)((1.0e-20 * 1.0e3 * 6.0221415e23) * delp / (100.0 * 9.80665 * tem0 * (1.0 + h2ovmr)));
-        float raw[NIN];
-        layer_features(pavel, tavel, h2ovmr, o3vmr, co2, ch4, n2o, raw);
-        // a layer outside the training envelope: list its column once for the fallback
-        if (!in_envelope(raw, a.norm) && atomicExch(a.fb_flag + c, 1u) == 0u) a.fb_list[atomicAdd(a.fb_count, 1)] = c;
-        float x[KIN];
-#pragma unroll
-        for (int j = 0; j < 7; ++j) x[j] = (raw[j] - snorm[j]) / snorm[8 + j];
-        x[7] = 1.0f;
-#pragma unroll
-        for (int j = 8; j < KIN; ++j) x[j] = 0.0f;
-        umma::st_canon8(pbase + HPO_X, t, 0, KIN, x);
-        umma::st_canon8(pbase + HPO_X, t, 8, KIN, x + 8);
-      } else {
-        double aod[NBANDS], ssa[NBANDS];
-#pragma unroll
-        for (int b = 0; b < NBANDS; ++b) {   // every load first, so their latencies overlap
-          const size_t ab = o + ld * (size_t)nlay * (size_t)b;
-          aod[b] = B->in[F_AERAOD][ab];
-          ssa[b] = B->in[F_AERSSA][ab];
-        }
-#pragma unroll
-        for (int b = 0; b < NBANDS; ++b) saer[b * 128 + t] = (float)(aod[b] * (1.0 - ssa[b]));
+    // ---------------- the column's packed inputs -> X (features), coldry, aerosol depths ----------------
+    {
+      const unsigned char* rec = a.pk + (size_t)cc * kSgPackBytes;
+      if (h == 0) {   // row t: its 8 feature columns and coldry
+        *reinterpret_cast<uint4*>(pbase + HPO_X + umma::canon_off(t, 0, KIN)) =
+            __ldg(reinterpret_cast<const uint4*>(rec + PK_X) + t);
+        scd[t] = __ldg(reinterpret_cast<const float*>(rec + PK_CD) + t);
+      } else {        // 32 bytes of the aerosol block each
+        const int q = ptid - HP_THREADS / 2;
+        const uint4* src = reinterpret_cast<const uint4*>(rec + PK_AER) + 2 * q;
+        const uint4 v0 = __ldg(src), v1 = __ldg(src + 1);
+        reinterpret_cast<uint4*>(saer)[2 * q] = v0;
+        reinterpret_cast<uint4*>(saer)[2 * q + 1] = v1;
       }
-    } else if (h == 0) {
-      const float x[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-      umma::st_canon8(pbase + HPO_X, t, 0, KIN, x);
-      umma::st_canon8(pbase + HPO_X, t, 8, KIN, x);
     }
     sync_for_mma();
     if (issuer) {
       umma::fence_after_sync();
-      umma::mma(tb, umma::tile_desc(sX, KIN, 0), umma::tile_desc(sbase + HSM_W1, KIN, 0), ID128, 0u);
+      umma::mma(tb, umma::tile_desc(sX, KIN, 0), umma::tile_desc(sbase + HSM_W1, KIN, 0), ID1, 0u);
       umma::commit(mbar);
     }
     if (!wait_mma()) break;
@@ -736,7 +856,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
     // ---------------- hidden layers: half h owns hidden units [64h, 64h+64) ----------------
 #pragma unroll 1
     for (int layer = 0; layer < 2; ++layer) {
-      const int KH = layer == 0 ? HID : KH3;   // H1 feeds MMA2 (K = 128), H2 feeds MMA3 (K = 144)
+      // H1 feeds MMA2 and H2 feeds MMA3, both with the biases against the constant columns
 #pragma unroll 1
       for (int part = 0; part < 2; ++part) {
         const int u0 = 64 * h + 32 * part;
@@ -747,28 +867,17 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
           const int c0 = u0 + 8 * h8;
           uint32_t w[4];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const float z0 = v32[8 * h8 + 2 * j] + (layer == 1 ? sb2[c0 + 2 * j] : 0.0f);
-            const float z1 = v32[8 * h8 + 2 * j + 1] + (layer == 1 ? sb2[c0 + 2 * j + 1] : 0.0f);
-            w[j] = silu_bf16x2(z0, z1);
-          }
-          *reinterpret_cast<uint4*>(pbase + HPO_H + umma::canon_off(t, c0, KH)) = make_uint4(w[0], w[1], w[2], w[3]);
+          for (int j = 0; j < 4; ++j) w[j] = silu_f16x2(v32[8 * h8 + 2 * j], v32[8 * h8 + 2 * j + 1]);
+          *reinterpret_cast<uint4*>(pbase + HPO_H + umma::canon_off(t, c0, KH3)) = make_uint4(w[0], w[1], w[2], w[3]);
         }
-      }
-      if (layer == 1 && h == 0) {
-        // the constant-one columns of H2 that carry the output shift
-        const float one[8] = {1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-        const float zero[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-        umma::st_canon8(pbase + HPO_H, t, HID, KH3, one);
-        umma::st_canon8(pbase + HPO_H, t, HID + 8, KH3, zero);
       }
       sync_for_mma();
       if (layer == 0) {
         if (issuer) {
           umma::fence_after_sync();
 #pragma unroll 1
-          for (int s = 0; s < HID / 16; ++s)
-            umma::mma(tb, umma::tile_desc(sH, HID, s), umma::tile_desc(sbase + HSM_W2, HID, s), ID128, s > 0 ? 1u : 0u);
+          for (int s = 0; s < KH3 / 16; ++s)
+            umma::mma(tb, umma::tile_desc(sH, KH3, s), umma::tile_desc(sbase + HSM_W2, KH3, s), ID128, s > 0 ? 1u : 0u);
           umma::commit(mbar);
         }
       } else {
@@ -782,25 +891,25 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
     // this row's slot of g-point 0 in its 8-layer block; g-point g at [8 g]
     __half* hrow = a.hnd + ((size_t)cc * nchk + (t >> 3)) * (2 * NGPT * 8) + (t & 7);
     const float cd = live ? scd[t] : 0.0f;
-    const float* ar = saer + t;
+    const __half* ar = saer + t;
     // the two halves of a row own whole bands: g-points [0, 68) and [68, 140), in two passes each
     if (h == 0) {
-      h_out_tau<0, 38>(tb, wl, 8, live, hrow, ar, cd);
-      h_out_tau<38, 68>(tb, wl, 8, live, hrow, ar, cd);
+      h_out_tau<0, 38>(tb, wl, 8, live, odd, inblk, hrow, ar, cd);
+      h_out_tau<38, 68>(tb, wl, 8, live, odd, inblk, hrow, ar, cd);
     } else {
-      h_out_tau<68, 108>(tb, wl, 8, live, hrow, ar, cd);
-      h_out_tau<108, 140>(tb, wl, 8, live, hrow, ar, cd);
+      h_out_tau<68, 108>(tb, wl, 8, live, odd, inblk, hrow, ar, cd);
+      h_out_tau<108, 140>(tb, wl, 8, live, odd, inblk, hrow, ar, cd);
     }
     sync_for_mma();   // the optical depths are read out of TMEM
     mma3(W3H_HALF);   // fractions: W3 rows [144, 288)
     if (!wait_mma()) break;
     hrow += 8 * NGPT;
     if (h == 0) {
-      h_out_frac<0, 38>(tb, wl, 8, live, hrow);
-      h_out_frac<38, 68>(tb, wl, 8, live, hrow);
+      h_out_frac<0, 38>(tb, wl, 8, live, odd, inblk, hrow);
+      h_out_frac<38, 68>(tb, wl, 8, live, odd, inblk, hrow);
     } else {
-      h_out_frac<68, 108>(tb, wl, 8, live, hrow);
-      h_out_frac<108, 140>(tb, wl, 8, live, hrow);
+      h_out_frac<68, 108>(tb, wl, 8, live, odd, inblk, hrow);
+      h_out_frac<108, 140>(tb, wl, 8, live, odd, inblk, hrow);
     }
     // the accumulators and this tile's rows are free for the next tile
     umma::fence_before_sync();
@@ -1225,8 +1334,8 @@ cudaError_t mlp_lw_launch(const Block* blocks, int nblocks, const Block& b0, int
 // hand-off of chunk columns [c0, c0 + nc) and the list of columns with a
 // layer outside the envelope.  Enqueue only.
 cudaError_t mlp_h_launch(const Block* blocks, int nblocks, const Block& b0, const int* colmap, int c0, int nc,
-                         const Flags& f, __half* hnd, unsigned int* fb_flag, int* fb_list, int* fb_count, int num_sms,
-                         cudaStream_t st) {
+                         const Flags& f, __half* hnd, unsigned int* fb_flag, int* fb_list, int* fb_count,
+                         unsigned char* pack, int num_sms, cudaStream_t st) {
   if (!net.ready || !net.attrs) return cudaErrorNotReady;
   FwdArgs a = base_args();
   a.blocks = blocks;
@@ -1240,9 +1349,15 @@ cudaError_t mlp_h_launch(const Block* blocks, int nblocks, const Block& b0, cons
   a.fb_flag = fb_flag;
   a.fb_list = fb_list;
   a.fb_count = fb_count;
+  a.pk = pack;
   if (f.nlay > 127) return cudaErrorInvalidValue;   // one column per 128-row tile
   const int grid = std::min((nc + HP - 1) / HP, num_sms);
   if (grid < 1) return cudaSuccess;
+  // two resident pack CTAs per SM (their registers: the 40 input loads of a layer are in flight at once)
+  const int pgrid = std::min((nc + PK_COLS - 1) / PK_COLS, 2 * num_sms);
+  mlp_h_pack_kernel<<<pgrid, PK_THREADS, 0, st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   mlp_h_kernel<<<grid, FWD_THREADS, H_SMEM, st>>>(a);
   return cudaGetLastError();
 }

@@ -2,11 +2,14 @@
 // (RRTMG_LW_SURROGATE calls with McICA clouds, up to 127 layers, no hlwb).
 //
 // Per chunk of columns, after the McICA kernel (lw_mcica.cu):
-//   mlp_fwd_kernel<MODE_H> (lw_mlp.cu)  the network: per layer the 140 gas +
-//       aerosol optical depths and band-normalised Planck fractions (taumol
+//   mlp_h_pack_kernel (lw_mlp.cu)  the network inputs of every column
+//       (normalised features, coldry, aerosol depths) as one contiguous
+//       record, and the list of the columns that have a layer outside the
+//       training envelope;
+//   mlp_h_kernel (lw_mlp.cu)  the network: per layer the 140 gas + aerosol
+//       optical depths and band-normalised Planck fractions (taumol
 //       outputs, RLM:3836-4013) in a compact FP16 hand-off
-//       hnd[column][8-layer block][{tau, frac} x 140 g-points][8 layers], and the list of the
-//       columns that have a layer outside the training envelope;
+//       hnd[column][8-layer block][{tau, frac} x 140 g-points][8 layers];
 //   lw_sg_fallback_kernel  plain FP32 setcoef + taumol (lw_gas.cuh) for the
 //       layers of the listed columns that lie outside the envelope, written
 //       over the network's values in the hand-off;
@@ -658,10 +661,10 @@ __global__ void lw_colmap_kernel(const Block* blocks, int nblocks, int* colmap) 
 bool s_prepared = false;
 
 // Work area layout (bytes, each part 256-aligned): colmap [ncols] int,
-// flags [ncols] u32, count, list [chunk] int, fallback slots, hand-off
-// [chunk][nlay/8][280][8] half.
+// flags [ncols] u32, count, list [chunk] int, fallback slots, packed network
+// inputs [chunk] x kSgPackBytes, hand-off [chunk][nlay/8][280][8] half.
 struct SgLayout {
-  size_t colmap, flag, count, list, fb, hnd, total;
+  size_t colmap, flag, count, list, fb, pk, hnd, total;
   long chunk;
 };
 size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -671,7 +674,7 @@ SgLayout layout(int ncols, int nlay, int num_sms, size_t budget) {
   L.flag = L.colmap + al((size_t)ncols * sizeof(int));
   L.count = L.flag + al((size_t)ncols * sizeof(unsigned));
   L.list = L.count + 256;
-  const size_t per_col = (size_t)((nlay + SR_CH - 1) / SR_CH) * SR_HCH * sizeof(__half);
+  const size_t per_col = (size_t)((nlay + SR_CH - 1) / SR_CH) * SR_HCH * sizeof(__half) + kSgPackBytes;
   const size_t fb_bytes = al((size_t)FB_GRID * FB_SLOT_BYTES);
   const size_t fixed = L.list + al((size_t)ncols * sizeof(int)) + fb_bytes;
   long chunk = (long)ncols;
@@ -680,8 +683,9 @@ SgLayout layout(int ncols, int nlay, int num_sms, size_t budget) {
   if (chunk < 1) chunk = 1;
   L.chunk = chunk;
   L.fb = L.list + al((size_t)chunk * sizeof(int));
-  L.hnd = L.fb + fb_bytes;
-  L.total = L.hnd + al((size_t)chunk * per_col);
+  L.pk = L.fb + fb_bytes;
+  L.hnd = L.pk + al((size_t)chunk * kSgPackBytes);
+  L.total = L.hnd + al((size_t)chunk * (per_col - kSgPackBytes));
   return L;
 }
 
@@ -698,7 +702,7 @@ size_t sg_path_bytes(int ncols, int nlay, int num_sms, size_t budget) {
 int sg_path_launches(int ncols, int nlay, int num_sms, size_t budget, int nblocks) {
   const SgLayout L = layout(ncols, nlay, num_sms, budget);
   const int nchunks = (int)((ncols + L.chunk - 1) / L.chunk);
-  return (nblocks > 1 ? 1 : 0) + 3 * nchunks;
+  return (nblocks > 1 ? 1 : 0) + 4 * nchunks;
 }
 
 cudaError_t sg_path_prepare() {
@@ -728,6 +732,7 @@ cudaError_t sg_path_launch(const Block* blocks, int nblocks, const Block& b0, in
   int* count = reinterpret_cast<int*>(base + L.count);
   int* list = reinterpret_cast<int*>(base + L.list);
   unsigned char* fbs = base + L.fb;
+  unsigned char* pk = base + L.pk;
   __half* hnd = reinterpret_cast<__half*>(base + L.hnd);
   cudaError_t e;
   if (nblocks > 1) {
@@ -738,7 +743,7 @@ cudaError_t sg_path_launch(const Block* blocks, int nblocks, const Block& b0, in
   for (long c0 = 0; c0 < ncols; c0 += L.chunk) {
     const int nc = (int)std::min<long>(L.chunk, ncols - c0);
     if ((e = cudaMemsetAsync(count, 0, sizeof(int), st)) != cudaSuccess) return e;
-    if ((e = mlp_h_launch(blocks, nblocks, b0, colmap, (int)c0, nc, f, hnd, flag, list, count, num_sms, st)) !=
+    if ((e = mlp_h_launch(blocks, nblocks, b0, colmap, (int)c0, nc, f, hnd, flag, list, count, pk, num_sms, st)) !=
         cudaSuccess)
       return e;
     FbArgs fa;

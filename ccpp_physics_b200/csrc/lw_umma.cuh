@@ -21,6 +21,7 @@
 
 #include <cstdint>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 namespace lw {
 namespace umma {
@@ -51,6 +52,10 @@ __device__ __forceinline__ uint64_t tile_desc(uint32_t saddr, int K, int s) {
 // instruction descriptor: kind::f16, A = B = BF16, D = F32, both K-major
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+// instruction descriptor: kind::f16, A = B = FP16, D = F32, both K-major
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
+  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {   // whole warp
@@ -185,6 +190,13 @@ __device__ __forceinline__ void st_canon8(unsigned char* tile, int r, int k, int
   __nv_bfloat162 p[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) p[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+  *reinterpret_cast<uint4*>(tile + canon_off(r, k, K)) = *reinterpret_cast<uint4*>(p);
+}
+// the same with FP16 elements
+__device__ __forceinline__ void st_canon8_h(unsigned char* tile, int r, int k, int K, const float* v) {
+  __half2 p[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) p[j] = __floats2half2_rn(v[2 * j], v[2 * j + 1]);
   *reinterpret_cast<uint4*>(tile + canon_off(r, k, K)) = *reinterpret_cast<uint4*>(p);
 }
 

@@ -115,6 +115,29 @@ def test_surrogate_path_meets_accuracy_bounds(sg, trained):
     assert torch.equal(s["cldtau"], r["cldtau"]) or _rmse(s["cldtau"], r["cldtau"]) < 1e-5
 
 
+@pytest.mark.parametrize("nlay", [64, 100])
+def test_surrogate_path_short_columns(sg, trained, nlay):
+    """Columns of fewer layers than the network's 128-row tile: the padding
+    rows past a column's last 8-layer hand-off block must write nothing (the
+    next column's hand-off follows), so two runs agree bit for bit and every
+    column stays close to the FP64 path (a column whose hand-off was
+    overwritten is off by tens of W/m2)."""
+    import torch
+    from ccpp_physics_b200 import rrtmg_lw as lw
+    n = 2048
+    prof = lw.to_device(synthetic.make_profiles(n, nlay, seed=5))
+    s1 = _run(lw, prof, "surrogate", n, nlay)
+    s2 = _run(lw, prof, "surrogate", n, nlay)
+    r = _run(lw, prof, "fp64", n, nlay)
+    for k in ("topflx", "sfcflx", "hlwc"):
+        assert torch.equal(s1[k], s2[k]), k
+    flux = torch.cat([s1["topflx"], s1["sfcflx"]], 1) - torch.cat([r["topflx"], r["sfcflx"]], 1)
+    assert bool(torch.isfinite(flux).all())
+    assert float(flux.abs().max()) <= 10.0, float(flux.abs().max())
+    assert _rmse(flux, torch.zeros_like(flux)) <= 1.0
+    assert _rmse(s1["hlwc"], r["hlwc"]) <= 0.2
+
+
 def test_out_of_envelope_layers_fall_back_to_taumol(sg, trained):
     """Doubled CO2 (the training set holds 400 ppmv) puts every layer outside
     the envelope: every layer's optical depths and Planck fractions then come
