@@ -623,25 +623,28 @@ __device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool
 //   [16 bands][128] FP16 aerosol optical depth aod (1 - ssa) (RLM:1000-1012)
 // The inputs lie column-fastest ((ldim, nlay) arrays), so the network's
 // one-column tiles read them at a stride of a whole layer row; the pack
-// kernel reads them four columns at a time (one 32-byte sector per layer and
-// field), stages four records in shared memory and writes them contiguously,
-// and the network then reads a column's 6.5 KB record with coalesced
-// 16-byte loads.  The same kernel runs the envelope test and lists the
-// columns that need the fallback.
+// kernel reads them 16 columns at a time (one whole 128-byte line per layer
+// and field), stages 16 records in shared memory and writes them
+// contiguously, and the network then reads a column's 6.5 KB record with
+// coalesced 16-byte loads.  The same kernel runs the envelope test and lists
+// the columns that need the fallback.
 constexpr uint32_t PK_X = 0, PK_CD = 128 * 16, PK_AER = PK_CD + 128 * 4;
 static_assert(PK_AER + NBANDS * 128 * 2 == kSgPackBytes, "packed column record");
-constexpr int PK_COLS = 4, PK_THREADS = 256;   // 4 columns x 64 layers per step
+constexpr int PK_COLS = 16, PK_THREADS = 256;   // 16 columns x 16 layers per step
+// staged records 16 bytes apart in shared-memory banks (the record size is a multiple of 128 bytes)
+constexpr uint32_t PK_STRIDE = kSgPackBytes + 16;
+constexpr uint32_t PK_SMEM = PK_COLS * PK_STRIDE + 64;
 
 __global__ void __launch_bounds__(PK_THREADS, 2) mlp_h_pack_kernel(FwdArgs a) {
-  __shared__ __align__(16) unsigned char st[PK_COLS * kSgPackBytes];
-  __shared__ float snorm[16];   // input mean, 1 / std
+  extern __shared__ __align__(16) unsigned char st[];   // PK_COLS records of PK_STRIDE bytes, then snorm
+  float* snorm = reinterpret_cast<float*>(st + PK_COLS * PK_STRIDE);   // input mean, 1 / std
   if (threadIdx.x < 16)
     snorm[threadIdx.x] = threadIdx.x < 8 ? a.norm[SG_IN_MEAN + threadIdx.x] : 1.0f / a.norm[SG_IN_STD + threadIdx.x - 8];
   __syncthreads();
   const int j = threadIdx.x & (PK_COLS - 1), tl = threadIdx.x / PK_COLS;
   const int nlay = a.f.nlay;
   const bool top = a.f.top_at_1 != 0;
-  unsigned char* rec = st + j * kSgPackBytes;
+  unsigned char* rec = st + j * PK_STRIDE;
   for (int cb = blockIdx.x * PK_COLS; cb < a.nc; cb += gridDim.x * PK_COLS) {
     const int cc = cb + j;
     const int c = a.c0 + cc;
@@ -704,9 +707,10 @@ __global__ void __launch_bounds__(PK_THREADS, 2) mlp_h_pack_kernel(FwdArgs a) {
     __syncthreads();
     // the records of chunk columns [cb, cb + n) are contiguous in the work area
     const int n = min(PK_COLS, a.nc - cb);
-    const uint4* src = reinterpret_cast<const uint4*>(st);
+    constexpr int Q = (int)(kSgPackBytes / 16);   // 16-byte pieces of a record
     uint4* dst = reinterpret_cast<uint4*>(a.pk + (size_t)cb * kSgPackBytes);
-    for (int q = threadIdx.x; q < n * (int)(kSgPackBytes / 16); q += PK_THREADS) dst[q] = src[q];
+    for (int q = threadIdx.x; q < n * Q; q += PK_THREADS)
+      dst[q] = *reinterpret_cast<const uint4*>(st + (q / Q) * PK_STRIDE + 16 * (q % Q));
     __syncthreads();
   }
 }
@@ -1166,6 +1170,7 @@ cudaError_t set_attrs() {
   if ((e = cudaFuncSetAttribute(mlp_fwd_kernel<MODE_LW>, cudaFuncAttributeMaxDynamicSharedMemorySize, FWD_SMEM)))
     return e;
   if ((e = cudaFuncSetAttribute(mlp_h_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, H_SMEM))) return e;
+  if ((e = cudaFuncSetAttribute(mlp_h_pack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, PK_SMEM))) return e;
   if ((e = cudaFuncSetAttribute(gemm_tn_kernel<EPI_ATOMIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM)))
     return e;
   if ((e = cudaFuncSetAttribute(gemm_tn_kernel<EPI_DACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM)))
@@ -1355,7 +1360,7 @@ cudaError_t mlp_h_launch(const Block* blocks, int nblocks, const Block& b0, cons
   if (grid < 1) return cudaSuccess;
   // two resident pack CTAs per SM (their registers: the 40 input loads of a layer are in flight at once)
   const int pgrid = std::min((nc + PK_COLS - 1) / PK_COLS, 2 * num_sms);
-  mlp_h_pack_kernel<<<pgrid, PK_THREADS, 0, st>>>(a);
+  mlp_h_pack_kernel<<<pgrid, PK_THREADS, PK_SMEM, st>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   mlp_h_kernel<<<grid, FWD_THREADS, H_SMEM, st>>>(a);

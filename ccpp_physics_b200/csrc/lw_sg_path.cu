@@ -68,10 +68,10 @@ struct SrGroup {
   union {
     struct {
       float pkv[SR_NL + 1][NBANDS];     // pklev(b, l) (prologue)
-      double red[2][SR_NL];             // coldry, colh2o per layer (prologue)
     } p;
     double fn[2][SR_NL + 1];            // net flux (total, clear sky; output)
   } u;
+  double pw[SR_WARPS][2];               // per-warp sums of coldry + colh2o and of colh2o (prologue)
   float secd[NBANDS];                   // diffusivity angle per band
   float pk0[NBANDS];                    // pklay(b, 0) (surface temperature)
   float semis;
@@ -270,6 +270,7 @@ __global__ void __launch_bounds__(SR_THREADS, 1) lw_sg_rt_kernel(SrArgs a) {
       const int rl = top ? nlay - 1 - t : t + 1;
       float pkl[NBANDS];
       bool cldk = false;
+      double colw = 0.0, colh = 0.0;   // this layer's coldry and water column
       double cf = 0.0, clwp = 0.0, relw = 0.0, ciwp = 0.0, reiw = 0.0, cda1 = 0.0, cda3 = 0.0, cda4 = 0.0;
       if (live) {
         const double delp = IN(F_DELPIN, r), q = IN(F_QLYR, r), tavel = IN(F_TLYR, r), tz = IN(F_TLVL, rl);
@@ -286,8 +287,8 @@ __global__ void __launch_bounds__(SR_THREADS, 1) lw_sg_rt_kernel(SrArgs a) {
         const double tem0 = (1.0 - h2ovmr) * kConAmd + h2ovmr * kConAmw;
         const double tem1c = 100.0 * kConG, tem2c = 1.0e-20 * 1.0e3 * kConAvgd;
         const double coldry = tem2c * delp / (tem1c * tem0 * (1.0 + h2ovmr));
-        S.u.p.red[0][t] = coldry;
-        S.u.p.red[1][t] = fmax(0.0, coldry * h2ovmr);
+        colw = coldry;
+        colh = fmax(0.0, coldry * h2ovmr);
         const int indlay = min(180, max(1, (int)(tavel - 159.0)));
         const double tlyrfr = tavel - (int)tavel;
         const int indlev = min(180, max(1, (int)(tz - 159.0)));
@@ -306,14 +307,30 @@ __global__ void __launch_bounds__(SR_THREADS, 1) lw_sg_rt_kernel(SrArgs a) {
         S.u.p.pkv[0][t] = (float)planck_int(kt64, t, min(180, max(1, (int)(tz0 - 159.0))), tz0 - (int)tz0);
         S.pk0[t] = (float)planck_int(kt64, t, min(180, max(1, (int)(stemp - 159.0))), stemp - (int)stemp);
       }
-      const int lcf1 = sync.any(live && cldk);   // also: red[] and pkv[] complete
+      // the column sums of the precipitable water (RLM:910-919) as a warp
+      // tree, then over the group's warps: the reference adds layer by layer,
+      // which kept one warp in a serial FP64 chain while the group waited
+      {
+        double s1 = colw + colh, s2 = colh;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+          s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        }
+        if (lane == 0) {
+          S.pw[gw][0] = s1;
+          S.pw[gw][1] = s2;
+        }
+      }
+      const int lcf1 = sync.any(live && cldk);   // also: pw[] and pkv[] complete
       if (t < NBANDS) {
-        // precipitable water (RLM:910-919, in the reference's order; every band's
-        // thread forms the same sum) and the diffusivity angle (RLM:1041-1050)
+        // precipitable water (every band's thread forms the same sum) and the
+        // diffusivity angle (RLM:1041-1050)
         double tem1 = 0.0, tem2 = 0.0;
-        for (int k = 0; k < nlay; ++k) {
-          tem1 = tem1 + S.u.p.red[0][k] + S.u.p.red[1][k];
-          tem2 = tem2 + S.u.p.red[1][k];
+#pragma unroll
+        for (int w = 0; w < SR_WARPS; ++w) {
+          tem1 += S.pw[w][0];
+          tem2 += S.pw[w][1];
         }
         const double amdw = kConAmd / kConAmw;
         const double tem0 = 10.0 * tem2 / (amdw * tem1 * kConG);
