@@ -32,6 +32,8 @@ __device__ __constant__ uint32_t c_pow69069[624];
 
 constexpr uint32_t kMata = 0x9908B0DFu, kUmask = 0x80000000u, kLmask = 0x7FFFFFFFu;
 constexpr uint32_t kTmaskB = 0x9D2C5680u, kTmaskC = 0xEFC60000u;
+// untempered word whose tempering is 2^32 - 1 (the only draw equal to 1)
+constexpr uint32_t kRawAllOnes = 0x12DD9BB3u;
 
 __device__ __forceinline__ uint32_t mt_word(uint32_t a, uint32_t b, uint32_t c) {
   uint32_t y = (a & kUmask) | (b & kLmask);
@@ -73,19 +75,33 @@ __device__ __forceinline__ double u32_unit(uint32_t u) {
 // (MT:341-356): words 0..226 of the block from the previous block, 227..453
 // and 454..622 from words 227 back in this block, 623 from x_{j-1}, x_j and
 // x_{j+396}; one barrier per dependency phase.
-__device__ void twist_ring(uint32_t* ring, int cap, int jp, int lane) {
+// With HIT, also returns whether this lane wrote the one word that tempers to
+// 2^32 - 1 (kRawAllOnes).
+template <bool HIT = false>
+__device__ bool twist_ring(uint32_t* ring, int cap, int jp, int lane) {
   const uint32_t* o = ring + ((jp == 0 ? cap : jp) - 624);
   uint32_t* w = ring + jp;
+  bool hit = false;
   // fully unrolled, so each phase's shared-memory loads issue together
 #pragma unroll
-  for (int t = lane; t < 227; t += 32) w[t] = mt_word(o[t], o[t + 1], o[t + 397]);
+  for (int t = lane; t < 227; t += 32) {
+    w[t] = mt_word(o[t], o[t + 1], o[t + 397]);
+    if (HIT) hit |= w[t] == kRawAllOnes;
+  }
   __syncwarp();
 #pragma unroll
-  for (int t = 227 + lane; t < 454; t += 32) w[t] = mt_word(o[t], o[t + 1], w[t - 227]);
+  for (int t = 227 + lane; t < 454; t += 32) {
+    w[t] = mt_word(o[t], o[t + 1], w[t - 227]);
+    if (HIT) hit |= w[t] == kRawAllOnes;
+  }
   __syncwarp();
 #pragma unroll
-  for (int t = 454 + lane; t < 624; t += 32) w[t] = mt_word(o[t], (t == 623) ? w[0] : o[t + 1], w[t - 227]);
+  for (int t = 454 + lane; t < 624; t += 32) {
+    w[t] = mt_word(o[t], (t == 623) ? w[0] : o[t + 1], w[t - 227]);
+    if (HIT) hit |= w[t] == kRawAllOnes;
+  }
   __syncwarp();
+  return hit;
 }
 
 struct McicaArgs {
@@ -257,8 +273,6 @@ __device__ void mcica_two_set(uint32_t* mtA, uint32_t* mtB, const long long* clr
 // holds one round's draws plus the twist history.
 constexpr int kMcicaRound = 28;
 
-// untempered word whose tempering is 2^32 - 1 (the only draw equal to 1)
-constexpr uint32_t kRawAllOnes = 0x12DD9BB3u;
 __host__ __device__ constexpr uint32_t temper_c(uint32_t y) {
   return ((((y ^ (y >> 11)) ^ (((y ^ (y >> 11)) << 7) & kTmaskB)) ^
            ((((y ^ (y >> 11)) ^ (((y ^ (y >> 11)) << 7) & kTmaskB)) << 15) & kTmaskC)) ^
@@ -408,16 +422,53 @@ lw_mcica_kernel(const Block* __restrict__ blocks, int nblocks, const Block b0, i
     // random (iovr=0) and maximum-random (iovr=1): draw n*nlay+k (RLM:1920-1941)
     long long gen = 624;       // sequence indices generated so far
     int jp = 624;              // gen mod cap
+    bool hit = false;          // warp-uniform: some generated word tempers to 2^32 - 1
     static_assert(NG % kMcicaRound == 0, "whole rounds of g-points");
     for (int n0 = 0; n0 < NG; n0 += kMcicaRound) {
       const long long need = 624 + (long long)(n0 + kMcicaRound) * nlay;
       while (gen < need) {
-        twist_ring(ring, cap, jp, lane);
+        hit |= __any_sync(0xffffffffu, twist_ring<true>(ring, cap, jp, lane));
         gen += 624;
         jp += 624;
         if (jp == cap) jp = 0;
       }
       const int n = n0 + lane;
+      if (!hit) {
+        // No draw so far is 1 (only that word tempers to 2^32 - 1), so every
+        // cdf stays below 1: a clear layer's flag (cdf >= 1, see below) is 0
+        // and the layer after it starts afresh (cdf = r * 1).  Only the
+        // cloudy layers are walked, word by word from the warp's mask of them;
+        // the flags are those of the walk below, bit for bit.
+        const int q0 = (int)((624 + (long long)n * nlay) % cap);
+        double cdf = 0.0;
+        int kprev = -2;
+        for (int w = 0; w < a.nw; ++w) {
+          const int kk = 32 * w + lane;
+          uint32_t m = __ballot_sync(0xffffffffu, kk < nlay && clr[kk] != 1.0);   // the word's cloudy layers
+          if (lane < kMcicaRound) {
+            uint32_t word = 0;
+            while (m) {
+              const int b = __ffs(m) - 1;
+              m &= m - 1;
+              const int k = 32 * w + b;
+              int q = q0 + k;
+              if (q >= cap) q -= cap;
+              const double r = u32_unit(temper(ring[q]));
+              if (k == 0 || a.iovr == 0 || kprev != k - 1) {
+                cdf = r;
+              } else {
+                const double tem1 = clr[k - 1];        // max-random walk (RLM:1949-1960)
+                cdf = (cdf > tem1) ? cdf : r * tem1;
+              }
+              if (cdf >= clr[k]) word |= 1u << b;      // RLM:2097-2103
+              kprev = k;
+            }
+            out[n * a.nw + w] = word;
+          }
+        }
+        __syncwarp();
+        continue;
+      }
       if (lane < kMcicaRound) {
         int q = (int)((624 + (long long)n * nlay) % cap);
         double cdf = 0.0;

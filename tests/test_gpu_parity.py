@@ -196,6 +196,43 @@ def test_mcica_bits_exact(gpu, orc, nlay):
             assert np.array_equal(got, ref), (iovr, i)
 
 
+def test_mcica_draw_of_one(gpu, orc):
+    """A twister draw of exactly 1 (the one word that tempers to 2^32 - 1)
+    flags even a clear layer (cdf >= 1 - 0), and under maximum-random overlap
+    it carries through the cloudy layers below and into the clear layer
+    after them.  The kernel walks only the cloudy layers while no draw of the
+    column is 1 and hands a column with such a draw to the full walk.  The
+    seeds below have a draw of 1 at draw index P (found by a search of the
+    oracle's twister), i.e. at g-point P // nlay, layer P % nlay."""
+    import torch
+    nlay = 127
+    cases = [(2944804, 2448), (2944804, 2448), (3658552, 3428), (2093810, 7220)]
+    for sd, p in cases:
+        u, _, _ = orc.mt_stream(sd, p + 1)
+        assert u[p] == 0xFFFFFFFF
+    rng = np.random.default_rng(17)
+    cldf = np.where(rng.random((nlay, 4)) < 0.3, rng.random((nlay, 4)), 0.0)
+    k0 = 2448 % nlay
+    cldf[k0 - 1:k0 + 1, 0] = 0.0                  # clear, after a clear layer
+    cldf[k0 - 1, 1] = 0.0
+    cldf[k0:k0 + 2, 1] = 0.5                      # cloudy, cloudy, then clear
+    cldf[k0 + 2, 1] = 0.0
+    cldf[3428 % nlay, 2] = 0.0
+    cldf[7220 % nlay - 1:7220 % nlay + 1, 3] = 0.0
+    seeds = np.array([c[0] for c in cases], dtype=np.int32)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    for iovr in (0, 1):
+        bits = gpu.mcica_bits(t(cldf), t(seeds), iovr=iovr).cpu().numpy().view(np.uint32)
+        for i, (sd, p) in enumerate(cases):
+            ref = orc.mcica(cldf[:, i], int(sd), iovr=iovr)                  # (nlay, 140) bool
+            assert ref[p % nlay, p // nlay]                                  # the draw of 1 flags its layer
+            got = ((bits[i][:, np.arange(nlay) >> 5] >> (np.arange(nlay) & 31)) & 1).astype(bool).T
+            assert np.array_equal(got, ref), (iovr, i)
+        if iovr == 1:
+            ref = orc.mcica(cldf[:, 1], int(cases[1][0]), iovr=1)
+            assert ref[k0 + 1, 2448 // nlay] and ref[k0 + 2, 2448 // nlay]   # carried into the clear layer
+
+
 def test_mcica_comparison_boundaries(gpu, orc):
     """The exponential overlaps compare draws with alpha and with 1 - cldf on
     the GPU as integers against exact thresholds; put those values exactly on
