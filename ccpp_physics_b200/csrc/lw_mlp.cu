@@ -833,22 +833,22 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
   const bool live = t < nlay, odd = t & 1;
   const bool inblk = t < 8 * nchk;   // the row lies in one of the column's 8-layer hand-off blocks
 
-  for (int cc = HP * blockIdx.x + P; cc < a.nc; cc += HP * gridDim.x) {
-    // ---------------- the column's packed inputs -> X (features), coldry, aerosol depths ----------------
-    {
-      const unsigned char* rec = a.pk + (size_t)cc * kSgPackBytes;
-      if (h == 0) {   // row t: its 8 feature columns and coldry
-        *reinterpret_cast<uint4*>(pbase + HPO_X + umma::canon_off(t, 0, KIN)) =
-            __ldg(reinterpret_cast<const uint4*>(rec + PK_X) + t);
-        scd[t] = __ldg(reinterpret_cast<const float*>(rec + PK_CD) + t);
-      } else {        // 32 bytes of the aerosol block each
-        const int q = ptid - HP_THREADS / 2;
-        const uint4* src = reinterpret_cast<const uint4*>(rec + PK_AER) + 2 * q;
-        const uint4 v0 = __ldg(src), v1 = __ldg(src + 1);
-        reinterpret_cast<uint4*>(saer)[2 * q] = v0;
-        reinterpret_cast<uint4*>(saer)[2 * q + 1] = v1;
-      }
-    }
+  // The column's packed inputs -> X (its feature columns), coldry and aerosol
+  // rows, as 16-byte asynchronous copies issued a tile ahead: for the next
+  // tile once this one's optical depths are out (X has been free since MMA1),
+  // so they land during MMA3 and the fractions.
+  auto prefetch = [&](int col) {
+    const unsigned char* rec = a.pk + (size_t)col * kSgPackBytes;
+    if (h == 0) umma::cp_async16(pbase + HPO_X + umma::canon_off(t, 0, KIN), rec + PK_X + 16 * t);
+    umma::cp_async16(reinterpret_cast<unsigned char*>(saer) + 16 * ptid, rec + PK_AER + 16 * ptid);
+    if (ptid < 32) umma::cp_async16(reinterpret_cast<unsigned char*>(scd) + 16 * ptid, rec + PK_CD + 16 * ptid);
+    umma::cp_async_commit();
+  };
+  const int cstep = HP * gridDim.x;
+  if (HP * (int)blockIdx.x + P < a.nc) prefetch(HP * blockIdx.x + P);
+
+  for (int cc = HP * blockIdx.x + P; cc < a.nc; cc += cstep) {
+    umma::cp_async_wait_all();   // this thread's copies of the tile's inputs
     sync_for_mma();
     if (issuer) {
       umma::fence_after_sync();
@@ -904,7 +904,8 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
       h_out_tau<68, 108>(tb, wl, 8, live, odd, inblk, hrow, ar, cd);
       h_out_tau<108, 140>(tb, wl, 8, live, odd, inblk, hrow, ar, cd);
     }
-    sync_for_mma();   // the optical depths are read out of TMEM
+    sync_for_mma();   // the optical depths are read out of TMEM; coldry and aerosol rows are free
+    if (cc + cstep < a.nc) prefetch(cc + cstep);
     mma3(W3H_HALF);   // fractions: W3 rows [144, 288)
     if (!wait_mma()) break;
     hrow += 8 * NGPT;
@@ -920,6 +921,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
     psync.sync();
   }
   if (failed) umma::mbar_wait(mbar, phase ^ 1u, 1u << 20);   // one more bounded wait for the MMA in flight
+  umma::cp_async_wait_all();   // no copy still in flight after a time-out
   umma::fence_before_sync();
   __syncthreads();
   if (tid == 0 && *sfail && a.err) atomicCAS(a.err, 0, 1);

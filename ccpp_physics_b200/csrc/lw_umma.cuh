@@ -192,6 +192,13 @@ __device__ __forceinline__ void st_canon8(unsigned char* tile, int r, int k, int
   for (int j = 0; j < 4; ++j) p[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
   *reinterpret_cast<uint4*>(tile + canon_off(r, k, K)) = *reinterpret_cast<uint4*>(p);
 }
+// 16-byte asynchronous copy global -> shared (L2 only), its commit and the
+// wait for every copy this thread committed
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 // the same with FP16 elements
 __device__ __forceinline__ void st_canon8_h(unsigned char* tile, int r, int k, int K, const float* v) {
   __half2 p[4];
