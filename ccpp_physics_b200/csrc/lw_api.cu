@@ -462,8 +462,10 @@ cudaError_t enqueue(Workspace* w, cudaStream_t st, const Block* dblk, const Bloc
                                                 : launches_column_fp32(V, ncols, w->scratch_bytes, sh);
     w->last_launches = (f.isubclw > 0 && !f.gas_only ? 1 : 0) + col + (f.surrogate ? col / 2 : 0);
   }
+  NvtxRange run_range("rrtmg_lw_run");
   if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return e;
   if (f.isubclw > 0 && !f.gas_only) {
+    NvtxRange r("mcica_subcol");
     e = mcica_launch(dblk, nblocks, b0, ncols, f.nlay, f.iovr, f.isubclw, f.top_at_1, McicaStage(), w->bits,
                      g.num_sms, st);
     if (e != cudaSuccess) return e;
@@ -478,9 +480,11 @@ cudaError_t enqueue(Workspace* w, cudaStream_t st, const Block* dblk, const Bloc
                        scratch_budget(), g.num_sms, st);
     if (e == cudaSuccess && ev) e = cudaEventRecord(ev[3], st);
   } else if (precision == RRTMG_LW_FP64) {
+    NvtxRange r("setcoef+taumol+rtrnmc (FP64)");
     e = launch_column_fp64(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t64, t64, w->bits, w->scratch,
                            w->scratch_bytes, nullptr, nullptr, g.num_sms, sh, st, ev ? ev[3] : nullptr);
   } else {
+    NvtxRange r(f.surrogate ? "learned gas optics+rtrnmc (FP32)" : "setcoef+taumol+rtrnmc (FP32)");
     Tables<float> t{g.kt32, g.tbl32};
     e = launch_column_fp32(V, hlwb, dblk, nblocks, b0, ncols, f, g.cs, t, t64, w->bits, w->scratch,
                            w->scratch_bytes, nullptr, nullptr, g.num_sms, sh, st, ev ? ev[3] : nullptr);
@@ -1052,6 +1056,42 @@ extern "C" int rrtmg_lw_gpu_autotune(const rrtmg_lw_run_args* blocks, int32_t nb
     best->use_graph = 0;
   }
   if (best_ms) *best_ms = best_t;
+  return 0;
+}
+
+// Sets (or with t == NULL clears) the default launch shape of later calls
+// with this layer count and precision, as rrtmg_lw_gpu_autotune does after
+// timing: a host that keeps the autotuner's choice (per layer count,
+// precision and GPU) restores it without re-timing.
+extern "C" int rrtmg_lw_gpu_set_tuning(int32_t nlay, int32_t precision, const rrtmg_lw_tuning* t, char* errmsg,
+                                       int32_t errmsg_len) {
+  set_msg(errmsg, errmsg_len, "");
+  if (nlay < 1 || nlay > 255) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_set_tuning: nlay must be 1..255 (got %d)", nlay);
+    return 1;
+  }
+  if (precision != RRTMG_LW_FP64 && precision != RRTMG_LW_FP32 && precision != RRTMG_LW_SURROGATE) {
+    set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_set_tuning: unknown precision %d", precision);
+    return 1;
+  }
+  Shape s;
+  if (t) {
+    if (t->rt_warps) s.rt_warps = t->rt_warps;
+    if (t->gas_per_sm) s.gas_per_sm = t->gas_per_sm;
+    if (t->chunk_cols) s.chunk = t->chunk_cols;
+    if (s.rt_warps != 1 && s.rt_warps != 2 && s.rt_warps != 4) {
+      set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_set_tuning: rt_warps must be 1, 2 or 4 (got %d)", s.rt_warps);
+      return 1;
+    }
+    if (s.gas_per_sm < 0 || s.chunk < 0) {
+      set_msg(errmsg, errmsg_len, "rrtmg_lw_gpu_set_tuning: negative tuning value");
+      return 1;
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int pi = precision == RRTMG_LW_FP64 ? 0 : 1, V = pick_v(nlay);
+  g.tuned[pi][V] = s;
+  g.has_tuned[pi][V] = t != nullptr;
   return 0;
 }
 

@@ -760,9 +760,12 @@ cudaError_t sg_path_launch(const Block* blocks, int nblocks, const Block& b0, in
   for (long c0 = 0; c0 < ncols; c0 += L.chunk) {
     const int nc = (int)std::min<long>(L.chunk, ncols - c0);
     if ((e = cudaMemsetAsync(count, 0, sizeof(int), st)) != cudaSuccess) return e;
-    if ((e = mlp_h_launch(blocks, nblocks, b0, colmap, (int)c0, nc, f, hnd, flag, list, count, pk, num_sms, st)) !=
-        cudaSuccess)
-      return e;
+    {
+      NvtxRange r("learned gas optics (taumol network)");
+      if ((e = mlp_h_launch(blocks, nblocks, b0, colmap, (int)c0, nc, f, hnd, flag, list, count, pk, num_sms,
+                            st)) != cudaSuccess)
+        return e;
+    }
     FbArgs fa;
     fa.blocks = blocks;
     fa.nblocks = nblocks;
@@ -776,8 +779,11 @@ cudaError_t sg_path_launch(const Block* blocks, int nblocks, const Block& b0, in
     fa.flag = flag;
     fa.hnd = hnd;
     fa.slots = fbs;
-    lw_sg_fallback_kernel<<<FB_GRID, 32 * FB_V, gas_smem_bytes<float>(FB_V), st>>>(fa);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    {
+      NvtxRange r("taumol fallback (out of envelope)");
+      lw_sg_fallback_kernel<<<FB_GRID, 32 * FB_V, gas_smem_bytes<float>(FB_V), st>>>(fa);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     SrArgs ra;
     ra.blocks = blocks;
     ra.nblocks = nblocks;
@@ -792,8 +798,11 @@ cudaError_t sg_path_launch(const Block* blocks, int nblocks, const Block& b0, in
     ra.bits = bits;
     ra.hnd = hnd;
     const int grid = std::min(num_sms, (nc + SR_GROUPS - 1) / SR_GROUPS);
-    lw_sg_rt_kernel<<<grid, SR_THREADS, SR_SMEM, st>>>(ra);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    {
+      NvtxRange r("cldprop+rtrnmc");
+      lw_sg_rt_kernel<<<grid, SR_THREADS, SR_SMEM, st>>>(ra);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
   }
   return cudaSuccess;
 }

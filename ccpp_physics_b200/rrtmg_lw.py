@@ -47,6 +47,7 @@ def lib():
                                               C.c_void_p, C.c_char_p, C.c_int32]
         L.rrtmg_lw_gpu_run_blocks.argtypes = [C.POINTER(abi.RunArgs), C.c_int32, C.POINTER(abi.ExecArgs),
                                               C.POINTER(abi.Tuning), C.c_char_p, C.c_int32]
+        L.rrtmg_lw_gpu_set_tuning.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_char_p, C.c_int32]
         L.rrtmg_lw_gpu_autotune.argtypes = [C.POINTER(abi.RunArgs), C.c_int32, C.c_int32, C.c_void_p,
                                             C.c_int64, C.POINTER(abi.Tuning), C.POINTER(C.c_float),
                                             C.c_char_p, C.c_int32]
@@ -313,9 +314,45 @@ def run_blocks(prof: dict, out: dict, sizes, *, precision="fp64", tuning=None, s
     return msg.value.decode(), rc
 
 
-def autotune(prof: dict, out: dict, sizes, *, precision="fp32", sample_cols=0, stream=None):
+def tuning_key(nlay: int, precision: str, device_name: str) -> str:
+    """Key of a launch shape in the autotuner's JSON cache: the kernels'
+    shape depends on the layer count (layers per lane), the precision and
+    the GPU."""
+    return f"{device_name}|nlay={int(nlay)}|{precision}"
+
+
+def set_tuning(nlay: int, precision: str, tuning):
+    """Default launch shape of later calls with this layer count and
+    precision (rrtmg_lw_gpu_set_tuning); None clears it."""
+    t = None if tuning is None else abi.Tuning(**{n: int(tuning.get(n, 0)) for n, _ in abi.Tuning._fields_})
+    msg = C.create_string_buffer(512)
+    rc = lib().rrtmg_lw_gpu_set_tuning(int(nlay), PRECISIONS[precision], None if t is None else C.byref(t), msg, 512)
+    if rc:
+        raise RRTMGLWError(msg.value.decode())
+
+
+def autotune(prof: dict, out: dict, sizes, *, precision="fp32", sample_cols=0, stream=None, cache=None,
+             device_name=None):
     """Autotune the launch shape on the physics blocks of ``sizes`` columns;
-    returns (tuning dict, ms per call)."""
+    returns (tuning dict, ms per call).
+
+    cache: path of a JSON file of chosen shapes keyed by (GPU, layer count,
+    precision).  A hit sets that shape as the default of later calls
+    (set_tuning) without timing and returns (tuning, ms recorded when it was
+    chosen); a miss times the candidates and adds the choice to the file."""
+    nlay = int(prof["nlay"])
+    key = None
+    if cache is not None:
+        if device_name is None:
+            import torch
+            device_name = torch.cuda.get_device_name(prof["plyr"].device) if hasattr(prof["plyr"], "device") \
+                else torch.cuda.get_device_name()
+        key = tuning_key(nlay, precision, device_name)
+        table = _read_tuning_cache(cache)
+        if key in table:
+            hit = table[key]
+            set_tuning(nlay, precision, hit["tuning"])
+            return dict(hit["tuning"]), float(hit["ms"])
     arr, keep = block_args(prof, out, sizes)
     stream = torch_stream(stream, prof["plyr"])
     best = abi.Tuning()
@@ -325,7 +362,32 @@ def autotune(prof: dict, out: dict, sizes, *, precision="fp32", sample_cols=0, s
                                      C.c_void_p(stream), int(sample_cols), C.byref(best), C.byref(ms), msg, 512)
     if rc:
         raise RRTMGLWError(msg.value.decode())
-    return {n: getattr(best, n) for n, _ in abi.Tuning._fields_}, ms.value
+    tuning = {n: getattr(best, n) for n, _ in abi.Tuning._fields_}
+    if key is not None:
+        table = _read_tuning_cache(cache)
+        table[key] = {"tuning": tuning, "ms": float(ms.value)}
+        _write_tuning_cache(cache, table)
+    return tuning, ms.value
+
+
+def _read_tuning_cache(path) -> dict:
+    import json
+    try:
+        with open(path) as fh:
+            table = json.load(fh)
+    except FileNotFoundError:
+        return {}
+    if not isinstance(table, dict):
+        raise RRTMGLWError(f"{path}: not a tuning cache (a JSON object is expected)")
+    return table
+
+
+def _write_tuning_cache(path, table: dict):
+    import json
+    tmp = f"{path}.tmp{os.getpid()}"
+    with open(tmp, "w") as fh:
+        json.dump(table, fh, indent=1, sort_keys=True)
+    os.replace(tmp, path)   # readers never see a half-written file
 
 
 def to_device(prof: dict, device="cuda"):

@@ -213,6 +213,14 @@ int rrtmg_lw_gpu_autotune(const rrtmg_lw_run_args *blocks, int32_t nblocks,
                           int32_t precision, void *stream,
                           int64_t sample_cols, rrtmg_lw_tuning *best,
                           float *best_ms, char *errmsg, int32_t errmsg_len);
+/* Sets the default launch shape of later calls with this layer count and
+ * precision, as the autotuner does after timing (NULL clears it): a host
+ * that saved the autotuner's choice per layer count, precision and GPU
+ * restores it without re-timing (ccpp_physics_b200.rrtmg_lw.autotune keeps
+ * such a JSON cache).  No counterpart in the reference.  Returns errflg. */
+int rrtmg_lw_gpu_set_tuning(int32_t nlay, int32_t precision,
+                            const rrtmg_lw_tuning *tune, char *errmsg,
+                            int32_t errmsg_len);
 
 /* ---- Learned gas optics (no counterpart in the reference) -------------
  * A BF16 MLP 8 -> 128 -> 128 -> 288 (SiLU) on the tensor cores replaces
