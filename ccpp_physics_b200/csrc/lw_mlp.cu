@@ -1441,6 +1441,7 @@ extern "C" int rrtmg_lw_gpu_surrogate_init(const float* norm, uint64_t seed, cha
   pack_kernel<<<64, 256>>>(net.P, net.ops);
   SG_CK(cudaGetLastError(), "pack kernel");
   SG_CK(cudaDeviceSynchronize(), "pack kernel");
+  SG_CK(cudaMemset(net.Madam, 0, sizeof(float) * P_N * 2), "cudaMemset(adam moments)");   // a fresh optimizer
   net.adam_t = 0;
   net.ready = true;
   return 0;
@@ -1472,6 +1473,7 @@ extern "C" int rrtmg_lw_gpu_surrogate_set(const float* w, const float* norm, cha
   pack_kernel<<<64, 256>>>(net.P, net.ops);
   SG_CK(cudaGetLastError(), "pack kernel");
   SG_CK(cudaDeviceSynchronize(), "pack kernel");
+  SG_CK(cudaMemset(net.Madam, 0, sizeof(float) * P_N * 2), "cudaMemset(adam moments)");   // a fresh optimizer
   net.adam_t = 0;
   net.ready = true;
   return 0;
@@ -1493,6 +1495,48 @@ extern "C" int rrtmg_lw_gpu_surrogate_get(float* w, float* norm, char* errmsg, i
       if (!pad_out_row(r)) w[k++] = P[P_B3 + r];
   }
   if (norm) SG_CK(cudaMemcpy(norm, net.norm, sizeof(float) * SG_NORM_FLOATS, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  return 0;
+}
+
+static_assert(RRTMG_LW_SURROGATE_NSTATE == P_N, "training-state size in the C ABI");
+
+// Training state for a checkpoint: the FP32 master parameters and Adam's
+// first and second moment estimates, each float[P_N] in the padded layout,
+// the step count and the normalisation.
+extern "C" int rrtmg_lw_gpu_surrogate_get_state(float* params, float* m, float* v, int64_t* step, float* norm,
+                                                char* errmsg, int32_t errmsg_len) {
+  smsg(errmsg, errmsg_len, "");
+  std::lock_guard<std::mutex> lk(net_mu);
+  if (check_ready(errmsg, errmsg_len)) return 1;
+  if (params) SG_CK(cudaMemcpy(params, net.P, sizeof(float) * P_N, cudaMemcpyDeviceToHost), "cudaMemcpy(params)");
+  if (m) SG_CK(cudaMemcpy(m, net.Madam, sizeof(float) * P_N, cudaMemcpyDeviceToHost), "cudaMemcpy(adam m)");
+  if (v) SG_CK(cudaMemcpy(v, net.Vadam, sizeof(float) * P_N, cudaMemcpyDeviceToHost), "cudaMemcpy(adam v)");
+  if (step) *step = net.adam_t;
+  if (norm) SG_CK(cudaMemcpy(norm, net.norm, sizeof(float) * SG_NORM_FLOATS, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  return 0;
+}
+
+extern "C" int rrtmg_lw_gpu_surrogate_set_state(const float* params, const float* m, const float* v, int64_t step,
+                                                const float* norm, char* errmsg, int32_t errmsg_len) {
+  smsg(errmsg, errmsg_len, "");
+  if (!params || !m || !v || !norm || step < 0) {
+    smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_set_state: NULL argument or negative step");
+    return 1;
+  }
+  std::lock_guard<std::mutex> lk(net_mu);
+  int dev = 0, sms = 0;
+  if (dev_of_init(&dev, &sms)) { smsg(errmsg, errmsg_len, "rrtmg_lw_gpu_surrogate_set_state: no CUDA device"); return 1; }
+  SG_CK(set_attrs(), "kernel attributes (one CTA per SM)");
+  SG_CK(ensure_net(dev, sms), "cudaMalloc(network)");
+  SG_CK(cudaMemcpy(net.P, params, sizeof(float) * P_N, cudaMemcpyHostToDevice), "cudaMemcpy(params)");
+  SG_CK(cudaMemcpy(net.Madam, m, sizeof(float) * P_N, cudaMemcpyHostToDevice), "cudaMemcpy(adam m)");
+  SG_CK(cudaMemcpy(net.Vadam, v, sizeof(float) * P_N, cudaMemcpyHostToDevice), "cudaMemcpy(adam v)");
+  SG_CK(cudaMemcpy(net.norm, norm, sizeof(float) * SG_NORM_FLOATS, cudaMemcpyHostToDevice), "cudaMemcpy(norm)");
+  pack_kernel<<<64, 256>>>(net.P, net.ops);
+  SG_CK(cudaGetLastError(), "pack kernel");
+  SG_CK(cudaDeviceSynchronize(), "pack kernel");
+  net.adam_t = (long)step;
+  net.ready = true;
   return 0;
 }
 

@@ -25,6 +25,7 @@ from . import abi, synthetic
 NORM = 608
 NPARAM = 53656
 NGRAD = 54688
+NSTATE = 54688   # parameters and each Adam moment, padded layout (rrtmg_lw_gpu_surrogate_get_state)
 NOUTP = 288
 NGPT = 140
 TAU = slice(0, 140)
@@ -55,6 +56,10 @@ def _lib():
         L.rrtmg_lw_gpu_surrogate_grads.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
                                                    C.c_void_p, C.c_char_p, C.c_int32]
         L.rrtmg_lw_gpu_surrogate_stats.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_int32), C.c_int32]
+        L.rrtmg_lw_gpu_surrogate_get_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int64),
+                                                       C.c_void_p, C.c_char_p, C.c_int32]
+        L.rrtmg_lw_gpu_surrogate_set_state.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                                       C.c_char_p, C.c_int32]
         L._sg_bound = True
     return L
 
@@ -232,6 +237,45 @@ def stats(reset=False):
     if _lib().rrtmg_lw_gpu_surrogate_stats(C.byref(n), C.byref(e), int(reset)):
         raise RuntimeError("surrogate stats unavailable")
     return int(n.value), int(e.value)
+
+
+def get_state():
+    """Training state: dict(params, m, v: float32[NSTATE], step, norm)."""
+    st = {k: np.zeros(NSTATE, dtype=np.float32) for k in ("params", "m", "v")}
+    norm = np.zeros(NORM, dtype=np.float32)
+    step = C.c_int64(0)
+    msg = C.create_string_buffer(512)
+    _check(_lib().rrtmg_lw_gpu_surrogate_get_state(_np_ptr(st["params"]), _np_ptr(st["m"]), _np_ptr(st["v"]),
+                                                   C.byref(step), _np_ptr(norm), msg, 512), msg)
+    st.update(step=int(step.value), norm=norm)
+    return st
+
+
+def set_state(params, m, v, step, norm):
+    """Restore a training state (get_state's fields): training resumes
+    with the same parameters, Adam moments and step count."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (params, m, v)]
+    n = np.ascontiguousarray(norm, dtype=np.float32)
+    if any(a.size != NSTATE for a in arrs) or n.size != NORM:
+        raise ValueError(f"training state arrays must hold {NSTATE} values (norm {NORM})")
+    msg = C.create_string_buffer(512)
+    _check(_lib().rrtmg_lw_gpu_surrogate_set_state(_np_ptr(arrs[0]), _np_ptr(arrs[1]), _np_ptr(arrs[2]),
+                                                   int(step), _np_ptr(n), msg, 512), msg)
+
+
+def save_checkpoint(path, **meta):
+    """Training checkpoint (.npz): parameters, Adam moments, step,
+    normalisation and any extra metadata."""
+    st = get_state()
+    np.savez_compressed(path, params=st["params"], m=st["m"], v=st["v"], step=np.int64(st["step"]),
+                        norm=st["norm"], **meta)
+
+
+def load_checkpoint(path):
+    """Restore a checkpoint written by save_checkpoint; returns its contents."""
+    d = np.load(path)
+    set_state(d["params"], d["m"], d["v"], int(d["step"]), d["norm"])
+    return d
 
 
 def save(path=WEIGHTS_PATH, **meta):

@@ -267,6 +267,19 @@ int rrtmg_lw_gpu_surrogate_train(const float *feats, const float *targets,
                                  int32_t flags, float *loss_per_epoch,
                                  void *stream,
                                  char *errmsg, int32_t errmsg_len);
+/* Training checkpoint: the FP32 master parameters and Adam's first and
+ * second moment estimates, each host float[RRTMG_LW_SURROGATE_NSTATE] in the
+ * padded layout of the gradient export, the optimizer step count and the
+ * normalisation (float[608]).  get_state fills any non-NULL argument;
+ * set_state restores all of them, so training resumes where it stopped. */
+#define RRTMG_LW_SURROGATE_NSTATE 54688
+int rrtmg_lw_gpu_surrogate_get_state(float *params, float *m, float *v,
+                                     int64_t *step, float *norm, char *errmsg,
+                                     int32_t errmsg_len);
+int rrtmg_lw_gpu_surrogate_set_state(const float *params, const float *m,
+                                     const float *v, int64_t step,
+                                     const float *norm, char *errmsg,
+                                     int32_t errmsg_len);
 /* Network outputs (normalised) for device features: y[n][288]. */
 int rrtmg_lw_gpu_surrogate_forward(const float *feats, int64_t n, float *y,
                                    void *stream, char *errmsg,

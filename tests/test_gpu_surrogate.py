@@ -75,6 +75,39 @@ def test_training_reduces_loss(sg, small_set):
     assert losses[-1] < 0.25 * losses[0], losses
 
 
+def test_training_checkpoint_resumes(sg, small_set, tmp_path):
+    """A training checkpoint holds the FP32 parameters, both Adam moments, the
+    step count and the normalisation: restored after other weights were
+    loaded (which also resets the optimizer), it gives back the same state
+    bit for bit and the same forward outputs, and training continues from
+    its step."""
+    feats, targ, norm = small_set
+    sg.init(norm, seed=13)
+    y = sg.normalise_targets(targ, norm)
+    batch = 1024
+    sg.train(feats, y, epochs=2, batch=batch, lr=3e-3, lr_final=1e-3)
+    st = sg.get_state()
+    steps = feats.shape[0] // batch
+    assert st["step"] == 2 * steps
+    assert np.any(st["m"] != 0) and np.any(st["v"] != 0)
+    x = feats[:1024].contiguous()
+    y0 = sg.forward(x).cpu().numpy()
+    path = tmp_path / "ckpt.npz"
+    sg.save_checkpoint(path)
+    sg.init(norm, seed=99)                      # other weights and a fresh optimizer
+    fresh = sg.get_state()
+    assert fresh["step"] == 0 and not np.any(fresh["m"]) and not np.any(fresh["v"])
+    sg.load_checkpoint(path)
+    st2 = sg.get_state()
+    for k in ("params", "m", "v", "norm"):
+        assert np.array_equal(st[k], st2[k]), k
+    assert st2["step"] == st["step"]
+    assert np.array_equal(sg.forward(x).cpu().numpy(), y0)
+    losses = sg.train(feats, y, epochs=1, batch=batch, lr=1e-3, lr_final=1e-4)
+    assert np.all(np.isfinite(losses))
+    assert sg.get_state()["step"] == 3 * steps
+
+
 @pytest.fixture(scope="module")
 def trained(sg):
     """The committed network, trained on the GPU by ccpp_physics_b200.train_surrogate."""
