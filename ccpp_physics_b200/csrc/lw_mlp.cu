@@ -567,12 +567,32 @@ __device__ __forceinline__ void st_pair(__half* dst_g, int stride, bool odd, boo
   if (store) *reinterpret_cast<uint32_t*>(odd ? dst_g + stride - 1 : dst_g) = __byte_perm(W, X, odd ? 0x3276u : 0x5410u);
 }
 
+// FP16 values of g-points g..g+3 of this row and of the other rows of its
+// 4-row group (lanes 4k..4k+3, layers of one 8-layer block) as one 8-byte
+// store each: row q of the group stores g-point g + q of the group's four
+// layers.  Two exchanges: rows q and q^2 swap one g-point pair, then rows q
+// and q^1 swap halves.
+__device__ __forceinline__ void st_quad(__half* dst_g, int stride, int q, bool store, float v0, float v1, float v2,
+                                        float v3) {
+  const __half2 a = __floats2half2_rn(v0, v1), b = __floats2half2_rn(v2, v3);
+  const uint32_t w0 = *reinterpret_cast<const uint32_t*>(&a), w1 = *reinterpret_cast<const uint32_t*>(&b);
+  const bool hi = q & 2, odd = q & 1;
+  const uint32_t r1 = __shfl_xor_sync(0xffffffffu, hi ? w0 : w1, 2);
+  // pair P (g, g+1 for rows 0-1; g+2, g+3 for rows 2-3) at layers (q & 1) and (q & 1) + 2
+  const uint32_t x0 = hi ? r1 : w0, x1 = hi ? w1 : r1;
+  const uint32_t r2 = __shfl_xor_sync(0xffffffffu, __byte_perm(x0, x1, odd ? 0x5410u : 0x7632u), 1);
+  uint2 out;
+  out.x = __byte_perm(x0, r2, odd ? 0x3254u : 0x5410u);
+  out.y = __byte_perm(x1, r2, odd ? 0x3276u : 0x7610u);
+  if (store) *reinterpret_cast<uint2*>(dst_g + q * stride - q) = out;
+}
+
 // optical depths of g-points [GA, GB) of this thread's row, FP16 at
 // dst[g stride]: 2^acc * coldry + aerosol.  Every lane runs the TMEM loads
-// (tcgen05.ld is a warp-wide instruction) and the pair exchanges; padding
+// (tcgen05.ld is a warp-wide instruction) and the store exchanges; padding
 // rows inside the column's last 8-layer block store zeros.
 template <int GA, int GB>
-__device__ __forceinline__ void h_out_tau(uint32_t tb, int wl, int stride, bool live, bool odd, bool store, __half* dst,
+__device__ __forceinline__ void h_out_tau(uint32_t tb, int wl, int stride, bool live, int q, bool store, __half* dst,
                                           const __half* aer_row, float cd) {
   static_assert((GB - GA) % 2 == 0, "g-point pairs");
   constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
@@ -586,12 +606,14 @@ __device__ __forceinline__ void h_out_tau(uint32_t tb, int wl, int stride, bool 
                      : 0.0f;   // below the FP16 maximum
   }
 #pragma unroll
-  for (int g = GA; g < GB; g += 2) st_pair(dst + g * stride, stride, odd, store, v[g - C0], v[g + 1 - C0]);
+  for (int g = GA; g + 4 <= GB; g += 4)
+    st_quad(dst + g * stride, stride, q, store, v[g - C0], v[g + 1 - C0], v[g + 2 - C0], v[g + 3 - C0]);
+  if ((GB - GA) % 4) st_pair(dst + (GB - 2) * stride, stride, q & 1, store, v[GB - 2 - C0], v[GB - 1 - C0]);
 }
 
 // band-normalised Planck fractions of g-points [GA, GB) (whole bands), FP16 at dst[g stride]
 template <int GA, int GB>
-__device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool live, bool odd, bool store,
+__device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool live, int q, bool store,
                                            __half* dst) {
   static_assert((GB - GA) % 2 == 0, "g-point pairs");
   constexpr int C0 = GA & ~15, NCH = (GB - C0 + 15) / 16;
@@ -610,9 +632,11 @@ __device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool
 #pragma unroll
   for (int b = 0; b < NBANDS; ++b) bsum[b] = bsum[b] > 0.0f ? __fdividef(1.0f, bsum[b]) : 1.0f;   // FP16 results
 #pragma unroll
-  for (int g = GA; g < GB; g += 2)
-    st_pair(dst + g * stride, stride, odd, store, live ? v[g - C0] * bsum[band_of_g(g)] : 0.0f,
-            live ? v[g + 1 - C0] * bsum[band_of_g(g + 1)] : 0.0f);
+  for (int g = GA; g < GB; ++g) v[g - C0] = live ? v[g - C0] * bsum[band_of_g(g)] : 0.0f;
+#pragma unroll
+  for (int g = GA; g + 4 <= GB; g += 4)
+    st_quad(dst + g * stride, stride, q, store, v[g - C0], v[g + 1 - C0], v[g + 2 - C0], v[g + 3 - C0]);
+  if ((GB - GA) % 4) st_pair(dst + (GB - 2) * stride, stride, q & 1, store, v[GB - 2 - C0], v[GB - 1 - C0]);
 }
 
 // Per-column network inputs of the column path, packed by mlp_h_pack_kernel
@@ -830,7 +854,8 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
   };
 
   const int nlay = a.f.nlay, nchk = (nlay + 7) >> 3;
-  const bool live = t < nlay, odd = t & 1;
+  const bool live = t < nlay;
+  const int q4 = t & 3;   // row within its 4-row group of the hand-off stores
   const bool inblk = t < 8 * nchk;   // the row lies in one of the column's 8-layer hand-off blocks
 
   // The column's packed inputs -> X (its feature columns), coldry and aerosol
@@ -898,11 +923,11 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
     const __half* ar = saer + t;
     // the two halves of a row own whole bands: g-points [0, 68) and [68, 140), in two passes each
     if (h == 0) {
-      h_out_tau<0, 38>(tb, wl, 8, live, odd, inblk, hrow, ar, cd);
-      h_out_tau<38, 68>(tb, wl, 8, live, odd, inblk, hrow, ar, cd);
+      h_out_tau<0, 38>(tb, wl, 8, live, q4, inblk, hrow, ar, cd);
+      h_out_tau<38, 68>(tb, wl, 8, live, q4, inblk, hrow, ar, cd);
     } else {
-      h_out_tau<68, 108>(tb, wl, 8, live, odd, inblk, hrow, ar, cd);
-      h_out_tau<108, 140>(tb, wl, 8, live, odd, inblk, hrow, ar, cd);
+      h_out_tau<68, 108>(tb, wl, 8, live, q4, inblk, hrow, ar, cd);
+      h_out_tau<108, 140>(tb, wl, 8, live, q4, inblk, hrow, ar, cd);
     }
     sync_for_mma();   // the optical depths are read out of TMEM; coldry and aerosol rows are free
     if (cc + cstep < a.nc) prefetch(cc + cstep);
@@ -910,11 +935,11 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) mlp_h_kernel(FwdArgs a) {
     if (!wait_mma()) break;
     hrow += 8 * NGPT;
     if (h == 0) {
-      h_out_frac<0, 38>(tb, wl, 8, live, odd, inblk, hrow);
-      h_out_frac<38, 68>(tb, wl, 8, live, odd, inblk, hrow);
+      h_out_frac<0, 38>(tb, wl, 8, live, q4, inblk, hrow);
+      h_out_frac<38, 68>(tb, wl, 8, live, q4, inblk, hrow);
     } else {
-      h_out_frac<68, 108>(tb, wl, 8, live, odd, inblk, hrow);
-      h_out_frac<108, 140>(tb, wl, 8, live, odd, inblk, hrow);
+      h_out_frac<68, 108>(tb, wl, 8, live, q4, inblk, hrow);
+      h_out_frac<108, 140>(tb, wl, 8, live, q4, inblk, hrow);
     }
     // the accumulators and this tile's rows are free for the next tile
     umma::fence_before_sync();
