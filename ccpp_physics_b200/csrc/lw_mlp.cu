@@ -643,8 +643,8 @@ __device__ __forceinline__ void h_out_frac(uint32_t tb, int wl, int stride, bool
 // into the work area (kSgPackBytes per chunk column):
 //   [128 rows][8] BF16  the normalised features x0..x6 and the constant 1
 //                       (padding rows zero): the first 8 columns of the X tile
-//   [128] FP32          coldry (RLM:823-836)
-//   [16 bands][128] FP16 aerosol optical depth aod (1 - ssa) (RLM:1000-1012)
+//   [128] FP32          coldry (RLM:835, 947)
+//   [16 bands][128] FP16 aerosol optical depth aod (1 - ssa) (RLM:877-880, 986-989)
 // The inputs lie column-fastest ((ldim, nlay) arrays), so the network's
 // one-column tiles read them at a stride of a whole layer row; the pack
 // kernel reads them 16 columns at a time (one whole 128-byte line per layer
