@@ -127,10 +127,12 @@ __device__ __forceinline__ float warp_sum_all(float v) {
 }
 
 // record index it = int(10000 x / (bpade + x) + 0.5) of an optical depth
-// (RLM:3602-3603); x is finite and >= 0 here (the hand-off clamps optical
-// depths below the FP16 maximum), so the index is >= 0
+// (RLM:3602-3603).  x is finite, >= 0 and at most ~1e10 here (the hand-off
+// clamps optical depths below the FP16 maximum; a cloudy layer past the
+// table's end adds 1e10), so x / (bpade + x) <= 1 and the index lies in
+// [0, NTBL] without a clamp.
 __device__ __forceinline__ int tbl_index(float x) {
-  return min(NTBL, (int)(float(kTblint) * __fdividef(x, float(kBpade) + x) + 0.5f));
+  return (int)(float(kTblint) * __fdividef(x, float(kBpade) + x) + 0.5f);
 }
 
 // Total-sky terms of a cloudy sub-column layer (RLM:3627-3660, clfm = 1):
